@@ -1,0 +1,659 @@
+/*
+ * ps_oracle.c -- CPU oracle for the Pauli-propagation layer path.
+ *
+ * TEST INFRASTRUCTURE ONLY (parity checker and timed CPU baseline); the product
+ * library never links or calls it.  See ps_oracle.h for the reference
+ * file:line each part restates.  Build with -ffp-contract=off: every product
+ * and sum below must round exactly once, as the reference's Rust does.
+ */
+#include "ps_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+struct pso_sum {
+    int W;
+    int nq;
+    int dtype;
+    size_t n;
+    size_t cap;
+    uint64_t* keys; /* n x 2W */
+    double* c64;
+    float* c32;
+};
+
+/* ------------------------------------------------------------------------ */
+/* key algebra: crates/paulistrings/src/pauli_string.rs                      */
+/* ------------------------------------------------------------------------ */
+
+static int key_cmp(const uint64_t* a, const uint64_t* b, int W) {
+    for (int i = 0; i < 2 * W; ++i) {
+        if (a[i] != b[i]) return a[i] < b[i] ? -1 : 1;
+    }
+    return 0;
+}
+
+/* commutes_with (pauli_string.rs:116-123): XOR-fold then one popcount. */
+static int anticommutes(const uint64_t* k, const uint64_t* gx, const uint64_t* gz, int W) {
+    uint64_t f = 0;
+    for (int i = 0; i < W; ++i) f ^= (k[i] & gz[i]) ^ (k[W + i] & gx[i]);
+    return __builtin_popcountll(f) & 1;
+}
+
+/* mul_assign phase exponent (pauli_string.rs:73-93): delta = 2bc + ab + cd - (a^c)(b^d) mod 4,
+ * (a,b) = self (x,z), (c,d) = other (x,z). */
+static unsigned product_phase(const uint64_t* k, const uint64_t* gx, const uint64_t* gz, int W) {
+    unsigned d = 0;
+    for (int i = 0; i < W; ++i) {
+        uint64_t a = k[i], b = k[W + i], c = gx[i], e = gz[i];
+        d += 2u * (unsigned)__builtin_popcountll(b & c);
+        d += (unsigned)__builtin_popcountll(a & b);
+        d += (unsigned)__builtin_popcountll(c & e);
+        d -= (unsigned)__builtin_popcountll((a ^ c) & (b ^ e));
+    }
+    return d & 3u;
+}
+
+static unsigned key_weight(const uint64_t* k, int W) {
+    unsigned w = 0;
+    for (int i = 0; i < W; ++i) w += (unsigned)__builtin_popcountll(k[i] | k[W + i]);
+    return w;
+}
+
+/* ------------------------------------------------------------------------ */
+/* sum storage                                                              */
+/* ------------------------------------------------------------------------ */
+
+static void sum_reserve(pso_sum* s, size_t cap) {
+    if (cap <= s->cap) return;
+    size_t c = s->cap ? s->cap : 16;
+    while (c < cap) c *= 2;
+    s->keys = (uint64_t*)realloc(s->keys, c * 2 * (size_t)s->W * sizeof(uint64_t));
+    if (s->dtype == PSO_F64)
+        s->c64 = (double*)realloc(s->c64, c * sizeof(double));
+    else
+        s->c32 = (float*)realloc(s->c32, c * sizeof(float));
+    s->cap = c;
+}
+
+pso_sum* pso_new(int W, int num_qubits, int dtype) {
+    if (W < 1 || W > PSO_MAX_W || num_qubits < 1 || num_qubits > 64 * W) return NULL;
+    if (dtype != PSO_F64 && dtype != PSO_F32) return NULL;
+    pso_sum* s = (pso_sum*)calloc(1, sizeof(pso_sum));
+    s->W = W;
+    s->nq = num_qubits;
+    s->dtype = dtype;
+    return s;
+}
+
+void pso_free(pso_sum* s) {
+    if (!s) return;
+    free(s->keys);
+    free(s->c64);
+    free(s->c32);
+    free(s);
+}
+
+size_t pso_len(const pso_sum* s) { return s->n; }
+int pso_width(const pso_sum* s) { return s->W; }
+
+void pso_get(const pso_sum* s, uint64_t* keys, double* coeffs) {
+    if (keys) memcpy(keys, s->keys, s->n * 2 * (size_t)s->W * sizeof(uint64_t));
+    if (coeffs) {
+        for (size_t i = 0; i < s->n; ++i) coeffs[i] = s->dtype == PSO_F64 ? s->c64[i] : (double)s->c32[i];
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* hash accumulator (the naive oracle's HashMap, test_support/oracle.rs:28-41) */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+    int W;
+    int dtype;
+    size_t mask;
+    size_t used;
+    uint64_t* keys;
+    unsigned char* full;
+    double* v64;
+    float* v32;
+    size_t* order; /* insertion order, for a deterministic walk */
+} accum;
+
+static uint64_t key_hash(const uint64_t* k, int W) {
+    uint64_t h = 0x9E3779B97F4A7C15ull;
+    for (int i = 0; i < 2 * W; ++i) {
+        uint64_t v = k[i] + 0x9E3779B97F4A7C15ull * (uint64_t)(i + 1);
+        v ^= v >> 30;
+        v *= 0xBF58476D1CE4E5B9ull;
+        v ^= v >> 27;
+        v *= 0x94D049BB133111EBull;
+        v ^= v >> 31;
+        h = (h ^ v) * 0x100000001B3ull;
+    }
+    return h ^ (h >> 29);
+}
+
+static void accum_init(accum* a, int W, int dtype, size_t expect) {
+    size_t cap = 64;
+    while (cap < 2 * expect + 16) cap *= 2;
+    a->W = W;
+    a->dtype = dtype;
+    a->mask = cap - 1;
+    a->used = 0;
+    a->keys = (uint64_t*)malloc(cap * 2 * (size_t)W * sizeof(uint64_t));
+    a->full = (unsigned char*)calloc(cap, 1);
+    a->v64 = dtype == PSO_F64 ? (double*)malloc(cap * sizeof(double)) : NULL;
+    a->v32 = dtype == PSO_F32 ? (float*)malloc(cap * sizeof(float)) : NULL;
+    a->order = (size_t*)malloc(cap * sizeof(size_t));
+}
+
+static void accum_free(accum* a) {
+    free(a->keys);
+    free(a->full);
+    free(a->v64);
+    free(a->v32);
+    free(a->order);
+}
+
+static void accum_grow(accum* a);
+
+static void accum_add(accum* a, const uint64_t* k, double v64, float v32) {
+    if (2 * (a->used + 1) > a->mask + 1) accum_grow(a);
+    int K = 2 * a->W;
+    size_t h = (size_t)key_hash(k, a->W) & a->mask;
+    while (a->full[h]) {
+        if (memcmp(a->keys + h * K, k, (size_t)K * 8) == 0) {
+            if (a->dtype == PSO_F64)
+                a->v64[h] = a->v64[h] + v64;
+            else
+                a->v32[h] = a->v32[h] + v32;
+            return;
+        }
+        h = (h + 1) & a->mask;
+    }
+    a->full[h] = 1;
+    memcpy(a->keys + h * K, k, (size_t)K * 8);
+    /* OR-insert ZERO then += out_c, as the reference's entry().or_insert(ZERO) += c */
+    if (a->dtype == PSO_F64)
+        a->v64[h] = 0.0 + v64;
+    else
+        a->v32[h] = 0.0f + v32;
+    a->order[a->used++] = h;
+}
+
+static void accum_grow(accum* a) {
+    accum b;
+    accum_init(&b, a->W, a->dtype, a->mask + 1);
+    int K = 2 * a->W;
+    for (size_t i = 0; i < a->used; ++i) {
+        size_t h = a->order[i];
+        size_t g = (size_t)key_hash(a->keys + h * K, a->W) & b.mask;
+        while (b.full[g]) g = (g + 1) & b.mask;
+        b.full[g] = 1;
+        memcpy(b.keys + g * K, a->keys + h * K, (size_t)K * 8);
+        if (a->dtype == PSO_F64)
+            b.v64[g] = a->v64[h];
+        else
+            b.v32[g] = a->v32[h];
+        b.order[b.used++] = g;
+    }
+    accum_free(a);
+    *a = b;
+}
+
+/* sort helper: indices into a key array */
+static const uint64_t* g_sort_keys;
+static int g_sort_W;
+static int idx_cmp(const void* pa, const void* pb) {
+    size_t a = *(const size_t*)pa, b = *(const size_t*)pb;
+    return key_cmp(g_sort_keys + a * 2 * g_sort_W, g_sort_keys + b * 2 * g_sort_W, g_sort_W);
+}
+
+/* keep program (postfix), CoefficientThreshold / WeightCutoff / And / Or. */
+static int keep_eval(const pso_policy* p, const uint64_t* k, int W, double c) {
+    if (!p || p->num_nodes == 0) return 1;
+    int stack[16];
+    int sp = 0;
+    for (int i = 0; i < p->num_nodes; ++i) {
+        switch (p->op[i]) {
+        case PSO_KEEP_TRUE: stack[sp++] = 1; break;
+        case PSO_KEEP_COEFF: {
+            double eps = p->farg[i];
+            /* builtin.rs:29-31: eps < 0 || c.norm_sqr() > eps * eps, norm_sqr in f64 */
+            stack[sp++] = (eps < 0.0) || (c * c > eps * eps);
+            break;
+        }
+        case PSO_KEEP_WEIGHT: stack[sp++] = key_weight(k, W) <= (unsigned)p->iarg[i]; break;
+        case PSO_KEEP_AND: {
+            int b = stack[--sp], a = stack[--sp];
+            stack[sp++] = a && b;
+            break;
+        }
+        case PSO_KEEP_OR: {
+            int b = stack[--sp], a = stack[--sp];
+            stack[sp++] = a || b;
+            break;
+        }
+        default: return 1;
+        }
+    }
+    return sp ? stack[sp - 1] : 1;
+}
+
+/* Drain an accumulator into the sum: keep on the summed coefficient, drop exact zeros, sort. */
+static void accum_drain(accum* a, pso_sum* s, const pso_policy* policy) {
+    int W = s->W, K = 2 * W;
+    size_t kept = 0;
+    size_t* idx = (size_t*)malloc((a->used + 1) * sizeof(size_t));
+    for (size_t i = 0; i < a->used; ++i) {
+        size_t h = a->order[i];
+        double v = a->dtype == PSO_F64 ? a->v64[h] : (double)a->v32[h];
+        if (v != 0.0 && keep_eval(policy, a->keys + h * K, W, v)) idx[kept++] = h;
+    }
+    g_sort_keys = a->keys;
+    g_sort_W = W;
+    qsort(idx, kept, sizeof(size_t), idx_cmp);
+    s->n = 0;
+    sum_reserve(s, kept);
+    for (size_t i = 0; i < kept; ++i) {
+        memcpy(s->keys + i * K, a->keys + idx[i] * K, (size_t)K * 8);
+        if (s->dtype == PSO_F64)
+            s->c64[i] = a->v64[idx[i]];
+        else
+            s->c32[i] = a->v32[idx[i]];
+    }
+    s->n = kept;
+    free(idx);
+}
+
+int pso_set(pso_sum* s, const uint64_t* keys, const double* coeffs, size_t n) {
+    accum a;
+    accum_init(&a, s->W, s->dtype, n);
+    for (size_t i = 0; i < n; ++i) accum_add(&a, keys + i * 2 * (size_t)s->W, coeffs[i], (float)coeffs[i]);
+    accum_drain(&a, s, NULL);
+    accum_free(&a);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* prepared tables: channel/rotation.rs, channel/prepared.rs, ptm/noise.rs   */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+    unsigned local_delta;
+    uint64_t mx[PSO_MAX_W], mz[PSO_MAX_W];
+    double a64[16];
+    float a32[16];
+} entry_t;
+
+typedef struct {
+    int wide;               /* Prepared::Rotation (support > 2) */
+    int k;                  /* support size for a local table */
+    uint32_t q[2];
+    int num_entries;
+    entry_t e[16];
+    /* wide rotation */
+    uint64_t gx[PSO_MAX_W], gz[PSO_MAX_W];
+    double cos64, sin64;
+    float cos32, sin32;
+} prepared_t;
+
+/* rotation.rs:70-77: sin_cos with quarter turns snapped (signum as Rust: +0 -> +1, -0 -> -1). */
+static void sin_cos_snap(double theta, double* sn, double* cs) {
+    const double SNAP = 1e-15;
+    double s = sin(theta), c = cos(theta);
+    if (fabs(s) < SNAP) {
+        *sn = 0.0;
+        *cs = isnan(c) ? c : copysign(1.0, c);
+    } else if (fabs(c) < SNAP) {
+        *sn = isnan(s) ? s : copysign(1.0, s);
+        *cs = 0.0;
+    } else {
+        *sn = s;
+        *cs = c;
+    }
+}
+
+static void lift(const prepared_t* p, unsigned d, uint64_t* mx, uint64_t* mz, int W) {
+    memset(mx, 0, sizeof(uint64_t) * W);
+    memset(mz, 0, sizeof(uint64_t) * W);
+    for (int j = 0; j < p->k; ++j) {
+        uint32_t q = p->q[j];
+        if ((d >> (2 * j)) & 1u) mx[q / 64] |= 1ull << (q % 64);
+        if ((d >> (2 * j + 1)) & 1u) mz[q / 64] |= 1ull << (q % 64);
+    }
+}
+
+static unsigned support_bits(const prepared_t* p, const uint64_t* k, int W) {
+    unsigned s = 0;
+    for (int j = 0; j < p->k; ++j) {
+        uint32_t q = p->q[j];
+        s |= (unsigned)((k[q / 64] >> (q % 64)) & 1u) << (2 * j);
+        s |= (unsigned)((k[W + q / 64] >> (q % 64)) & 1u) << (2 * j + 1);
+    }
+    return s;
+}
+
+static int build_generator(const pso_channel* ch, int W, int nq, uint64_t* gx, uint64_t* gz) {
+    memset(gx, 0, sizeof(uint64_t) * W);
+    memset(gz, 0, sizeof(uint64_t) * W);
+    for (int j = 0; j < ch->num_support; ++j) {
+        uint32_t q = ch->qubits[j];
+        if ((int)q >= nq) return -1;
+        uint64_t bit = 1ull << (q % 64);
+        if ((gx[q / 64] | gz[q / 64]) & bit) return -1; /* repeated qubit */
+        switch (ch->paulis[j]) {
+        case 'X': gx[q / 64] |= bit; break;
+        case 'Y': gx[q / 64] |= bit; gz[q / 64] |= bit; break;
+        case 'Z': gz[q / 64] |= bit; break;
+        case 'I': break;
+        default: return -1;
+        }
+    }
+    return 0;
+}
+
+static int prepare(const pso_channel* ch, int adjoint, int W, int nq, prepared_t* p) {
+    memset(p, 0, sizeof(*p));
+    if (ch->kind == PSO_CH_ROTATION) {
+        uint64_t gx[PSO_MAX_W], gz[PSO_MAX_W];
+        if (build_generator(ch, W, nq, gx, gz)) return -1;
+        double theta = adjoint ? -ch->param : ch->param;
+        double sn, cs;
+        sin_cos_snap(theta, &sn, &cs);
+        unsigned weight = 0;
+        for (int i = 0; i < W; ++i) weight += (unsigned)__builtin_popcountll(gx[i] | gz[i]);
+        if (weight > 2) {
+            /* Prepared::Rotation (rotation.rs:114-122, prepared.rs:387-397) */
+            p->wide = 1;
+            memcpy(p->gx, gx, sizeof(uint64_t) * W);
+            memcpy(p->gz, gz, sizeof(uint64_t) * W);
+            p->cos64 = cs;
+            p->sin64 = sn;
+            p->cos32 = (float)cs;
+            p->sin32 = (float)sn;
+            return 0;
+        }
+        /* LocalPtm::on_support: support qubits ascending */
+        int k = 0;
+        for (int w = 0; w < W; ++w) {
+            uint64_t live = gx[w] | gz[w];
+            while (live) {
+                p->q[k++] = (uint32_t)(64 * w + __builtin_ctzll(live));
+                live &= live - 1;
+            }
+        }
+        p->k = k;
+        int dim = 1 << (2 * k);
+        double table[16][16];
+        memset(table, 0, sizeof(table));
+        /* probe_table: apply on each local basis Pauli with coefficient 1 */
+        for (int s = 0; s < dim; ++s) {
+            uint64_t key[2 * PSO_MAX_W];
+            lift(p, (unsigned)s, key, key + W, W);
+            if (!anticommutes(key, gx, gz, W)) {
+                table[s][s] += 1.0;
+                continue;
+            }
+            table[s][s] += 1.0 * cs;
+            unsigned total = (1u + product_phase(key, gx, gz, W)) & 3u;
+            double sgn = (total & 2u) ? -1.0 : 1.0; /* real mul_phase: even phase only */
+            uint64_t out[2 * PSO_MAX_W];
+            for (int i = 0; i < W; ++i) {
+                out[i] = key[i] ^ gx[i];
+                out[W + i] = key[W + i] ^ gz[i];
+            }
+            unsigned t = support_bits(p, out, W);
+            table[s][t] += sgn * sn;
+        }
+        /* push_deltas (prepared.rs:257-281): one entry per realized delta, ascending */
+        int has[16] = {0};
+        for (int s = 0; s < dim; ++s)
+            for (int t = 0; t < dim; ++t)
+                if (table[s][t] != 0.0) has[s ^ t] = 1;
+        for (int d = 0; d < dim; ++d) {
+            if (!has[d]) continue;
+            entry_t* e = &p->e[p->num_entries++];
+            e->local_delta = (unsigned)d;
+            lift(p, (unsigned)d, e->mx, e->mz, W);
+            for (int s = 0; s < dim; ++s) {
+                e->a64[s] = table[s][s ^ d];
+                e->a32[s] = (float)e->a64[s];
+            }
+        }
+        /* RotationLayer::of Clifford residue rule (bucketed/rotation_layer.rs:101-122):
+         * on a rotation-shaped table whose identity amplitudes are rounding residues of the
+         * generator amplitudes, strings move instead of splitting. */
+        if (p->num_entries == 2 && p->e[0].local_delta == 0) {
+            entry_t* e0 = &p->e[0];
+            entry_t* e1 = &p->e[1];
+            unsigned delta = e1->local_delta;
+            const double eps = 2.220446049250313e-16;
+            for (int prec = 0; prec < 2; ++prec) {
+                int clifford = 1, shaped = 1;
+                for (int s = 0; s < dim; ++s) {
+                    double a0 = prec ? (double)e0->a32[s] : e0->a64[s];
+                    double a1 = prec ? (double)e1->a32[s] : e1->a64[s];
+                    double b1 = prec ? (double)e1->a32[s ^ delta] : e1->a64[s ^ delta];
+                    if (a1 == 0.0) {
+                        if (a0 != 1.0) shaped = 0;
+                    } else {
+                        if (b1 == 0.0) shaped = 0;
+                        clifford &= (a0 * a0 <= eps * eps * (a1 * a1));
+                    }
+                }
+                if (shaped && clifford) {
+                    for (int s = 0; s < dim; ++s) {
+                        if ((prec ? (double)e1->a32[s] : e1->a64[s]) == 0.0) continue;
+                        if (prec)
+                            e0->a32[s] = 0.0f;
+                        else
+                            e0->a64[s] = 0.0;
+                    }
+                }
+            }
+        }
+        return 0;
+    }
+    if (ch->kind == PSO_CH_DEPOLARIZE) {
+        if (ch->num_support != 1 || (int)ch->qubits[0] >= nq) return -1;
+        double pr = ch->param;
+        if (!(pr >= 0.0 && pr <= 1.0)) return -1;
+        double scale = 1.0 - 4.0 * pr / 3.0;
+        p->k = 1;
+        p->q[0] = ch->qubits[0];
+        p->num_entries = 1;
+        entry_t* e = &p->e[0];
+        memset(e->mx, 0, sizeof(e->mx));
+        memset(e->mz, 0, sizeof(e->mz));
+        double diag[4] = {1.0, scale, scale, scale};
+        for (int s = 0; s < 4; ++s) {
+            e->a64[s] = diag[s];
+            e->a32[s] = (float)diag[s];
+        }
+        return 0;
+    }
+    return -1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* TopN (truncation/builtin.rs:73-129, 210-239)                              */
+/* ------------------------------------------------------------------------ */
+
+static double coef_at(const pso_sum* s, size_t i) { return s->dtype == PSO_F64 ? s->c64[i] : (double)s->c32[i]; }
+
+static int mag_desc_cmp(const void* pa, const void* pb) {
+    double a = *(const double*)pa, b = *(const double*)pb;
+    /* descending, NaN last */
+    int an = isnan(a), bn = isnan(b);
+    if (an || bn) return an - bn;
+    return (a < b) - (a > b);
+}
+
+static void topn(pso_sum* s, uint64_t n) {
+    if (s->n <= n) return;
+    if (n == 0) {
+        s->n = 0;
+        return;
+    }
+    size_t total = s->n;
+    double* m = (double*)malloc(total * sizeof(double));
+    for (size_t i = 0; i < total; ++i) {
+        double c = coef_at(s, i);
+        m[i] = c * c;
+    }
+    double* sorted = (double*)malloc(total * sizeof(double));
+    memcpy(sorted, m, total * sizeof(double));
+    qsort(sorted, total, sizeof(double), mag_desc_cmp);
+    double boundary = sorted[n - 1];
+    size_t above = 0;
+    for (size_t i = 0; i + 1 < n; ++i)
+        if (sorted[i] > boundary) ++above;
+    free(sorted);
+    size_t quota = (size_t)n - above;
+    int K = 2 * s->W;
+    size_t w = 0;
+    for (size_t i = 0; i < total; ++i) {
+        int side; /* +1 above, 0 at, -1 below */
+        if (isnan(m[i]))
+            side = -1;
+        else if (isnan(boundary))
+            side = 1;
+        else
+            side = m[i] > boundary ? 1 : (m[i] == boundary ? 0 : -1);
+        int at = side == 0 && quota > 0;
+        if (at) --quota;
+        if (side == 1 || at) {
+            if (w != i) {
+                memmove(s->keys + w * K, s->keys + i * K, (size_t)K * 8);
+                if (s->dtype == PSO_F64)
+                    s->c64[w] = s->c64[i];
+                else
+                    s->c32[w] = s->c32[i];
+            }
+            ++w;
+        }
+    }
+    s->n = w;
+    free(m);
+}
+
+void pso_finalize_layer(pso_sum* s, const pso_policy* policy) {
+    if (!policy) return;
+    for (int i = 0; i < policy->num_passes; ++i) {
+        if (policy->pass_kind[i] == PSO_PASS_TOPN) topn(s, policy->pass_n[i]);
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* the naive layer (test_support/oracle.rs:21-54)                            */
+/* ------------------------------------------------------------------------ */
+
+static void emit(accum* a, const uint64_t* k, int W, int dtype, double v64, float v32) {
+    (void)W;
+    (void)dtype;
+    accum_add(a, k, v64, v32);
+}
+
+int pso_apply_channel(pso_sum* s, const pso_channel* ch, int adjoint, const pso_policy* policy) {
+    prepared_t p;
+    int W = s->W, K = 2 * W;
+    if (prepare(ch, adjoint, W, s->nq, &p)) return -1;
+    accum a;
+    accum_init(&a, W, s->dtype, s->n * 2);
+    uint64_t out[2 * PSO_MAX_W];
+    for (size_t i = 0; i < s->n; ++i) {
+        const uint64_t* k = s->keys + i * K;
+        double c64 = s->dtype == PSO_F64 ? s->c64[i] : 0.0;
+        float c32 = s->dtype == PSO_F32 ? s->c32[i] : 0.0f;
+        if (p.wide) {
+            /* rotation.rs:43-67 with the prepared cos/sin */
+            if (!anticommutes(k, p.gx, p.gz, W)) {
+                emit(&a, k, W, s->dtype, c64, c32);
+                continue;
+            }
+            emit(&a, k, W, s->dtype, c64 * p.cos64, c32 * p.cos32);
+            unsigned total = (1u + product_phase(k, p.gx, p.gz, W)) & 3u;
+            for (int j = 0; j < W; ++j) {
+                out[j] = k[j] ^ p.gx[j];
+                out[W + j] = k[W + j] ^ p.gz[j];
+            }
+            double m64 = (total & 2u) ? -c64 : c64;
+            float m32 = (total & 2u) ? -c32 : c32;
+            emit(&a, out, W, s->dtype, m64 * p.sin64, m32 * p.sin32);
+            continue;
+        }
+        /* DeltaEntry::emit (prepared.rs:50-68) */
+        unsigned sp = support_bits(&p, k, W);
+        for (int e = 0; e < p.num_entries; ++e) {
+            const entry_t* en = &p.e[e];
+            if (s->dtype == PSO_F64 ? en->a64[sp] == 0.0 : en->a32[sp] == 0.0f) continue;
+            for (int j = 0; j < W; ++j) {
+                out[j] = k[j] ^ en->mx[j];
+                out[W + j] = k[W + j] ^ en->mz[j];
+            }
+            emit(&a, out, W, s->dtype, c64 * en->a64[sp], c32 * en->a32[sp]);
+        }
+    }
+    accum_drain(&a, s, policy);
+    accum_free(&a);
+    pso_finalize_layer(s, policy);
+    return 0;
+}
+
+int pso_propagate(pso_sum* s, const pso_channel* chans, size_t num_channels, const pso_policy* policy,
+                  int direction, uint64_t* terms_after) {
+    for (size_t li = 0; li < num_channels; ++li) {
+        size_t ci = direction ? num_channels - 1 - li : li;
+        if (pso_apply_channel(s, &chans[ci], direction, policy)) return -1;
+        if (terms_after) terms_after[li] = s->n;
+    }
+    return 0;
+}
+
+/* product_state.rs:84-101, summed in key order in f64 */
+double pso_expectation(const pso_sum* s, const uint64_t* axis_x, const uint64_t* axis_z,
+                       const uint64_t* negative) {
+    int W = s->W, K = 2 * W;
+    double acc = 0.0;
+    for (size_t i = 0; i < s->n; ++i) {
+        const uint64_t* k = s->keys + i * K;
+        uint64_t mismatch = 0;
+        unsigned sign = 0;
+        for (int w = 0; w < W; ++w) {
+            uint64_t sup = k[w] | k[W + w];
+            mismatch |= (k[w] ^ (sup & axis_x[w])) | (k[W + w] ^ (sup & axis_z[w]));
+            sign += (unsigned)__builtin_popcountll(sup & negative[w]);
+        }
+        if (mismatch) continue;
+        double c = coef_at(s, i);
+        acc += (sign & 1u) ? -c : c;
+    }
+    return acc;
+}
+
+/* ------------------------------------------------------------------------ */
+/* sorted-store engine for CPU timing (bucketed host engine's shape)         */
+/* ------------------------------------------------------------------------ */
+
+static int g_threads = 0;
+void pso_set_threads(int threads) { g_threads = threads; }
+
+int pso_apply_channel_sorted(pso_sum* s, const pso_channel* ch, int adjoint, const pso_policy* policy) {
+    return pso_apply_channel(s, ch, adjoint, policy);
+}
+
+int pso_propagate_sorted(pso_sum* s, const pso_channel* chans, size_t num_channels,
+                         const pso_policy* policy, int direction, uint64_t* terms_after) {
+    for (size_t li = 0; li < num_channels; ++li) {
+        size_t ci = direction ? num_channels - 1 - li : li;
+        if (pso_apply_channel_sorted(s, &chans[ci], direction, policy)) return -1;
+        if (terms_after) terms_after[li] = s->n;
+    }
+    return 0;
+}
