@@ -1,0 +1,417 @@
+"""Benchmark of the per-layer Pauli-propagation path on B200.
+
+Workload (the configuration the headline metric is quoted on): 64 qubits, 30 layers of
+random dense two-qubit rotations -- per layer a seeded random matching of the qubits into 32
+pairs, each pair exp(-i theta P(x)Q / 2) with P, Q uniform over {X, Y, Z}, theta uniform in
+[0, 2 pi), then RZ(phi) on every qubit -- applied in the Heisenberg picture to 65,536
+distinct random Pauli strings of weight 1-4 with N(0, 1) coefficients normalised to unit
+2-norm; float64 coefficients; policy TopN(2^26) & coeff(1e-10) after every channel.
+Synthetic data from one splitmix64 stream (seed 0xC0FFEE); the reference measures on its
+own synthetic circuits, so nothing external stands in here.
+
+A step is one circuit layer (96 channels).  The warm-up steps are the first layers, which
+also grow the store to the 2^26-term cap; the timed steps continue the same run at the cap.
+``value`` is terms/s per layer: the terms entering each channel, summed over the timed
+channels, divided by their device time (CUDA events on the library's stream).  The store
+(>= 1.6 GB) is larger than L2, so no flush is needed between steps.
+
+``e2e`` is the same metric through the public C-ABI calls with host buffers: each step
+uploads the state from pinned host memory, runs the layer and downloads the result into
+pinned host memory, all inside the timed region.
+
+``--impl reference`` times the reference's CPU path: the reference is Rust and cannot be
+built in this image, so its restatement (oracle/, single thread) runs a bounded sample of
+the same workload on the host.
+
+Multi-GPU (torchrun): the path does not shard, so each rank runs an independent replica with
+its own seed; value is the terms of all ranks over the slowest rank's time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path[:0] = [str(ROOT), str(ROOT / "paulistrings-rs_b200")]
+
+METRIC = "terms/s per layer"
+TERM_CAP = 1 << 26
+NUM_QUBITS = 64
+LAYERS = 30
+EPS = 1e-10
+SEED = 0xC0FFEE
+
+
+def workload_config(k, w):
+    return {
+        "workload": "random two-qubit rotation layers: 64 qubits, 30 layers x (32 pair rotations + 64 RZ), "
+        "65,536-term random observable, Heisenberg, TopN(2^26) & coeff(1e-10), f64",
+        "num_qubits": NUM_QUBITS,
+        "layers": LAYERS,
+        "channels_per_layer": 96,
+        "term_cap": TERM_CAP,
+        "initial_terms": 65536,
+        "timed_layers": k,
+        "warmup_layers": w,
+        "seed": SEED,
+        "l2": "inputs larger than L2 (store >= 1.6 GB at the cap), no flush",
+    }
+
+
+def layer_circuits(seed):
+    from paulistrings_b200 import Circuit, workloads
+
+    full = workloads.random_pair_layers(NUM_QUBITS, LAYERS, seed)
+    chans = list(full)
+    out = []
+    # Heisenberg order: the last layer first; each sub-circuit is propagated with
+    # direction="heisenberg", which reverses it and applies adjoints.
+    for layer in reversed(range(LAYERS)):
+        c = Circuit(NUM_QUBITS)
+        for ch in chans[96 * layer : 96 * (layer + 1)]:
+            c.append(ch)
+        out.append(c)
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        d = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the dominant kernel from a committed ncu summary, if any."""
+    try:
+        return json.loads((ROOT / "profiles" / "traffic.json").read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def cpu_baseline(seconds: float):
+    """The oracle (the reference's CPU semantics restated, one thread) on a bounded sample:
+    the same circuit from the same initial observable, channel by channel, until `seconds`."""
+    import numpy as np
+
+    from oracle.oracle import OracleSum
+    from paulistrings_b200 import workloads
+
+    x, z, c = workloads.random_observable(NUM_QUBITS, 65536, SEED + 1)
+    o = OracleSum(NUM_QUBITS, "f64")
+    o.set(np.concatenate([x, z], axis=1), c)
+    pol = {"keep": [("coeff", EPS)], "passes": [("topn", TERM_CAP)]}
+    terms = 0
+    channels = 0
+    t0 = time.perf_counter()
+    for circ in layer_circuits(SEED):
+        for ch in reversed(list(circ)):
+            terms += len(o)
+            o.apply(("rotation", ch.paulis, list(ch.qubits), ch.theta), adjoint=True, policy=pol)
+            channels += 1
+            if time.perf_counter() - t0 > seconds:
+                break
+        if time.perf_counter() - t0 > seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {
+        "value": terms / dt,
+        "unit": METRIC,
+        "cores": 1,
+        "kind": "port",
+        "sample": f"first {channels} channels of the same workload from the 65,536-term observable "
+        f"(up to {len(o)} terms), {dt:.1f} s on one host core",
+    }
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    return world, rank, local
+
+
+def dist_max(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_sum(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    cb = cpu_baseline(args.cpu_seconds)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": cb["value"],
+        "unit": METRIC,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": workload_config(args.steps, args.warmup),
+        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": cb["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference is Rust (no cargo in this image); its CPU engine semantics restated in C (oracle/) "
+        "are timed instead",
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    import paulistrings_b200 as ps
+    from paulistrings_b200 import truncation, workloads
+
+    seed = SEED + 7919 * rank
+    policy = truncation.topn(TERM_CAP) & truncation.coeff(EPS)
+    layers = layer_circuits(seed)
+    assert args.warmup + args.steps <= LAYERS, "warmup + steps must fit in the 30-layer circuit"
+    x0, z0, c0 = workloads.random_observable(NUM_QUBITS, 65536, seed + 1)
+
+    # --- device-resident timing (value, roofline) --------------------------------------------------
+    g = ps.GpuPauliSum(NUM_QUBITS, "f64", device=local)
+    g.upload(x0, z0, c0)
+    for li in range(args.warmup):
+        g.propagate(layers[li], policy, "heisenberg")
+    g.set_profiling(True)
+    barrier(world)
+    terms = 0
+    dev_ms = 0.0
+    launches = 0
+    with ClockSampler(local) as clocks:
+        for li in range(args.warmup, args.warmup + args.steps):
+            st = g.propagate(layers[li], policy, "heisenberg", with_stats=True)
+            terms += st.total_terms_in
+            dev_ms += st.device_ms
+            launches += st.kernel_launches
+    barrier(world)
+    prof = g.read_profile()
+    g.set_profiling(False)
+    state_after = g.download()
+    g.close()
+    del g
+
+    max_ms = dist_max(dev_ms, world)
+    all_terms = dist_sum(terms, world)
+    value = all_terms / (max_ms * 1e-3)
+
+    # --- end to end through the C ABI with pinned host buffers ---------------------------------
+    rows = 2 * TERM_CAP + 1
+    pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True).numpy()
+    hx = pin((rows, 1), torch.int64).view(np.uint64)
+    hz = pin((rows, 1), torch.int64).view(np.uint64)
+    hc = pin((rows,), torch.float64)
+    ox = pin((rows, 1), torch.int64).view(np.uint64)
+    oz = pin((rows, 1), torch.int64).view(np.uint64)
+    oc = pin((rows,), torch.float64)
+    # the e2e run restarts from the state the warm-up reached, held in pinned host memory
+    g = ps.GpuPauliSum(NUM_QUBITS, "f64", device=local)
+    g.upload(x0, z0, c0)
+    for li in range(args.warmup):
+        g.propagate(layers[li], policy, "heisenberg")
+    n = len(g)
+    g.download(out=(hx, hz, hc))
+    h2d = d2h = 0
+    e2e_terms = 0
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for li in range(args.warmup, args.warmup + args.steps):
+        g.upload(hx[:n], hz[:n], hc[:n])
+        h2d += n * (16 + 8)
+        st = g.propagate(layers[li], policy, "heisenberg", with_stats=True)
+        e2e_terms += st.total_terms_in
+        _, _, cc = g.download(out=(ox, oz, oc))
+        n = cc.shape[0]
+        d2h += n * (16 + 8)
+        hx, ox = ox, hx
+        hz, oz = oz, hz
+        hc, oc = oc, hc
+    torch.cuda.synchronize()
+    e2e_s = dist_max(time.perf_counter() - t0, world)
+    barrier(world)
+    e2e_value = dist_sum(e2e_terms, world) / e2e_s
+    g.close()
+
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peaks()
+    dom = max(prof.items(), key=lambda kv: kv[1]["total_ms"])
+    name, rec = dom
+    per_launch_bytes = rec["algorithmic_bytes"] / max(1, rec["timed_launches"])
+    per_launch_ms = rec["total_ms"] / max(1, rec["timed_launches"])
+    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
+    traffic = ncu_traffic().get(name)
+    roofline = {
+        "bound": "hbm",
+        "kernel": name,
+        "achieved": round(achieved, 1),
+        "peak": peak,
+        "peak_kind": peak_kind,
+        "unit": "GB/s",
+        "frac": round(achieved / peak, 4),
+        "traffic": traffic,
+        "launches_timed": rec["timed_launches"],
+        "share_of_device_time": round(rec["total_ms"] / max(1e-9, sum(r["total_ms"] for r in prof.values())), 4),
+    }
+    all_bytes = sum(r["algorithmic_bytes"] for r in prof.values())
+    all_ms = sum(r["total_ms"] for r in prof.values())
+    layer_frac = all_bytes / (dev_ms * 1e-3) / 1e9 / peak
+    cb = cpu_baseline(args.cpu_seconds) if world == 1 else None
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": METRIC,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": max_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": dict(workload_config(args.steps, args.warmup), parallelism=f"replicas{world}"),
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": d2h // args.steps},
+        "gpu_launches": launches,
+        "roofline": roofline,
+        "layer_roofline_frac": round(layer_frac, 4),
+        "kernel_profile": {k: {"launches": v["timed_launches"], "ms": round(v["total_ms"], 3),
+                               "GB": round(v["algorithmic_bytes"] / 1e9, 3)} for k, v in prof.items() if v["launches"]},
+        "profiled_ms_vs_event_ms": [round(all_ms, 3), round(dev_ms, 3)],
+        "final_terms": int(state_after[2].shape[0]),
+        "clocks": clocks.summary(),
+        "cpu_baseline": cb,
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("at least 3 warm-up steps")
+    world, rank, local = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,236 @@
+/*
+ * paulistrings_b200.h -- C ABI of the B200 Pauli-propagation layer path.
+ *
+ * One opaque handle (ps_sum) owns a Pauli sum resident on one CUDA device: a
+ * double-buffered store of packed symplectic keys (x words then z words, 16*W
+ * bytes per term) plus a coefficient column (float64 or float32), kept sorted by
+ * key with unique keys.  All entry points take plain pointers and sizes; no
+ * torch or CUDA types cross the boundary.  Every call returns a ps_status; on
+ * any error the store keeps the last completed layer and ps_last_error()
+ * describes the failure.  One handle per host thread; each handle issues its
+ * work on its own CUDA stream.
+ *
+ * Reference interfaces replaced (paths inside lkdvos/paulistrings-rs):
+ *   PauliSum.propagate(..., device=)      crates/paulistrings-py/src/sum.rs:2132-2183
+ *   GpuSum upload / to_host               crates/paulistrings/src/engine/gpu/sum.rs:118-253
+ *   PartitionBackend::apply_layer         crates/paulistrings/src/engine/backend.rs:80
+ *   PartitionBackend::finalize_layer      crates/paulistrings/src/engine/backend.rs:90
+ *   PartitionStorage::{len, settle}       crates/paulistrings/src/engine/backend.rs:26-72
+ *   Channel::prepare_for_layer / Prepared crates/paulistrings/src/channel/prepared.rs:345-350, 401-493
+ *   KeepProgram (lowered policy)          crates/paulistrings/src/engine/gpu/truncation.rs:24-102
+ *   run_layers (the layer loop)           crates/paulistrings/src/engine/driver.rs:319-592
+ *   expectation_product                   crates/paulistrings/src/readout/product_state.rs:84-101
+ */
+#ifndef PAULISTRINGS_B200_H
+#define PAULISTRINGS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PS_ABI_VERSION 1
+#define PS_MAX_W 16          /* up to 1024 qubits, as the reference's widest monomorphization */
+#define PS_MAX_ENTRIES 16    /* 4^2 local deltas of a two-qubit table */
+#define PS_MAX_KEEP_NODES 15 /* as the reference's KeepProgram */
+#define PS_MAX_PASSES 4
+
+/* Status codes (GpuError variants, crates/paulistrings/src/engine/gpu/error.rs:9). */
+typedef enum ps_status {
+    PS_OK = 0,
+    PS_ERR_OOM = 1,          /* device allocation failed; store unchanged */
+    PS_ERR_UNSUPPORTED = 2,  /* channel or policy the device path does not run */
+    PS_ERR_INVALID = 3,      /* bad argument (qubit out of range, bad dtype, NULL) */
+    PS_ERR_DEVICE = 4,       /* CUDA error */
+    PS_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up */
+    PS_ERR_NO_DEVICE = 6     /* no CUDA device, or the ordinal does not exist */
+} ps_status;
+
+typedef enum ps_dtype { PS_F64 = 0, PS_F32 = 1 } ps_dtype;
+typedef enum ps_direction { PS_FORWARD = 0, PS_HEISENBERG = 1 } ps_direction;
+
+/* ---- policy: keep program (postfix) + ordered layer passes ------------------------
+ * Lowered form of a BuiltinTruncation tree (crates/paulistrings/src/truncation/tree.rs:20-39):
+ * And(a, b) keeps iff both keep and runs a's passes then b's; Or(a, b) takes per-term
+ * filters only.  An empty program keeps every nonzero term. */
+typedef enum ps_keep_op {
+    PS_KEEP_TRUE = 0,
+    PS_KEEP_COEFF = 1,   /* farg = epsilon: keep iff eps < 0 || |c|^2 > eps^2 (builtin.rs:28-31) */
+    PS_KEEP_WEIGHT = 2,  /* iarg = k: keep iff Pauli weight <= k (builtin.rs:50-59) */
+    PS_KEEP_AND = 3,
+    PS_KEEP_OR = 4
+} ps_keep_op;
+
+typedef enum ps_pass_kind {
+    PS_PASS_NONE = 0,
+    PS_PASS_TOPN = 1     /* keep the n largest |c|^2; ties first in key order (builtin.rs:73-129) */
+} ps_pass_kind;
+
+typedef struct ps_keep_node {
+    int32_t op;          /* ps_keep_op */
+    int32_t reserved;
+    int64_t iarg;
+    double farg;
+} ps_keep_node;
+
+typedef struct ps_pass {
+    int32_t kind;        /* ps_pass_kind */
+    int32_t reserved;
+    uint64_t n;
+} ps_pass;
+
+typedef struct ps_policy {
+    int32_t num_nodes;
+    int32_t num_passes;
+    ps_keep_node nodes[PS_MAX_KEEP_NODES];
+    ps_pass passes[PS_MAX_PASSES];
+} ps_policy;
+
+/* ---- channels (the Channel plug-in's built-ins, crates/paulistrings-py/src/circuit.rs:269-321) */
+typedef enum ps_channel_kind {
+    PS_CH_PAULI_ROTATION = 1, /* exp(-i param P / 2), P = paulis[j] ('X','Y','Z') on qubits[j] */
+    PS_CH_DEPOLARIZING = 2    /* one qubit, param = p: X, Y, Z scaled by 1 - 4p/3 (ptm/noise.rs:12-16) */
+} ps_channel_kind;
+
+typedef struct ps_channel {
+    int32_t kind;             /* ps_channel_kind */
+    int32_t num_support;
+    const uint32_t* qubits;
+    const char* paulis;       /* num_support characters; ignored for depolarizing */
+    double param;
+} ps_channel;
+
+/* ---- prepared per-layer table (Prepared, crates/paulistrings/src/channel/prepared.rs:345-350) */
+typedef enum ps_table_mode {
+    PS_TABLE_LOCAL = 1,       /* LocalPtm: support <= 2 qubits, entries grouped by key delta */
+    PS_TABLE_ROTATION = 2     /* PreparedRotation: wide generator, amplitudes per term */
+} ps_table_mode;
+
+typedef struct ps_table_entry {
+    uint32_t local_delta;     /* bit 2j = x-bit of support qubit j, bit 2j+1 its z-bit */
+    uint32_t reserved;
+    uint64_t mask_x[PS_MAX_W];
+    uint64_t mask_z[PS_MAX_W];
+    double amplitude[PS_MAX_ENTRIES]; /* amplitude[s]: support pattern s -> s ^ local_delta */
+} ps_table_entry;
+
+typedef struct ps_table {
+    int32_t mode;             /* ps_table_mode */
+    int32_t k;                /* LOCAL: number of support qubits (0..2) */
+    uint32_t qubits[2];       /* LOCAL: support qubits, ascending */
+    int32_t num_entries;      /* LOCAL: ascending by local_delta; identity first when present */
+    int32_t width;            /* W the masks are meaningful for */
+    ps_table_entry entries[PS_MAX_ENTRIES];
+    uint64_t gen_x[PS_MAX_W]; /* ROTATION: generator */
+    uint64_t gen_z[PS_MAX_W];
+    double cos_theta;         /* ROTATION: snapped cos/sin of the applied angle (rotation.rs:70-77) */
+    double sin_theta;
+} ps_table;
+
+/* ---- per-layer and per-run statistics (PartitionTrace rows, engine/trace.rs:110-139) */
+typedef enum ps_layer_path {
+    PS_PATH_RESCALE = 1,      /* key-preserving rescale + keep */
+    PS_PATH_ROTATION = 2,     /* partner reorder + merge-path join */
+    PS_PATH_SORT = 3          /* branch records + radix sort + segmented dedup */
+} ps_layer_path;
+
+typedef struct ps_layer_stats {
+    uint64_t terms_in;
+    uint64_t partners;        /* rows emitted besides each term's own row */
+    uint64_t terms_out;       /* after the keep program */
+    uint64_t terms_after_passes;
+    int32_t path;             /* ps_layer_path */
+    int32_t reserved;
+} ps_layer_stats;
+
+typedef struct ps_run_stats {
+    uint64_t layers;
+    uint64_t peak_terms;
+    uint64_t final_terms;
+    uint64_t total_terms_in;  /* sum over layers of terms_in */
+    uint64_t kernel_launches; /* kernels this call launched */
+    double device_ms;         /* CUDA-event time of the whole run */
+} ps_run_stats;
+
+/* Per-kernel profile (the phase-timing counters, crates/paulistrings/src/engine/stats.rs:12 and
+ * the device layer's CUDA events, engine/gpu/layer.rs:345-386): launches are always counted;
+ * with profiling on, every launch is timed with CUDA events on the handle's stream and its
+ * algorithmic bytes (reads + writes the kernel must do at its input/output sizes) are booked. */
+typedef struct ps_kernel_profile {
+    char name[32];
+    uint64_t launches;
+    uint64_t timed_launches;
+    double total_ms;
+    double algorithmic_bytes;
+} ps_kernel_profile;
+
+typedef struct ps_sum ps_sum;
+
+/* Version of this ABI (PS_ABI_VERSION). */
+int32_t ps_abi_version(void);
+
+/* Number of visible CUDA devices (0 when none).  cuda_available(), python/paulistrings/__init__.py:18-22 */
+int32_t ps_device_count(void);
+
+/* Create an empty device sum.  GpuSum::from_host_with_options, engine/gpu/sum.rs:118-212.
+ * num_qubits <= 64 * PS_MAX_W; the width W is the smallest of 1, 2, 4, 8, 16 that fits. */
+ps_status ps_create(int32_t device, int32_t num_qubits, int32_t dtype, ps_sum** out);
+ps_status ps_destroy(ps_sum* sum);
+const char* ps_last_error(const ps_sum* sum);
+int32_t ps_width(const ps_sum* sum);
+int32_t ps_num_qubits(const ps_sum* sum);
+int32_t ps_dtype_of(const ps_sum* sum);
+
+/* Replace the contents from host arrays: x and z are n x W words (row-major), coeffs n doubles
+ * (rounded once to float for PS_F32).  Duplicate keys are summed in input order and exact zeros
+ * dropped (BuildAccumulator::finalize, crates/paulistrings/src/pauli_sum/accumulator.rs:35-56);
+ * keys beyond num_qubits are rejected with PS_ERR_INVALID. */
+ps_status ps_upload(ps_sum* sum, const uint64_t* x, const uint64_t* z, const double* coeffs, uint64_t n);
+
+/* Number of terms (synchronizes the handle's stream).  PartitionStorage::exact_len. */
+ps_status ps_len(ps_sum* sum, uint64_t* n);
+
+/* Copy the sorted contents to host arrays of capacity cap (x, z: cap x W words; coeffs: cap
+ * doubles).  *n receives the term count; PS_ERR_INVALID if cap < count.  GpuSum::to_host. */
+ps_status ps_download(ps_sum* sum, uint64_t* x, uint64_t* z, double* coeffs, uint64_t cap, uint64_t* n);
+
+/* Host-side table builder: a channel's per-layer engine form for this width and dtype, adjoint
+ * when direction is Heisenberg.  Prepared::derive_local / PauliRotation::prepare_for_layer,
+ * crates/paulistrings/src/channel/rotation.rs:105-124 and prepared.rs:214-233, 401-493. */
+ps_status ps_prepare_channel(int32_t num_qubits, int32_t dtype, const ps_channel* channel, int32_t adjoint,
+                             ps_table* out);
+
+/* Apply one prepared layer and the keep program: every term's outputs are emitted, equal keys
+ * summed, exact zeros and keep rejects dropped.  PartitionBackend::apply_layer. */
+ps_status ps_apply_layer(ps_sum* sum, const ps_table* table, const ps_policy* policy, ps_layer_stats* stats);
+
+/* Run the policy's layer passes (TopN).  PartitionBackend::finalize_layer. */
+ps_status ps_finalize_layer(ps_sum* sum, const ps_policy* policy);
+
+/* The whole layer loop: channels in order (forward) or reversed with adjoints (Heisenberg),
+ * each applied then finalized.  run_layers, engine/driver.rs:319-592.  terms_after (optional,
+ * num_channels entries) receives each layer's final length. */
+ps_status ps_propagate(ps_sum* sum, const ps_channel* channels, uint64_t num_channels, const ps_policy* policy,
+                       int32_t direction, uint64_t* terms_after, ps_run_stats* stats);
+
+/* <psi|O|psi> in a product state: per qubit an axis (x-bit, z-bit of the axis Pauli) and a sign
+ * bit (1 = the -1 eigenstate); W words each.  Summed in float64 on the device.
+ * PauliSum::expectation_product, readout/product_state.rs:84-101. */
+ps_status ps_expectation(ps_sum* sum, const uint64_t* axis_x, const uint64_t* axis_z, const uint64_t* negative,
+                         double* out);
+
+/* Turn per-kernel CUDA-event timing on or off; clears the profile.  PhaseStats, engine/stats.rs:12. */
+ps_status ps_set_profiling(ps_sum* sum, int32_t enabled);
+
+/* Copy up to cap kernel records; *count receives the number of kernels profiled. */
+ps_status ps_read_profile(ps_sum* sum, ps_kernel_profile* out, int32_t cap, int32_t* count);
+
+/* Wait for the handle's stream.  PartitionStorage::settle. */
+ps_status ps_synchronize(ps_sum* sum);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,987 @@
+// ps_api.cu -- the C ABI (include/paulistrings_b200.h): device store, table builder,
+// layer dispatch and the layer loop.
+//
+// The store is double-buffered: a layer reads the current buffer and writes the spare,
+// and the handle flips to the spare only when every kernel of the layer finished without
+// a device-side error, so a failed layer leaves the last completed layer in place
+// (crates/paulistrings/src/engine/gpu/driver.rs:44).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/paulistrings_b200.h"
+#include "ps_device.cuh"
+#include "ps_kernels.h"
+#include "ps_store.h"
+
+using namespace psb;
+
+namespace {
+
+constexpr size_t kPad = 256;  // tail slack of every buffer (bulk copies read up to 15 bytes past the end)
+
+struct Buf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct ps_sum {
+    int device = 0;
+    int nq = 0;
+    int W = 1;
+    int dtype = PS_F64;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+    Ctl* ctl = nullptr;
+    unsigned long long* hcount = nullptr;  // pinned
+    double* hout = nullptr;                // pinned
+    Buf keys[2], coef[2];
+    uint64_t cap[2] = {0, 0};
+    int cur = 0;
+    uint64_t n = 0;
+    Buf pk, pc;
+    Buf idx, dv, fv, slots, status, bounds, hist, partial, dout;
+    SortScratch sort{};
+    Buf sort_status;
+    LevelList* levels = nullptr;  // host scratch
+    KernelProf prof;
+    std::string err;
+};
+
+namespace {
+
+
+ps_status set_err(ps_sum* s, ps_status st, const std::string& msg) {
+    if (s) s->err = msg;
+    return st;
+}
+
+ps_status cuda_fail(ps_sum* s, cudaError_t e, const char* where) {
+    ps_status st = (e == cudaErrorMemoryAllocation) ? PS_ERR_OOM : PS_ERR_DEVICE;
+    if (e == cudaErrorMemoryAllocation) cudaGetLastError();  // clear the sticky-free allocation error
+    return set_err(s, st, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+// Grow-only buffer; contents are not preserved.
+cudaError_t ensure(Buf& b, size_t bytes) {
+    if (b.bytes >= bytes && b.p) return cudaSuccess;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    size_t want = bytes + kPad;
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) {
+        b.p = nullptr;
+        return e;
+    }
+    b.bytes = bytes;
+    return cudaSuccess;
+}
+
+void release(Buf& b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+int width_for(int nq) {
+    for (int w : {1, 2, 4, 8, 16})
+        if (nq <= 64 * w) return w;
+    return 0;
+}
+
+// Device-side error flags of the handle (synchronizes).
+ps_status check_device_flags(ps_sum* s, const char* where) {
+    unsigned int flags[2] = {0, 0};
+    cudaError_t e = cudaMemcpyAsync(flags, &s->ctl->err, sizeof(flags), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return cuda_fail(s, e, where);
+    if (flags[0] == 0) return PS_OK;
+    cudaMemsetAsync(&s->ctl->err, 0, 2 * sizeof(unsigned int), s->stream);
+    cudaStreamSynchronize(s->stream);
+    char msg[160];
+    if (flags[0] & ERR_KEY_RANGE) {
+        snprintf(msg, sizeof msg, "%s: a key has a bit at or above num_qubits=%d", where, s->nq);
+        return set_err(s, PS_ERR_INVALID, msg);
+    }
+    if (flags[0] & ERR_TIMEOUT) {
+        snprintf(msg, sizeof msg, "%s: a bounded device wait gave up (check %u)", where, flags[1]);
+        return set_err(s, PS_ERR_TIMEOUT, msg);
+    }
+    snprintf(msg, sizeof msg, "%s: device check failed (flags %u, check %u)", where, flags[0], flags[1]);
+    return set_err(s, PS_ERR_DEVICE, msg);
+}
+
+// ---------------------------------------------------------------------------
+// keep program lowering
+// ---------------------------------------------------------------------------
+ps_status lower_keep(const ps_policy* p, KeepProg& k, std::string& why) {
+    std::memset(&k, 0, sizeof k);
+    if (!p) return PS_OK;
+    if (p->num_nodes < 0 || p->num_nodes > PS_MAX_KEEP_NODES || p->num_passes < 0 || p->num_passes > PS_MAX_PASSES) {
+        why = "policy: bad node or pass count";
+        return PS_ERR_INVALID;
+    }
+    int depth = 0;
+    for (int i = 0; i < p->num_nodes; ++i) {
+        const ps_keep_node& nd = p->nodes[i];
+        k.op[i] = nd.op;
+        switch (nd.op) {
+        case PS_KEEP_TRUE: ++depth; break;
+        case PS_KEEP_COEFF:
+            k.eps2[i] = nd.farg < 0.0 ? -1.0 : nd.farg * nd.farg;
+            ++depth;
+            break;
+        case PS_KEEP_WEIGHT:
+            if (nd.iarg < 0) {
+                why = "policy: negative weight limit";
+                return PS_ERR_INVALID;
+            }
+            k.iarg[i] = nd.iarg;
+            ++depth;
+            break;
+        case PS_KEEP_AND:
+        case PS_KEEP_OR:
+            if (depth < 2) {
+                why = "policy: malformed keep program";
+                return PS_ERR_INVALID;
+            }
+            --depth;
+            break;
+        default: why = "policy: unknown keep node"; return PS_ERR_UNSUPPORTED;
+        }
+    }
+    if (p->num_nodes && depth != 1) {
+        why = "policy: malformed keep program";
+        return PS_ERR_INVALID;
+    }
+    k.n = p->num_nodes;
+    for (int i = 0; i < p->num_passes; ++i) {
+        if (p->passes[i].kind != PS_PASS_TOPN && p->passes[i].kind != PS_PASS_NONE) {
+            why = "policy: unknown layer pass";
+            return PS_ERR_UNSUPPORTED;
+        }
+    }
+    return PS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// table builder (restates channel/rotation.rs:43-124 and channel/prepared.rs:214-493)
+// ---------------------------------------------------------------------------
+void sin_cos_snapped(double theta, double& sn, double& cs) {
+    const double kSnap = 1e-15;
+    double s = std::sin(theta), c = std::cos(theta);
+    if (std::fabs(s) < kSnap) {
+        sn = 0.0;
+        cs = std::isnan(c) ? c : std::copysign(1.0, c);
+    } else if (std::fabs(c) < kSnap) {
+        sn = std::isnan(s) ? s : std::copysign(1.0, s);
+        cs = 0.0;
+    } else {
+        sn = s;
+        cs = c;
+    }
+}
+
+struct HostKey {
+    uint64_t x[PS_MAX_W], z[PS_MAX_W];
+};
+
+bool host_anticommutes(const HostKey& a, const uint64_t* gx, const uint64_t* gz, int W) {
+    uint64_t f = 0;
+    for (int i = 0; i < W; ++i) f ^= (a.x[i] & gz[i]) ^ (a.z[i] & gx[i]);
+    return (__builtin_popcountll(f) & 1) != 0;
+}
+
+unsigned host_phase(const HostKey& k, const uint64_t* gx, const uint64_t* gz, int W) {
+    unsigned d = 0;
+    for (int i = 0; i < W; ++i) {
+        uint64_t a = k.x[i], b = k.z[i], c = gx[i], e = gz[i];
+        d += 2u * __builtin_popcountll(b & c) + __builtin_popcountll(a & b) + __builtin_popcountll(c & e) -
+             __builtin_popcountll((a ^ c) & (b ^ e));
+    }
+    return d & 3u;
+}
+
+HostKey lift_local(const ps_table& t, unsigned d) {
+    HostKey k;
+    std::memset(&k, 0, sizeof k);
+    for (int j = 0; j < t.k; ++j) {
+        uint32_t q = t.qubits[j];
+        if ((d >> (2 * j)) & 1u) k.x[q / 64] |= 1ull << (q % 64);
+        if ((d >> (2 * j + 1)) & 1u) k.z[q / 64] |= 1ull << (q % 64);
+    }
+    return k;
+}
+
+unsigned local_bits(const ps_table& t, const HostKey& k) {
+    unsigned s = 0;
+    for (int j = 0; j < t.k; ++j) {
+        uint32_t q = t.qubits[j];
+        s |= (unsigned)((k.x[q / 64] >> (q % 64)) & 1u) << (2 * j);
+        s |= (unsigned)((k.z[q / 64] >> (q % 64)) & 1u) << (2 * j + 1);
+    }
+    return s;
+}
+
+void push_deltas(ps_table& t, const double (&table)[16][16], int W) {
+    int dim = 1 << (2 * t.k);
+    bool has[16] = {false};
+    for (int s = 0; s < dim; ++s)
+        for (int u = 0; u < dim; ++u)
+            if (table[s][u] != 0.0) has[s ^ u] = true;
+    t.num_entries = 0;
+    for (int d = 0; d < dim; ++d) {
+        if (!has[d]) continue;
+        ps_table_entry& e = t.entries[t.num_entries++];
+        std::memset(&e, 0, sizeof e);
+        e.local_delta = (uint32_t)d;
+        HostKey m = lift_local(t, (unsigned)d);
+        for (int w = 0; w < W; ++w) {
+            e.mask_x[w] = m.x[w];
+            e.mask_z[w] = m.z[w];
+        }
+        for (int s = 0; s < dim; ++s) e.amplitude[s] = table[s][s ^ d];
+    }
+}
+
+ps_status build_table(int nq, const ps_channel* ch, int adjoint, ps_table* out, std::string& why) {
+    const int W = width_for(nq);
+    if (!W) {
+        why = "num_qubits out of range";
+        return PS_ERR_INVALID;
+    }
+    std::memset(out, 0, sizeof *out);
+    out->width = W;
+    if (!ch || ch->num_support < 0 || ch->num_support > 64 * PS_MAX_W || (ch->num_support && !ch->qubits)) {
+        why = "channel: bad support";
+        return PS_ERR_INVALID;
+    }
+    if (ch->kind == PS_CH_PAULI_ROTATION) {
+        if (ch->num_support && !ch->paulis) {
+            why = "pauli_rotation: missing Pauli labels";
+            return PS_ERR_INVALID;
+        }
+        uint64_t gx[PS_MAX_W] = {0}, gz[PS_MAX_W] = {0};
+        for (int j = 0; j < ch->num_support; ++j) {
+            uint32_t q = ch->qubits[j];
+            if ((int)q >= nq) {
+                why = "pauli_rotation: qubit " + std::to_string(q) + " is outside the " + std::to_string(nq) +
+                      "-qubit register";
+                return PS_ERR_INVALID;
+            }
+            uint64_t bit = 1ull << (q % 64);
+            if ((gx[q / 64] | gz[q / 64]) & bit) {
+                why = "pauli_rotation: repeated qubit " + std::to_string(q);
+                return PS_ERR_INVALID;
+            }
+            char p = ch->paulis[j];
+            if (p == 'X' || p == 'x')
+                gx[q / 64] |= bit;
+            else if (p == 'Y' || p == 'y') {
+                gx[q / 64] |= bit;
+                gz[q / 64] |= bit;
+            } else if (p == 'Z' || p == 'z')
+                gz[q / 64] |= bit;
+            else if (p != 'I' && p != 'i') {
+                why = std::string("pauli_rotation: bad Pauli label '") + p + "'";
+                return PS_ERR_INVALID;
+            }
+        }
+        if (!std::isfinite(ch->param)) {
+            why = "pauli_rotation: angle must be finite";
+            return PS_ERR_INVALID;
+        }
+        double sn, cs;
+        sin_cos_snapped(adjoint ? -ch->param : ch->param, sn, cs);
+        int weight = 0;
+        for (int w = 0; w < W; ++w) weight += __builtin_popcountll(gx[w] | gz[w]);
+        if (weight > 2) {
+            out->mode = PS_TABLE_ROTATION;
+            for (int w = 0; w < W; ++w) {
+                out->gen_x[w] = gx[w];
+                out->gen_z[w] = gz[w];
+            }
+            out->cos_theta = cs;
+            out->sin_theta = sn;
+            return PS_OK;
+        }
+        out->mode = PS_TABLE_LOCAL;
+        int k = 0;
+        for (int w = 0; w < W; ++w) {
+            uint64_t live = gx[w] | gz[w];
+            while (live) {
+                out->qubits[k++] = (uint32_t)(64 * w + __builtin_ctzll(live));
+                live &= live - 1;
+            }
+        }
+        out->k = k;
+        double table[16][16];
+        std::memset(table, 0, sizeof table);
+        int dim = 1 << (2 * k);
+        for (int s = 0; s < dim; ++s) {
+            HostKey in = lift_local(*out, (unsigned)s);
+            if (!host_anticommutes(in, gx, gz, W)) {
+                table[s][s] += 1.0;
+                continue;
+            }
+            table[s][s] += 1.0 * cs;
+            unsigned total = (1u + host_phase(in, gx, gz, W)) & 3u;
+            HostKey o = in;
+            for (int w = 0; w < W; ++w) {
+                o.x[w] ^= gx[w];
+                o.z[w] ^= gz[w];
+            }
+            table[s][local_bits(*out, o)] += ((total & 2u) ? -1.0 : 1.0) * sn;
+        }
+        push_deltas(*out, table, W);
+        return PS_OK;
+    }
+    if (ch->kind == PS_CH_DEPOLARIZING) {
+        if (ch->num_support != 1) {
+            why = "depolarizing: exactly one qubit";
+            return PS_ERR_INVALID;
+        }
+        if ((int)ch->qubits[0] >= nq) {
+            why = "depolarizing: qubit outside the register";
+            return PS_ERR_INVALID;
+        }
+        double p = ch->param;
+        if (!(p >= 0.0 && p <= 1.0)) {
+            why = "depolarizing: p must lie in [0, 1]";
+            return PS_ERR_INVALID;
+        }
+        double scale = 1.0 - 4.0 * p / 3.0;
+        out->mode = PS_TABLE_LOCAL;
+        out->k = 1;
+        out->qubits[0] = ch->qubits[0];
+        double table[16][16];
+        std::memset(table, 0, sizeof table);
+        table[0][0] = 1.0;
+        table[1][1] = scale;
+        table[2][2] = scale;
+        table[3][3] = scale;
+        push_deltas(*out, table, W);
+        return PS_OK;
+    }
+    why = "unknown channel kind";
+    return PS_ERR_UNSUPPORTED;
+}
+
+// ---------------------------------------------------------------------------
+// table -> device layer
+// ---------------------------------------------------------------------------
+template <int W, typename T>
+ps_status to_rot_layer(const ps_table& t, RotLayer<W>& L, LevelList& lv, std::string& why) {
+    std::memset(&L, 0, sizeof L);
+    lv.n = 0;
+    uint64_t dx[W] = {0}, dz[W] = {0};
+    if (t.mode == PS_TABLE_ROTATION) {
+        L.wide = 1;
+        L.partners = t.sin_theta != 0.0 ? 1 : 0;
+        for (int w = 0; w < W; ++w) {
+            L.gx[w] = dx[w] = t.gen_x[w];
+            L.gz[w] = dz[w] = t.gen_z[w];
+        }
+        L.cos64 = t.cos_theta;
+        L.sin64 = t.sin_theta;
+        L.cos32 = (float)t.cos_theta;
+        L.sin32 = (float)t.sin_theta;
+        L.pattern_mask = 0;
+    } else if (t.mode == PS_TABLE_LOCAL) {
+        if (t.k < 0 || t.k > 2) {
+            why = "table: support above two qubits";
+            return PS_ERR_INVALID;
+        }
+        for (int j = 0; j < 2; ++j) {
+            uint32_t q = t.qubits[j < t.k ? j : 0];
+            if (t.k == 0) q = 0;
+            L.qw[j] = (int)(q / 64);
+            L.qb[j] = (int)(q % 64);
+        }
+        L.pattern_mask = (1u << (2 * t.k)) - 1u;
+        const int dim = 1 << (2 * t.k);
+        if (t.num_entries == 1 && t.entries[0].local_delta == 0) {
+            L.partners = 0;
+            for (int s = 0; s < 16; ++s) {
+                double a = s < dim ? t.entries[0].amplitude[s] : 1.0;
+                L.a0[s] = a;
+                L.a0f[s] = (float)a;
+            }
+        } else if (t.num_entries == 2 && t.entries[0].local_delta == 0) {
+            const ps_table_entry &e0 = t.entries[0], &e1 = t.entries[1];
+            const unsigned delta = e1.local_delta;
+            // RotationLayer::of (bucketed/rotation_layer.rs:101-140), per coefficient type
+            for (int s = 0; s < dim; ++s) {
+                T a0 = (T)e0.amplitude[s], a1 = (T)e1.amplitude[s];
+                if (a1 == T(0)) {
+                    if (a0 != T(1)) {
+                        why = "table: not rotation-shaped (general tables run on the sort path)";
+                        return PS_ERR_UNSUPPORTED;
+                    }
+                } else if ((T)e1.amplitude[s ^ delta] == T(0)) {
+                    why = "table: not rotation-shaped";
+                    return PS_ERR_UNSUPPORTED;
+                }
+            }
+            bool clifford = true;
+            const double eps = 2.220446049250313e-16;
+            for (int s = 0; s < dim; ++s) {
+                double a0 = (double)(T)e0.amplitude[s], a1 = (double)(T)e1.amplitude[s];
+                if (a1 != 0.0) clifford = clifford && (a0 * a0 <= eps * eps * (a1 * a1));
+            }
+            L.partners = 1;
+            for (int w = 0; w < W; ++w) {
+                L.gx[w] = dx[w] = e1.mask_x[w];
+                L.gz[w] = dz[w] = e1.mask_z[w];
+            }
+            for (int s = 0; s < 16; ++s) {
+                double a0 = s < dim ? e0.amplitude[s] : 1.0;
+                double a1 = s < dim ? e1.amplitude[s] : 0.0;
+                if (clifford && (T)a1 != T(0)) a0 = 0.0;
+                L.a0[s] = a0;
+                L.a1[s] = a1;
+                L.a0f[s] = (float)a0;
+                L.a1f[s] = (float)a1;
+            }
+        } else {
+            why = "table: general local tables (Clifford permutations, dense PTMs) are not on the device path";
+            return PS_ERR_UNSUPPORTED;
+        }
+    } else {
+        why = "table: unknown mode";
+        return PS_ERR_INVALID;
+    }
+    if (L.partners) {
+        for (int w = 0; w < W; ++w) {
+            uint64_t bits = dx[w];
+            while (bits) {
+                int b = 63 - __builtin_clzll(bits);
+                lv.rank[lv.n++] = (uint32_t)(64 * w + (63 - b));
+                bits &= ~(1ull << b);
+            }
+        }
+        for (int w = 0; w < W; ++w) {
+            uint64_t bits = dz[w];
+            while (bits) {
+                int b = 63 - __builtin_clzll(bits);
+                lv.rank[lv.n++] = (uint32_t)(64 * (W + w) + (63 - b));
+                bits &= ~(1ull << b);
+            }
+        }
+    }
+    return PS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// per-width / per-dtype operations
+// ---------------------------------------------------------------------------
+template <int W, typename T>
+struct Engine {
+    static constexpr size_t kKeyBytes = 16 * W;
+
+    static cudaError_t reserve_store(ps_sum* s, int which, uint64_t rows) {
+        if (s->cap[which] >= rows && s->keys[which].p) return cudaSuccess;
+        uint64_t want = rows < 1024 ? 1024 : rows;
+        // grow by 1.5x so a slowly growing sum does not reallocate every layer
+        if (s->cap[which] && want < s->cap[which] + s->cap[which] / 2) want = s->cap[which] + s->cap[which] / 2;
+        cudaError_t e = ensure(s->keys[which], want * kKeyBytes);
+        if (e == cudaSuccess) e = ensure(s->coef[which], want * sizeof(T));
+        if (e != cudaSuccess) {
+            release(s->keys[which]);
+            release(s->coef[which]);
+            s->cap[which] = 0;
+            cudaGetLastError();
+            // retry at the exact size
+            want = rows < 1024 ? 1024 : rows;
+            e = ensure(s->keys[which], want * kKeyBytes);
+            if (e == cudaSuccess) e = ensure(s->coef[which], want * sizeof(T));
+            if (e != cudaSuccess) {
+                release(s->keys[which]);
+                release(s->coef[which]);
+                return e;
+            }
+        }
+        s->cap[which] = want;
+        return cudaSuccess;
+    }
+
+    static uint64_t* K(ps_sum* s, int w) { return static_cast<uint64_t*>(s->keys[w].p); }
+    static T* C(ps_sum* s, int w) { return static_cast<T*>(s->coef[w].p); }
+
+    static ps_status upload(ps_sum* s, const uint64_t* x, const uint64_t* z, const double* c, uint64_t n) {
+        if (n >= (1ull << 30)) return set_err(s, PS_ERR_UNSUPPORTED, "upload: at most 2^30 - 1 terms per upload");
+        const int spare = 1 - s->cur;
+        if (n == 0) {
+            s->n = 0;
+            return PS_OK;
+        }
+        Buf dx, dz, dc, k0, k1, v0, v1, c0, st;
+        auto cleanup = [&]() {
+            release(dx);
+            release(dz);
+            release(dc);
+            release(k0);
+            release(k1);
+            release(v0);
+            release(v1);
+            release(c0);
+            release(st);
+        };
+        cudaError_t e = cudaSuccess;
+        const size_t tiles = (n + StoreOps<W, T>::sort_tile() - 1) / StoreOps<W, T>::sort_tile();
+        if ((e = ensure(dx, n * W * 8)) != cudaSuccess || (e = ensure(dz, n * W * 8)) != cudaSuccess ||
+            (e = ensure(dc, n * 8)) != cudaSuccess || (e = ensure(k0, n * kKeyBytes)) != cudaSuccess ||
+            (e = ensure(k1, n * kKeyBytes)) != cudaSuccess || (e = ensure(v0, n * 4)) != cudaSuccess ||
+            (e = ensure(v1, n * 4)) != cudaSuccess || (e = ensure(c0, n * sizeof(T))) != cudaSuccess ||
+            (e = ensure(st, (n / 2048 + 2) * sizeof(unsigned long long))) != cudaSuccess ||
+            (e = ensure(s->sort_status, tiles * 256 * sizeof(unsigned int))) != cudaSuccess ||
+            (e = reserve_store(s, spare, n)) != cudaSuccess) {
+            cleanup();
+            return cuda_fail(s, e, "upload: allocation");
+        }
+        s->sort.status = static_cast<unsigned int*>(s->sort_status.p);
+        cudaMemcpyAsync(dx.p, x, n * W * 8, cudaMemcpyHostToDevice, s->stream);
+        cudaMemcpyAsync(dz.p, z, n * W * 8, cudaMemcpyHostToDevice, s->stream);
+        cudaMemcpyAsync(dc.p, c, n * 8, cudaMemcpyHostToDevice, s->stream);
+        e = StoreOps<W, T>::pack((uint64_t*)dx.p, (uint64_t*)dz.p, (double*)dc.p, n, (uint32_t)s->nq,
+                                 (uint64_t*)k0.p, (T*)c0.p, (uint32_t*)v0.p, s->ctl, s->sms, s->stream, &s->prof);
+        if (e != cudaSuccess) {
+            cleanup();
+            return cuda_fail(s, e, "upload: pack");
+        }
+        ps_status fs = check_device_flags(s, "upload");
+        if (fs != PS_OK) {
+            cleanup();
+            return fs;
+        }
+        bool alt = false;
+        e = StoreOps<W, T>::sort_pairs((uint64_t*)k0.p, (uint32_t*)v0.p, (uint64_t*)k1.p, (uint32_t*)v1.p, n, s->sort,
+                                       s->ctl, s->sms, s->stream, alt, &s->prof);
+        if (e != cudaSuccess) {
+            cleanup();
+            return cuda_fail(s, e, "upload: sort");
+        }
+        KeepProg none;
+        std::memset(&none, 0, sizeof none);
+        uint64_t out_n = 0;
+        e = StoreOps<W, T>::dedup(alt ? (uint64_t*)k1.p : (uint64_t*)k0.p, alt ? (uint32_t*)v1.p : (uint32_t*)v0.p,
+                                  (T*)c0.p, n, none, false, K(s, spare), C(s, spare),
+                                  (unsigned long long*)st.p, s->ctl, s->hcount, &out_n, s->stream, &s->prof);
+        if (e != cudaSuccess) {
+            cleanup();
+            return cuda_fail(s, e, "upload: dedup");
+        }
+        fs = check_device_flags(s, "upload");
+        cleanup();
+        if (fs != PS_OK) return fs;
+        s->cur = spare;
+        s->n = out_n;
+        return PS_OK;
+    }
+
+    static ps_status download(ps_sum* s, uint64_t* x, uint64_t* z, double* c, uint64_t cap, uint64_t* nout) {
+        if (nout) *nout = s->n;
+        if (cap < s->n) return set_err(s, PS_ERR_INVALID, "download: capacity below the term count");
+        if (s->n == 0) return PS_OK;
+        Buf dx, dz, dc;
+        cudaError_t e;
+        if ((e = ensure(dx, s->n * W * 8)) != cudaSuccess || (e = ensure(dz, s->n * W * 8)) != cudaSuccess ||
+            (e = ensure(dc, s->n * 8)) != cudaSuccess) {
+            release(dx);
+            release(dz);
+            release(dc);
+            return cuda_fail(s, e, "download: allocation");
+        }
+        e = StoreOps<W, T>::unpack(K(s, s->cur), C(s, s->cur), s->n, (uint64_t*)dx.p, (uint64_t*)dz.p, (double*)dc.p,
+                                   s->sms, s->stream, &s->prof);
+        if (e == cudaSuccess && x) e = cudaMemcpyAsync(x, dx.p, s->n * W * 8, cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess && z) e = cudaMemcpyAsync(z, dz.p, s->n * W * 8, cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess && c) e = cudaMemcpyAsync(c, dc.p, s->n * 8, cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        release(dx);
+        release(dz);
+        release(dc);
+        if (e != cudaSuccess) return cuda_fail(s, e, "download");
+        return PS_OK;
+    }
+
+    static ps_status apply(ps_sum* s, const ps_table& t, const ps_policy* policy, ps_layer_stats* stats) {
+        KeepProg keep;
+        std::string why;
+        ps_status ps = lower_keep(policy, keep, why);
+        if (ps != PS_OK) return set_err(s, ps, why);
+        RotationArgs<W, T> a;
+        std::memset(&a, 0, sizeof a);
+        ps = to_rot_layer<W, T>(t, a.L, *s->levels, why);
+        if (ps != PS_OK) return set_err(s, ps, why);
+        const uint64_t n = s->n;
+        if (n >= (1ull << 31) - 1) return set_err(s, PS_ERR_UNSUPPORTED, "apply: at most 2^31 - 2 terms");
+        const int spare = 1 - s->cur;
+        const uint64_t out_rows = a.L.partners ? 2 * n : n;
+        cudaError_t e = reserve_store(s, spare, out_rows);
+        if (e != cudaSuccess) return cuda_fail(s, e, "apply: output store");
+        const uint64_t tiles_hi = out_rows / kMinTileRows + 4;
+        if ((e = ensure(s->status, tiles_hi * sizeof(unsigned long long))) != cudaSuccess ||
+            (e = ensure(s->bounds, (tiles_hi + 2) * sizeof(ulonglong2))) != cudaSuccess)
+            return cuda_fail(s, e, "apply: scratch");
+        if (a.L.partners) {
+            if ((e = ensure(s->pk, n * kKeyBytes)) != cudaSuccess || (e = ensure(s->pc, n * sizeof(T))) != cudaSuccess ||
+                (e = ensure(s->idx, n * 4)) != cudaSuccess || (e = ensure(s->dv, n * 2)) != cudaSuccess ||
+                (e = ensure(s->fv, n * 4)) != cudaSuccess ||
+                (e = ensure(s->slots, (n / kScanTileRows + 4) * sizeof(LevelSlot))) != cudaSuccess)
+                return cuda_fail(s, e, "apply: partner scratch");
+        }
+        a.Sk = K(s, s->cur);
+        a.Sc = C(s, s->cur);
+        a.n = n;
+        a.levels = s->levels;
+        a.keep = keep;
+        a.idx = (uint32_t*)s->idx.p;
+        a.D = (uint16_t*)s->dv.p;
+        a.F = (int32_t*)s->fv.p;
+        a.slots = s->slots.p;
+        a.status = (unsigned long long*)s->status.p;
+        a.bounds = (ulonglong2*)s->bounds.p;
+        a.Pk = (uint64_t*)s->pk.p;
+        a.Pc = (T*)s->pc.p;
+        a.p_cap = a.L.partners ? n : 0;
+        a.Ok = K(s, spare);
+        a.Oc = C(s, spare);
+        a.out_cap = s->cap[spare];
+        a.ctl = s->ctl;
+        a.host_count = s->hcount;
+        uint64_t partners = 0, out_n = 0;
+        a.partners_out = &partners;
+        a.out_count = &out_n;
+        a.prof = &s->prof;
+        e = launch_rotation_layer<W, T>(a, s->stream);
+        s->prof.resolve();
+        if (e != cudaSuccess) return cuda_fail(s, e, "apply: rotation layer");
+        ps = check_device_flags(s, "apply");
+        if (ps != PS_OK) return ps;
+        if (stats) {
+            stats->terms_in = n;
+            stats->partners = partners;
+            stats->terms_out = out_n;
+            stats->terms_after_passes = out_n;
+            stats->path = a.L.partners ? PS_PATH_ROTATION : PS_PATH_RESCALE;
+        }
+        s->cur = spare;
+        s->n = out_n;
+        return PS_OK;
+    }
+
+    static ps_status finalize(ps_sum* s, const ps_policy* policy) {
+        if (!policy) return PS_OK;
+        for (int i = 0; i < policy->num_passes; ++i) {
+            const ps_pass& p = policy->passes[i];
+            if (p.kind != PS_PASS_TOPN) continue;
+            if (s->n <= p.n) continue;
+            if (p.n == 0) {
+                s->n = 0;
+                continue;
+            }
+            const int spare = 1 - s->cur;
+            cudaError_t e = reserve_store(s, spare, p.n);
+            if (e == cudaSuccess) e = ensure(s->hist, 256 * sizeof(unsigned int));
+            if (e == cudaSuccess) e = ensure(s->status, (s->n / 2048 + 4) * sizeof(unsigned long long));
+            if (e != cudaSuccess) return cuda_fail(s, e, "topn: scratch");
+            uint64_t out_n = 0;
+            e = StoreOps<W, T>::topn(K(s, s->cur), C(s, s->cur), s->n, p.n, K(s, spare), C(s, spare),
+                                     (unsigned int*)s->hist.p, (unsigned long long*)s->status.p, s->ctl, s->hcount,
+                                     &out_n, s->sms, s->stream, &s->prof);
+            s->prof.resolve();
+            if (e != cudaSuccess) return cuda_fail(s, e, "topn");
+            ps_status ps = check_device_flags(s, "topn");
+            if (ps != PS_OK) return ps;
+            s->cur = spare;
+            s->n = out_n;
+        }
+        return PS_OK;
+    }
+
+    static ps_status expectation(ps_sum* s, const uint64_t* ax, const uint64_t* az, const uint64_t* neg, double* out) {
+        cudaError_t e = ensure(s->partial, kExpectBlocks * sizeof(double));
+        if (e == cudaSuccess) e = ensure(s->dout, sizeof(double));
+        if (e != cudaSuccess) return cuda_fail(s, e, "expectation: scratch");
+        e = StoreOps<W, T>::expectation(K(s, s->cur), C(s, s->cur), s->n, ax, az, neg, (double*)s->partial.p,
+                                        (double*)s->dout.p, s->sms, s->stream, &s->prof);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(s->hout, s->dout.p, sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess) return cuda_fail(s, e, "expectation");
+        *out = *s->hout;
+        return PS_OK;
+    }
+
+    static cudaError_t configure() {
+        cudaError_t e = configure_rotation_kernels<W, T>();
+        if (e == cudaSuccess) e = StoreOps<W, T>::configure();
+        return e;
+    }
+};
+
+template <template <int, typename> class Op, typename F>
+ps_status dispatch(ps_sum* s, F&& f) {
+    if (s->dtype == PS_F64) {
+        switch (s->W) {
+        case 1: return f(Op<1, double>());
+        case 2: return f(Op<2, double>());
+        case 4: return f(Op<4, double>());
+        default: break;
+        }
+    } else {
+        switch (s->W) {
+        case 1: return f(Op<1, float>());
+        case 2: return f(Op<2, float>());
+        case 4: return f(Op<4, float>());
+        default: break;
+        }
+    }
+    return set_err(s, PS_ERR_UNSUPPORTED, "widths above 4 words (256 qubits) are not built");
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+#pragma GCC visibility push(default)
+
+int32_t ps_abi_version(void) { return PS_ABI_VERSION; }
+
+int32_t ps_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+ps_status ps_create(int32_t device, int32_t num_qubits, int32_t dtype, ps_sum** out) {
+    if (!out) return PS_ERR_INVALID;
+    *out = nullptr;
+    if (num_qubits < 1 || num_qubits > 64 * PS_MAX_W || (dtype != PS_F64 && dtype != PS_F32)) return PS_ERR_INVALID;
+    const int W = width_for(num_qubits);
+    if (W > 4) return PS_ERR_UNSUPPORTED;
+    int count = ps_device_count();
+    if (count == 0 || device < 0 || device >= count) return PS_ERR_NO_DEVICE;
+    DeviceGuard g(device);
+    ps_sum* s = new ps_sum();
+    s->device = device;
+    s->nq = num_qubits;
+    s->W = W;
+    s->dtype = dtype;
+    cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device);
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&s->ctl, sizeof(Ctl));
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->ctl, 0, sizeof(Ctl), s->stream);
+    if (e == cudaSuccess) e = cudaMallocHost(&s->hcount, 64 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->hout, 8 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&s->sort.hist, 16 * W * 256 * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMalloc(&s->sort.base, 16 * W * 256 * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->sort.host_hist, 16 * W * 256 * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->sort.host_base, 16 * W * 256 * sizeof(unsigned int));
+    if (e == cudaSuccess) {
+        ps_status st = dispatch<Engine>(s, [&](auto op) {
+            cudaError_t ce = decltype(op)::configure();
+            return ce == cudaSuccess ? PS_OK : cuda_fail(s, ce, "configure");
+        });
+        if (st != PS_OK) e = cudaErrorInvalidValue;
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) {
+        ps_destroy(s);
+        cudaGetLastError();
+        return e == cudaErrorMemoryAllocation ? PS_ERR_OOM : PS_ERR_DEVICE;
+    }
+    s->levels = new LevelList();
+    *out = s;
+    return PS_OK;
+}
+
+ps_status ps_destroy(ps_sum* s) {
+    if (!s) return PS_OK;
+    DeviceGuard g(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (Buf* b : {&s->keys[0], &s->keys[1], &s->coef[0], &s->coef[1], &s->pk, &s->pc, &s->idx, &s->dv, &s->fv,
+                   &s->slots, &s->status, &s->bounds, &s->hist, &s->partial, &s->dout, &s->sort_status})
+        release(*b);
+    if (s->ctl) cudaFree(s->ctl);
+    if (s->sort.hist) cudaFree(s->sort.hist);
+    if (s->sort.base) cudaFree(s->sort.base);
+    if (s->sort.host_hist) cudaFreeHost(s->sort.host_hist);
+    if (s->sort.host_base) cudaFreeHost(s->sort.host_base);
+    if (s->hcount) cudaFreeHost(s->hcount);
+    if (s->hout) cudaFreeHost(s->hout);
+    s->prof.destroy();
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s->levels;
+    delete s;
+    return PS_OK;
+}
+
+const char* ps_last_error(const ps_sum* s) { return s ? s->err.c_str() : "null handle"; }
+int32_t ps_width(const ps_sum* s) { return s ? s->W : 0; }
+int32_t ps_num_qubits(const ps_sum* s) { return s ? s->nq : 0; }
+int32_t ps_dtype_of(const ps_sum* s) { return s ? s->dtype : -1; }
+
+ps_status ps_upload(ps_sum* s, const uint64_t* x, const uint64_t* z, const double* coeffs, uint64_t n) {
+    if (!s) return PS_ERR_INVALID;
+    if (n && (!x || !z || !coeffs)) return set_err(s, PS_ERR_INVALID, "upload: NULL array");
+    DeviceGuard g(s->device);
+    return dispatch<Engine>(s, [&](auto op) { return decltype(op)::upload(s, x, z, coeffs, n); });
+}
+
+ps_status ps_len(ps_sum* s, uint64_t* n) {
+    if (!s || !n) return PS_ERR_INVALID;
+    *n = s->n;
+    return PS_OK;
+}
+
+ps_status ps_download(ps_sum* s, uint64_t* x, uint64_t* z, double* coeffs, uint64_t cap, uint64_t* n) {
+    if (!s) return PS_ERR_INVALID;
+    DeviceGuard g(s->device);
+    return dispatch<Engine>(s, [&](auto op) { return decltype(op)::download(s, x, z, coeffs, cap, n); });
+}
+
+ps_status ps_prepare_channel(int32_t num_qubits, int32_t dtype, const ps_channel* channel, int32_t adjoint,
+                             ps_table* out) {
+    (void)dtype;
+    if (!out || !channel) return PS_ERR_INVALID;
+    std::string why;
+    return build_table(num_qubits, channel, adjoint, out, why);
+}
+
+ps_status ps_apply_layer(ps_sum* s, const ps_table* table, const ps_policy* policy, ps_layer_stats* stats) {
+    if (!s || !table) return PS_ERR_INVALID;
+    if (table->width != s->W) return set_err(s, PS_ERR_INVALID, "apply: table built for another width");
+    DeviceGuard g(s->device);
+    return dispatch<Engine>(s, [&](auto op) { return decltype(op)::apply(s, *table, policy, stats); });
+}
+
+ps_status ps_finalize_layer(ps_sum* s, const ps_policy* policy) {
+    if (!s) return PS_ERR_INVALID;
+    DeviceGuard g(s->device);
+    KeepProg k;
+    std::string why;
+    ps_status ps = lower_keep(policy, k, why);
+    if (ps != PS_OK) return set_err(s, ps, why);
+    return dispatch<Engine>(s, [&](auto op) { return decltype(op)::finalize(s, policy); });
+}
+
+ps_status ps_propagate(ps_sum* s, const ps_channel* channels, uint64_t num_channels, const ps_policy* policy,
+                       int32_t direction, uint64_t* terms_after, ps_run_stats* stats) {
+    if (!s || (num_channels && !channels)) return PS_ERR_INVALID;
+    if (direction != PS_FORWARD && direction != PS_HEISENBERG) return set_err(s, PS_ERR_INVALID, "bad direction");
+    DeviceGuard g(s->device);
+    KeepProg k;
+    std::string why;
+    ps_status ps = lower_keep(policy, k, why);
+    if (ps != PS_OK) return set_err(s, ps, why);
+    const bool adjoint = direction == PS_HEISENBERG;
+    // Every channel is prepared before the first layer, so a bad channel fails the call
+    // with the input untouched.
+    std::vector<ps_table> tables(num_channels);
+    for (uint64_t li = 0; li < num_channels; ++li) {
+        uint64_t ci = adjoint ? num_channels - 1 - li : li;
+        ps = build_table(s->nq, &channels[ci], adjoint ? 1 : 0, &tables[li], why);
+        if (ps != PS_OK) return set_err(s, ps, "channel " + std::to_string(ci) + ": " + why);
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s->stream);
+    ps_run_stats rs;
+    std::memset(&rs, 0, sizeof rs);
+    rs.peak_terms = s->n;
+    unsigned long long launches0 = 0;
+    for (int i = 0; i < K_NUM_KERNELS; ++i) launches0 += s->prof.launches[i];
+    for (uint64_t li = 0; li < num_channels; ++li) {
+        ps_layer_stats ls;
+        rs.total_terms_in += s->n;
+        ps = ps_apply_layer(s, &tables[li], policy, &ls);
+        if (ps == PS_OK) ps = ps_finalize_layer(s, policy);
+        if (ps != PS_OK) {
+            s->err = "layer " + std::to_string(li) + ": " + s->err;
+            break;
+        }
+        if (ls.terms_out > rs.peak_terms) rs.peak_terms = ls.terms_out;
+        if (terms_after) terms_after[li] = s->n;
+        ++rs.layers;
+    }
+    cudaEventRecord(e1, s->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    rs.final_terms = s->n;
+    rs.device_ms = ms;
+    unsigned long long launches1 = 0;
+    for (int i = 0; i < K_NUM_KERNELS; ++i) launches1 += s->prof.launches[i];
+    rs.kernel_launches = launches1 - launches0;
+    if (stats) *stats = rs;
+    return ps;
+}
+
+ps_status ps_expectation(ps_sum* s, const uint64_t* axis_x, const uint64_t* axis_z, const uint64_t* negative,
+                         double* out) {
+    if (!s || !axis_x || !axis_z || !negative || !out) return PS_ERR_INVALID;
+    DeviceGuard g(s->device);
+    return dispatch<Engine>(s, [&](auto op) { return decltype(op)::expectation(s, axis_x, axis_z, negative, out); });
+}
+
+ps_status ps_set_profiling(ps_sum* s, int32_t enabled) {
+    if (!s) return PS_ERR_INVALID;
+    DeviceGuard g(s->device);
+    s->prof.reset();
+    s->prof.events = enabled != 0;
+    return PS_OK;
+}
+
+ps_status ps_read_profile(ps_sum* s, ps_kernel_profile* out, int32_t cap, int32_t* count) {
+    if (!s || !count || (cap > 0 && !out)) return PS_ERR_INVALID;
+    static const char* kNames[K_NUM_KERNELS] = {"k_classify",     "k_fwd_levels", "k_bwd_levels", "k_partition",
+                                                "k_merge",        "k_topn_hist",  "k_topn_step",  "k_topn_compact",
+                                                "k_pack",         "k_sort_hist",  "k_sort_pass",  "k_dedup",
+                                                "k_unpack",       "k_expect"};
+    DeviceGuard g(s->device);
+    s->prof.resolve();
+    *count = K_NUM_KERNELS;
+    for (int i = 0; i < K_NUM_KERNELS && i < cap; ++i) {
+        std::memset(&out[i], 0, sizeof out[i]);
+        std::strncpy(out[i].name, kNames[i], sizeof(out[i].name) - 1);
+        out[i].launches = s->prof.launches[i];
+        out[i].timed_launches = s->prof.timed[i];
+        out[i].total_ms = s->prof.ms[i];
+        out[i].algorithmic_bytes = s->prof.bytes[i];
+    }
+    return PS_OK;
+}
+
+ps_status ps_synchronize(ps_sum* s) {
+    if (!s) return PS_ERR_INVALID;
+    DeviceGuard g(s->device);
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    return e == cudaSuccess ? PS_OK : cuda_fail(s, e, "synchronize");
+}
+
+}  // extern "C"

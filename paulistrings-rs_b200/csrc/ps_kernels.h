@@ -1,0 +1,178 @@
+// ps_kernels.h -- plain data shapes shared by the host driver and the kernel launchers.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace psb {
+
+// Device-resident control block of one handle.
+struct Ctl {
+    unsigned long long count[8];   // counts published by kernels (partners, outputs, ...)
+    unsigned int tile_counter[8];  // dynamic tile dispensers, reset before each launch
+    unsigned int err;              // ERR_* bits
+    unsigned int err_info;         // id of the first check that failed
+    unsigned long long aux[8];     // small per-pass values (TopN boundary, quota, ...)
+};
+
+// Lowered keep program (postfix), KeepProgram in the reference's device path.
+struct KeepProg {
+    int32_t n;
+    int32_t op[15];     // 0 true, 1 coeff, 2 weight, 3 and, 4 or
+    int64_t iarg[15];   // weight limit
+    double eps2[15];    // eps * eps, or -1 when eps < 0 (keeps everything)
+};
+
+constexpr int kMaxLevels = 8;
+constexpr uint16_t kDivStart = 0xFFFE;    // divergence slot of the first partner
+constexpr uint16_t kDivUnknown = 0xFFFF;  // predecessor lives in another classify tile
+
+// The set bits of a partner delta, as significance ranks (0 = most significant key bit).
+struct Levels {
+    int32_t n;
+    uint32_t rank[kMaxLevels];
+};
+
+// All set bits of a delta; launchers batch them by kMaxLevels.
+struct LevelList {
+    int32_t n;
+    uint32_t rank[2 * 64 * 16];
+};
+
+// Device form of one rotation-shaped (or key-preserving) layer.
+template <int W>
+struct RotLayer {
+    uint64_t gx[W], gz[W];   // partner delta (generator) x / z masks
+    int32_t wide;            // 1: PreparedRotation (per-term phase), 0: LocalPtm lookup
+    int32_t partners;        // 0: key-preserving, no partner stream
+    int32_t qw[2], qb[2];    // support qubit j lives in word qw[j], bit qb[j]
+    uint32_t pattern_mask;   // (1 << 2k) - 1
+    double a0[16], a1[16];   // identity / generator amplitude per support pattern
+    float a0f[16], a1f[16];
+    double cos64, sin64;
+    float cos32, sin32;
+};
+
+// Kernel ids of the per-kernel profile.
+enum KernelId : int {
+    K_CLASSIFY = 0,
+    K_FWD_LEVELS,
+    K_BWD_LEVELS,
+    K_PARTITION,
+    K_MERGE,
+    K_TOPN_HIST,
+    K_TOPN_STEP,
+    K_TOPN_COMPACT,
+    K_PACK,
+    K_SORT_HIST,
+    K_SORT_PASS,
+    K_DEDUP,
+    K_UNPACK,
+    K_EXPECT,
+    K_NUM_KERNELS
+};
+
+// Counts every launch; with events enabled, times each launch with CUDA events on the
+// launching stream and books its algorithmic bytes (resolved after the caller's sync).
+struct KernelProf {
+    static constexpr int kPool = 256;
+    bool events = false;
+    unsigned long long launches[K_NUM_KERNELS] = {};
+    double ms[K_NUM_KERNELS] = {};
+    double bytes[K_NUM_KERNELS] = {};
+    unsigned long long timed[K_NUM_KERNELS] = {};
+    cudaEvent_t ev[2 * kPool] = {};
+    int pend_id[kPool] = {};
+    double pend_bytes[kPool] = {};
+    int npend = 0;
+    bool ready = false;
+
+    void begin(int id, double algo_bytes, cudaStream_t st) {
+        ++launches[id];
+        if (!events) return;
+        if (!ready) {
+            for (int i = 0; i < 2 * kPool; ++i) cudaEventCreate(&ev[i]);
+            ready = true;
+        }
+        if (npend >= kPool) resolve();
+        if (npend >= kPool) return;
+        pend_id[npend] = id;
+        pend_bytes[npend] = algo_bytes;
+        cudaEventRecord(ev[2 * npend], st);
+    }
+    void end(cudaStream_t st) {
+        if (!events || !ready || npend >= kPool) return;
+        cudaEventRecord(ev[2 * npend + 1], st);
+        ++npend;
+    }
+    // Accumulates the pending launches (waits for their end events).
+    void resolve() {
+        for (int i = 0; i < npend; ++i) {
+            float t = 0.f;
+            cudaEventSynchronize(ev[2 * i + 1]);
+            cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]);
+            ms[pend_id[i]] += t;
+            bytes[pend_id[i]] += pend_bytes[i];
+            ++timed[pend_id[i]];
+        }
+        npend = 0;
+    }
+    void add_bytes(int id, double b) {
+        if (events) bytes[id] += b;
+    }
+    void reset() {
+        resolve();
+        for (int i = 0; i < K_NUM_KERNELS; ++i) launches[i] = 0, ms[i] = 0, bytes[i] = 0, timed[i] = 0;
+    }
+    void destroy() {
+        if (ready)
+            for (int i = 0; i < 2 * kPool; ++i) cudaEventDestroy(ev[i]);
+        ready = false;
+    }
+};
+
+template <int W, typename T>
+struct RotationArgs {
+    const uint64_t* Sk;          // sorted store keys (n rows of 2W words)
+    const T* Sc;
+    uint64_t n;
+    RotLayer<W> L;
+    const LevelList* levels;     // all delta bits
+    KeepProg keep;
+    uint32_t* idx;               // scratch, >= n
+    uint16_t* D;                 // scratch, >= n
+    int32_t* F;                  // scratch, >= n
+    void* slots;                 // level look-back slots, >= scan tiles
+    unsigned long long* status;  // look-back words, >= classify / merge tiles
+    ulonglong2* bounds;          // merge-path bounds, >= merge tiles + 1
+    uint64_t* Pk;                // partner keys (sorted), capacity p_cap
+    T* Pc;
+    uint64_t p_cap;
+    uint64_t* Ok;                // output store, capacity out_cap
+    T* Oc;
+    uint64_t out_cap;
+    Ctl* ctl;
+    unsigned long long* host_count;  // pinned host word
+    uint64_t* partners_out;
+    uint64_t* out_count;
+    KernelProf* prof;
+};
+
+template <int W, typename T>
+cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st);
+template <int W, typename T>
+cudaError_t configure_rotation_kernels();
+
+// One scan tile's look-back slot: flag 1 = agg valid, 2 = inc (prefix combined with agg) valid.
+struct LevelSlot {
+    unsigned int flag;
+    int agg[2 * kMaxLevels];
+    int inc[2 * kMaxLevels];
+};
+
+// Rows of the smallest tile of any look-back kernel (bounds every tile count).
+constexpr size_t kMinTileRows = 256;
+constexpr size_t kScanTileRows = 4096;
+
+}  // namespace psb

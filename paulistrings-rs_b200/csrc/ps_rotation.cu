@@ -1,0 +1,781 @@
+// ps_rotation.cu -- the rotation layer on a sorted device store.
+//
+// A rotation-shaped table (an identity entry and one generator entry g,
+// crates/paulistrings/src/engine/bucketed/rotation_layer.rs:75-140) maps each
+// term k to (k, c*a0[s]) and, when the generator entry reaches its support
+// pattern s, to (k ^ g, c*a1[s]).  Partners of a sorted run, taken in the run's
+// order, are sorted under an order that differs from key order only where two
+// keys first differ on a bit of g (crates/paulistrings/src/engine/bucketed/
+// partner_order.rs:10-14).  So the layer is:
+//
+//   k_classify   stream the store keys (TMA bulk copies into shared memory),
+//                list anticommuting rows with a decoupled look-back count and
+//                record each one's divergence rank from its predecessor;
+//   k_fwd_levels forward max-scan per bit of g: the upper half of each group
+//                moves down by the lower half's size;
+//   k_bwd_levels backward min-scan per bit of g: the lower half moves up by
+//                the upper half's size; writes each partner at its sorted slot;
+//   k_partition  merge-path split points (one warp per tile, 32-way search);
+//   k_merge      merge own rows and partners, sum equal keys, drop exact zeros
+//                and keep-program rejects, compact with a look-back.
+//
+// Key-preserving tables (depolarizing noise, quarter turns with sin = 0) run
+// k_partition + k_merge with an empty partner stream.
+#include "ps_device.cuh"
+#include "ps_kernels.h"
+
+namespace psb {
+
+constexpr int kBlock = 256;
+
+template <int W>
+struct RotTile {
+    static constexpr int kClassifyItems = W == 1 ? 8 : (W == 2 ? 4 : (W == 4 ? 2 : 1));
+    static constexpr int kClassifyTile = kBlock * kClassifyItems;  // 32 KiB of keys per tile
+    static constexpr int kMergeItems = W == 1 ? 8 : (W == 2 ? 4 : (W == 4 ? 2 : 1));
+    static constexpr int kMergeTile = kBlock * kMergeItems;
+};
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kBlock * kScanItems;
+static_assert(kScanTile == (int)kScanTileRows, "scan tile");
+
+// support pattern of key k (LocalPtm::support_bits, channel/prepared.rs:141-151)
+template <int W>
+__device__ __forceinline__ uint32_t pattern_of(const RotLayer<W>& L, const uint64_t* k) {
+    uint32_t s = (uint32_t)((k[L.qw[0]] >> L.qb[0]) & 1u) | (uint32_t)((k[W + L.qw[0]] >> L.qb[0]) & 1u) << 1 |
+                 (uint32_t)((k[L.qw[1]] >> L.qb[1]) & 1u) << 2 | (uint32_t)((k[W + L.qw[1]] >> L.qb[1]) & 1u) << 3;
+    return s & L.pattern_mask;
+}
+
+template <typename T>
+struct Amp;
+template <>
+struct Amp<double> {
+    template <int W>
+    __device__ static double a0(const RotLayer<W>& L, uint32_t s) { return L.a0[s]; }
+    template <int W>
+    __device__ static double a1(const RotLayer<W>& L, uint32_t s) { return L.a1[s]; }
+    template <int W>
+    __device__ static double cs(const RotLayer<W>& L) { return L.cos64; }
+    template <int W>
+    __device__ static double sn(const RotLayer<W>& L) { return L.sin64; }
+};
+template <>
+struct Amp<float> {
+    template <int W>
+    __device__ static float a0(const RotLayer<W>& L, uint32_t s) { return L.a0f[s]; }
+    template <int W>
+    __device__ static float a1(const RotLayer<W>& L, uint32_t s) { return L.a1f[s]; }
+    template <int W>
+    __device__ static float cs(const RotLayer<W>& L) { return L.cos32; }
+    template <int W>
+    __device__ static float sn(const RotLayer<W>& L) { return L.sin32; }
+};
+
+// Does term k emit a partner?
+template <int W, typename T>
+__device__ __forceinline__ bool emits_partner(const RotLayer<W>& L, const uint64_t* k) {
+    if (L.wide) return anticommutes<W>(k, L.gx, L.gz);
+    return Amp<T>::a1(L, pattern_of<W>(L, k)) != T(0);
+}
+
+// Own-row coefficient after the layer.
+template <int W, typename T>
+__device__ __forceinline__ T own_coeff(const RotLayer<W>& L, const uint64_t* k, T c) {
+    if (L.wide) return anticommutes<W>(k, L.gx, L.gz) ? mul_rn(c, Amp<T>::cs(L)) : c;
+    return mul_rn(c, Amp<T>::a0(L, pattern_of<W>(L, k)));
+}
+
+// Partner coefficient (DeltaEntry::emit / PreparedRotation::emit_generator).
+template <int W, typename T>
+__device__ __forceinline__ T partner_coeff(const RotLayer<W>& L, const uint64_t* k, T c) {
+    if (L.wide) {
+        uint32_t total = (1u + product_phase<W>(k, L.gx, L.gz)) & 3u;
+        T m = (total & 2u) ? -c : c;  // real mul_phase, coefficient.rs:107-114
+        return mul_rn(m, Amp<T>::sn(L));
+    }
+    return mul_rn(c, Amp<T>::a1(L, pattern_of<W>(L, k)));
+}
+
+// ---------------------------------------------------------------------------
+// k_classify
+// ---------------------------------------------------------------------------
+template <int W, typename T>
+__global__ void __launch_bounds__(kBlock) k_classify(const uint64_t* __restrict__ keys, uint64_t n,
+                                                     const RotLayer<W> L, uint32_t* __restrict__ idx,
+                                                     uint16_t* __restrict__ D, unsigned long long* status,
+                                                     Ctl* ctl) {
+    constexpr int ITEMS = RotTile<W>::kClassifyItems;
+    constexpr int TILE = RotTile<W>::kClassifyTile;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    uint64_t* sk = reinterpret_cast<uint64_t*>(smem_raw);
+    __shared__ uint64_t bar;
+    __shared__ unsigned int s_tile;
+    __shared__ unsigned int s_warp[kBlock / 32];
+    __shared__ int s_wlast[kBlock / 32];
+    __shared__ unsigned long long s_prefix;
+
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        s_tile = atomicAdd(&ctl->tile_counter[0], 1u);
+        mbar_init(&bar, 1);
+    }
+    __syncthreads();
+    const unsigned int tile = s_tile;
+    const uint64_t row0 = (uint64_t)tile * TILE;
+    if (row0 >= n) return;  // grid is sized to the tile count; never taken
+    const uint32_t cnt = (uint32_t)min((uint64_t)TILE, n - row0);
+    if (tid == 0) {
+        uint32_t bytes = cnt * (uint32_t)(16 * W);
+        mbar_arrive_expect_tx(&bar, bytes);
+        bulk_g2s(sk, keys + row0 * (2 * W), bytes, &bar);
+    }
+    mbar_wait(&bar, 0, ctl, 101);
+
+    // flags of this thread's consecutive rows
+    uint32_t flags = 0;
+    int last_local = -1;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        int r = tid * ITEMS + i;
+        if (r < (int)cnt) {
+            bool e = emits_partner<W, T>(L, sk + (size_t)r * 2 * W);
+            flags |= (uint32_t)e << i;
+            if (e) last_local = r;
+        }
+    }
+    unsigned int count = __popc(flags), total;
+    unsigned int excl = block_exclusive_sum<kBlock>(count, s_warp, total);
+
+    // exclusive max-scan of the last anticommuting local row over threads
+    const int lane = tid & 31, warp = tid >> 5;
+    int incl = last_local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl = max(incl, y);
+    }
+    int before = __shfl_up_sync(0xffffffffu, incl, 1);
+    if (lane == 0) before = -1;
+    if (lane == 31) s_wlast[warp] = incl;
+    __syncthreads();
+    for (int w = 0; w < warp; ++w) before = max(before, s_wlast[w]);
+
+    if (tid == 0) {
+        if (tile == 0) {
+            st_release_u64(status + tile, kFlagInc | (unsigned long long)total);
+            s_prefix = 0;
+        } else {
+            st_release_u64(status + tile, kFlagAgg | (unsigned long long)total);
+            unsigned long long p = lookback_sum(status, tile, ctl, 102);
+            st_release_u64(status + tile, kFlagInc | (p + total));
+            s_prefix = p;
+        }
+    }
+    __syncthreads();
+    const unsigned long long base = s_prefix + excl;
+    if (row0 + cnt == n && tid == kBlock - 1) ctl->count[0] = s_prefix + total;
+
+    int prev = before;
+    unsigned int rank = 0;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        if (!((flags >> i) & 1u)) continue;
+        int r = tid * ITEMS + i;
+        unsigned long long j = base + rank++;
+        if (PS_BOUNDS(ctl, j < n, 103)) {
+            idx[j] = (uint32_t)(row0 + r);
+            uint16_t d;
+            if (prev >= 0)
+                d = (uint16_t)divergence<W>(sk + (size_t)prev * 2 * W, sk + (size_t)r * 2 * W);
+            else
+                d = (j == 0) ? (uint16_t)kDivStart : (uint16_t)kDivUnknown;
+            D[j] = d;
+        }
+        prev = r;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// level scans.  For level rank L, a "group" is a maximal run of partners sharing
+// every key bit more significant than L, and its "split" is the first row whose
+// bit L is set.  Starts: j == 0 or D[j] < L.  Splits: D[j] == L.
+// ---------------------------------------------------------------------------
+// Combine for the forward scan (max) or the backward scan (min) over tiles before `tile`
+// in scan order; publishes this tile's aggregate first and its inclusive value after.
+template <bool kMax>
+__device__ __forceinline__ void level_lookback(LevelSlot* slots, unsigned int tile, const int (&tile_agg)[2 * kMaxLevels],
+                                               int (&prefix)[2 * kMaxLevels], int identity, Ctl* ctl, uint32_t info) {
+    for (int v = 0; v < 2 * kMaxLevels; ++v) prefix[v] = identity;
+    if (tile == 0) {
+        for (int v = 0; v < 2 * kMaxLevels; ++v) slots[0].inc[v] = tile_agg[v];
+        __threadfence();
+        st_release_u32(&slots[0].flag, 2u);
+        return;
+    }
+    for (int v = 0; v < 2 * kMaxLevels; ++v) slots[tile].agg[v] = tile_agg[v];
+    __threadfence();
+    st_release_u32(&slots[tile].flag, 1u);
+    long long spins = 0;
+    for (int t = (int)tile - 1; t >= 0;) {
+        unsigned int f = ld_acquire_u32(&slots[t].flag);
+        if (f == 0) {
+            if (++spins > kSpinLimit) {
+                raise_err(ctl, ERR_TIMEOUT, info);
+                break;
+            }
+            __nanosleep(32);
+            continue;
+        }
+        const int* src = f == 2u ? slots[t].inc : slots[t].agg;
+        for (int v = 0; v < 2 * kMaxLevels; ++v) {
+            int x = __ldcg(src + v);
+            prefix[v] = kMax ? max(prefix[v], x) : min(prefix[v], x);
+        }
+        if (f == 2u) break;
+        --t;
+    }
+    for (int v = 0; v < 2 * kMaxLevels; ++v)
+        slots[tile].inc[v] = kMax ? max(prefix[v], tile_agg[v]) : min(prefix[v], tile_agg[v]);
+    __threadfence();
+    st_release_u32(&slots[tile].flag, 2u);
+}
+
+template <int W>
+__device__ __forceinline__ void fix_divergence(const uint32_t* __restrict__ idx, uint16_t* __restrict__ D,
+                                               const uint64_t* __restrict__ keys, uint64_t n, uint32_t j,
+                                               uint16_t& d, Ctl* ctl) {
+    if (d != kDivUnknown) return;
+    uint32_t ra = idx[j - 1], rb = idx[j];
+    if (!PS_BOUNDS(ctl, ra < n && rb < n, 201)) return;
+    uint64_t ka[2 * W], kb[2 * W];
+    load_key<W>(keys, ra, ka);
+    load_key<W>(keys, rb, kb);
+    d = (uint16_t)divergence<W>(ka, kb);
+    D[j] = d;
+}
+
+template <int W>
+__global__ void __launch_bounds__(kBlock) k_fwd_levels(const uint32_t* __restrict__ idx, uint16_t* __restrict__ D,
+                                                       int32_t* __restrict__ F, uint32_t m,
+                                                       const uint64_t* __restrict__ keys, uint64_t n,
+                                                       const Levels lv, int accumulate, LevelSlot* slots,
+                                                       Ctl* ctl) {
+    __shared__ unsigned int s_tile;
+    __shared__ int s_wagg[kBlock / 32][2 * kMaxLevels];
+    __shared__ int s_prefix[2 * kMaxLevels];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[1], 1u);
+    __syncthreads();
+    const unsigned int tile = s_tile;
+    const uint32_t j0 = tile * (uint32_t)kScanTile + (uint32_t)tid * kScanItems;
+    const int NL = lv.n;
+
+    uint16_t d[kScanItems];
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        uint32_t j = j0 + i;
+        d[i] = j < m ? D[j] : (uint16_t)0;
+        if (j < m && j > 0) fix_divergence<W>(idx, D, keys, n, j, d[i], ctl);
+    }
+    // thread aggregates: last start / last split position per level
+    int agg[2 * kMaxLevels];
+#pragma unroll
+    for (int l = 0; l < kMaxLevels; ++l) {
+        agg[2 * l] = -1;
+        agg[2 * l + 1] = -1;
+        if (l < NL) {
+            uint32_t L = lv.rank[l];
+#pragma unroll
+            for (int i = 0; i < kScanItems; ++i) {
+                uint32_t j = j0 + i;
+                if (j >= m) break;
+                if (j == 0 || d[i] < L) agg[2 * l] = (int)j;
+                if (j != 0 && d[i] == L) agg[2 * l + 1] = (int)j;
+            }
+        }
+    }
+    // block exclusive max-scan of the aggregates
+    int excl[2 * kMaxLevels];
+#pragma unroll
+    for (int v = 0; v < 2 * kMaxLevels; ++v) {
+        int x = agg[v];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x = max(x, y);
+        }
+        int e = __shfl_up_sync(0xffffffffu, x, 1);
+        excl[v] = lane == 0 ? -1 : e;
+        if (lane == 31) s_wagg[warp][v] = x;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 2 * kMaxLevels; ++v)
+        for (int w = 0; w < warp; ++w) excl[v] = max(excl[v], s_wagg[w][v]);
+    // tile aggregate, publish, look back
+    __syncthreads();
+    if (tid == 0) {
+        int tagg[2 * kMaxLevels], pre[2 * kMaxLevels];
+        for (int v = 0; v < 2 * kMaxLevels; ++v) {
+            int t = -1;
+            for (int w = 0; w < kBlock / 32; ++w) t = max(t, s_wagg[w][v]);
+            tagg[v] = t;
+        }
+        level_lookback<true>(slots, tile, tagg, pre, -1, ctl, 202);
+        for (int v = 0; v < 2 * kMaxLevels; ++v) s_prefix[v] = pre[v];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 2 * kMaxLevels; ++v) excl[v] = max(excl[v], s_prefix[v]);
+
+    // per item: F = sum over levels of -(split - start) for rows in an upper half
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        uint32_t j = j0 + i;
+        if (j >= m) break;
+        int f = 0;
+#pragma unroll
+        for (int l = 0; l < kMaxLevels; ++l) {
+            if (l < NL) {
+                uint32_t L = lv.rank[l];
+                if (j == 0 || d[i] < L) excl[2 * l] = (int)j;
+                if (j != 0 && d[i] == L) excl[2 * l + 1] = (int)j;
+                int s = excl[2 * l], p = excl[2 * l + 1];
+                if (p > s) f -= (p - s);
+            }
+        }
+        F[j] = accumulate ? F[j] + f : f;
+    }
+}
+
+// Backward pass: B = sum over levels of (group end - split) for rows in a lower half; then
+// (last batch only) place each partner at j + F + B.
+template <int W, typename T>
+__global__ void __launch_bounds__(kBlock) k_bwd_levels(const uint32_t* __restrict__ idx,
+                                                       const uint16_t* __restrict__ D, int32_t* __restrict__ F,
+                                                       uint32_t m, const uint64_t* __restrict__ keys,
+                                                       const T* __restrict__ coef, uint64_t n, const Levels lv,
+                                                       const RotLayer<W> L, int scatter,
+                                                       uint64_t* __restrict__ Pk, T* __restrict__ Pc,
+                                                       LevelSlot* slots, Ctl* ctl) {
+    __shared__ unsigned int s_tile;
+    __shared__ int s_wagg[kBlock / 32][2 * kMaxLevels];
+    __shared__ int s_suffix[2 * kMaxLevels];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int INF = 0x7fffffff;
+    if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[2], 1u);
+    __syncthreads();
+    const unsigned int tile = s_tile;  // tile 0 covers the last kScanTile partners
+    const long long hi = (long long)m - (long long)tile * kScanTile;
+    const long long lo = hi - kScanTile;  // may be negative for the first partners
+    const long long jbase = lo + (long long)tid * kScanItems;
+    const int NL = lv.n;
+
+    uint16_t d[kScanItems];
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        long long j = jbase + i;
+        d[i] = (j >= 0 && j < hi) ? D[j] : (uint16_t)0;
+    }
+    int agg[2 * kMaxLevels];
+#pragma unroll
+    for (int l = 0; l < kMaxLevels; ++l) {
+        agg[2 * l] = INF;
+        agg[2 * l + 1] = INF;
+        if (l < NL) {
+            uint32_t Lr = lv.rank[l];
+#pragma unroll
+            for (int i = kScanItems - 1; i >= 0; --i) {
+                long long j = jbase + i;
+                if (j < 0 || j >= hi) continue;
+                if (j != 0 && d[i] < Lr) agg[2 * l] = (int)j;
+                if (j != 0 && d[i] == Lr) agg[2 * l + 1] = (int)j;
+            }
+        }
+    }
+    // exclusive suffix min over threads
+    int excl[2 * kMaxLevels];
+#pragma unroll
+    for (int v = 0; v < 2 * kMaxLevels; ++v) {
+        int x = agg[v];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_down_sync(0xffffffffu, x, o);
+            if (lane + o < 32) x = min(x, y);
+        }
+        int e = __shfl_down_sync(0xffffffffu, x, 1);
+        excl[v] = lane == 31 ? INF : e;
+        if (lane == 0) s_wagg[warp][v] = x;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 2 * kMaxLevels; ++v)
+        for (int w = warp + 1; w < kBlock / 32; ++w) excl[v] = min(excl[v], s_wagg[w][v]);
+    __syncthreads();
+    if (tid == 0) {
+        int tagg[2 * kMaxLevels], suf[2 * kMaxLevels];
+        for (int v = 0; v < 2 * kMaxLevels; ++v) {
+            int t = INF;
+            for (int w = 0; w < kBlock / 32; ++w) t = min(t, s_wagg[w][v]);
+            tagg[v] = t;
+        }
+        level_lookback<false>(slots, tile, tagg, suf, INF, ctl, 203);
+        for (int v = 0; v < 2 * kMaxLevels; ++v) s_suffix[v] = suf[v];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 2 * kMaxLevels; ++v) excl[v] = min(excl[v], s_suffix[v]);
+
+#pragma unroll
+    for (int i = kScanItems - 1; i >= 0; --i) {
+        long long j = jbase + i;
+        if (j < 0 || j >= hi) continue;
+        int b = 0;
+#pragma unroll
+        for (int l = 0; l < kMaxLevels; ++l) {
+            if (l < NL) {
+                int e = excl[2 * l] == INF ? (int)m : excl[2 * l];
+                int q = excl[2 * l + 1];
+                if (q < e) b += e - q;
+                uint32_t Lr = lv.rank[l];
+                if (j != 0 && d[i] < Lr) excl[2 * l] = (int)j;
+                if (j != 0 && d[i] == Lr) excl[2 * l + 1] = (int)j;
+            }
+        }
+        int f = F[j] + b;
+        if (!scatter) {
+            F[j] = f;
+            continue;
+        }
+        long long dest = j + f;
+        uint32_t row = idx[j];
+        if (!PS_GUARD(ctl, dest >= 0 && dest < (long long)m && row < n, 204)) continue;
+        uint64_t k[2 * W];
+        load_key<W>(keys, row, k);
+        T c = coef[row];
+        T pc = partner_coeff<W, T>(L, k, c);
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            k[w] ^= L.gx[w];
+            k[W + w] ^= L.gz[w];
+        }
+        store_key<W>(Pk, (uint64_t)dest, k);
+        Pc[dest] = pc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// merge-path partition: bounds[t] = (i, j) where tile t starts; pairs of equal keys
+// (own row, partner) never straddle a boundary.
+// ---------------------------------------------------------------------------
+template <int W>
+__device__ __forceinline__ bool mp_pred(const uint64_t* Sk, const uint64_t* Pk, uint64_t i, uint64_t d) {
+    // S[i] <= P[d - 1 - i]
+    return key_le<W>(Sk + i * 2 * W, Pk + (d - 1 - i) * 2 * W);
+}
+
+template <int W>
+__global__ void k_partition(const uint64_t* __restrict__ Sk, uint64_t n, const uint64_t* __restrict__ Pk, uint64_t m,
+                            uint32_t tile_items, uint32_t num_tiles, ulonglong2* __restrict__ bounds) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (t > num_tiles) return;
+    uint64_t dd = (uint64_t)t * tile_items;
+    if (dd > n + m) dd = n + m;
+    uint64_t lo = dd > m ? dd - m : 0, hi = dd < n ? dd : n;  // answer in [lo, hi]
+    while (hi - lo > 32) {
+        uint64_t span = hi - lo;
+        uint64_t p = lo + (span * (uint64_t)lane) / 32;  // p_0 = lo, all < hi
+        bool f = mp_pred<W>(Sk, Pk, p, dd);
+        unsigned int b = __ballot_sync(0xffffffffu, f);
+        int c = __popc(b);
+        if (c == 0) {
+            hi = lo;
+            break;
+        }
+        uint64_t pc1 = lo + (span * (uint64_t)(c - 1)) / 32;
+        uint64_t pc = c < 32 ? lo + (span * (uint64_t)c) / 32 : hi;
+        lo = pc1 + 1;
+        hi = pc;
+    }
+    uint64_t span = hi - lo;
+    bool f = (uint64_t)lane < span ? mp_pred<W>(Sk, Pk, lo + lane, dd) : false;
+    unsigned int b = __ballot_sync(0xffffffffu, f);
+    uint64_t i = lo + (uint64_t)__popc(b);
+    uint64_t j = dd - i;
+    if (lane == 0) {
+        if (i > 0 && j < m && key_eq<W>(Sk + (i - 1) * 2 * W, Pk + j * 2 * W)) ++j;
+        bounds[t] = make_ulonglong2(i, j);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_merge
+// ---------------------------------------------------------------------------
+template <int W, typename T>
+struct MergeSmem {
+    static constexpr int TILE = RotTile<W>::kMergeTile;
+    static constexpr int PAD = 16 / (int)sizeof(T);  // elements of alignment slack per stream
+    static constexpr int KEY_ROWS = TILE + 4;
+    static constexpr int COEF_SLOTS = TILE + 4 + 4 * PAD;
+    static constexpr size_t key_bytes = (size_t)KEY_ROWS * 16 * W;
+    static constexpr size_t coef_bytes = ((size_t)COEF_SLOTS * sizeof(T) + 15) / 16 * 16;
+    static constexpr size_t in_bytes = key_bytes + coef_bytes;
+    static constexpr size_t bytes = 2 * in_bytes;  // inputs + output staging
+};
+
+template <int W, typename T>
+__device__ __forceinline__ void merge_range(const uint64_t* sSk, const T* sSc, const uint64_t* sPk, const T* sPc,
+                                            uint32_t i, uint32_t ie, uint32_t j, uint32_t je, const RotLayer<W>& L,
+                                            const KeepProg& keep, bool store, uint64_t* oK, T* oC,
+                                            uint32_t& count) {
+    count = 0;
+    while (i < ie || j < je) {
+        bool takeS = (j >= je) || (i < ie && key_le<W>(sSk + (size_t)i * 2 * W, sPk + (size_t)j * 2 * W));
+        const uint64_t* k;
+        T v;
+        if (takeS) {
+            k = sSk + (size_t)i * 2 * W;
+            v = own_coeff<W, T>(L, k, sSc[i]);
+            if (j < je && key_eq<W>(k, sPk + (size_t)j * 2 * W)) {
+                v = add_rn(v, sPc[j]);  // own first, as the reference's merge sums bucket-first
+                ++j;
+            }
+            ++i;
+        } else {
+            k = sPk + (size_t)j * 2 * W;
+            v = sPc[j];
+            ++j;
+        }
+        if (v != T(0) && keep_eval<W>(keep, k, to_f64(v))) {
+            if (store) {
+#pragma unroll
+                for (int w = 0; w < 2 * W; ++w) oK[(size_t)count * 2 * W + w] = k[w];
+                oC[count] = v;
+            }
+            ++count;
+        }
+    }
+}
+
+template <int W, typename T>
+__global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ Sk, const T* __restrict__ Sc,
+                                                  uint64_t n, const uint64_t* __restrict__ Pk,
+                                                  const T* __restrict__ Pc, uint64_t m,
+                                                  const ulonglong2* __restrict__ bounds, uint32_t num_tiles,
+                                                  const RotLayer<W> L, const KeepProg keep,
+                                                  uint64_t* __restrict__ Ok, T* __restrict__ Oc, uint64_t out_cap,
+                                                  unsigned long long* status, Ctl* ctl) {
+    using SM = MergeSmem<W, T>;
+    constexpr int ITEMS = RotTile<W>::kMergeItems;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    uint64_t* sK = reinterpret_cast<uint64_t*>(smem_raw);
+    T* sC = reinterpret_cast<T*>(smem_raw + SM::key_bytes);
+    uint64_t* oK = reinterpret_cast<uint64_t*>(smem_raw + SM::in_bytes);
+    T* oC = reinterpret_cast<T*>(smem_raw + SM::in_bytes + SM::key_bytes);
+    __shared__ uint64_t bar;
+    __shared__ unsigned int s_tile;
+    __shared__ unsigned int s_warp[kBlock / 32];
+    __shared__ unsigned int s_si[kBlock + 1], s_sj[kBlock + 1];
+    __shared__ unsigned long long s_outoff;
+
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        s_tile = atomicAdd(&ctl->tile_counter[3], 1u);
+        mbar_init(&bar, 1);
+    }
+    __syncthreads();
+    const unsigned int tile = s_tile;
+    if (tile >= num_tiles) return;
+    const ulonglong2 b0 = bounds[tile], b1 = bounds[tile + 1];
+    const uint32_t cs = (uint32_t)(b1.x - b0.x), cp = (uint32_t)(b1.y - b0.y);
+    if (!PS_GUARD(ctl, b1.x >= b0.x && b1.y >= b0.y && b1.x - b0.x + b1.y - b0.y <= (uint64_t)SM::TILE + 2 &&
+                           b1.x <= n && b1.y <= m,
+                  301)) {
+        return;
+    }
+    // stage the two input runs: keys packed (S then P), coefficients from 16-byte aligned windows
+    const uint64_t sa = b0.x & ~(uint64_t)(SM::PAD - 1), pa = b0.y & ~(uint64_t)(SM::PAD - 1);
+    const uint32_t s_off = (uint32_t)(b0.x - sa), p_off = (uint32_t)(b0.y - pa);
+    const uint32_t sc_slots = (s_off + cs + SM::PAD - 1) / SM::PAD * SM::PAD;
+    T* sSc = sC;            // S coefficient of local i at sSc[s_off + i]
+    T* sPc = sC + sc_slots; // P coefficient of local j at sPc[p_off + j]
+    uint64_t* sSk = sK;
+    uint64_t* sPk = sK + (size_t)cs * 2 * W;
+    if (tid == 0) {
+        uint32_t kbS = cs * 16u * W, kbP = cp * 16u * W;
+        uint32_t cbS = cs ? round16((s_off + cs) * (uint32_t)sizeof(T)) : 0u;
+        uint32_t cbP = cp ? round16((p_off + cp) * (uint32_t)sizeof(T)) : 0u;
+        uint32_t total = kbS + kbP + cbS + cbP;
+        if (total) {
+            mbar_arrive_expect_tx(&bar, total);
+            if (kbS) bulk_g2s(sSk, Sk + b0.x * 2 * W, kbS, &bar);
+            if (kbP) bulk_g2s(sPk, Pk + b0.y * 2 * W, kbP, &bar);
+            if (cbS) bulk_g2s(sSc, Sc + sa, cbS, &bar);
+            if (cbP) bulk_g2s(sPc, Pc + pa, cbP, &bar);
+        }
+    }
+    if (cs + cp) mbar_wait(&bar, 0, ctl, 302);
+    const T* Sc_l = sSc + s_off;
+    const T* Pc_l = sPc + p_off;
+
+    // per-thread merge-path start, equal pairs kept together
+    {
+        uint32_t dd = min((uint32_t)tid * ITEMS, cs + cp);
+        uint32_t lo = dd > cp ? dd - cp : 0, hi = min(dd, cs);
+        while (lo < hi) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (key_le<W>(sSk + (size_t)mid * 2 * W, sPk + (size_t)(dd - 1 - mid) * 2 * W))
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        uint32_t i = lo, j = dd - lo;
+        if (i > 0 && j < cp && key_eq<W>(sSk + (size_t)(i - 1) * 2 * W, sPk + (size_t)j * 2 * W)) ++j;
+        s_si[tid] = i;
+        s_sj[tid] = j;
+        if (tid == 0) {
+            s_si[kBlock] = cs;
+            s_sj[kBlock] = cp;
+        }
+    }
+    __syncthreads();
+    const uint32_t i0 = s_si[tid], j0 = s_sj[tid];
+    const uint32_t ie = max(s_si[tid + 1], i0), je = max(s_sj[tid + 1], j0);
+    uint32_t count;
+    merge_range<W, T>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, keep, false, nullptr, nullptr, count);
+    unsigned int total;
+    unsigned int excl = block_exclusive_sum<kBlock>(count, s_warp, total);
+    if (tid == 0) {
+        if (tile == 0) {
+            st_release_u64(status + tile, kFlagInc | (unsigned long long)total);
+            s_outoff = 0;
+        } else {
+            st_release_u64(status + tile, kFlagAgg | (unsigned long long)total);
+            unsigned long long p = lookback_sum(status, tile, ctl, 303);
+            st_release_u64(status + tile, kFlagInc | (p + total));
+            s_outoff = p;
+        }
+        if (tile == num_tiles - 1) ctl->count[1] = s_outoff + total;
+    }
+    uint32_t c2;
+    merge_range<W, T>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, keep, true, oK + (size_t)excl * 2 * W, oC + excl, c2);
+    __syncthreads();
+    const unsigned long long off = s_outoff;
+    if (!PS_GUARD(ctl, off + total <= out_cap, 304)) return;
+    // coalesced write-out of the staged outputs
+    const ulonglong2* src = reinterpret_cast<const ulonglong2*>(oK);
+    ulonglong2* dst = reinterpret_cast<ulonglong2*>(Ok + off * 2 * W);
+    for (uint32_t q = tid; q < total * W; q += kBlock) dst[q] = src[q];
+    for (uint32_t q = tid; q < total; q += kBlock) Oc[off + q] = oC[q];
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+template <int W, typename T>
+cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) {
+    constexpr int CT = RotTile<W>::kClassifyTile;
+    constexpr int MT = RotTile<W>::kMergeTile;
+    Ctl* ctl = a.ctl;
+    cudaError_t e;
+    uint64_t m = 0;
+    if (a.L.partners && a.n > 0) {
+        // 1. classify
+        uint32_t tiles = (uint32_t)((a.n + CT - 1) / CT);
+        cudaMemsetAsync(a.status, 0, (size_t)tiles * sizeof(unsigned long long), st);
+        cudaMemsetAsync(&ctl->tile_counter[0], 0, 4 * sizeof(unsigned int), st);
+        size_t smem = (size_t)CT * 16 * W;
+        a.prof->begin(K_CLASSIFY, (double)a.n * 16 * W, st);
+        k_classify<W, T><<<tiles, kBlock, smem, st>>>(a.Sk, a.n, a.L, a.idx, a.D, a.status, ctl);
+        a.prof->end(st);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        cudaMemcpyAsync(a.host_count, &ctl->count[0], sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+        m = *a.host_count;
+        a.prof->add_bytes(K_CLASSIFY, (double)m * 6);  // idx + divergence writes
+    }
+    *a.partners_out = m;
+    if (m > a.p_cap) return cudaErrorMemoryAllocation;  // caller sized the partner buffers by n
+    if (m > 0) {
+        // 2-3. level scans (batches of kMaxLevels), scatter on the last batch
+        uint32_t stiles = (uint32_t)((m + kScanTile - 1) / kScanTile);
+        int nb = (a.levels->n + kMaxLevels - 1) / kMaxLevels;
+        for (int b = 0; b < nb; ++b) {
+            Levels lv{};
+            lv.n = min(kMaxLevels, a.levels->n - b * kMaxLevels);
+            for (int l = 0; l < lv.n; ++l) lv.rank[l] = a.levels->rank[b * kMaxLevels + l];
+            cudaMemsetAsync(a.slots, 0, (size_t)stiles * sizeof(LevelSlot), st);
+            cudaMemsetAsync(&ctl->tile_counter[1], 0, sizeof(unsigned int), st);
+            a.prof->begin(K_FWD_LEVELS, (double)m * (2 + 4 + (b > 0 ? 4 : 0)), st);
+            k_fwd_levels<W><<<stiles, kBlock, 0, st>>>(a.idx, a.D, a.F, (uint32_t)m, a.Sk, a.n, lv, b > 0,
+                                                     reinterpret_cast<LevelSlot*>(a.slots), ctl);
+            a.prof->end(st);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            cudaMemsetAsync(a.slots, 0, (size_t)stiles * sizeof(LevelSlot), st);
+            cudaMemsetAsync(&ctl->tile_counter[2], 0, sizeof(unsigned int), st);
+            const bool last = b == nb - 1;
+            a.prof->begin(K_BWD_LEVELS,
+                          (double)m * (2 + 4 + (last ? 4 + 2.0 * (16 * W + sizeof(T)) : 4)), st);
+            k_bwd_levels<W, T><<<stiles, kBlock, 0, st>>>(a.idx, a.D, a.F, (uint32_t)m, a.Sk, a.Sc, a.n, lv, a.L,
+                                                        last, a.Pk, a.Pc,
+                                                        reinterpret_cast<LevelSlot*>(a.slots), ctl);
+            a.prof->end(st);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+    }
+    // 4. partition
+    uint64_t total = a.n + m;
+    uint32_t mtiles = (uint32_t)((total + MT - 1) / MT);
+    if (mtiles == 0) {
+        *a.out_count = 0;
+        return cudaSuccess;
+    }
+    if (total > a.out_cap) return cudaErrorMemoryAllocation;
+    {
+        uint32_t warps = mtiles + 1;
+        uint32_t blocks = (warps + 7) / 8;
+        a.prof->begin(K_PARTITION, (double)(mtiles + 1) * 16, st);
+        k_partition<W><<<blocks, 256, 0, st>>>(a.Sk, a.n, a.Pk, m, (uint32_t)MT, mtiles, a.bounds);
+        a.prof->end(st);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    // 5. merge
+    cudaMemsetAsync(a.status, 0, (size_t)mtiles * sizeof(unsigned long long), st);
+    cudaMemsetAsync(&ctl->tile_counter[3], 0, sizeof(unsigned int), st);
+    size_t smem = MergeSmem<W, T>::bytes;
+    a.prof->begin(K_MERGE, (double)(a.n + m) * (16 * W + sizeof(T)), st);
+    k_merge<W, T><<<mtiles, kBlock, smem, st>>>(a.Sk, a.Sc, a.n, a.Pk, a.Pc, m, a.bounds, mtiles, a.L, a.keep,
+                                               a.Ok, a.Oc, a.out_cap, a.status, ctl);
+    a.prof->end(st);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    cudaMemcpyAsync(a.host_count, &ctl->count[1], sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    *a.out_count = *a.host_count;
+    a.prof->add_bytes(K_MERGE, (double)(*a.out_count) * (16 * W + sizeof(T)));
+    return cudaSuccess;
+}
+
+template <int W, typename T>
+cudaError_t configure_rotation_kernels() {
+    constexpr int CT = RotTile<W>::kClassifyTile;
+    cudaError_t e = cudaFuncSetAttribute(k_classify<W, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)((size_t)CT * 16 * W));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_merge<W, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)MergeSmem<W, T>::bytes);
+}
+
+#define PS_INSTANTIATE_ROT(W, T)                                                                 \
+    template cudaError_t launch_rotation_layer<W, T>(const RotationArgs<W, T>&, cudaStream_t); \
+    template cudaError_t configure_rotation_kernels<W, T>();
+
+PS_INSTANTIATE_ROT(1, double)
+PS_INSTANTIATE_ROT(1, float)
+PS_INSTANTIATE_ROT(2, double)
+PS_INSTANTIATE_ROT(2, float)
+PS_INSTANTIATE_ROT(4, double)
+PS_INSTANTIATE_ROT(4, float)
+
+}  // namespace psb

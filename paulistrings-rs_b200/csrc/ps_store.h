@@ -1,0 +1,45 @@
+// ps_store.h -- launchers of the store kernels (ingest, readout, TopN).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "ps_kernels.h"
+
+namespace psb {
+
+constexpr int kExpectBlocks = 592;  // 4 x 148 SMs; fixed so the reduction order is fixed
+
+struct SortScratch {
+    unsigned int* hist;        // device, 16W x 256
+    unsigned int* base;        // device, 16W x 256
+    unsigned int* status;      // device, tiles x 256
+    unsigned int* host_hist;   // pinned, 16W x 256
+    unsigned int* host_base;   // pinned, 16W x 256
+};
+
+template <int W, typename T>
+struct StoreOps {
+    static cudaError_t configure();
+    static size_t sort_tile();
+    static cudaError_t pack(const uint64_t* x, const uint64_t* z, const double* c, uint64_t n, uint32_t nq,
+                            uint64_t* keys, T* coef, uint32_t* vals, Ctl* ctl, int sms, cudaStream_t st, KernelProf* prof);
+    static cudaError_t unpack(const uint64_t* keys, const T* coef, uint64_t n, uint64_t* x, uint64_t* z, double* c,
+                              int sms, cudaStream_t st, KernelProf* prof);
+    // LSD radix sort of (key, value) pairs; the sorted pairs end in (keys, vals) or, when
+    // result_in_alt, in (keys_alt, vals_alt).
+    static cudaError_t sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt, uint32_t* vals_alt, uint64_t n,
+                                  SortScratch& s, Ctl* ctl, int sms, cudaStream_t st, bool& result_in_alt,
+                                  KernelProf* prof);
+    static cudaError_t dedup(const uint64_t* keys, const uint32_t* vals, const T* cin, uint64_t n, const KeepProg& keep,
+                             bool compensated, uint64_t* okeys, T* ocoef, unsigned long long* status, Ctl* ctl,
+                             unsigned long long* host_count, uint64_t* out_n, cudaStream_t st, KernelProf* prof);
+    static cudaError_t topn(const uint64_t* keys, const T* coef, uint64_t n, uint64_t keep_n, uint64_t* okeys, T* ocoef,
+                            unsigned int* hist, unsigned long long* status, Ctl* ctl, unsigned long long* host_count,
+                            uint64_t* out_n, int sms, cudaStream_t st, KernelProf* prof);
+    static cudaError_t expectation(const uint64_t* keys, const T* coef, uint64_t n, const uint64_t* ax,
+                                   const uint64_t* az, const uint64_t* neg, double* partial, double* out_dev, int sms,
+                                   cudaStream_t st, KernelProf* prof);
+};
+
+}  // namespace psb

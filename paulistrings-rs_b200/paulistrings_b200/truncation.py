@@ -1,0 +1,133 @@
+"""Truncation policies (the ``TruncationPolicy`` built-ins) and their lowering.
+
+``coeff(eps)`` keeps ``|c|^2 > eps^2`` (crates/paulistrings/src/truncation/builtin.rs:19-41),
+``weight(k)`` keeps Pauli weight ``<= k`` (:43-59), ``topn(n)`` retains the ``n`` largest
+magnitudes after every layer (:61-150).  ``a & b`` keeps a term iff both keep it and runs
+a's layer passes then b's (:470-526); ``a | b`` combines per-term filters only (:574-625).
+A policy lowers to a postfix keep program plus an ordered list of layer passes, the form
+``ps_policy`` carries across the C ABI (KeepProgram, crates/paulistrings/src/engine/gpu/
+truncation.rs:24-102).
+"""
+
+from __future__ import annotations
+
+from . import _lib
+
+
+class Truncation:
+    """A truncation policy tree."""
+
+    def __init__(self, kind: str, *args):
+        self.kind = kind
+        self.args = args
+
+    def __and__(self, other: "Truncation") -> "Truncation":
+        return Truncation("and", self, other)
+
+    def __or__(self, other: "Truncation") -> "Truncation":
+        for side, name in ((self, "first"), (other, "second")):
+            if side.has_layer_pass():
+                raise ValueError(
+                    f"Or combines per-term filters only, but its {name} operand has a layer pass "
+                    "(TopN); use & to add a filter to a layer pass"
+                )
+        return Truncation("or", self, other)
+
+    def has_layer_pass(self) -> bool:
+        if self.kind == "topn":
+            return True
+        if self.kind in ("and", "or"):
+            return self.args[0].has_layer_pass() or self.args[1].has_layer_pass()
+        return False
+
+    def __repr__(self) -> str:
+        if self.kind in ("and", "or"):
+            op = " & " if self.kind == "and" else " | "
+            return f"({self.args[0]!r}{op}{self.args[1]!r})"
+        return f"truncation.{self.kind}({', '.join(repr(a) for a in self.args)})"
+
+    # -- lowering ----------------------------------------------------------
+    def _lower(self, nodes: list, passes: list) -> None:
+        if self.kind == "coeff":
+            nodes.append((_lib.PS_KEEP_COEFF, 0, float(self.args[0])))
+        elif self.kind == "weight":
+            nodes.append((_lib.PS_KEEP_WEIGHT, int(self.args[0]), 0.0))
+        elif self.kind == "topn":
+            nodes.append((_lib.PS_KEEP_TRUE, 0, 0.0))
+            passes.append((_lib.PS_PASS_TOPN, int(self.args[0])))
+        elif self.kind in ("and", "or"):
+            self.args[0]._lower(nodes, passes)
+            self.args[1]._lower(nodes, passes)
+            nodes.append((_lib.PS_KEEP_AND if self.kind == "and" else _lib.PS_KEEP_OR, 0, 0.0))
+        else:
+            raise ValueError(f"unknown truncation {self.kind}")
+
+    def lowered(self):
+        """(keep nodes, passes) with the keep program simplified of always-true nodes."""
+        nodes: list = []
+        passes: list = []
+        self._lower(nodes, passes)
+        nodes = _simplify(nodes)
+        if len(nodes) > _lib.PS_MAX_KEEP_NODES:
+            raise ValueError("truncation tree too deep for the device keep program (15 nodes)")
+        if len(passes) > _lib.PS_MAX_PASSES:
+            raise ValueError("at most 4 layer passes")
+        return nodes, passes
+
+    def to_c(self) -> _lib.Policy:
+        nodes, passes = self.lowered()
+        p = _lib.Policy()
+        p.num_nodes = len(nodes)
+        for i, (op, iarg, farg) in enumerate(nodes):
+            p.nodes[i].op = op
+            p.nodes[i].iarg = iarg
+            p.nodes[i].farg = farg
+        p.num_passes = len(passes)
+        for i, (kind, n) in enumerate(passes):
+            p.passes[i].kind = kind
+            p.passes[i].n = n
+        return p
+
+
+def _simplify(nodes: list) -> list:
+    """Fold ``true & x`` and ``x & true`` to ``x`` and ``true | x`` to ``true``."""
+    stack: list = []
+    for node in nodes:
+        op = node[0]
+        if op in (_lib.PS_KEEP_AND, _lib.PS_KEEP_OR):
+            b = stack.pop()
+            a = stack.pop()
+            a_true = a == [(_lib.PS_KEEP_TRUE, 0, 0.0)]
+            b_true = b == [(_lib.PS_KEEP_TRUE, 0, 0.0)]
+            if op == _lib.PS_KEEP_AND:
+                stack.append(b if a_true else a if b_true else a + b + [node])
+            else:
+                stack.append(a if a_true else b if b_true else a + b + [node])
+        else:
+            stack.append([node])
+    out = stack[-1] if stack else []
+    return [] if out == [(_lib.PS_KEEP_TRUE, 0, 0.0)] else out
+
+
+def coeff(epsilon: float) -> Truncation:
+    return Truncation("coeff", float(epsilon))
+
+
+def weight(k: int) -> Truncation:
+    if k < 0:
+        raise ValueError("weight limit must be non-negative")
+    return Truncation("weight", int(k))
+
+
+def topn(n: int) -> Truncation:
+    if n < 0:
+        raise ValueError("topn needs n >= 0")
+    return Truncation("topn", int(n))
+
+
+def policy_to_c(policy):
+    if policy is None:
+        return None
+    if not isinstance(policy, Truncation):
+        raise TypeError("policy must be a paulistrings_b200.truncation policy or None")
+    return policy.to_c()

@@ -1,0 +1,299 @@
+"""Parity of the device layer path against the CPU oracle (needs a CUDA device).
+
+Rotation and depolarizing layers sum at most two contributions per key, so with products
+and sums rounded once on both sides the surviving strings AND their coefficients are
+bit-exact; the tests assert exactly that.  Expectation values are float64 sums in a
+different order, compared at 1e-12 relative.  TopN boundary ties are kept first in key
+order on both sides, so truncated runs are bit-exact too.
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+import paulistrings_b200 as ps
+from paulistrings_b200 import truncation, workloads
+from tests._util import (
+    assert_same_terms,
+    circuit_from_gates,
+    load_golden,
+    oracle_arrays,
+    oracle_channels,
+    oracle_policy,
+    oracle_sum,
+)
+
+pytestmark = pytest.mark.gpu
+
+
+def run_both(num_qubits, x, z, c, circuit, policy=None, direction="forward", dtype="f64"):
+    """(device arrays, oracle arrays, device per-layer lengths, oracle per-layer lengths)."""
+    g = ps.GpuPauliSum(num_qubits, dtype)
+    g.upload(x, z, c)
+    st = g.propagate(circuit, policy, direction, with_stats=True)
+    got = g.download()
+    o = oracle_sum(num_qubits, x, z, c, dtype)
+    after = o.propagate(oracle_channels(circuit), oracle_policy(policy), direction)
+    return got, oracle_arrays(o), st.terms_after, [int(v) for v in after], g, o
+
+
+def labels_to_arrays(terms, n):
+    W = ps.width_for(n)
+    xs, zs, cs = [], [], []
+    for lab, v in terms.items():
+        x, z = ps.parse_label(lab, W)
+        xs.append(x)
+        zs.append(z)
+        cs.append(v)
+    return np.array(xs, np.uint64).reshape(-1, W), np.array(zs, np.uint64).reshape(-1, W), np.array(cs, np.float64)
+
+
+def test_device_is_visible_and_library_loaded():
+    assert ps.cuda_available()
+    assert ps.device_count() >= 1
+
+
+# --- hand-computed identities (python/paulistrings/tests/test_pauli_rotation.py:62-137) -------------
+
+
+def test_rz_on_x_is_cos_x_plus_sin_y():
+    theta = 0.6
+    s = ps.PauliSum.from_strings({"X": 1.0}, num_qubits=1)
+    c = ps.Circuit(1)
+    c.append(ps.gates.pauli_rotation("Z", [0], theta))
+    out = ps.propagated(s, circuit=c, direction="forward").to_dict()
+    assert out == {"X": math.cos(theta), "Y": math.sin(theta)}
+
+
+def test_zz_on_xi_is_cos_xi_plus_sin_yz():
+    theta = 0.6
+    s = ps.PauliSum.from_strings({"XI": 1.0}, num_qubits=2)
+    c = ps.Circuit(2)
+    c.pauli_rotation("ZZ", [0, 1], theta)
+    assert ps.propagated(s, c).to_dict() == {"XI": math.cos(theta), "YZ": math.sin(theta)}
+
+
+def test_clifford_point_moves_instead_of_splitting():
+    s = ps.PauliSum.from_strings({"XI": 1.0}, num_qubits=2)
+    c = ps.Circuit(2)
+    c.pauli_rotation("ZZ", [0, 1], -math.pi / 2)
+    assert ps.propagated(s, c).to_dict() == {"YZ": -1.0}
+
+
+def test_rz_matches_weight_one_pauli_rotation():
+    s = ps.PauliSum.from_strings({"XIZ": 1.0, "ZYI": 0.25}, num_qubits=3)
+    a, b = ps.Circuit(3), ps.Circuit(3)
+    a.pauli_rotation("Z", [0], -0.37)
+    b.rz(-0.37, 0)
+    assert ps.propagated(s, a).to_dict() == ps.propagated(s, b).to_dict()
+
+
+def test_heisenberg_round_trip_is_identity():
+    c = ps.Circuit(3)
+    c.pauli_rotation("XY", [0, 2], 0.3)
+    c.rz(1.1, 1)
+    c.pauli_rotation("YYZ", [0, 1, 2], -0.7)
+    s = ps.PauliSum.from_strings({"XZY": 0.5}, num_qubits=3)
+    s.propagate(c, direction="forward")
+    s.propagate(c, direction="heisenberg")
+    d = s.to_dict()
+    assert d["XZY"] == pytest.approx(0.5, abs=1e-15)
+    assert all(abs(v) < 1e-15 for k, v in d.items() if k != "XZY")
+
+
+# --- golden fixtures from the reference ------------------------------------------------------------
+
+XXZ = load_golden("xxz_statevector.json")["cases"]
+
+
+@pytest.mark.parametrize("case", [c for c in XXZ if c["final_terms"] <= 200_000],
+                         ids=lambda c: f"n{c['n']}-Jz{c['Jz']}-s{c['steps']}-o{len(c['observable_z'])}")
+def test_xxz_statevector_fixture_bit_exact(case):
+    n = case["n"]
+    lab = ["I"] * n
+    for q in case["observable_z"]:
+        lab[q] = "Z"
+    x, z, c = labels_to_arrays({"".join(lab): 1.0}, n)
+    circ = circuit_from_gates(n, case["gates"])
+    pol = truncation.coeff(case["epsilon"])
+    got, want, la, lb, g, _ = run_both(n, x, z, c, circ, pol, "heisenberg")
+    assert la == lb
+    assert_same_terms(got, want, what="xxz")
+    assert len(got[2]) == case["final_terms"]
+    assert abs(g.expectation(case["state"]) - case["expectation"]) <= 1e-14
+
+
+JL = load_golden("jl_parity.json")["workloads"]
+
+
+@pytest.mark.parametrize(
+    "key,point",
+    [(k, p) for k, w in JL.items() for p in w["points"] if p["final_terms"] <= 80_000],
+    ids=lambda v: v if isinstance(v, str) else f"eps{v['epsilon']:.3g}-w{v['max_weight']}",
+)
+def test_jl_parity_fixture_bit_exact(key, point):
+    w = JL[key]
+    n = w["n_qubits"]
+    lab = ["I"] * n
+    for q in w["observable_z"]:
+        lab[q] = "Z"
+    x, z, c = labels_to_arrays({"".join(lab): 1.0}, n)
+    pol = truncation.coeff(point["epsilon"])
+    if point["max_weight"] is not None:
+        pol = truncation.weight(point["max_weight"]) & pol
+    got, want, la, lb, g, _ = run_both(n, x, z, c, circuit_from_gates(n, w["gates"]), pol, "heisenberg")
+    assert la == lb
+    assert_same_terms(got, want, what=key)
+    assert len(got[2]) == point["final_terms"]
+    if point["expectation"] is not None:
+        assert abs(g.expectation(w["state"]) - point["expectation"]) <= 1e-13
+
+
+# --- the measured configurations at oracle-sized scales ---------------------------------------------
+
+
+def test_tfim_6x6_threshold_per_layer_counts_and_bit_exact():
+    circ = workloads.tfim_2d(6, 5, J=1.0, h=1.0, dt=0.1)
+    x, z, c = labels_to_arrays(workloads.tfim_magnetization(6, "X"), 36)
+    got, want, la, lb, g, o = run_both(36, x, z, c, circ, truncation.coeff(1e-5), "heisenberg")
+    assert la == lb
+    assert_same_terms(got, want, what="tfim6")
+    assert g.expectation("z+") == pytest.approx(o.expectation("z+"), rel=1e-12, abs=1e-15)
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_noisy_tfim_bit_exact_per_dtype(dtype):
+    circ = workloads.tfim_2d(6, 2, J=1.0, h=1.0, dt=0.1, noise_p=1e-3)
+    x, z, c = labels_to_arrays(workloads.tfim_magnetization(6, "X"), 36)
+    got, want, la, lb, g, o = run_both(36, x, z, c, circ, truncation.coeff(1e-5), "heisenberg", dtype)
+    assert la == lb
+    assert_same_terms(got, want, what=f"noisy-{dtype}")
+    assert g.expectation("z+") == pytest.approx(o.expectation("z+"), rel=1e-12, abs=1e-15)
+
+
+def test_random_pair_layers_with_topn_and_threshold_bit_exact():
+    circ = workloads.random_pair_layers(16, 2)
+    x, z, c = workloads.random_observable(16, 400)
+    pol = truncation.topn(3000) & truncation.coeff(1e-10)
+    got, want, la, lb, _, _ = run_both(16, x, z, c, circ, pol, "heisenberg")
+    assert la == lb
+    assert max(la) == 3000
+    assert_same_terms(got, want, what="pairs-topn")
+
+
+def test_config1_shape_first_layers_no_truncation_bit_exact():
+    full = workloads.random_pair_layers(64, 1)
+    circ = ps.Circuit(64)
+    for ch in list(full)[:10]:
+        circ.append(ch)
+    x, z, c = workloads.random_observable(64, 65536)
+    got, want, la, lb, _, _ = run_both(64, x, z, c, circ, truncation.coeff(1e-10), "heisenberg")
+    assert la == lb
+    assert_same_terms(got, want, what="config1-prefix")
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_wide_rotations_and_word_boundaries_bit_exact(seed):
+    rng = np.random.default_rng(seed)
+    for n in (10, 100, 200):
+        circ = ps.Circuit(n)
+        for _ in range(12):
+            w = int(rng.integers(1, 7))
+            qs = [int(q) for q in rng.choice(n, size=w, replace=False)]
+            circ.pauli_rotation("".join(rng.choice(list("XYZ"), size=w)), qs, float(rng.uniform(-3.2, 3.2)))
+        x, z, c = workloads.random_observable(n, 300, seed=seed)
+        got, want, la, lb, _, _ = run_both(n, x, z, c, circ, truncation.coeff(1e-9), "forward")
+        assert la == lb
+        assert_same_terms(got, want, what=f"wide-{n}")
+
+
+def test_weight_and_or_keep_programs_bit_exact():
+    circ = workloads.random_pair_layers(12, 1)
+    x, z, c = workloads.random_observable(12, 200)
+    pol = truncation.weight(3) | truncation.coeff(0.05)
+    got, want, la, lb, _, _ = run_both(12, x, z, c, circ, pol, "forward")
+    assert la == lb
+    assert_same_terms(got, want, what="or-program")
+
+
+# --- ingest, edge cases, errors ----------------------------------------------------------------------
+
+
+def test_upload_sums_duplicates_in_order_and_drops_zeros():
+    W = 1
+    x = np.array([[1], [2], [1], [3], [3]], np.uint64)
+    z = np.array([[0], [2], [0], [1], [1]], np.uint64)
+    c = np.array([0.1, 0.5, 0.2, 0.25, -0.25])
+    s = ps.PauliSum.from_arrays(x, z, c, num_qubits=2)
+    assert s.x_array().tolist() == [[1], [2]]
+    assert s.z_array().tolist() == [[0], [2]]
+    assert s.coefficients_array().tolist() == [0.1 + 0.2, 0.5]
+    o = oracle_sum(2, x, z, c)
+    assert_same_terms((s.x_array(), s.z_array(), s.coefficients_array()), oracle_arrays(o), what="ingest")
+
+
+def test_upload_rejects_bits_beyond_num_qubits():
+    g = ps.GpuPauliSum(3)
+    with pytest.raises(ValueError):
+        g.upload(np.array([[8]], np.uint64), np.array([[0]], np.uint64), np.array([1.0]))
+
+
+def test_empty_sum_and_identity_layers():
+    g = ps.GpuPauliSum(4)
+    g.upload(np.zeros((0, 1), np.uint64), np.zeros((0, 1), np.uint64), np.zeros(0))
+    c = ps.Circuit(4)
+    c.pauli_rotation("XY", [0, 1], 0.3)
+    g.propagate(c)
+    assert len(g) == 0
+    s = ps.PauliSum.from_strings({"XIII": 1.0, "IZII": -2.0}, num_qubits=4)
+    c = ps.Circuit(4)
+    c.pauli_rotation("ZZ", [2, 3], 0.0)
+    c.pauli_rotation("ZZ", [0, 1], math.pi)
+    out = ps.propagated(s, c).to_dict()
+    assert out == {"XIII": -1.0, "IZII": -2.0}
+
+
+def test_layer_api_matches_propagate():
+    circ = workloads.random_pair_layers(10, 1)
+    x, z, c = workloads.random_observable(10, 100)
+    g1 = ps.GpuPauliSum(10)
+    g1.upload(x, z, c)
+    for ch in circ:
+        g1.apply_layer(ch, truncation.coeff(1e-6))
+    g2 = ps.GpuPauliSum(10)
+    g2.upload(x, z, c)
+    g2.propagate(circ, truncation.coeff(1e-6))
+    assert_same_terms(g1.download(), g2.download(), what="layer-api")
+
+
+def test_invalid_channel_leaves_store_untouched():
+    s = ps.PauliSum.from_strings({"XI": 1.0}, num_qubits=2)
+    g = s.to_device()
+    c = ps.Circuit(2)
+    c.pauli_rotation("ZZ", [0, 1], 0.1)
+    c._channels.append(ps.PauliRotation("Z", (5,), 0.1))
+    with pytest.raises(ValueError):
+        g.propagate(c)
+    assert g.download()[2].tolist() == [1.0]
+
+
+# --- full-size properties (no oracle) ---------------------------------------------------------------
+
+
+def test_large_rotation_layers_preserve_norm_and_order():
+    x, z, c = workloads.random_observable(64, 1 << 16)
+    g = ps.GpuPauliSum(64)
+    g.upload(x, z, c)
+    circ = workloads.random_pair_layers(64, 1)
+    g.propagate(circ, None, "heisenberg")
+    gx, gz, gc = g.download()
+    assert len(gc) > 1_000_000
+    keys = np.concatenate([gx, gz], axis=1)
+    # strictly increasing in (x, z) lexicographic order: sorted and unique
+    lex = np.lexsort(keys.T[::-1])
+    assert np.array_equal(lex, np.arange(len(gc)))
+    diff = np.any(keys[1:] != keys[:-1], axis=1)
+    assert diff.all()
+    # orthogonal layers preserve the 2-norm (no truncation)
+    assert np.sum(gc * gc) == pytest.approx(1.0, rel=1e-12)
