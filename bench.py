@@ -299,7 +299,7 @@ def run_ours(args, world, rank, local):
     value = all_terms / (max_ms * 1e-3)
 
     # --- end to end through the C ABI with pinned host buffers ---------------------------------
-    rows = 2 * TERM_CAP + 1
+    rows = TERM_CAP + 1024
     pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True).numpy()
     hx = pin((rows, 1), torch.int64).view(np.uint64)
     hz = pin((rows, 1), torch.int64).view(np.uint64)
