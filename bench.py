@@ -49,14 +49,15 @@ EPS = 1e-10
 SEED = 0xC0FFEE
 
 
-def workload_config(k, w):
+def workload_config(k, w, cap=None):
+    cap = cap or TERM_CAP
     return {
         "workload": "random two-qubit rotation layers: 64 qubits, 30 layers x (32 pair rotations + 64 RZ), "
         "65,536-term random observable, Heisenberg, TopN(2^26) & coeff(1e-10), f64",
         "num_qubits": NUM_QUBITS,
         "layers": LAYERS,
         "channels_per_layer": 96,
-        "term_cap": TERM_CAP,
+        "term_cap": cap,
         "initial_terms": 65536,
         "timed_layers": k,
         "warmup_layers": w,
@@ -266,7 +267,8 @@ def run_ours(args, world, rank, local):
     from paulistrings_b200 import truncation, workloads
 
     seed = SEED + 7919 * rank
-    policy = truncation.topn(TERM_CAP) & truncation.coeff(EPS)
+    cap = args.term_cap
+    policy = truncation.topn(cap) & truncation.coeff(EPS)
     layers = layer_circuits(seed)
     assert args.warmup + args.steps <= LAYERS, "warmup + steps must fit in the 30-layer circuit"
     x0, z0, c0 = workloads.random_observable(NUM_QUBITS, 65536, seed + 1)
@@ -281,12 +283,16 @@ def run_ours(args, world, rank, local):
     terms = 0
     dev_ms = 0.0
     launches = 0
+    torch.cuda.synchronize()
+    # ncu --profile-from-start off captures exactly the timed steps
+    torch.cuda.cudart().cudaProfilerStart()
     with ClockSampler(local) as clocks:
         for li in range(args.warmup, args.warmup + args.steps):
             st = g.propagate(layers[li], policy, "heisenberg", with_stats=True)
             terms += st.total_terms_in
             dev_ms += st.device_ms
             launches += st.kernel_launches
+    torch.cuda.cudart().cudaProfilerStop()
     barrier(world)
     prof = g.read_profile()
     g.set_profiling(False)
@@ -299,7 +305,11 @@ def run_ours(args, world, rank, local):
     value = all_terms / (max_ms * 1e-3)
 
     # --- end to end through the C ABI with pinned host buffers ---------------------------------
-    rows = TERM_CAP + 1024
+    if args.no_e2e:
+        e2e_value, h2d, d2h = None, 0, 0
+        return finish(args, world, rank, value, max_ms, launches, prof, dev_ms, clocks, state_after, cap,
+                      e2e_value, h2d, d2h)
+    rows = cap + 1024
     pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True).numpy()
     hx = pin((rows, 1), torch.int64).view(np.uint64)
     hz = pin((rows, 1), torch.int64).view(np.uint64)
@@ -335,7 +345,11 @@ def run_ours(args, world, rank, local):
     barrier(world)
     e2e_value = dist_sum(e2e_terms, world) / e2e_s
     g.close()
+    return finish(args, world, rank, value, max_ms, launches, prof, dev_ms, clocks, state_after, cap, e2e_value,
+                  h2d, d2h)
 
+
+def finish(args, world, rank, value, max_ms, launches, prof, dev_ms, clocks, state_after, cap, e2e_value, h2d, d2h):
     if rank != 0:
         return
     peak, peak_kind = measured_peaks()
@@ -360,7 +374,7 @@ def run_ours(args, world, rank, local):
     all_bytes = sum(r["algorithmic_bytes"] for r in prof.values())
     all_ms = sum(r["total_ms"] for r in prof.values())
     layer_frac = all_bytes / (dev_ms * 1e-3) / 1e9 / peak
-    cb = cpu_baseline(args.cpu_seconds) if world == 1 else None
+    cb = cpu_baseline(args.cpu_seconds) if world == 1 and args.cpu_seconds > 0 else None
     line = {
         "metric": METRIC,
         "value": value,
@@ -374,9 +388,10 @@ def run_ours(args, world, rank, local):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": dict(workload_config(args.steps, args.warmup), parallelism=f"replicas{world}"),
-        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d // args.steps,
-                "d2h_bytes_per_step": d2h // args.steps},
+        "config": dict(workload_config(args.steps, args.warmup, cap), parallelism=f"replicas{world}"),
+        "e2e": None if e2e_value is None else {"value": e2e_value, "unit": METRIC,
+                                              "h2d_bytes_per_step": h2d // args.steps,
+                                              "d2h_bytes_per_step": d2h // args.steps},
         "gpu_launches": launches,
         "roofline": roofline,
         "layer_roofline_frac": round(layer_frac, 4),
@@ -397,6 +412,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--term-cap", type=int, default=TERM_CAP,
+                    help="TopN cap; smaller values give the small cases profiled under ncu")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")

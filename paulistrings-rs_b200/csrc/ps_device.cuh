@@ -264,26 +264,38 @@ constexpr unsigned long long kFlagAgg = 1ull << 62;
 constexpr unsigned long long kFlagInc = 2ull << 62;
 constexpr unsigned long long kValMask = (1ull << 62) - 1;
 
-// Exclusive prefix of tile `tile` (called by one thread after it published its aggregate).
-__device__ __forceinline__ unsigned long long lookback_sum(const unsigned long long* status, unsigned int tile,
-                                                          Ctl* ctl, uint32_t info) {
+// Exclusive prefix of tile `tile`, computed by one full warp after the tile published its
+// aggregate: each poll reads 32 predecessors at once, sums the aggregates up to the nearest
+// inclusive prefix, and moves the window back only when none of the 32 holds one.
+// Returns the same value in every lane.
+__device__ __forceinline__ unsigned long long lookback_sum_warp(const unsigned long long* status, unsigned int tile,
+                                                               Ctl* ctl, uint32_t info) {
+    const int lane = threadIdx.x & 31;
     unsigned long long acc = 0;
+    long long base = (long long)tile - 1;
     long long spins = 0;
-    int t = (int)tile - 1;
-    while (t >= 0) {
-        unsigned long long v = ld_acquire_u64(status + t);
-        unsigned long long f = v & ~kValMask;
-        if (f == 0) {
+    while (base >= 0) {
+        const long long t = base - lane;
+        unsigned long long v = t >= 0 ? ld_acquire_u64(status + t) : kFlagInc;  // before tile 0: prefix 0
+        const unsigned long long f = v & ~kValMask;
+        const unsigned int empty = __ballot_sync(0xffffffffu, f == 0);
+        const unsigned int inc = __ballot_sync(0xffffffffu, f == kFlagInc);
+        const int first_inc = inc ? __ffs(inc) - 1 : 32;
+        const unsigned int need = first_inc >= 31 ? 0xffffffffu : ((2u << first_inc) - 1u);
+        if (empty & need) {
             if (++spins > kSpinLimit) {
-                raise_err(ctl, ERR_TIMEOUT, info);
+                if (lane == 0) raise_err(ctl, ERR_TIMEOUT, info);
                 return acc;
             }
-            __nanosleep(32);
+            __nanosleep(20);
             continue;
         }
-        acc += v & kValMask;
-        if (f == kFlagInc) break;
-        --t;
+        unsigned long long val = lane <= first_inc ? (v & kValMask) : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+        acc += val;
+        if (first_inc < 32) break;
+        base -= 32;
     }
     return acc;
 }

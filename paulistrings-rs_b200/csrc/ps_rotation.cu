@@ -161,16 +161,16 @@ __global__ void __launch_bounds__(kBlock) k_classify(const uint64_t* __restrict_
     __syncthreads();
     for (int w = 0; w < warp; ++w) before = max(before, s_wlast[w]);
 
-    if (tid == 0) {
+    if (tid < 32) {
+        unsigned long long p = 0;
         if (tile == 0) {
-            st_release_u64(status + tile, kFlagInc | (unsigned long long)total);
-            s_prefix = 0;
+            if (tid == 0) st_release_u64(status + tile, kFlagInc | (unsigned long long)total);
         } else {
-            st_release_u64(status + tile, kFlagAgg | (unsigned long long)total);
-            unsigned long long p = lookback_sum(status, tile, ctl, 102);
-            st_release_u64(status + tile, kFlagInc | (p + total));
-            s_prefix = p;
+            if (tid == 0) st_release_u64(status + tile, kFlagAgg | (unsigned long long)total);
+            p = lookback_sum_warp(status, tile, ctl, 102);
+            if (tid == 0) st_release_u64(status + tile, kFlagInc | (p + total));
         }
+        if (tid == 0) s_prefix = p;
     }
     __syncthreads();
     const unsigned long long base = s_prefix + excl;
@@ -201,44 +201,66 @@ __global__ void __launch_bounds__(kBlock) k_classify(const uint64_t* __restrict_
 // every key bit more significant than L, and its "split" is the first row whose
 // bit L is set.  Starts: j == 0 or D[j] < L.  Splits: D[j] == L.
 // ---------------------------------------------------------------------------
-// Combine for the forward scan (max) or the backward scan (min) over tiles before `tile`
-// in scan order; publishes this tile's aggregate first and its inclusive value after.
+// Look-back over the tiles before `tile` in scan order for the forward (max) or backward
+// (min) level scans, by one full warp: each poll reads 32 predecessors' slots, combines their
+// aggregates up to the nearest inclusive value, and moves back only when none of the 32 has
+// one.  Publishes this tile's aggregate first and its inclusive value after.
 template <bool kMax>
 __device__ __forceinline__ void level_lookback(LevelSlot* slots, unsigned int tile, const int (&tile_agg)[2 * kMaxLevels],
                                                int (&prefix)[2 * kMaxLevels], int identity, Ctl* ctl, uint32_t info) {
+    const int lane = threadIdx.x & 31;
+    auto comb = [](int a, int b) { return kMax ? max(a, b) : min(a, b); };
+#pragma unroll
     for (int v = 0; v < 2 * kMaxLevels; ++v) prefix[v] = identity;
     if (tile == 0) {
-        for (int v = 0; v < 2 * kMaxLevels; ++v) slots[0].inc[v] = tile_agg[v];
-        __threadfence();
-        st_release_u32(&slots[0].flag, 2u);
+        if (lane == 0) {
+            for (int v = 0; v < 2 * kMaxLevels; ++v) slots[0].inc[v] = tile_agg[v];
+            __threadfence();
+            st_release_u32(&slots[0].flag, 2u);
+        }
+        __syncwarp();
         return;
     }
-    for (int v = 0; v < 2 * kMaxLevels; ++v) slots[tile].agg[v] = tile_agg[v];
-    __threadfence();
-    st_release_u32(&slots[tile].flag, 1u);
+    if (lane == 0) {
+        for (int v = 0; v < 2 * kMaxLevels; ++v) slots[tile].agg[v] = tile_agg[v];
+        __threadfence();
+        st_release_u32(&slots[tile].flag, 1u);
+    }
+    long long base = (long long)tile - 1;
     long long spins = 0;
-    for (int t = (int)tile - 1; t >= 0;) {
-        unsigned int f = ld_acquire_u32(&slots[t].flag);
-        if (f == 0) {
+    while (base >= 0) {
+        const long long t = base - lane;
+        const unsigned int f = t >= 0 ? ld_acquire_u32(&slots[t].flag) : 2u;
+        const unsigned int empty = __ballot_sync(0xffffffffu, f == 0u);
+        const unsigned int inc = __ballot_sync(0xffffffffu, f == 2u);
+        const int first_inc = inc ? __ffs(inc) - 1 : 32;
+        const unsigned int need = first_inc >= 31 ? 0xffffffffu : ((2u << first_inc) - 1u);
+        if (empty & need) {
             if (++spins > kSpinLimit) {
-                raise_err(ctl, ERR_TIMEOUT, info);
+                if (lane == 0) raise_err(ctl, ERR_TIMEOUT, info);
                 break;
             }
-            __nanosleep(32);
+            __nanosleep(20);
             continue;
         }
-        const int* src = f == 2u ? slots[t].inc : slots[t].agg;
+        const bool use = lane <= first_inc && t >= 0;
+        const int* src = f == 2u ? slots[t >= 0 ? t : 0].inc : slots[t >= 0 ? t : 0].agg;
+#pragma unroll
         for (int v = 0; v < 2 * kMaxLevels; ++v) {
-            int x = __ldcg(src + v);
-            prefix[v] = kMax ? max(prefix[v], x) : min(prefix[v], x);
+            int x = use ? __ldcg(src + v) : identity;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x = comb(x, __shfl_xor_sync(0xffffffffu, x, o));
+            prefix[v] = comb(prefix[v], x);
         }
-        if (f == 2u) break;
-        --t;
+        if (first_inc < 32) break;
+        base -= 32;
     }
-    for (int v = 0; v < 2 * kMaxLevels; ++v)
-        slots[tile].inc[v] = kMax ? max(prefix[v], tile_agg[v]) : min(prefix[v], tile_agg[v]);
-    __threadfence();
-    st_release_u32(&slots[tile].flag, 2u);
+    if (lane == 0) {
+        for (int v = 0; v < 2 * kMaxLevels; ++v) slots[tile].inc[v] = comb(prefix[v], tile_agg[v]);
+        __threadfence();
+        st_release_u32(&slots[tile].flag, 2u);
+    }
+    __syncwarp();
 }
 
 template <int W>
@@ -315,7 +337,7 @@ __global__ void __launch_bounds__(kBlock) k_fwd_levels(const uint32_t* __restric
         for (int w = 0; w < warp; ++w) excl[v] = max(excl[v], s_wagg[w][v]);
     // tile aggregate, publish, look back
     __syncthreads();
-    if (tid == 0) {
+    if (tid < 32) {
         int tagg[2 * kMaxLevels], pre[2 * kMaxLevels];
         for (int v = 0; v < 2 * kMaxLevels; ++v) {
             int t = -1;
@@ -323,7 +345,8 @@ __global__ void __launch_bounds__(kBlock) k_fwd_levels(const uint32_t* __restric
             tagg[v] = t;
         }
         level_lookback<true>(slots, tile, tagg, pre, -1, ctl, 202);
-        for (int v = 0; v < 2 * kMaxLevels; ++v) s_prefix[v] = pre[v];
+        if (tid == 0)
+            for (int v = 0; v < 2 * kMaxLevels; ++v) s_prefix[v] = pre[v];
     }
     __syncthreads();
 #pragma unroll
@@ -413,7 +436,7 @@ __global__ void __launch_bounds__(kBlock) k_bwd_levels(const uint32_t* __restric
     for (int v = 0; v < 2 * kMaxLevels; ++v)
         for (int w = warp + 1; w < kBlock / 32; ++w) excl[v] = min(excl[v], s_wagg[w][v]);
     __syncthreads();
-    if (tid == 0) {
+    if (tid < 32) {
         int tagg[2 * kMaxLevels], suf[2 * kMaxLevels];
         for (int v = 0; v < 2 * kMaxLevels; ++v) {
             int t = INF;
@@ -421,7 +444,8 @@ __global__ void __launch_bounds__(kBlock) k_bwd_levels(const uint32_t* __restric
             tagg[v] = t;
         }
         level_lookback<false>(slots, tile, tagg, suf, INF, ctl, 203);
-        for (int v = 0; v < 2 * kMaxLevels; ++v) s_suffix[v] = suf[v];
+        if (tid == 0)
+            for (int v = 0; v < 2 * kMaxLevels; ++v) s_suffix[v] = suf[v];
     }
     __syncthreads();
 #pragma unroll
@@ -647,17 +671,19 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
     merge_range<W, T>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, keep, false, nullptr, nullptr, count);
     unsigned int total;
     unsigned int excl = block_exclusive_sum<kBlock>(count, s_warp, total);
-    if (tid == 0) {
+    if (tid < 32) {
+        unsigned long long p = 0;
         if (tile == 0) {
-            st_release_u64(status + tile, kFlagInc | (unsigned long long)total);
-            s_outoff = 0;
+            if (tid == 0) st_release_u64(status + tile, kFlagInc | (unsigned long long)total);
         } else {
-            st_release_u64(status + tile, kFlagAgg | (unsigned long long)total);
-            unsigned long long p = lookback_sum(status, tile, ctl, 303);
-            st_release_u64(status + tile, kFlagInc | (p + total));
-            s_outoff = p;
+            if (tid == 0) st_release_u64(status + tile, kFlagAgg | (unsigned long long)total);
+            p = lookback_sum_warp(status, tile, ctl, 303);
+            if (tid == 0) st_release_u64(status + tile, kFlagInc | (p + total));
         }
-        if (tile == num_tiles - 1) ctl->count[1] = s_outoff + total;
+        if (tid == 0) {
+            s_outoff = p;
+            if (tile == num_tiles - 1) ctl->count[1] = p + total;
+        }
     }
     uint32_t c2;
     merge_range<W, T>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, keep, true, oK + (size_t)excl * 2 * W, oC + excl, c2);

@@ -244,17 +244,19 @@ __global__ void __launch_bounds__(kThreads) k_dedup(const uint64_t* __restrict__
     }
     unsigned int count = __popc(keepmask), total;
     unsigned int excl = block_exclusive_sum<kThreads>(count, s_warp, total);
-    if (tid == 0) {
+    if (tid < 32) {
+        unsigned long long p = 0;
         if (tile == 0) {
-            st_release_u64(status + tile, kFlagInc | (unsigned long long)total);
-            s_off = 0;
+            if (tid == 0) st_release_u64(status + tile, kFlagInc | (unsigned long long)total);
         } else {
-            st_release_u64(status + tile, kFlagAgg | (unsigned long long)total);
-            unsigned long long p = lookback_sum(status, tile, ctl, 601);
-            st_release_u64(status + tile, kFlagInc | (p + total));
-            s_off = p;
+            if (tid == 0) st_release_u64(status + tile, kFlagAgg | (unsigned long long)total);
+            p = lookback_sum_warp(status, tile, ctl, 601);
+            if (tid == 0) st_release_u64(status + tile, kFlagInc | (p + total));
         }
-        if ((uint64_t)(tile + 1) * (kThreads * ITEMS) >= n) ctl->count[2] = s_off + total;
+        if (tid == 0) {
+            s_off = p;
+            if ((uint64_t)(tile + 1) * (kThreads * ITEMS) >= n) ctl->count[2] = p + total;
+        }
     }
     __syncthreads();
     unsigned long long o = s_off + excl;
@@ -351,21 +353,23 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
     unsigned int ta, tt;
     unsigned int ea = block_exclusive_sum<kThreads>(__popc(amask), s_warp, ta);
     unsigned int et = block_exclusive_sum<kThreads>(__popc(tmask), s_warp, tt);
-    if (tid == 0) {
+    if (tid < 32) {
         unsigned long long agg = (unsigned long long)ta | ((unsigned long long)tt << 31);
         unsigned long long pre = 0;
         if (tile == 0) {
-            st_release_u64(status + tile, kFlagInc | agg);
+            if (tid == 0) st_release_u64(status + tile, kFlagInc | agg);
         } else {
-            st_release_u64(status + tile, kFlagAgg | agg);
-            pre = lookback_sum(status, tile, ctl, 701);
-            st_release_u64(status + tile, kFlagInc | (pre + agg));
+            if (tid == 0) st_release_u64(status + tile, kFlagAgg | agg);
+            pre = lookback_sum_warp(status, tile, ctl, 701);
+            if (tid == 0) st_release_u64(status + tile, kFlagInc | (pre + agg));
         }
-        s_above = pre & ((1ull << 31) - 1);
-        s_ties = pre >> 31;
-        if ((uint64_t)(tile + 1) * (kThreads * ITEMS) >= n) {
-            unsigned long long tot_ties = s_ties + tt;
-            ctl->count[3] = s_above + ta + (tot_ties < quota ? tot_ties : quota);
+        if (tid == 0) {
+            s_above = pre & ((1ull << 31) - 1);
+            s_ties = pre >> 31;
+            if ((uint64_t)(tile + 1) * (kThreads * ITEMS) >= n) {
+                unsigned long long tot_ties = s_ties + tt;
+                ctl->count[3] = s_above + ta + (tot_ties < quota ? tot_ties : quota);
+            }
         }
     }
     __syncthreads();
