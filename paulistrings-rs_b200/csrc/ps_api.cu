@@ -44,7 +44,8 @@ struct ps_sum {
     int cur = 0;
     uint64_t n = 0;
     Buf pk, pc;
-    Buf idx, dv, fv, slots, status, bounds, hist, partial, dout;
+    Buf idx, dv, fv, slots, status, bounds, hist, cand, partial, dout;
+    bool hist_ready = false;  // hist holds the TopN digit-1 histogram of the current store
     SortScratch sort{};
     Buf sort_status;
     LevelList* levels = nullptr;  // host scratch
@@ -581,6 +582,10 @@ struct Engine {
         if (fs != PS_OK) return fs;
         s->cur = spare;
         s->n = out_n;
+        if (s->hist_ready) {
+            cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+            s->hist_ready = false;
+        }
         return PS_OK;
     }
 
@@ -659,11 +664,23 @@ struct Engine {
         a.partners_out = &partners;
         a.out_count = &out_n;
         a.prof = &s->prof;
+        // the first layer pass is TopN and could trigger: the merge builds its first select digit
+        const bool fuse_topn = policy && policy->num_passes > 0 && policy->passes[0].kind == PS_PASS_TOPN &&
+                               out_rows > policy->passes[0].n;
+        if (s->hist_ready) {
+            cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+            s->hist_ready = false;
+        }
+        a.topn_hist = fuse_topn ? (unsigned int*)s->hist.p : nullptr;
         e = launch_rotation_layer<W, T>(a, s->stream);
         s->prof.resolve();
         if (e != cudaSuccess) return cuda_fail(s, e, "apply: rotation layer");
         ps = check_device_flags(s, "apply");
-        if (ps != PS_OK) return ps;
+        if (ps != PS_OK) {
+            if (fuse_topn) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+            return ps;
+        }
+        s->hist_ready = fuse_topn;
         if (stats) {
             stats->terms_in = n;
             stats->partners = partners;
@@ -677,32 +694,46 @@ struct Engine {
     }
 
     static ps_status finalize(ps_sum* s, const ps_policy* policy) {
-        if (!policy) return PS_OK;
-        for (int i = 0; i < policy->num_passes; ++i) {
+        const bool ready = s->hist_ready;
+        if (ready) s->hist_ready = false;
+        ps_status result = PS_OK;
+        for (int i = 0; policy && i < policy->num_passes; ++i) {
             const ps_pass& p = policy->passes[i];
             if (p.kind != PS_PASS_TOPN) continue;
-            if (s->n <= p.n) continue;
+            const bool use_hist = ready && i == 0;
+            if (s->n <= p.n) {
+                if (use_hist) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+                continue;
+            }
             if (p.n == 0) {
+                if (use_hist) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
                 s->n = 0;
                 continue;
             }
             const int spare = 1 - s->cur;
             cudaError_t e = reserve_store(s, spare, p.n);
-            if (e == cudaSuccess) e = ensure(s->hist, 256 * sizeof(unsigned int));
-            if (e == cudaSuccess) e = ensure(s->status, (s->n / 2048 + 4) * sizeof(unsigned long long));
-            if (e != cudaSuccess) return cuda_fail(s, e, "topn: scratch");
+            if (e == cudaSuccess) e = ensure(s->cand, s->n * sizeof(uint64_t));
+            if (e == cudaSuccess) e = ensure(s->status, (s->n / 4096 + 4) * sizeof(unsigned long long));
+            if (e != cudaSuccess) {
+                if (use_hist) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+                return cuda_fail(s, e, "topn: scratch");
+            }
             uint64_t out_n = 0;
             e = StoreOps<W, T>::topn(K(s, s->cur), C(s, s->cur), s->n, p.n, K(s, spare), C(s, spare),
-                                     (unsigned int*)s->hist.p, (unsigned long long*)s->status.p, s->ctl, s->hcount,
-                                     &out_n, s->sms, s->stream, &s->prof);
+                                     (unsigned int*)s->hist.p, use_hist, (uint64_t*)s->cand.p, s->n,
+                                     (unsigned long long*)s->status.p, s->ctl, s->hcount, &out_n, s->sms,
+                                     s->stream, &s->prof);
             s->prof.resolve();
             if (e != cudaSuccess) return cuda_fail(s, e, "topn");
             ps_status ps = check_device_flags(s, "topn");
-            if (ps != PS_OK) return ps;
+            if (ps != PS_OK) {
+                cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+                return ps;
+            }
             s->cur = spare;
             s->n = out_n;
         }
-        return PS_OK;
+        return result;
     }
 
     static ps_status expectation(ps_sum* s, const uint64_t* ax, const uint64_t* az, const uint64_t* neg, double* out) {
@@ -799,6 +830,8 @@ ps_status ps_create(int32_t device, int32_t num_qubits, int32_t dtype, ps_sum** 
     if (e == cudaSuccess) e = cudaMalloc(&s->sort.base, 16 * W * 256 * sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMallocHost(&s->sort.host_hist, 16 * W * 256 * sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMallocHost(&s->sort.host_base, 16 * W * 256 * sizeof(unsigned int));
+    if (e == cudaSuccess) e = ensure(s->hist, kTopnBinsN * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
     if (e == cudaSuccess) {
         ps_status st = dispatch<Engine>(s, [&](auto op) {
             cudaError_t ce = decltype(op)::configure();
@@ -822,7 +855,7 @@ ps_status ps_destroy(ps_sum* s) {
     DeviceGuard g(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (Buf* b : {&s->keys[0], &s->keys[1], &s->coef[0], &s->coef[1], &s->pk, &s->pc, &s->idx, &s->dv, &s->fv,
-                   &s->slots, &s->status, &s->bounds, &s->hist, &s->partial, &s->dout, &s->sort_status})
+                   &s->slots, &s->status, &s->bounds, &s->hist, &s->cand, &s->partial, &s->dout, &s->sort_status})
         release(*b);
     if (s->ctl) cudaFree(s->ctl);
     if (s->sort.hist) cudaFree(s->sort.hist);

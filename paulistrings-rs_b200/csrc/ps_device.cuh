@@ -214,6 +214,16 @@ __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, 
 __device__ __forceinline__ double to_f64(double a) { return a; }
 __device__ __forceinline__ double to_f64(float a) { return (double)a; }
 
+// TopN select key of a coefficient: 0 for NaN, else bits(|c|^2) + 1 (monotone in |c|^2, as the
+// reference's norm_sqr ordering; crates/paulistrings/src/truncation/builtin.rs:107-110).
+template <typename T>
+__device__ __forceinline__ uint64_t mag_key(T c) {
+    double v = to_f64(c);
+    double m = __dmul_rn(v, v);
+    if (isnan(m)) return 0ull;
+    return (uint64_t)__double_as_longlong(m) + 1ull;
+}
+
 // Knuth TwoSum: s + e == a + b exactly.
 template <typename T>
 __device__ __forceinline__ void two_sum(T a, T b, T& s, T& e) {

@@ -157,6 +157,7 @@ struct RotationArgs {
     uint64_t* partners_out;
     uint64_t* out_count;
     KernelProf* prof;
+    unsigned int* topn_hist;  // when set, the merge histograms key >> 52 of its outputs (2048 bins)
 };
 
 template <int W, typename T>

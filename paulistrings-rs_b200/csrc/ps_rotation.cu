@@ -27,23 +27,37 @@
 namespace psb {
 
 constexpr int kBlock = 256;
+constexpr int kTopnHistBins = 2048;  // key >> 52 of |c|^2 (first TopN select digit)
 
 template <int W>
 struct RotTile {
-    static constexpr int kClassifyItems = W == 1 ? 8 : (W == 2 ? 4 : (W == 4 ? 2 : 1));
-    static constexpr int kClassifyTile = kBlock * kClassifyItems;  // 32 KiB of keys per tile
-    static constexpr int kMergeItems = W == 1 ? 8 : (W == 2 ? 4 : (W == 4 ? 2 : 1));
+    static constexpr int kClassifyItems = W == 1 ? 16 : (W == 2 ? 8 : (W == 4 ? 4 : 2));
+    static constexpr int kClassifyTile = kBlock * kClassifyItems;
+    // odd, so the threads' merge-path starts fall on different shared-memory bank groups
+    static constexpr int kMergeItems = W == 1 ? 7 : (W == 2 ? 5 : (W == 4 ? 3 : 1));
     static constexpr int kMergeTile = kBlock * kMergeItems;
 };
 constexpr int kScanItems = 16;
 constexpr int kScanTile = kBlock * kScanItems;
 static_assert(kScanTile == (int)kScanTileRows, "scan tile");
 
+// word `wi` of a key held in registers, by an unrolled select (a runtime index into a
+// register array would move the array to local memory)
+template <int W>
+__device__ __forceinline__ uint64_t pick(const uint64_t* k, int wi) {
+    uint64_t v = k[0];
+#pragma unroll
+    for (int w = 1; w < 2 * W; ++w) v = (w == wi) ? k[w] : v;
+    return v;
+}
+
 // support pattern of key k (LocalPtm::support_bits, channel/prepared.rs:141-151)
 template <int W>
 __device__ __forceinline__ uint32_t pattern_of(const RotLayer<W>& L, const uint64_t* k) {
-    uint32_t s = (uint32_t)((k[L.qw[0]] >> L.qb[0]) & 1u) | (uint32_t)((k[W + L.qw[0]] >> L.qb[0]) & 1u) << 1 |
-                 (uint32_t)((k[L.qw[1]] >> L.qb[1]) & 1u) << 2 | (uint32_t)((k[W + L.qw[1]] >> L.qb[1]) & 1u) << 3;
+    uint32_t s = (uint32_t)((pick<W>(k, L.qw[0]) >> L.qb[0]) & 1u) |
+                 (uint32_t)((pick<W>(k, W + L.qw[0]) >> L.qb[0]) & 1u) << 1 |
+                 (uint32_t)((pick<W>(k, L.qw[1]) >> L.qb[1]) & 1u) << 2 |
+                 (uint32_t)((pick<W>(k, W + L.qw[1]) >> L.qb[1]) & 1u) << 3;
     return s & L.pattern_mask;
 }
 
@@ -79,6 +93,28 @@ __device__ __forceinline__ bool emits_partner(const RotLayer<W>& L, const uint64
     return Amp<T>::a1(L, pattern_of<W>(L, k)) != T(0);
 }
 
+template <int W, typename T>
+__device__ __forceinline__ bool emits_partner_regs(const RotLayer<W>& L, const uint64_t (&k)[2 * W]) {
+    if (L.wide) {
+        uint64_t f = 0;
+#pragma unroll
+        for (int i = 0; i < W; ++i) f ^= (k[i] & L.gz[i]) ^ (k[W + i] & L.gx[i]);
+        return (__popcll(f) & 1) != 0;
+    }
+    return Amp<T>::a1(L, pattern_of<W>(L, k)) != T(0);
+}
+
+template <int W>
+__device__ __forceinline__ uint32_t div_regs(const uint64_t (&a)[2 * W], const uint64_t (&b)[2 * W]) {
+    uint32_t r = 0xFFFFu;
+#pragma unroll
+    for (int i = 2 * W - 1; i >= 0; --i) {
+        uint64_t d = a[i] ^ b[i];
+        if (d) r = 64u * i + (uint32_t)__clzll((long long)d);
+    }
+    return r;
+}
+
 // Own-row coefficient after the layer.
 template <int W, typename T>
 __device__ __forceinline__ T own_coeff(const RotLayer<W>& L, const uint64_t* k, T c) {
@@ -98,7 +134,10 @@ __device__ __forceinline__ T partner_coeff(const RotLayer<W>& L, const uint64_t*
 }
 
 // ---------------------------------------------------------------------------
-// k_classify
+// k_classify: warp-striped (lane l of warp w reads row base_w + 32 i + l, coalesced 16W-byte
+// loads), anticommuting rows compacted by ballot in row order; each listed row records its
+// divergence rank from the previous listed row (shuffled from the lane that holds it).  The
+// first listed row of each warp takes kDivUnknown and k_fwd_levels resolves it.
 // ---------------------------------------------------------------------------
 template <int W, typename T>
 __global__ void __launch_bounds__(kBlock) k_classify(const uint64_t* __restrict__ keys, uint64_t n,
@@ -107,60 +146,41 @@ __global__ void __launch_bounds__(kBlock) k_classify(const uint64_t* __restrict_
                                                      Ctl* ctl) {
     constexpr int ITEMS = RotTile<W>::kClassifyItems;
     constexpr int TILE = RotTile<W>::kClassifyTile;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    uint64_t* sk = reinterpret_cast<uint64_t*>(smem_raw);
-    __shared__ uint64_t bar;
     __shared__ unsigned int s_tile;
-    __shared__ unsigned int s_warp[kBlock / 32];
-    __shared__ int s_wlast[kBlock / 32];
+    __shared__ unsigned int s_wcount[kBlock / 32];
     __shared__ unsigned long long s_prefix;
-
-    const int tid = threadIdx.x;
-    if (tid == 0) {
-        s_tile = atomicAdd(&ctl->tile_counter[0], 1u);
-        mbar_init(&bar, 1);
-    }
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned int lanemask_lt = (1u << lane) - 1u;
+    if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[0], 1u);
     __syncthreads();
     const unsigned int tile = s_tile;
-    const uint64_t row0 = (uint64_t)tile * TILE;
-    if (row0 >= n) return;  // grid is sized to the tile count; never taken
-    const uint32_t cnt = (uint32_t)min((uint64_t)TILE, n - row0);
-    if (tid == 0) {
-        uint32_t bytes = cnt * (uint32_t)(16 * W);
-        mbar_arrive_expect_tx(&bar, bytes);
-        bulk_g2s(sk, keys + row0 * (2 * W), bytes, &bar);
-    }
-    mbar_wait(&bar, 0, ctl, 101);
-
-    // flags of this thread's consecutive rows
-    uint32_t flags = 0;
-    int last_local = -1;
+    const uint64_t wbase = (uint64_t)tile * TILE + (uint64_t)warp * 32 * ITEMS;
+    uint64_t k[ITEMS][2 * W];
+    unsigned int ball[ITEMS];
+    unsigned int wcount = 0;
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
-        int r = tid * ITEMS + i;
-        if (r < (int)cnt) {
-            bool e = emits_partner<W, T>(L, sk + (size_t)r * 2 * W);
-            flags |= (uint32_t)e << i;
-            if (e) last_local = r;
-        }
-    }
-    unsigned int count = __popc(flags), total;
-    unsigned int excl = block_exclusive_sum<kBlock>(count, s_warp, total);
-
-    // exclusive max-scan of the last anticommuting local row over threads
-    const int lane = tid & 31, warp = tid >> 5;
-    int incl = last_local;
+        const uint64_t row = wbase + (uint64_t)i * 32 + lane;
+        bool e = false;
+        if (row < n) {
+            load_key<W>(keys, row, k[i]);
+            e = emits_partner_regs<W, T>(L, k[i]);
+        } else {
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl = max(incl, y);
+            for (int w = 0; w < 2 * W; ++w) k[i][w] = 0;
+        }
+        ball[i] = __ballot_sync(0xffffffffu, e);
+        wcount += __popc(ball[i]);
     }
-    int before = __shfl_up_sync(0xffffffffu, incl, 1);
-    if (lane == 0) before = -1;
-    if (lane == 31) s_wlast[warp] = incl;
+    if (lane == 0) s_wcount[warp] = wcount;
     __syncthreads();
-    for (int w = 0; w < warp; ++w) before = max(before, s_wlast[w]);
-
+    unsigned int wexcl = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < kBlock / 32; ++w) {
+        unsigned int c = s_wcount[w];
+        wexcl += w < warp ? c : 0u;
+        total += c;
+    }
     if (tid < 32) {
         unsigned long long p = 0;
         if (tile == 0) {
@@ -170,29 +190,45 @@ __global__ void __launch_bounds__(kBlock) k_classify(const uint64_t* __restrict_
             p = lookback_sum_warp(status, tile, ctl, 102);
             if (tid == 0) st_release_u64(status + tile, kFlagInc | (p + total));
         }
-        if (tid == 0) s_prefix = p;
+        if (tid == 0) {
+            s_prefix = p;
+            if ((uint64_t)(tile + 1) * TILE >= n) ctl->count[0] = p + total;
+        }
     }
     __syncthreads();
-    const unsigned long long base = s_prefix + excl;
-    if (row0 + cnt == n && tid == kBlock - 1) ctl->count[0] = s_prefix + total;
-
-    int prev = before;
-    unsigned int rank = 0;
+    const unsigned long long base = s_prefix + wexcl;
+    uint64_t prev[2 * W];
+    bool have_prev = false;
+    unsigned int run = 0;
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
-        if (!((flags >> i) & 1u)) continue;
-        int r = tid * ITEMS + i;
-        unsigned long long j = base + rank++;
-        if (PS_BOUNDS(ctl, j < n, 103)) {
-            idx[j] = (uint32_t)(row0 + r);
-            uint16_t d;
-            if (prev >= 0)
-                d = (uint16_t)divergence<W>(sk + (size_t)prev * 2 * W, sk + (size_t)r * 2 * W);
-            else
-                d = (j == 0) ? (uint16_t)kDivStart : (uint16_t)kDivUnknown;
-            D[j] = d;
+        const unsigned int b = ball[i];
+        if (b != 0) {  // warp-uniform
+            const unsigned int lower = b & lanemask_lt;
+            const int src = lower ? 31 - __clz(lower) : lane;
+            const int hi = 31 - __clz(b);
+            uint64_t pk[2 * W];
+#pragma unroll
+            for (int w = 0; w < 2 * W; ++w) pk[w] = __shfl_sync(0xffffffffu, k[i][w], src);
+            if ((b >> lane) & 1u) {
+                const unsigned long long j = base + run + __popc(lower);
+                if (PS_BOUNDS(ctl, j < n, 103)) {
+                    idx[j] = (uint32_t)(wbase + (uint64_t)i * 32 + lane);
+                    uint16_t d;
+                    if (lower)
+                        d = (uint16_t)div_regs<W>(pk, k[i]);
+                    else if (have_prev)
+                        d = (uint16_t)div_regs<W>(prev, k[i]);
+                    else
+                        d = j == 0 ? kDivStart : kDivUnknown;
+                    D[j] = d;
+                }
+            }
+#pragma unroll
+            for (int w = 0; w < 2 * W; ++w) prev[w] = __shfl_sync(0xffffffffu, k[i][w], hi);
+            have_prev = true;
+            run += __popc(b);
         }
-        prev = r;
     }
 }
 
@@ -545,42 +581,78 @@ struct MergeSmem {
     static constexpr int COEF_SLOTS = TILE + 4 + 4 * PAD;
     static constexpr size_t key_bytes = (size_t)KEY_ROWS * 16 * W;
     static constexpr size_t coef_bytes = ((size_t)COEF_SLOTS * sizeof(T) + 15) / 16 * 16;
-    static constexpr size_t in_bytes = key_bytes + coef_bytes;
-    static constexpr size_t bytes = 2 * in_bytes;  // inputs + output staging
+    static constexpr size_t bytes = key_bytes + coef_bytes;
 };
 
-template <int W, typename T>
-__device__ __forceinline__ void merge_range(const uint64_t* sSk, const T* sSc, const uint64_t* sPk, const T* sPc,
-                                            uint32_t i, uint32_t ie, uint32_t j, uint32_t je, const RotLayer<W>& L,
-                                            const KeepProg& keep, bool store, uint64_t* oK, T* oC,
-                                            uint32_t& count) {
-    count = 0;
+template <int W>
+__device__ __forceinline__ void ld_row(const uint64_t* base, uint32_t r, uint64_t (&k)[2 * W]) {
+    const ulonglong2* p = reinterpret_cast<const ulonglong2*>(base + (size_t)r * 2 * W);
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+        ulonglong2 v = p[q];
+        k[2 * q] = v.x;
+        k[2 * q + 1] = v.y;
+    }
+}
+
+template <int W>
+__device__ __forceinline__ bool le_regs(const uint64_t (&a)[2 * W], const uint64_t (&b)[2 * W]) {
+#pragma unroll
+    for (int i = 0; i < 2 * W; ++i)
+        if (a[i] != b[i]) return a[i] < b[i];
+    return true;
+}
+template <int W>
+__device__ __forceinline__ bool eq_regs(const uint64_t (&a)[2 * W], const uint64_t (&b)[2 * W]) {
+    uint64_t d = 0;
+#pragma unroll
+    for (int i = 0; i < 2 * W; ++i) d |= a[i] ^ b[i];
+    return d == 0;
+}
+
+// Walk one thread's merge-path range with the two run heads held in registers (one shared
+// load per consumed item).  Own row first, partner second when their keys are equal, as the
+// reference's merge sums bucket-first.  With kStore, kept outputs go straight to the output
+// store starting at row `out`.
+template <int W, typename T, bool kStore>
+__device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc, const uint64_t* sPk, const T* sPc,
+                                               uint32_t i, uint32_t ie, uint32_t j, uint32_t je,
+                                               const RotLayer<W>& L, const KeepProg& keep,
+                                               uint64_t* __restrict__ Ok, T* __restrict__ Oc,
+                                               unsigned long long out, unsigned int* s_hist) {
+    uint32_t count = 0;
+    uint64_t a[2 * W], b[2 * W];
+    if (i < ie) ld_row<W>(sSk, i, a);
+    if (j < je) ld_row<W>(sPk, j, b);
     while (i < ie || j < je) {
-        bool takeS = (j >= je) || (i < ie && key_le<W>(sSk + (size_t)i * 2 * W, sPk + (size_t)j * 2 * W));
-        const uint64_t* k;
+        const bool takeS = (j >= je) || (i < ie && le_regs<W>(a, b));
+        uint64_t k[2 * W];
         T v;
         if (takeS) {
-            k = sSk + (size_t)i * 2 * W;
-            v = own_coeff<W, T>(L, k, sSc[i]);
-            if (j < je && key_eq<W>(k, sPk + (size_t)j * 2 * W)) {
-                v = add_rn(v, sPc[j]);  // own first, as the reference's merge sums bucket-first
-                ++j;
+#pragma unroll
+            for (int w = 0; w < 2 * W; ++w) k[w] = a[w];
+            v = own_coeff<W, T>(L, a, sSc[i]);
+            if (j < je && eq_regs<W>(a, b)) {
+                v = add_rn(v, sPc[j]);
+                if (++j < je) ld_row<W>(sPk, j, b);
             }
-            ++i;
+            if (++i < ie) ld_row<W>(sSk, i, a);
         } else {
-            k = sPk + (size_t)j * 2 * W;
+#pragma unroll
+            for (int w = 0; w < 2 * W; ++w) k[w] = b[w];
             v = sPc[j];
-            ++j;
+            if (++j < je) ld_row<W>(sPk, j, b);
         }
         if (v != T(0) && keep_eval<W>(keep, k, to_f64(v))) {
-            if (store) {
-#pragma unroll
-                for (int w = 0; w < 2 * W; ++w) oK[(size_t)count * 2 * W + w] = k[w];
-                oC[count] = v;
+            if (kStore) {
+                store_key<W>(Ok, out + count, k);
+                Oc[out + count] = v;
+                if (s_hist) atomicAdd(&s_hist[mag_key<T>(v) >> 52], 1u);
             }
             ++count;
         }
     }
+    return count;
 }
 
 template <int W, typename T>
@@ -590,50 +662,52 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
                                                   const ulonglong2* __restrict__ bounds, uint32_t num_tiles,
                                                   const RotLayer<W> L, const KeepProg keep,
                                                   uint64_t* __restrict__ Ok, T* __restrict__ Oc, uint64_t out_cap,
-                                                  unsigned long long* status, Ctl* ctl) {
+                                                  unsigned long long* status, Ctl* ctl,
+                                                  unsigned int* __restrict__ topn_hist) {
     using SM = MergeSmem<W, T>;
     constexpr int ITEMS = RotTile<W>::kMergeItems;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     uint64_t* sK = reinterpret_cast<uint64_t*>(smem_raw);
     T* sC = reinterpret_cast<T*>(smem_raw + SM::key_bytes);
-    uint64_t* oK = reinterpret_cast<uint64_t*>(smem_raw + SM::in_bytes);
-    T* oC = reinterpret_cast<T*>(smem_raw + SM::in_bytes + SM::key_bytes);
     __shared__ uint64_t bar;
     __shared__ unsigned int s_tile;
     __shared__ unsigned int s_warp[kBlock / 32];
     __shared__ unsigned int s_si[kBlock + 1], s_sj[kBlock + 1];
     __shared__ unsigned long long s_outoff;
+    __shared__ unsigned int s_hist[kTopnHistBins];
 
     const int tid = threadIdx.x;
     if (tid == 0) {
         s_tile = atomicAdd(&ctl->tile_counter[3], 1u);
         mbar_init(&bar, 1);
     }
+    if (topn_hist)
+        for (int q = tid; q < kTopnHistBins; q += kBlock) s_hist[q] = 0;
     __syncthreads();
     const unsigned int tile = s_tile;
     if (tile >= num_tiles) return;
     const ulonglong2 b0 = bounds[tile], b1 = bounds[tile + 1];
-    const uint32_t cs = (uint32_t)(b1.x - b0.x), cp = (uint32_t)(b1.y - b0.y);
     if (!PS_GUARD(ctl, b1.x >= b0.x && b1.y >= b0.y && b1.x - b0.x + b1.y - b0.y <= (uint64_t)SM::TILE + 2 &&
                            b1.x <= n && b1.y <= m,
                   301)) {
         return;
     }
+    const uint32_t cs = (uint32_t)(b1.x - b0.x), cp = (uint32_t)(b1.y - b0.y);
     // stage the two input runs: keys packed (S then P), coefficients from 16-byte aligned windows
     const uint64_t sa = b0.x & ~(uint64_t)(SM::PAD - 1), pa = b0.y & ~(uint64_t)(SM::PAD - 1);
     const uint32_t s_off = (uint32_t)(b0.x - sa), p_off = (uint32_t)(b0.y - pa);
     const uint32_t sc_slots = (s_off + cs + SM::PAD - 1) / SM::PAD * SM::PAD;
-    T* sSc = sC;            // S coefficient of local i at sSc[s_off + i]
-    T* sPc = sC + sc_slots; // P coefficient of local j at sPc[p_off + j]
+    T* sSc = sC;             // S coefficient of local i at sSc[s_off + i]
+    T* sPc = sC + sc_slots;  // P coefficient of local j at sPc[p_off + j]
     uint64_t* sSk = sK;
     uint64_t* sPk = sK + (size_t)cs * 2 * W;
     if (tid == 0) {
         uint32_t kbS = cs * 16u * W, kbP = cp * 16u * W;
         uint32_t cbS = cs ? round16((s_off + cs) * (uint32_t)sizeof(T)) : 0u;
         uint32_t cbP = cp ? round16((p_off + cp) * (uint32_t)sizeof(T)) : 0u;
-        uint32_t total = kbS + kbP + cbS + cbP;
-        if (total) {
-            mbar_arrive_expect_tx(&bar, total);
+        uint32_t tot = kbS + kbP + cbS + cbP;
+        if (tot) {
+            mbar_arrive_expect_tx(&bar, tot);
             if (kbS) bulk_g2s(sSk, Sk + b0.x * 2 * W, kbS, &bar);
             if (kbP) bulk_g2s(sPk, Pk + b0.y * 2 * W, kbP, &bar);
             if (cbS) bulk_g2s(sSc, Sc + sa, cbS, &bar);
@@ -667,8 +741,8 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
     __syncthreads();
     const uint32_t i0 = s_si[tid], j0 = s_sj[tid];
     const uint32_t ie = max(s_si[tid + 1], i0), je = max(s_sj[tid + 1], j0);
-    uint32_t count;
-    merge_range<W, T>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, keep, false, nullptr, nullptr, count);
+    const uint32_t count =
+        merge_walk<W, T, false>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, keep, nullptr, nullptr, 0ull, nullptr);
     unsigned int total;
     unsigned int excl = block_exclusive_sum<kBlock>(count, s_warp, total);
     if (tid < 32) {
@@ -685,16 +759,16 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
             if (tile == num_tiles - 1) ctl->count[1] = p + total;
         }
     }
-    uint32_t c2;
-    merge_range<W, T>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, keep, true, oK + (size_t)excl * 2 * W, oC + excl, c2);
     __syncthreads();
     const unsigned long long off = s_outoff;
     if (!PS_GUARD(ctl, off + total <= out_cap, 304)) return;
-    // coalesced write-out of the staged outputs
-    const ulonglong2* src = reinterpret_cast<const ulonglong2*>(oK);
-    ulonglong2* dst = reinterpret_cast<ulonglong2*>(Ok + off * 2 * W);
-    for (uint32_t q = tid; q < total * W; q += kBlock) dst[q] = src[q];
-    for (uint32_t q = tid; q < total; q += kBlock) Oc[off + q] = oC[q];
+    merge_walk<W, T, true>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, keep, Ok, Oc, off + excl,
+                           topn_hist ? s_hist : nullptr);
+    if (topn_hist) {
+        __syncthreads();
+        for (int q = tid; q < kTopnHistBins; q += kBlock)
+            if (s_hist[q]) atomicAdd(&topn_hist[q], s_hist[q]);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -712,9 +786,8 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
         uint32_t tiles = (uint32_t)((a.n + CT - 1) / CT);
         cudaMemsetAsync(a.status, 0, (size_t)tiles * sizeof(unsigned long long), st);
         cudaMemsetAsync(&ctl->tile_counter[0], 0, 4 * sizeof(unsigned int), st);
-        size_t smem = (size_t)CT * 16 * W;
         a.prof->begin(K_CLASSIFY, (double)a.n * 16 * W, st);
-        k_classify<W, T><<<tiles, kBlock, smem, st>>>(a.Sk, a.n, a.L, a.idx, a.D, a.status, ctl);
+        k_classify<W, T><<<tiles, kBlock, 0, st>>>(a.Sk, a.n, a.L, a.idx, a.D, a.status, ctl);
         a.prof->end(st);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         cudaMemcpyAsync(a.host_count, &ctl->count[0], sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
@@ -773,7 +846,7 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     size_t smem = MergeSmem<W, T>::bytes;
     a.prof->begin(K_MERGE, (double)(a.n + m) * (16 * W + sizeof(T)), st);
     k_merge<W, T><<<mtiles, kBlock, smem, st>>>(a.Sk, a.Sc, a.n, a.Pk, a.Pc, m, a.bounds, mtiles, a.L, a.keep,
-                                               a.Ok, a.Oc, a.out_cap, a.status, ctl);
+                                               a.Ok, a.Oc, a.out_cap, a.status, ctl, a.topn_hist);
     a.prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     cudaMemcpyAsync(a.host_count, &ctl->count[1], sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
@@ -785,10 +858,6 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
 
 template <int W, typename T>
 cudaError_t configure_rotation_kernels() {
-    constexpr int CT = RotTile<W>::kClassifyTile;
-    cudaError_t e = cudaFuncSetAttribute(k_classify<W, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)((size_t)CT * 16 * W));
-    if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_merge<W, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)MergeSmem<W, T>::bytes);
 }

@@ -20,6 +20,8 @@
 #include "ps_device.cuh"
 #include "ps_store.h"
 
+#include <type_traits>
+
 namespace psb {
 
 constexpr int kThreads = 256;
@@ -274,85 +276,166 @@ __global__ void __launch_bounds__(kThreads) k_dedup(const uint64_t* __restrict__
 }
 
 // ---------------------------------------------------------------------------
-// TopN radix-select on |c|^2 bits
+// TopN radix-select on the bit pattern of |c|^2.  The select key is mag_key(c): 0 for NaN,
+// else bits(|c|^2) + 1, so it is monotone in |c|^2 and NaN sorts lowest.  Digit 1 is
+// key >> 52 (2048 bins, the octave of |c|^2); it is histogrammed by the merge kernel of
+// the layer (or k_topn_hist1 when no merge ran), the boundary bin's keys are gathered into a
+// candidate buffer, and the remaining 52 bits are selected over the candidates in four
+// 13-bit digits.  aux[0] prefix, aux[1] mask, aux[2] remaining rank, aux[3] count above,
+// count[4] candidates.
 // ---------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ uint64_t mag_key(T c) {
-    double v = to_f64(c);
-    double m = __dmul_rn(v, v);
-    if (isnan(m)) return 0ull;  // NaN sorts below every number and is never kept
-    return (uint64_t)__double_as_longlong(m) + 1ull;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_topn_hist(const T* __restrict__ coef, uint64_t n, int byte,
-                                                        Ctl* ctl, unsigned int* __restrict__ hist) {
-    __shared__ unsigned int sh[256];
-    sh[threadIdx.x] = 0;
+__global__ void __launch_bounds__(kThreads) k_topn_hist1(const double* __restrict__ c64, const float* __restrict__ c32,
+                                                         uint64_t n, unsigned int* __restrict__ hist) {
+    __shared__ unsigned int sh[kTopnBins1];
+    for (int i = threadIdx.x; i < kTopnBins1; i += kThreads) sh[i] = 0;
     __syncthreads();
-    const uint64_t prefix = ctl->aux[0], mask = ctl->aux[1];
     for (uint64_t i = blockIdx.x * (uint64_t)kThreads + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kThreads) {
-        uint64_t mk = mag_key<T>(coef[i]);
-        if ((mk & mask) == prefix) atomicAdd(&sh[(mk >> (8 * byte)) & 0xFFu], 1u);
+        uint64_t mk = c64 ? mag_key<double>(c64[i]) : mag_key<float>(c32[i]);
+        atomicAdd(&sh[mk >> 52], 1u);
     }
     __syncthreads();
-    if (sh[threadIdx.x]) atomicAdd(&hist[threadIdx.x], sh[threadIdx.x]);
+    for (int i = threadIdx.x; i < kTopnBins1; i += kThreads)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
 }
 
-// aux[0] prefix, aux[1] mask, aux[2] remaining rank (1-based, among prefix matches),
-// aux[3] count strictly above the prefix so far.
-__global__ void k_topn_step(unsigned int* __restrict__ hist, int byte, Ctl* ctl) {
-    __shared__ unsigned int sh[256];
-    const int b = threadIdx.x;
-    sh[b] = hist[b];
-    hist[b] = 0;
+// One block: pick the bin holding the remaining rank, counting from the top; clears the histogram.
+template <int BINS>
+__global__ void __launch_bounds__(1024) k_topn_select(unsigned int* __restrict__ hist, int shift, int bits, Ctl* ctl) {
+    constexpr int PER = BINS / 1024;
+    __shared__ unsigned long long s_part[1024];
+    __shared__ int s_choice;
+    __shared__ unsigned long long s_above;
+    const int t = threadIdx.x;
+    if (t == 0) {
+        s_choice = 0;
+        s_above = 0;
+    }
+    // thread t owns bins [BINS - (t + 1) * PER, BINS - t * PER), highest first
+    unsigned long long mine = 0;
+    for (int q = 0; q < PER; ++q) mine += hist[BINS - 1 - (t * PER + q)];
+    s_part[t] = mine;
     __syncthreads();
-    if (b == 0) {
-        unsigned long long r = ctl->aux[2];
-        unsigned long long above = 0;
-        int chosen = 0;
-        for (int q = 255; q >= 0; --q) {
-            unsigned long long c = sh[q];
-            if (above + c >= r) {
-                chosen = q;
+    for (int o = 1; o < 1024; o <<= 1) {  // inclusive scan over threads (top bins first)
+        unsigned long long v = t >= o ? s_part[t - o] : 0ull;
+        __syncthreads();
+        s_part[t] += v;
+        __syncthreads();
+    }
+    const unsigned long long r = ctl->aux[2];
+    const unsigned long long before = t ? s_part[t - 1] : 0ull;
+    if (before < r && s_part[t] >= r) {
+        unsigned long long acc = before;
+        for (int q = 0; q < PER; ++q) {
+            const int bin = BINS - 1 - (t * PER + q);
+            const unsigned long long c = hist[bin];
+            if (acc + c >= r) {
+                s_choice = bin;
+                s_above = acc;
                 break;
             }
-            above += c;
+            acc += c;
         }
-        ctl->aux[0] |= (unsigned long long)chosen << (8 * byte);
-        ctl->aux[1] |= 0xFFull << (8 * byte);
+    }
+    __syncthreads();
+    for (int q = 0; q < PER; ++q) hist[t * PER + q] = 0;
+    if (t == 0) {
+        const unsigned long long above = s_above;
+        ctl->aux[0] |= (unsigned long long)s_choice << shift;
+        ctl->aux[1] |= ((1ull << bits) - 1ull) << shift;
         ctl->aux[2] = r - above;
         ctl->aux[3] += above;
     }
 }
 
+// Gather the keys of the boundary bin (order does not matter for the select).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_topn_cand(const T* __restrict__ coef, uint64_t n, Ctl* ctl,
+                                                        uint64_t* __restrict__ cand, uint64_t cand_cap) {
+    const uint64_t prefix = ctl->aux[0], mask = ctl->aux[1];
+    const int lane = threadIdx.x & 31;
+    for (uint64_t base = blockIdx.x * (uint64_t)kThreads; base < n; base += (uint64_t)gridDim.x * kThreads) {
+        const uint64_t i = base + threadIdx.x;
+        uint64_t mk = 0;
+        bool hit = false;
+        if (i < n) {
+            mk = mag_key<T>(coef[i]);
+            hit = (mk & mask) == prefix;
+        }
+        const unsigned int b = __ballot_sync(0xffffffffu, hit);
+        if (!b) continue;
+        unsigned long long slot = 0;
+        if (lane == __ffs(b) - 1) slot = atomicAdd(&ctl->count[4], (unsigned long long)__popc(b));
+        slot = __shfl_sync(0xffffffffu, slot, __ffs(b) - 1) + __popc(b & ((1u << lane) - 1u));
+        if (hit && PS_GUARD(ctl, slot < cand_cap, 703)) cand[slot] = mk;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_topn_hist_cand(const uint64_t* __restrict__ cand, Ctl* ctl, int shift,
+                                                             unsigned int* __restrict__ hist) {
+    __shared__ unsigned int sh[kTopnBinsN];
+    for (int i = threadIdx.x; i < kTopnBinsN; i += kThreads) sh[i] = 0;
+    __syncthreads();
+    const uint64_t prefix = ctl->aux[0], mask = ctl->aux[1], m = ctl->count[4];
+    for (uint64_t i = blockIdx.x * (uint64_t)kThreads + threadIdx.x; i < m; i += (uint64_t)gridDim.x * kThreads) {
+        uint64_t mk = cand[i];
+        if ((mk & mask) == prefix) atomicAdd(&sh[(mk >> shift) & (kTopnBinsN - 1)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kTopnBinsN; i += kThreads)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
+// Order-preserving compaction, warp-striped: keeps keys above the boundary and the first
+// `quota` boundary ties in key order.
 template <int W, typename T>
 __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __restrict__ keys, const T* __restrict__ coef,
                                                            uint64_t n, unsigned long long quota,
                                                            uint64_t* __restrict__ okeys, T* __restrict__ ocoef,
                                                            unsigned long long* status, Ctl* ctl) {
-    constexpr int ITEMS = 8;
+    constexpr int ITEMS = 16;
+    constexpr int TILE = kThreads * ITEMS;
     __shared__ unsigned int s_tile;
-    __shared__ unsigned int s_warp[kThreads / 32];
+    __shared__ unsigned int s_wa[kThreads / 32], s_wt[kThreads / 32];
     __shared__ unsigned long long s_above, s_ties;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned int lt = (1u << lane) - 1u;
     if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[6], 1u);
     __syncthreads();
     const unsigned int tile = s_tile;
     const uint64_t boundary = ctl->aux[0];
-    const uint64_t e0 = (uint64_t)tile * (kThreads * ITEMS) + (uint64_t)tid * ITEMS;
-    uint32_t amask = 0, tmask = 0;
+    const uint64_t wbase = (uint64_t)tile * TILE + (uint64_t)warp * 32 * ITEMS;
+    unsigned int ba[ITEMS], bt[ITEMS];
+    T cv[ITEMS];
+    unsigned int wa = 0, wt = 0;
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
-        uint64_t e = e0 + i;
-        if (e >= n) continue;
-        uint64_t mk = mag_key<T>(coef[e]);
-        if (mk > boundary) amask |= 1u << i;
-        else if (mk == boundary && boundary != 0) tmask |= 1u << i;
+        const uint64_t e = wbase + (uint64_t)i * 32 + lane;
+        bool isa = false, ist = false;
+        cv[i] = T(0);
+        if (e < n) {
+            cv[i] = coef[e];
+            const uint64_t mk = mag_key<T>(cv[i]);
+            isa = mk > boundary;
+            ist = mk == boundary && boundary != 0;
+        }
+        ba[i] = __ballot_sync(0xffffffffu, isa);
+        bt[i] = __ballot_sync(0xffffffffu, ist);
+        wa += __popc(ba[i]);
+        wt += __popc(bt[i]);
     }
-    unsigned int ta, tt;
-    unsigned int ea = block_exclusive_sum<kThreads>(__popc(amask), s_warp, ta);
-    unsigned int et = block_exclusive_sum<kThreads>(__popc(tmask), s_warp, tt);
+    if (lane == 0) {
+        s_wa[warp] = wa;
+        s_wt[warp] = wt;
+    }
+    __syncthreads();
+    unsigned int xa = 0, xt = 0, ta = 0, tt = 0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) {
+        xa += w < warp ? s_wa[w] : 0u;
+        xt += w < warp ? s_wt[w] : 0u;
+        ta += s_wa[w];
+        tt += s_wt[w];
+    }
     if (tid < 32) {
         unsigned long long agg = (unsigned long long)ta | ((unsigned long long)tt << 31);
         unsigned long long pre = 0;
@@ -366,31 +449,30 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
         if (tid == 0) {
             s_above = pre & ((1ull << 31) - 1);
             s_ties = pre >> 31;
-            if ((uint64_t)(tile + 1) * (kThreads * ITEMS) >= n) {
+            if ((uint64_t)(tile + 1) * TILE >= n) {
                 unsigned long long tot_ties = s_ties + tt;
                 ctl->count[3] = s_above + ta + (tot_ties < quota ? tot_ties : quota);
             }
         }
     }
     __syncthreads();
-    unsigned long long arank = s_above + ea, trank = s_ties + et;
+    unsigned long long arank = s_above + xa, trank = s_ties + xt;
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
-        bool isa = (amask >> i) & 1u, ist = (tmask >> i) & 1u;
-        if (!isa && !ist) continue;
-        bool keepit = isa || trank < quota;
-        unsigned long long tie_before = trank < quota ? trank : quota;
-        unsigned long long pos = arank + tie_before;
-        if (keepit) {
+        const bool isa = (ba[i] >> lane) & 1u, ist = (bt[i] >> lane) & 1u;
+        const unsigned long long ar = arank + __popc(ba[i] & lt), tr = trank + __popc(bt[i] & lt);
+        if (isa || (ist && tr < quota)) {
+            const unsigned long long pos = ar + (tr < quota ? tr : quota);
+            const uint64_t e = wbase + (uint64_t)i * 32 + lane;
             uint64_t k[2 * W];
-            load_key<W>(keys, e0 + i, k);
+            load_key<W>(keys, e, k);
             if (PS_GUARD(ctl, pos < n, 702)) {
                 store_key<W>(okeys, pos, k);
-                ocoef[pos] = coef[e0 + i];
+                ocoef[pos] = cv[i];
             }
         }
-        if (isa) ++arank;
-        if (ist) ++trank;
+        arank += __popc(ba[i]);
+        trank += __popc(bt[i]);
     }
 }
 
@@ -551,29 +633,48 @@ cudaError_t StoreOps<W, T>::dedup(const uint64_t* keys, const uint32_t* vals, co
 
 template <int W, typename T>
 cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n, uint64_t keep_n, uint64_t* okeys,
-                                 T* ocoef, unsigned int* hist, unsigned long long* status, Ctl* ctl,
-                                 unsigned long long* host_count, uint64_t* out_n, int sms, cudaStream_t st,
-                                 KernelProf* prof) {
-    // aux: prefix, mask, remaining rank, above
-    unsigned long long init[4] = {0ull, 0ull, (unsigned long long)keep_n, 0ull};
-    cudaMemcpyAsync(ctl->aux, init, sizeof(init), cudaMemcpyHostToDevice, st);
-    cudaMemsetAsync(hist, 0, 256 * sizeof(unsigned int), st);
+                                 T* ocoef, unsigned int* hist, bool hist_ready, uint64_t* cand, uint64_t cand_cap,
+                                 unsigned long long* status, Ctl* ctl, unsigned long long* host_count,
+                                 uint64_t* out_n, int sms, cudaStream_t st, KernelProf* prof) {
+    // aux: prefix, mask, remaining rank, above; count[4]: candidates
+    unsigned long long* init = host_count + 8;
+    init[0] = 0ull;
+    init[1] = 0ull;
+    init[2] = (unsigned long long)keep_n;
+    init[3] = 0ull;
+    cudaMemcpyAsync(ctl->aux, init, 4 * sizeof(unsigned long long), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(&ctl->count[4], 0, sizeof(unsigned long long), st);
     cudaError_t e;
-    for (int byte = 7; byte >= 0; --byte) {
+    if (!hist_ready) {
+        cudaMemsetAsync(hist, 0, kTopnBins1 * sizeof(unsigned int), st);
         prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
-        k_topn_hist<T><<<grid_for(n, sms), kThreads, 0, st>>>(coef, n, byte, ctl, hist);
+        k_topn_hist1<<<grid_for(n, sms), kThreads, 0, st>>>(std::is_same<T, double>::value ? (const double*)coef : nullptr,
+                                                            std::is_same<T, float>::value ? (const float*)coef : nullptr,
+                                                            n, hist);
         prof->end(st);
-        prof->begin(K_TOPN_STEP, 2048.0, st);
-        k_topn_step<<<1, 256, 0, st>>>(hist, byte, ctl);
+    }
+    prof->begin(K_TOPN_STEP, kTopnBins1 * 8.0, st);
+    k_topn_select<kTopnBins1><<<1, 1024, 0, st>>>(hist, 52, 12, ctl);
+    prof->end(st);
+    prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
+    k_topn_cand<T><<<grid_for(n, sms), kThreads, 0, st>>>(coef, n, ctl, cand, cand_cap);
+    prof->end(st);
+    // 52 remaining bits: digits at 39, 26, 13, 0 (13 bits each)
+    for (int shift = 39; shift >= 0; shift -= 13) {
+        prof->begin(K_TOPN_HIST, 0.0, st);
+        k_topn_hist_cand<<<2 * sms, kThreads, 0, st>>>(cand, ctl, shift, hist);
+        prof->end(st);
+        prof->begin(K_TOPN_STEP, kTopnBinsN * 8.0, st);
+        k_topn_select<kTopnBinsN><<<1, 1024, 0, st>>>(hist, shift, 13, ctl);
         prof->end(st);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    unsigned long long aux[4];
-    cudaMemcpyAsync(aux, ctl->aux, sizeof(aux), cudaMemcpyDeviceToHost, st);
+    unsigned long long* aux = host_count + 16;
+    cudaMemcpyAsync(aux, ctl->aux, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
     unsigned long long quota = keep_n - aux[3];
     if (aux[0] == 0) quota = 0;  // NaN boundary: only the non-NaN terms stay
-    const uint32_t tiles = (uint32_t)((n + kThreads * 8 - 1) / (kThreads * 8));
+    const uint32_t tiles = (uint32_t)((n + kThreads * 16 - 1) / (kThreads * 16));
     cudaMemsetAsync(status, 0, (size_t)tiles * sizeof(unsigned long long), st);
     cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
@@ -583,7 +684,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     cudaMemcpyAsync(host_count, &ctl->count[3], sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
     *out_n = *host_count;
-    prof->add_bytes(K_TOPN_COMPACT, (double)*out_n * 2 * (16 * W + sizeof(T)));
+    prof->add_bytes(K_TOPN_COMPACT, (double)*out_n * (2 * 16 * W + sizeof(T)));
     return cudaSuccess;
 }
 

@@ -9,6 +9,8 @@
 namespace psb {
 
 constexpr int kExpectBlocks = 592;  // 4 x 148 SMs; fixed so the reduction order is fixed
+constexpr int kTopnBins1 = 2048;    // first select digit: |c|^2 key >> 52
+constexpr int kTopnBinsN = 8192;    // later digits: 13 bits over the boundary-bin candidates
 
 struct SortScratch {
     unsigned int* hist;        // device, 16W x 256
@@ -34,9 +36,13 @@ struct StoreOps {
     static cudaError_t dedup(const uint64_t* keys, const uint32_t* vals, const T* cin, uint64_t n, const KeepProg& keep,
                              bool compensated, uint64_t* okeys, T* ocoef, unsigned long long* status, Ctl* ctl,
                              unsigned long long* host_count, uint64_t* out_n, cudaStream_t st, KernelProf* prof);
+    // hist: kTopnBinsN words, zero on entry and on exit; when hist_ready its first kTopnBins1
+    // words already hold the digit-1 histogram of coef (built by the layer's merge).
+    // host_count: pinned scratch of at least 20 words.
     static cudaError_t topn(const uint64_t* keys, const T* coef, uint64_t n, uint64_t keep_n, uint64_t* okeys, T* ocoef,
-                            unsigned int* hist, unsigned long long* status, Ctl* ctl, unsigned long long* host_count,
-                            uint64_t* out_n, int sms, cudaStream_t st, KernelProf* prof);
+                            unsigned int* hist, bool hist_ready, uint64_t* cand, uint64_t cand_cap,
+                            unsigned long long* status, Ctl* ctl, unsigned long long* host_count, uint64_t* out_n,
+                            int sms, cudaStream_t st, KernelProf* prof);
     static cudaError_t expectation(const uint64_t* keys, const T* coef, uint64_t n, const uint64_t* ax,
                                    const uint64_t* az, const uint64_t* neg, double* partial, double* out_dev, int sms,
                                    cudaStream_t st, KernelProf* prof);

@@ -297,3 +297,27 @@ def test_large_rotation_layers_preserve_norm_and_order():
     assert diff.all()
     # orthogonal layers preserve the 2-norm (no truncation)
     assert np.sum(gc * gc) == pytest.approx(1.0, rel=1e-12)
+
+
+def test_topn_nan_and_boundary_ties_match_the_oracle():
+    labels = ["XI", "YI", "ZI", "IX", "IY", "IZ"]
+    x, z, c = labels_to_arrays(dict(zip(labels, [0.5, -0.5, 0.1, 0.5, 0.9, float("nan")])), 2)
+    circ = ps.Circuit(2)
+    circ.rz(0.0, 0)
+    for n_keep in (0, 1, 2, 3, 4, 5, 6, 7):
+        got, want, la, lb, _, _ = run_both(2, x, z, c, circ, truncation.topn(n_keep))
+        assert la == lb, n_keep
+        assert_same_terms(got, want, what=f"topn{n_keep}")
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_topn_many_ties_bit_exact(dtype):
+    # coefficients from a small set of values, so whole blocks tie at the boundary
+    rng = np.random.default_rng(7)
+    x, z, _ = workloads.random_observable(20, 5000, seed=11)
+    c = rng.choice([0.25, -0.25, 0.5, 0.125, -0.0625], size=len(x))
+    circ = workloads.random_pair_layers(20, 1)
+    pol = truncation.topn(2500) & truncation.coeff(1e-12)
+    got, want, la, lb, _, _ = run_both(20, x, z, c, circ, pol, "heisenberg", dtype)
+    assert la == lb
+    assert_same_terms(got, want, what=f"ties-{dtype}")
