@@ -48,6 +48,7 @@ struct ps_sum {
     bool hist_ready = false;  // hist holds the TopN digit-1 histogram of the current store
     SortScratch sort{};
     Buf sort_status;
+    Buf up_x, up_z, up_c, up_k, up_v0, up_v1, up_c0, up_st;  // ingest / readout staging, grow-only
     LevelList* levels = nullptr;  // host scratch
     KernelProf prof;
     std::string err;
@@ -521,65 +522,51 @@ struct Engine {
             s->n = 0;
             return PS_OK;
         }
-        Buf dx, dz, dc, k0, k1, v0, v1, c0, st;
-        auto cleanup = [&]() {
-            release(dx);
-            release(dz);
-            release(dc);
-            release(k0);
-            release(k1);
-            release(v0);
-            release(v1);
-            release(c0);
-            release(st);
-        };
         cudaError_t e = cudaSuccess;
-        const size_t tiles = (n + StoreOps<W, T>::sort_tile() - 1) / StoreOps<W, T>::sort_tile();
-        if ((e = ensure(dx, n * W * 8)) != cudaSuccess || (e = ensure(dz, n * W * 8)) != cudaSuccess ||
-            (e = ensure(dc, n * 8)) != cudaSuccess || (e = ensure(k0, n * kKeyBytes)) != cudaSuccess ||
-            (e = ensure(k1, n * kKeyBytes)) != cudaSuccess || (e = ensure(v0, n * 4)) != cudaSuccess ||
-            (e = ensure(v1, n * 4)) != cudaSuccess || (e = ensure(c0, n * sizeof(T))) != cudaSuccess ||
-            (e = ensure(st, (n / 2048 + 2) * sizeof(unsigned long long))) != cudaSuccess ||
-            (e = ensure(s->sort_status, tiles * 256 * sizeof(unsigned int))) != cudaSuccess ||
-            (e = reserve_store(s, spare, n)) != cudaSuccess) {
-            cleanup();
+        if ((e = ensure(s->up_x, n * W * 8)) != cudaSuccess || (e = ensure(s->up_z, n * W * 8)) != cudaSuccess ||
+            (e = ensure(s->up_c, n * 8)) != cudaSuccess || (e = ensure(s->up_v0, n * 4)) != cudaSuccess ||
+            (e = reserve_store(s, spare, n)) != cudaSuccess)
             return cuda_fail(s, e, "upload: allocation");
-        }
-        s->sort.status = static_cast<unsigned int*>(s->sort_status.p);
-        cudaMemcpyAsync(dx.p, x, n * W * 8, cudaMemcpyHostToDevice, s->stream);
-        cudaMemcpyAsync(dz.p, z, n * W * 8, cudaMemcpyHostToDevice, s->stream);
-        cudaMemcpyAsync(dc.p, c, n * 8, cudaMemcpyHostToDevice, s->stream);
-        e = StoreOps<W, T>::pack((uint64_t*)dx.p, (uint64_t*)dz.p, (double*)dc.p, n, (uint32_t)s->nq,
-                                 (uint64_t*)k0.p, (T*)c0.p, (uint32_t*)v0.p, s->ctl, s->sms, s->stream, &s->prof);
-        if (e != cudaSuccess) {
-            cleanup();
-            return cuda_fail(s, e, "upload: pack");
-        }
+        cudaMemcpyAsync(s->up_x.p, x, n * W * 8, cudaMemcpyHostToDevice, s->stream);
+        cudaMemcpyAsync(s->up_z.p, z, n * W * 8, cudaMemcpyHostToDevice, s->stream);
+        cudaMemcpyAsync(s->up_c.p, c, n * 8, cudaMemcpyHostToDevice, s->stream);
+        // pack straight into the spare store; an input already in store form (sorted, unique,
+        // no zeros, as every download is) needs nothing more
+        e = StoreOps<W, T>::pack((uint64_t*)s->up_x.p, (uint64_t*)s->up_z.p, (double*)s->up_c.p, n, (uint32_t)s->nq,
+                                 K(s, spare), C(s, spare), (uint32_t*)s->up_v0.p, s->ctl, s->sms, s->stream, &s->prof);
+        if (e != cudaSuccess) return cuda_fail(s, e, "upload: pack");
         ps_status fs = check_device_flags(s, "upload");
-        if (fs != PS_OK) {
-            cleanup();
-            return fs;
-        }
-        bool alt = false;
-        e = StoreOps<W, T>::sort_pairs((uint64_t*)k0.p, (uint32_t*)v0.p, (uint64_t*)k1.p, (uint32_t*)v1.p, n, s->sort,
-                                       s->ctl, s->sms, s->stream, alt, &s->prof);
-        if (e != cudaSuccess) {
-            cleanup();
-            return cuda_fail(s, e, "upload: sort");
-        }
-        KeepProg none;
-        std::memset(&none, 0, sizeof none);
-        uint64_t out_n = 0;
-        e = StoreOps<W, T>::dedup(alt ? (uint64_t*)k1.p : (uint64_t*)k0.p, alt ? (uint32_t*)v1.p : (uint32_t*)v0.p,
-                                  (T*)c0.p, n, none, false, K(s, spare), C(s, spare),
-                                  (unsigned long long*)st.p, s->ctl, s->hcount, &out_n, s->stream, &s->prof);
-        if (e != cudaSuccess) {
-            cleanup();
-            return cuda_fail(s, e, "upload: dedup");
-        }
-        fs = check_device_flags(s, "upload");
-        cleanup();
         if (fs != PS_OK) return fs;
+        bool sorted = false;
+        e = StoreOps<W, T>::check_sorted(K(s, spare), C(s, spare), n, s->ctl, s->hcount, &sorted, s->sms, s->stream,
+                                         &s->prof);
+        if (e != cudaSuccess) return cuda_fail(s, e, "upload: check");
+        uint64_t out_n = n;
+        if (!sorted) {
+            const size_t tiles = (n + StoreOps<W, T>::sort_tile() - 1) / StoreOps<W, T>::sort_tile();
+            if ((e = ensure(s->up_k, 2 * n * kKeyBytes)) != cudaSuccess || (e = ensure(s->up_v1, n * 4)) != cudaSuccess ||
+                (e = ensure(s->up_c0, n * sizeof(T))) != cudaSuccess ||
+                (e = ensure(s->up_st, (n / 2048 + 2) * sizeof(unsigned long long))) != cudaSuccess ||
+                (e = ensure(s->sort_status, tiles * 256 * sizeof(unsigned int))) != cudaSuccess)
+                return cuda_fail(s, e, "upload: sort scratch");
+            s->sort.status = static_cast<unsigned int*>(s->sort_status.p);
+            uint64_t* k0 = (uint64_t*)s->up_k.p;
+            uint64_t* k1 = k0 + n * 2 * W;
+            cudaMemcpyAsync(k0, K(s, spare), n * kKeyBytes, cudaMemcpyDeviceToDevice, s->stream);
+            cudaMemcpyAsync(s->up_c0.p, C(s, spare), n * sizeof(T), cudaMemcpyDeviceToDevice, s->stream);
+            bool alt = false;
+            e = StoreOps<W, T>::sort_pairs(k0, (uint32_t*)s->up_v0.p, k1, (uint32_t*)s->up_v1.p, n, s->sort, s->ctl,
+                                           s->sms, s->stream, alt, &s->prof);
+            if (e != cudaSuccess) return cuda_fail(s, e, "upload: sort");
+            KeepProg none;
+            std::memset(&none, 0, sizeof none);
+            e = StoreOps<W, T>::dedup(alt ? k1 : k0, alt ? (uint32_t*)s->up_v1.p : (uint32_t*)s->up_v0.p,
+                                      (T*)s->up_c0.p, n, none, false, K(s, spare), C(s, spare),
+                                      (unsigned long long*)s->up_st.p, s->ctl, s->hcount, &out_n, s->stream, &s->prof);
+            if (e != cudaSuccess) return cuda_fail(s, e, "upload: dedup");
+            fs = check_device_flags(s, "upload");
+            if (fs != PS_OK) return fs;
+        }
         s->cur = spare;
         s->n = out_n;
         if (s->hist_ready) {
@@ -593,24 +580,16 @@ struct Engine {
         if (nout) *nout = s->n;
         if (cap < s->n) return set_err(s, PS_ERR_INVALID, "download: capacity below the term count");
         if (s->n == 0) return PS_OK;
-        Buf dx, dz, dc;
         cudaError_t e;
-        if ((e = ensure(dx, s->n * W * 8)) != cudaSuccess || (e = ensure(dz, s->n * W * 8)) != cudaSuccess ||
-            (e = ensure(dc, s->n * 8)) != cudaSuccess) {
-            release(dx);
-            release(dz);
-            release(dc);
+        if ((e = ensure(s->up_x, s->n * W * 8)) != cudaSuccess || (e = ensure(s->up_z, s->n * W * 8)) != cudaSuccess ||
+            (e = ensure(s->up_c, s->n * 8)) != cudaSuccess)
             return cuda_fail(s, e, "download: allocation");
-        }
-        e = StoreOps<W, T>::unpack(K(s, s->cur), C(s, s->cur), s->n, (uint64_t*)dx.p, (uint64_t*)dz.p, (double*)dc.p,
-                                   s->sms, s->stream, &s->prof);
-        if (e == cudaSuccess && x) e = cudaMemcpyAsync(x, dx.p, s->n * W * 8, cudaMemcpyDeviceToHost, s->stream);
-        if (e == cudaSuccess && z) e = cudaMemcpyAsync(z, dz.p, s->n * W * 8, cudaMemcpyDeviceToHost, s->stream);
-        if (e == cudaSuccess && c) e = cudaMemcpyAsync(c, dc.p, s->n * 8, cudaMemcpyDeviceToHost, s->stream);
+        e = StoreOps<W, T>::unpack(K(s, s->cur), C(s, s->cur), s->n, (uint64_t*)s->up_x.p, (uint64_t*)s->up_z.p,
+                                   (double*)s->up_c.p, s->sms, s->stream, &s->prof);
+        if (e == cudaSuccess && x) e = cudaMemcpyAsync(x, s->up_x.p, s->n * W * 8, cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess && z) e = cudaMemcpyAsync(z, s->up_z.p, s->n * W * 8, cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess && c) e = cudaMemcpyAsync(c, s->up_c.p, s->n * 8, cudaMemcpyDeviceToHost, s->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-        release(dx);
-        release(dz);
-        release(dc);
         if (e != cudaSuccess) return cuda_fail(s, e, "download");
         return PS_OK;
     }
@@ -855,7 +834,8 @@ ps_status ps_destroy(ps_sum* s) {
     DeviceGuard g(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (Buf* b : {&s->keys[0], &s->keys[1], &s->coef[0], &s->coef[1], &s->pk, &s->pc, &s->idx, &s->dv, &s->fv,
-                   &s->slots, &s->status, &s->bounds, &s->hist, &s->cand, &s->partial, &s->dout, &s->sort_status})
+                   &s->slots, &s->status, &s->bounds, &s->hist, &s->cand, &s->partial, &s->dout, &s->sort_status,
+                   &s->up_x, &s->up_z, &s->up_c, &s->up_k, &s->up_v0, &s->up_v1, &s->up_c0, &s->up_st})
         release(*b);
     if (s->ctl) cudaFree(s->ctl);
     if (s->sort.hist) cudaFree(s->sort.hist);

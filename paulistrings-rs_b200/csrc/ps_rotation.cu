@@ -34,7 +34,7 @@ struct RotTile {
     static constexpr int kClassifyItems = W == 1 ? 16 : (W == 2 ? 8 : (W == 4 ? 4 : 2));
     static constexpr int kClassifyTile = kBlock * kClassifyItems;
     // odd, so the threads' merge-path starts fall on different shared-memory bank groups
-    static constexpr int kMergeItems = W == 1 ? 7 : (W == 2 ? 5 : (W == 4 ? 3 : 1));
+    static constexpr int kMergeItems = W == 1 ? 5 : (W == 2 ? 5 : (W == 4 ? 3 : 1));
     static constexpr int kMergeTile = kBlock * kMergeItems;
 };
 constexpr int kScanItems = 16;
@@ -155,7 +155,6 @@ __global__ void __launch_bounds__(kBlock) k_classify(const uint64_t* __restrict_
     __syncthreads();
     const unsigned int tile = s_tile;
     const uint64_t wbase = (uint64_t)tile * TILE + (uint64_t)warp * 32 * ITEMS;
-    uint64_t k[ITEMS][2 * W];
     unsigned int ball[ITEMS];
     unsigned int wcount = 0;
 #pragma unroll
@@ -163,11 +162,9 @@ __global__ void __launch_bounds__(kBlock) k_classify(const uint64_t* __restrict_
         const uint64_t row = wbase + (uint64_t)i * 32 + lane;
         bool e = false;
         if (row < n) {
-            load_key<W>(keys, row, k[i]);
-            e = emits_partner_regs<W, T>(L, k[i]);
-        } else {
-#pragma unroll
-            for (int w = 0; w < 2 * W; ++w) k[i][w] = 0;
+            uint64_t kk[2 * W];
+            load_key<W>(keys, row, kk);
+            e = emits_partner_regs<W, T>(L, kk);
         }
         ball[i] = __ballot_sync(0xffffffffu, e);
         wcount += __popc(ball[i]);
@@ -207,25 +204,34 @@ __global__ void __launch_bounds__(kBlock) k_classify(const uint64_t* __restrict_
             const unsigned int lower = b & lanemask_lt;
             const int src = lower ? 31 - __clz(lower) : lane;
             const int hi = 31 - __clz(b);
+            // keys are read again here (this tile was just streamed, so L2 holds it) rather
+            // than kept in registers across the look-back
+            const uint64_t row = wbase + (uint64_t)i * 32 + lane;
+            uint64_t ki[2 * W];
+            if (row < n)
+                load_key<W>(keys, row, ki);
+            else
+#pragma unroll
+                for (int w = 0; w < 2 * W; ++w) ki[w] = 0;
             uint64_t pk[2 * W];
 #pragma unroll
-            for (int w = 0; w < 2 * W; ++w) pk[w] = __shfl_sync(0xffffffffu, k[i][w], src);
+            for (int w = 0; w < 2 * W; ++w) pk[w] = __shfl_sync(0xffffffffu, ki[w], src);
             if ((b >> lane) & 1u) {
                 const unsigned long long j = base + run + __popc(lower);
                 if (PS_BOUNDS(ctl, j < n, 103)) {
                     idx[j] = (uint32_t)(wbase + (uint64_t)i * 32 + lane);
                     uint16_t d;
                     if (lower)
-                        d = (uint16_t)div_regs<W>(pk, k[i]);
+                        d = (uint16_t)div_regs<W>(pk, ki);
                     else if (have_prev)
-                        d = (uint16_t)div_regs<W>(prev, k[i]);
+                        d = (uint16_t)div_regs<W>(prev, ki);
                     else
                         d = j == 0 ? kDivStart : kDivUnknown;
                     D[j] = d;
                 }
             }
 #pragma unroll
-            for (int w = 0; w < 2 * W; ++w) prev[w] = __shfl_sync(0xffffffffu, k[i][w], hi);
+            for (int w = 0; w < 2 * W; ++w) prev[w] = __shfl_sync(0xffffffffu, ki[w], hi);
             have_prev = true;
             run += __popc(b);
         }

@@ -66,6 +66,27 @@ __global__ void k_unpack(const uint64_t* __restrict__ keys, const T* __restrict_
     }
 }
 
+// Counts rows that break "strictly increasing keys, nonzero coefficients" into count[5];
+// an upload that passes is already in store form and skips the sort.
+template <int W, typename T>
+__global__ void __launch_bounds__(kThreads) k_check_sorted(const uint64_t* __restrict__ keys,
+                                                           const T* __restrict__ coef, uint64_t n, Ctl* ctl) {
+    unsigned int bad = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)kThreads + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kThreads) {
+        uint64_t k[2 * W];
+        load_key<W>(keys, i, k);
+        bool ok = coef[i] != T(0);
+        if (i > 0) {
+            uint64_t p[2 * W];
+            load_key<W>(keys, i - 1, p);
+            ok = ok && key_lt<W>(p, k);
+        }
+        bad += ok ? 0u : 1u;
+    }
+    bad = __reduce_add_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0 && bad) atomicAdd(&ctl->count[5], (unsigned long long)bad);
+}
+
 // ---------------------------------------------------------------------------
 // onesweep radix sort
 // ---------------------------------------------------------------------------
@@ -347,26 +368,51 @@ __global__ void __launch_bounds__(1024) k_topn_select(unsigned int* __restrict__
     }
 }
 
-// Gather the keys of the boundary bin (order does not matter for the select).
+// Gather the keys of the boundary bin (order does not matter for the select): each block
+// takes chunks of kThreads * 16 elements and claims its output slots with one atomic per chunk.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_topn_cand(const T* __restrict__ coef, uint64_t n, Ctl* ctl,
                                                         uint64_t* __restrict__ cand, uint64_t cand_cap) {
+    constexpr int ITEMS = 16;
+    constexpr int CHUNK = kThreads * ITEMS;
+    __shared__ unsigned int s_w[kThreads / 32];
+    __shared__ unsigned long long s_base;
     const uint64_t prefix = ctl->aux[0], mask = ctl->aux[1];
-    const int lane = threadIdx.x & 31;
-    for (uint64_t base = blockIdx.x * (uint64_t)kThreads; base < n; base += (uint64_t)gridDim.x * kThreads) {
-        const uint64_t i = base + threadIdx.x;
-        uint64_t mk = 0;
-        bool hit = false;
-        if (i < n) {
-            mk = mag_key<T>(coef[i]);
-            hit = (mk & mask) == prefix;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned int lt = (1u << lane) - 1u;
+    for (uint64_t c0 = (uint64_t)blockIdx.x * CHUNK; c0 < n; c0 += (uint64_t)gridDim.x * CHUNK) {
+        const uint64_t wbase = c0 + (uint64_t)warp * 32 * ITEMS;
+        unsigned int ball[ITEMS];
+        unsigned int wc = 0;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            const uint64_t e = wbase + (uint64_t)i * 32 + lane;
+            bool hit = false;
+            if (e < n) hit = (mag_key<T>(coef[e]) & mask) == prefix;
+            ball[i] = __ballot_sync(0xffffffffu, hit);
+            wc += __popc(ball[i]);
         }
-        const unsigned int b = __ballot_sync(0xffffffffu, hit);
-        if (!b) continue;
-        unsigned long long slot = 0;
-        if (lane == __ffs(b) - 1) slot = atomicAdd(&ctl->count[4], (unsigned long long)__popc(b));
-        slot = __shfl_sync(0xffffffffu, slot, __ffs(b) - 1) + __popc(b & ((1u << lane) - 1u));
-        if (hit && PS_GUARD(ctl, slot < cand_cap, 703)) cand[slot] = mk;
+        if (lane == 0) s_w[warp] = wc;
+        __syncthreads();
+        unsigned int wx = 0, tot = 0;
+#pragma unroll
+        for (int w = 0; w < kThreads / 32; ++w) {
+            wx += w < warp ? s_w[w] : 0u;
+            tot += s_w[w];
+        }
+        if (tid == 0) s_base = tot ? atomicAdd(&ctl->count[4], (unsigned long long)tot) : 0ull;
+        __syncthreads();
+        unsigned long long slot = s_base + wx;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            if ((ball[i] >> lane) & 1u) {
+                const uint64_t e = wbase + (uint64_t)i * 32 + lane;
+                const unsigned long long q = slot + __popc(ball[i] & lt);
+                if (PS_GUARD(ctl, q < cand_cap, 703)) cand[q] = mag_key<T>(coef[e]);
+            }
+            slot += __popc(ball[i]);
+        }
+        __syncthreads();
     }
 }
 
@@ -405,16 +451,13 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
     const uint64_t boundary = ctl->aux[0];
     const uint64_t wbase = (uint64_t)tile * TILE + (uint64_t)warp * 32 * ITEMS;
     unsigned int ba[ITEMS], bt[ITEMS];
-    T cv[ITEMS];
     unsigned int wa = 0, wt = 0;
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
         const uint64_t e = wbase + (uint64_t)i * 32 + lane;
         bool isa = false, ist = false;
-        cv[i] = T(0);
         if (e < n) {
-            cv[i] = coef[e];
-            const uint64_t mk = mag_key<T>(cv[i]);
+            const uint64_t mk = mag_key<T>(coef[e]);
             isa = mk > boundary;
             ist = mk == boundary && boundary != 0;
         }
@@ -468,7 +511,7 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
             load_key<W>(keys, e, k);
             if (PS_GUARD(ctl, pos < n, 702)) {
                 store_key<W>(okeys, pos, k);
-                ocoef[pos] = cv[i];
+                ocoef[pos] = coef[e];
             }
         }
         arank += __popc(ba[i]);
@@ -545,6 +588,20 @@ cudaError_t StoreOps<W, T>::pack(const uint64_t* x, const uint64_t* z, const dou
     k_pack<W, T><<<grid_for(n, sms), kThreads, 0, st>>>(x, z, c, n, nq, keys, coef, vals, ctl);
     prof->end(st);
     return cudaGetLastError();
+}
+
+template <int W, typename T>
+cudaError_t StoreOps<W, T>::check_sorted(const uint64_t* keys, const T* coef, uint64_t n, Ctl* ctl,
+                                         unsigned long long* host_count, bool* sorted, int sms, cudaStream_t st,
+                                         KernelProf* prof) {
+    cudaMemsetAsync(&ctl->count[5], 0, sizeof(unsigned long long), st);
+    prof->begin(K_PACK, (double)n * (16 * W + sizeof(T)), st);
+    if (n) k_check_sorted<W, T><<<grid_for(n, sms), kThreads, 0, st>>>(keys, coef, n, ctl);
+    prof->end(st);
+    cudaMemcpyAsync(host_count, &ctl->count[5], sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    *sorted = e == cudaSuccess && *host_count == 0;
+    return e;
 }
 
 template <int W, typename T>

@@ -26,6 +26,10 @@ struct StoreOps {
     static size_t sort_tile();
     static cudaError_t pack(const uint64_t* x, const uint64_t* z, const double* c, uint64_t n, uint32_t nq,
                             uint64_t* keys, T* coef, uint32_t* vals, Ctl* ctl, int sms, cudaStream_t st, KernelProf* prof);
+    // *sorted = keys strictly increasing and no zero coefficient (synchronizes)
+    static cudaError_t check_sorted(const uint64_t* keys, const T* coef, uint64_t n, Ctl* ctl,
+                                    unsigned long long* host_count, bool* sorted, int sms, cudaStream_t st,
+                                    KernelProf* prof);
     static cudaError_t unpack(const uint64_t* keys, const T* coef, uint64_t n, uint64_t* x, uint64_t* z, double* c,
                               int sms, cudaStream_t st, KernelProf* prof);
     // LSD radix sort of (key, value) pairs; the sorted pairs end in (keys, vals) or, when

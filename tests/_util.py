@@ -77,7 +77,9 @@ def assert_same_terms(got, want, rtol=0.0, what=""):
     assert gx.shape == wx.shape, f"{what}: {gx.shape[0]} terms vs {wx.shape[0]} expected"
     assert np.array_equal(gx, wx) and np.array_equal(gz, wz), f"{what}: key sets differ"
     if rtol == 0.0:
-        bad = np.nonzero(gc != wc)[0]
+        # bit-exact; a NaN matches any NaN (payloads differ between host and device arithmetic)
+        both_nan = np.isnan(gc) & np.isnan(wc)
+        bad = np.nonzero((gc.view(np.uint64) != wc.view(np.uint64)) & ~both_nan)[0]
         assert bad.size == 0, f"{what}: {bad.size} coefficients differ, first {gc[bad[0]]!r} vs {wc[bad[0]]!r}"
     else:
         scale = np.maximum(np.abs(gc), np.abs(wc))

@@ -321,3 +321,23 @@ def test_topn_many_ties_bit_exact(dtype):
     got, want, la, lb, _, _ = run_both(20, x, z, c, circ, pol, "heisenberg", dtype)
     assert la == lb
     assert_same_terms(got, want, what=f"ties-{dtype}")
+
+
+def test_upload_fast_path_and_fallback_agree():
+    x, z, c = workloads.random_observable(64, 20000, seed=5)
+    g = ps.GpuPauliSum(64)
+    g.upload(x, z, c)  # unsorted: radix sort + dedup
+    sx, sz, sc = g.download()
+    g2 = ps.GpuPauliSum(64)
+    g2.upload(sx, sz, sc)  # already in store form: no sort
+    assert_same_terms(g2.download(), (sx, sz, sc), what="fast-path")
+    # sorted but with a zero coefficient and a duplicate: must take the general path
+    sc2 = sc.copy()
+    sc2[3] = 0.0
+    dx = np.concatenate([sx[:10], sx[9:10]])
+    dz = np.concatenate([sz[:10], sz[9:10]])
+    dc = np.concatenate([sc2[:10], sc2[9:10]])
+    g2.upload(dx, dz, dc)
+    o = oracle_sum(64, dx, dz, dc)
+    assert_same_terms(g2.download(), oracle_arrays(o), what="fallback")
+    assert len(g2) == 9
