@@ -86,22 +86,39 @@ struct Amp<float> {
     __device__ static float sn(const RotLayer<W>& L) { return L.sin32; }
 };
 
+// The layer's per-pattern amplitudes staged in shared memory: indexing the kernel-parameter
+// copy with a per-lane pattern would serialize on the constant cache.
+template <typename T>
+struct AmpTab {
+    T a0[16];
+    T a1[16];
+};
+
+template <int W, typename T>
+__device__ __forceinline__ void stage_amps(const RotLayer<W>& L, AmpTab<T>& t) {
+    if (threadIdx.x < 16) {
+        t.a0[threadIdx.x] = Amp<T>::a0(L, threadIdx.x);
+        t.a1[threadIdx.x] = Amp<T>::a1(L, threadIdx.x);
+    }
+}
+
 // Does term k emit a partner?
 template <int W, typename T>
-__device__ __forceinline__ bool emits_partner(const RotLayer<W>& L, const uint64_t* k) {
+__device__ __forceinline__ bool emits_partner(const RotLayer<W>& L, const AmpTab<T>& A, const uint64_t* k) {
     if (L.wide) return anticommutes<W>(k, L.gx, L.gz);
-    return Amp<T>::a1(L, pattern_of<W>(L, k)) != T(0);
+    return A.a1[pattern_of<W>(L, k)] != T(0);
 }
 
 template <int W, typename T>
-__device__ __forceinline__ bool emits_partner_regs(const RotLayer<W>& L, const uint64_t (&k)[2 * W]) {
+__device__ __forceinline__ bool emits_partner_regs(const RotLayer<W>& L, const AmpTab<T>& A,
+                                                   const uint64_t (&k)[2 * W]) {
     if (L.wide) {
         uint64_t f = 0;
 #pragma unroll
         for (int i = 0; i < W; ++i) f ^= (k[i] & L.gz[i]) ^ (k[W + i] & L.gx[i]);
         return (__popcll(f) & 1) != 0;
     }
-    return Amp<T>::a1(L, pattern_of<W>(L, k)) != T(0);
+    return A.a1[pattern_of<W>(L, k)] != T(0);
 }
 
 template <int W>
@@ -117,20 +134,20 @@ __device__ __forceinline__ uint32_t div_regs(const uint64_t (&a)[2 * W], const u
 
 // Own-row coefficient after the layer.
 template <int W, typename T>
-__device__ __forceinline__ T own_coeff(const RotLayer<W>& L, const uint64_t* k, T c) {
+__device__ __forceinline__ T own_coeff(const RotLayer<W>& L, const AmpTab<T>& A, const uint64_t* k, T c) {
     if (L.wide) return anticommutes<W>(k, L.gx, L.gz) ? mul_rn(c, Amp<T>::cs(L)) : c;
-    return mul_rn(c, Amp<T>::a0(L, pattern_of<W>(L, k)));
+    return mul_rn(c, A.a0[pattern_of<W>(L, k)]);
 }
 
 // Partner coefficient (DeltaEntry::emit / PreparedRotation::emit_generator).
 template <int W, typename T>
-__device__ __forceinline__ T partner_coeff(const RotLayer<W>& L, const uint64_t* k, T c) {
+__device__ __forceinline__ T partner_coeff(const RotLayer<W>& L, const AmpTab<T>& A, const uint64_t* k, T c) {
     if (L.wide) {
         uint32_t total = (1u + product_phase<W>(k, L.gx, L.gz)) & 3u;
         T m = (total & 2u) ? -c : c;  // real mul_phase, coefficient.rs:107-114
         return mul_rn(m, Amp<T>::sn(L));
     }
-    return mul_rn(c, Amp<T>::a1(L, pattern_of<W>(L, k)));
+    return mul_rn(c, A.a1[pattern_of<W>(L, k)]);
 }
 
 // ---------------------------------------------------------------------------
@@ -149,9 +166,11 @@ __global__ void __launch_bounds__(kBlock) k_classify(const uint64_t* __restrict_
     __shared__ unsigned int s_tile;
     __shared__ unsigned int s_wcount[kBlock / 32];
     __shared__ unsigned long long s_prefix;
+    __shared__ AmpTab<T> A;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned int lanemask_lt = (1u << lane) - 1u;
     if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[0], 1u);
+    stage_amps<W, T>(L, A);
     __syncthreads();
     const unsigned int tile = s_tile;
     const uint64_t wbase = (uint64_t)tile * TILE + (uint64_t)warp * 32 * ITEMS;
@@ -164,7 +183,7 @@ __global__ void __launch_bounds__(kBlock) k_classify(const uint64_t* __restrict_
         if (row < n) {
             uint64_t kk[2 * W];
             load_key<W>(keys, row, kk);
-            e = emits_partner_regs<W, T>(L, kk);
+            e = emits_partner_regs<W, T>(L, A, kk);
         }
         ball[i] = __ballot_sync(0xffffffffu, e);
         wcount += __popc(ball[i]);
@@ -427,9 +446,11 @@ __global__ void __launch_bounds__(kBlock) k_bwd_levels(const uint32_t* __restric
     __shared__ unsigned int s_tile;
     __shared__ int s_wagg[kBlock / 32][2 * kMaxLevels];
     __shared__ int s_suffix[2 * kMaxLevels];
+    __shared__ AmpTab<T> A;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int INF = 0x7fffffff;
     if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[2], 1u);
+    stage_amps<W, T>(L, A);
     __syncthreads();
     const unsigned int tile = s_tile;  // tile 0 covers the last kScanTile partners
     const long long hi = (long long)m - (long long)tile * kScanTile;
@@ -520,7 +541,7 @@ __global__ void __launch_bounds__(kBlock) k_bwd_levels(const uint32_t* __restric
         uint64_t k[2 * W];
         load_key<W>(keys, row, k);
         T c = coef[row];
-        T pc = partner_coeff<W, T>(L, k, c);
+        T pc = partner_coeff<W, T>(L, A, k, c);
 #pragma unroll
         for (int w = 0; w < W; ++w) {
             k[w] ^= L.gx[w];
@@ -623,7 +644,7 @@ __device__ __forceinline__ bool eq_regs(const uint64_t (&a)[2 * W], const uint64
 template <int W, typename T, bool kStore>
 __device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc, const uint64_t* sPk, const T* sPc,
                                                uint32_t i, uint32_t ie, uint32_t j, uint32_t je,
-                                               const RotLayer<W>& L, const KeepProg& keep,
+                                               const RotLayer<W>& L, const AmpTab<T>& A, const KeepProg& keep,
                                                uint64_t* __restrict__ Ok, T* __restrict__ Oc,
                                                unsigned long long out, unsigned int* s_hist) {
     uint32_t count = 0;
@@ -637,7 +658,7 @@ __device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc
         if (takeS) {
 #pragma unroll
             for (int w = 0; w < 2 * W; ++w) k[w] = a[w];
-            v = own_coeff<W, T>(L, a, sSc[i]);
+            v = own_coeff<W, T>(L, A, a, sSc[i]);
             if (j < je && eq_regs<W>(a, b)) {
                 v = add_rn(v, sPc[j]);
                 if (++j < je) ld_row<W>(sPk, j, b);
@@ -681,6 +702,7 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
     __shared__ unsigned int s_si[kBlock + 1], s_sj[kBlock + 1];
     __shared__ unsigned long long s_outoff;
     __shared__ unsigned int s_hist[kTopnHistBins];
+    __shared__ AmpTab<T> A;
 
     const int tid = threadIdx.x;
     if (tid == 0) {
@@ -689,6 +711,7 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
     }
     if (topn_hist)
         for (int q = tid; q < kTopnHistBins; q += kBlock) s_hist[q] = 0;
+    stage_amps<W, T>(L, A);
     __syncthreads();
     const unsigned int tile = s_tile;
     if (tile >= num_tiles) return;
@@ -748,7 +771,7 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
     const uint32_t i0 = s_si[tid], j0 = s_sj[tid];
     const uint32_t ie = max(s_si[tid + 1], i0), je = max(s_sj[tid + 1], j0);
     const uint32_t count =
-        merge_walk<W, T, false>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, keep, nullptr, nullptr, 0ull, nullptr);
+        merge_walk<W, T, false>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, A, keep, nullptr, nullptr, 0ull, nullptr);
     unsigned int total;
     unsigned int excl = block_exclusive_sum<kBlock>(count, s_warp, total);
     if (tid < 32) {
@@ -768,7 +791,7 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
     __syncthreads();
     const unsigned long long off = s_outoff;
     if (!PS_GUARD(ctl, off + total <= out_cap, 304)) return;
-    merge_walk<W, T, true>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, keep, Ok, Oc, off + excl,
+    merge_walk<W, T, true>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, A, keep, Ok, Oc, off + excl,
                            topn_hist ? s_hist : nullptr);
     if (topn_hist) {
         __syncthreads();
