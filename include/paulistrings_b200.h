@@ -227,6 +227,24 @@ ps_status ps_set_profiling(ps_sum* sum, int32_t enabled);
 /* Copy up to cap kernel records; *count receives the number of kernels profiled. */
 ps_status ps_read_profile(ps_sum* sum, ps_kernel_profile* out, int32_t cap, int32_t* count);
 
+/* Largest n ps_expectation_device_noalloc accepts (its scratch holds one partial per 16,384 terms). */
+#define PS_NOALLOC_MAX_TERMS (1ull << 30)
+
+/* The product-state expectation (as ps_expectation) of a sum the caller already holds in device
+ * memory, for callers that cannot allocate device memory themselves (a framework that owns the
+ * GPU's memory through its own pool, a service that forbids allocation after start-up).  This
+ * entry point allocates nothing: its scratch is a fixed 512 KiB device array inside the library,
+ * held by every GPU that loads it until the process exits.  keys: n rows of 2*width u64 (x words
+ * then z words) in device memory; coeffs: n float64 or float32 (dtype) in device memory; the
+ * axis/sign masks are host arrays of width words; out: one float64 in device memory, written on
+ * `stream` (a cudaStream_t, NULL for the default stream).  n above PS_NOALLOC_MAX_TERMS is
+ * rejected with PS_ERR_INVALID.  The first call on each device looks up the scratch address
+ * (make it before any stream capture); calls on one device share the scratch, so calls that
+ * overlap on the GPU race.  It has no counterpart in the reference. */
+ps_status ps_expectation_device_noalloc(const uint64_t* keys, const void* coeffs, int32_t dtype, int32_t width,
+                                        uint64_t n, const uint64_t* axis_x, const uint64_t* axis_z,
+                                        const uint64_t* negative, double* out, void* stream);
+
 /* Wait for the handle's stream.  PartitionStorage::settle. */
 ps_status ps_synchronize(ps_sum* sum);
 

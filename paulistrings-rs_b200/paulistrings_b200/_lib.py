@@ -48,8 +48,11 @@ EXPORTED = (
     "ps_expectation",
     "ps_set_profiling",
     "ps_read_profile",
+    "ps_expectation_device_noalloc",
     "ps_synchronize",
 )
+
+NOALLOC_MAX_TERMS = 1 << 30
 
 
 class KeepNode(ctypes.Structure):
@@ -186,6 +189,7 @@ def lib():
     L.ps_expectation.argtypes = [vp, vp, vp, vp, P(ctypes.c_double)]
     L.ps_set_profiling.argtypes = [vp, i32]
     L.ps_read_profile.argtypes = [vp, P(KernelProfile), i32, P(i32)]
+    L.ps_expectation_device_noalloc.argtypes = [vp, vp, i32, i32, u64, vp, vp, vp, vp, vp]
     L.ps_synchronize.argtypes = [vp]
     for name in EXPORTED:
         fn = getattr(L, name)
