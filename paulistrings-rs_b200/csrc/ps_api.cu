@@ -123,7 +123,7 @@ ps_status check_device_flags(ps_sum* s, const char* where) {
 // ---------------------------------------------------------------------------
 ps_status lower_keep(const ps_policy* p, KeepProg& k, std::string& why) {
     std::memset(&k, 0, sizeof k);
-    if (!p) return PS_OK;
+    if (!p) return PS_OK;  // fast = 0: keep every nonzero term
     if (p->num_nodes < 0 || p->num_nodes > PS_MAX_KEEP_NODES || p->num_passes < 0 || p->num_passes > PS_MAX_PASSES) {
         why = "policy: bad node or pass count";
         return PS_ERR_INVALID;
@@ -162,6 +162,24 @@ ps_status lower_keep(const ps_policy* p, KeepProg& k, std::string& why) {
         return PS_ERR_INVALID;
     }
     k.n = p->num_nodes;
+    // recognise the common programs so kernels skip the interpreter
+    k.fast = 4;
+    if (k.n == 0 || (k.n == 1 && k.op[0] == PS_KEEP_TRUE)) {
+        k.fast = 0;
+    } else if (k.n == 1 && k.op[0] == PS_KEEP_COEFF) {
+        k.fast = 1;
+        k.fast_eps2 = k.eps2[0];
+    } else if (k.n == 1 && k.op[0] == PS_KEEP_WEIGHT) {
+        k.fast = 2;
+        k.fast_k = k.iarg[0];
+    } else if (k.n == 3 && k.op[2] == PS_KEEP_AND &&
+               ((k.op[0] == PS_KEEP_COEFF && k.op[1] == PS_KEEP_WEIGHT) ||
+                (k.op[0] == PS_KEEP_WEIGHT && k.op[1] == PS_KEEP_COEFF))) {
+        k.fast = 3;
+        const int ci = k.op[0] == PS_KEEP_COEFF ? 0 : 1;
+        k.fast_eps2 = k.eps2[ci];
+        k.fast_k = k.iarg[1 - ci];
+    }
     for (int i = 0; i < p->num_passes; ++i) {
         if (p->passes[i].kind != PS_PASS_TOPN && p->passes[i].kind != PS_PASS_NONE) {
             why = "policy: unknown layer pass";

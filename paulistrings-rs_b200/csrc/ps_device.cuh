@@ -238,6 +238,13 @@ __device__ __forceinline__ void two_sum(T a, T b, T& s, T& e) {
 // ---------------------------------------------------------------------------
 template <int W>
 __device__ __forceinline__ bool keep_eval(const KeepProg& p, const uint64_t* k, double c) {
+    switch (p.fast) {  // uniform across the grid
+    case 0: return true;
+    case 1: return p.fast_eps2 < 0.0 || __dmul_rn(c, c) > p.fast_eps2;
+    case 2: return key_weight<W>(k) <= (uint64_t)p.fast_k;
+    case 3: return (p.fast_eps2 < 0.0 || __dmul_rn(c, c) > p.fast_eps2) && key_weight<W>(k) <= (uint64_t)p.fast_k;
+    default: break;
+    }
     if (p.n == 0) return true;
     uint32_t stack = 0;  // bit stack
     int sp = 0;

@@ -22,6 +22,11 @@ struct KeepProg {
     int32_t op[15];     // 0 true, 1 coeff, 2 weight, 3 and, 4 or
     int64_t iarg[15];   // weight limit
     double eps2[15];    // eps * eps, or -1 when eps < 0 (keeps everything)
+    // the common programs, recognised on the host: 0 keep all, 1 threshold, 2 weight,
+    // 3 threshold and weight, 4 interpret op[]
+    int32_t fast;
+    double fast_eps2;
+    int64_t fast_k;
 };
 
 constexpr int kMaxLevels = 8;

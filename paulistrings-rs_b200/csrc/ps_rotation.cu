@@ -266,16 +266,16 @@ __global__ void __launch_bounds__(kBlock) k_classify(const uint64_t* __restrict_
 // (min) level scans, by one full warp: each poll reads 32 predecessors' slots, combines their
 // aggregates up to the nearest inclusive value, and moves back only when none of the 32 has
 // one.  Publishes this tile's aggregate first and its inclusive value after.
-template <bool kMax>
-__device__ __forceinline__ void level_lookback(LevelSlot* slots, unsigned int tile, const int (&tile_agg)[2 * kMaxLevels],
-                                               int (&prefix)[2 * kMaxLevels], int identity, Ctl* ctl, uint32_t info) {
+template <bool kMax, int LV>
+__device__ __forceinline__ void level_lookback(LevelSlot* slots, unsigned int tile, const int (&tile_agg)[2 * LV],
+                                               int (&prefix)[2 * LV], int identity, Ctl* ctl, uint32_t info) {
     const int lane = threadIdx.x & 31;
     auto comb = [](int a, int b) { return kMax ? max(a, b) : min(a, b); };
 #pragma unroll
-    for (int v = 0; v < 2 * kMaxLevels; ++v) prefix[v] = identity;
+    for (int v = 0; v < 2 * LV; ++v) prefix[v] = identity;
     if (tile == 0) {
         if (lane == 0) {
-            for (int v = 0; v < 2 * kMaxLevels; ++v) slots[0].inc[v] = tile_agg[v];
+            for (int v = 0; v < 2 * LV; ++v) slots[0].inc[v] = tile_agg[v];
             __threadfence();
             st_release_u32(&slots[0].flag, 2u);
         }
@@ -283,7 +283,7 @@ __device__ __forceinline__ void level_lookback(LevelSlot* slots, unsigned int ti
         return;
     }
     if (lane == 0) {
-        for (int v = 0; v < 2 * kMaxLevels; ++v) slots[tile].agg[v] = tile_agg[v];
+        for (int v = 0; v < 2 * LV; ++v) slots[tile].agg[v] = tile_agg[v];
         __threadfence();
         st_release_u32(&slots[tile].flag, 1u);
     }
@@ -307,7 +307,7 @@ __device__ __forceinline__ void level_lookback(LevelSlot* slots, unsigned int ti
         const bool use = lane <= first_inc && t >= 0;
         const int* src = f == 2u ? slots[t >= 0 ? t : 0].inc : slots[t >= 0 ? t : 0].agg;
 #pragma unroll
-        for (int v = 0; v < 2 * kMaxLevels; ++v) {
+        for (int v = 0; v < 2 * LV; ++v) {
             int x = use ? __ldcg(src + v) : identity;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) x = comb(x, __shfl_xor_sync(0xffffffffu, x, o));
@@ -317,7 +317,7 @@ __device__ __forceinline__ void level_lookback(LevelSlot* slots, unsigned int ti
         base -= 32;
     }
     if (lane == 0) {
-        for (int v = 0; v < 2 * kMaxLevels; ++v) slots[tile].inc[v] = comb(prefix[v], tile_agg[v]);
+        for (int v = 0; v < 2 * LV; ++v) slots[tile].inc[v] = comb(prefix[v], tile_agg[v]);
         __threadfence();
         st_release_u32(&slots[tile].flag, 2u);
     }
@@ -338,15 +338,15 @@ __device__ __forceinline__ void fix_divergence(const uint32_t* __restrict__ idx,
     D[j] = d;
 }
 
-template <int W>
+template <int W, int LV>
 __global__ void __launch_bounds__(kBlock) k_fwd_levels(const uint32_t* __restrict__ idx, uint16_t* __restrict__ D,
                                                        int32_t* __restrict__ F, uint32_t m,
                                                        const uint64_t* __restrict__ keys, uint64_t n,
                                                        const Levels lv, int accumulate, LevelSlot* slots,
                                                        Ctl* ctl) {
     __shared__ unsigned int s_tile;
-    __shared__ int s_wagg[kBlock / 32][2 * kMaxLevels];
-    __shared__ int s_prefix[2 * kMaxLevels];
+    __shared__ int s_wagg[kBlock / 32][2 * LV];
+    __shared__ int s_prefix[2 * LV];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[1], 1u);
     __syncthreads();
@@ -362,9 +362,9 @@ __global__ void __launch_bounds__(kBlock) k_fwd_levels(const uint32_t* __restric
         if (j < m && j > 0) fix_divergence<W>(idx, D, keys, n, j, d[i], ctl);
     }
     // thread aggregates: last start / last split position per level
-    int agg[2 * kMaxLevels];
+    int agg[2 * LV];
 #pragma unroll
-    for (int l = 0; l < kMaxLevels; ++l) {
+    for (int l = 0; l < LV; ++l) {
         agg[2 * l] = -1;
         agg[2 * l + 1] = -1;
         if (l < NL) {
@@ -379,9 +379,9 @@ __global__ void __launch_bounds__(kBlock) k_fwd_levels(const uint32_t* __restric
         }
     }
     // block exclusive max-scan of the aggregates
-    int excl[2 * kMaxLevels];
+    int excl[2 * LV];
 #pragma unroll
-    for (int v = 0; v < 2 * kMaxLevels; ++v) {
+    for (int v = 0; v < 2 * LV; ++v) {
         int x = agg[v];
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -394,24 +394,24 @@ __global__ void __launch_bounds__(kBlock) k_fwd_levels(const uint32_t* __restric
     }
     __syncthreads();
 #pragma unroll
-    for (int v = 0; v < 2 * kMaxLevels; ++v)
+    for (int v = 0; v < 2 * LV; ++v)
         for (int w = 0; w < warp; ++w) excl[v] = max(excl[v], s_wagg[w][v]);
     // tile aggregate, publish, look back
     __syncthreads();
     if (tid < 32) {
-        int tagg[2 * kMaxLevels], pre[2 * kMaxLevels];
-        for (int v = 0; v < 2 * kMaxLevels; ++v) {
+        int tagg[2 * LV], pre[2 * LV];
+        for (int v = 0; v < 2 * LV; ++v) {
             int t = -1;
             for (int w = 0; w < kBlock / 32; ++w) t = max(t, s_wagg[w][v]);
             tagg[v] = t;
         }
-        level_lookback<true>(slots, tile, tagg, pre, -1, ctl, 202);
+        level_lookback<true, LV>(slots, tile, tagg, pre, -1, ctl, 202);
         if (tid == 0)
-            for (int v = 0; v < 2 * kMaxLevels; ++v) s_prefix[v] = pre[v];
+            for (int v = 0; v < 2 * LV; ++v) s_prefix[v] = pre[v];
     }
     __syncthreads();
 #pragma unroll
-    for (int v = 0; v < 2 * kMaxLevels; ++v) excl[v] = max(excl[v], s_prefix[v]);
+    for (int v = 0; v < 2 * LV; ++v) excl[v] = max(excl[v], s_prefix[v]);
 
     // per item: F = sum over levels of -(split - start) for rows in an upper half
 #pragma unroll
@@ -420,7 +420,7 @@ __global__ void __launch_bounds__(kBlock) k_fwd_levels(const uint32_t* __restric
         if (j >= m) break;
         int f = 0;
 #pragma unroll
-        for (int l = 0; l < kMaxLevels; ++l) {
+        for (int l = 0; l < LV; ++l) {
             if (l < NL) {
                 uint32_t L = lv.rank[l];
                 if (j == 0 || d[i] < L) excl[2 * l] = (int)j;
@@ -435,7 +435,7 @@ __global__ void __launch_bounds__(kBlock) k_fwd_levels(const uint32_t* __restric
 
 // Backward pass: B = sum over levels of (group end - split) for rows in a lower half; then
 // (last batch only) place each partner at j + F + B.
-template <int W, typename T>
+template <int W, typename T, int LV>
 __global__ void __launch_bounds__(kBlock) k_bwd_levels(const uint32_t* __restrict__ idx,
                                                        const uint16_t* __restrict__ D, int32_t* __restrict__ F,
                                                        uint32_t m, const uint64_t* __restrict__ keys,
@@ -444,8 +444,8 @@ __global__ void __launch_bounds__(kBlock) k_bwd_levels(const uint32_t* __restric
                                                        uint64_t* __restrict__ Pk, T* __restrict__ Pc,
                                                        LevelSlot* slots, Ctl* ctl) {
     __shared__ unsigned int s_tile;
-    __shared__ int s_wagg[kBlock / 32][2 * kMaxLevels];
-    __shared__ int s_suffix[2 * kMaxLevels];
+    __shared__ int s_wagg[kBlock / 32][2 * LV];
+    __shared__ int s_suffix[2 * LV];
     __shared__ AmpTab<T> A;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int INF = 0x7fffffff;
@@ -464,9 +464,9 @@ __global__ void __launch_bounds__(kBlock) k_bwd_levels(const uint32_t* __restric
         long long j = jbase + i;
         d[i] = (j >= 0 && j < hi) ? D[j] : (uint16_t)0;
     }
-    int agg[2 * kMaxLevels];
+    int agg[2 * LV];
 #pragma unroll
-    for (int l = 0; l < kMaxLevels; ++l) {
+    for (int l = 0; l < LV; ++l) {
         agg[2 * l] = INF;
         agg[2 * l + 1] = INF;
         if (l < NL) {
@@ -481,9 +481,9 @@ __global__ void __launch_bounds__(kBlock) k_bwd_levels(const uint32_t* __restric
         }
     }
     // exclusive suffix min over threads
-    int excl[2 * kMaxLevels];
+    int excl[2 * LV];
 #pragma unroll
-    for (int v = 0; v < 2 * kMaxLevels; ++v) {
+    for (int v = 0; v < 2 * LV; ++v) {
         int x = agg[v];
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -496,23 +496,23 @@ __global__ void __launch_bounds__(kBlock) k_bwd_levels(const uint32_t* __restric
     }
     __syncthreads();
 #pragma unroll
-    for (int v = 0; v < 2 * kMaxLevels; ++v)
+    for (int v = 0; v < 2 * LV; ++v)
         for (int w = warp + 1; w < kBlock / 32; ++w) excl[v] = min(excl[v], s_wagg[w][v]);
     __syncthreads();
     if (tid < 32) {
-        int tagg[2 * kMaxLevels], suf[2 * kMaxLevels];
-        for (int v = 0; v < 2 * kMaxLevels; ++v) {
+        int tagg[2 * LV], suf[2 * LV];
+        for (int v = 0; v < 2 * LV; ++v) {
             int t = INF;
             for (int w = 0; w < kBlock / 32; ++w) t = min(t, s_wagg[w][v]);
             tagg[v] = t;
         }
-        level_lookback<false>(slots, tile, tagg, suf, INF, ctl, 203);
+        level_lookback<false, LV>(slots, tile, tagg, suf, INF, ctl, 203);
         if (tid == 0)
-            for (int v = 0; v < 2 * kMaxLevels; ++v) s_suffix[v] = suf[v];
+            for (int v = 0; v < 2 * LV; ++v) s_suffix[v] = suf[v];
     }
     __syncthreads();
 #pragma unroll
-    for (int v = 0; v < 2 * kMaxLevels; ++v) excl[v] = min(excl[v], s_suffix[v]);
+    for (int v = 0; v < 2 * LV; ++v) excl[v] = min(excl[v], s_suffix[v]);
 
 #pragma unroll
     for (int i = kScanItems - 1; i >= 0; --i) {
@@ -520,7 +520,7 @@ __global__ void __launch_bounds__(kBlock) k_bwd_levels(const uint32_t* __restric
         if (j < 0 || j >= hi) continue;
         int b = 0;
 #pragma unroll
-        for (int l = 0; l < kMaxLevels; ++l) {
+        for (int l = 0; l < LV; ++l) {
             if (l < NL) {
                 int e = excl[2 * l] == INF ? (int)m : excl[2 * l];
                 int q = excl[2 * l + 1];
@@ -637,49 +637,52 @@ __device__ __forceinline__ bool eq_regs(const uint64_t (&a)[2 * W], const uint64
     return d == 0;
 }
 
+// One thread's merge outputs, held in registers between the walk and the write-out.  A
+// thread's range holds at most ITEMS + 1 merged items (its start and end may each move by one
+// to keep an equal pair together), so ITEMS + 2 fixed slots cover it with static indexing.
+template <int W, typename T, int SLOTS>
+struct WalkOut {
+    uint64_t k[SLOTS][2 * W];
+    T v[SLOTS];
+    uint32_t keep;  // bit s: slot s holds a kept output
+};
+
 // Walk one thread's merge-path range with the two run heads held in registers (one shared
 // load per consumed item).  Own row first, partner second when their keys are equal, as the
-// reference's merge sums bucket-first.  With kStore, kept outputs go straight to the output
-// store starting at row `out`.
-template <int W, typename T, bool kStore>
-__device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc, const uint64_t* sPk, const T* sPc,
-                                               uint32_t i, uint32_t ie, uint32_t j, uint32_t je,
-                                               const RotLayer<W>& L, const AmpTab<T>& A, const KeepProg& keep,
-                                               uint64_t* __restrict__ Ok, T* __restrict__ Oc,
-                                               unsigned long long out, unsigned int* s_hist) {
-    uint32_t count = 0;
+// reference's merge sums bucket-first.  Returns false if the range did not fit the slots.
+template <int W, typename T, int SLOTS>
+__device__ __forceinline__ bool merge_walk(const uint64_t* sSk, const T* sSc, const uint64_t* sPk, const T* sPc,
+                                           uint32_t i, uint32_t ie, uint32_t j, uint32_t je, const RotLayer<W>& L,
+                                           const AmpTab<T>& A, const KeepProg& keep, WalkOut<W, T, SLOTS>& out) {
+    out.keep = 0;
     uint64_t a[2 * W], b[2 * W];
     if (i < ie) ld_row<W>(sSk, i, a);
     if (j < je) ld_row<W>(sPk, j, b);
-    while (i < ie || j < je) {
-        const bool takeS = (j >= je) || (i < ie && le_regs<W>(a, b));
-        uint64_t k[2 * W];
-        T v;
-        if (takeS) {
 #pragma unroll
-            for (int w = 0; w < 2 * W; ++w) k[w] = a[w];
-            v = own_coeff<W, T>(L, A, a, sSc[i]);
-            if (j < je && eq_regs<W>(a, b)) {
-                v = add_rn(v, sPc[j]);
+    for (int st = 0; st < SLOTS; ++st) {
+        if (i < ie || j < je) {
+            const bool takeS = (j >= je) || (i < ie && le_regs<W>(a, b));
+            T v;
+            if (takeS) {
+#pragma unroll
+                for (int w = 0; w < 2 * W; ++w) out.k[st][w] = a[w];
+                v = own_coeff<W, T>(L, A, a, sSc[i]);
+                if (j < je && eq_regs<W>(a, b)) {
+                    v = add_rn(v, sPc[j]);
+                    if (++j < je) ld_row<W>(sPk, j, b);
+                }
+                if (++i < ie) ld_row<W>(sSk, i, a);
+            } else {
+#pragma unroll
+                for (int w = 0; w < 2 * W; ++w) out.k[st][w] = b[w];
+                v = sPc[j];
                 if (++j < je) ld_row<W>(sPk, j, b);
             }
-            if (++i < ie) ld_row<W>(sSk, i, a);
-        } else {
-#pragma unroll
-            for (int w = 0; w < 2 * W; ++w) k[w] = b[w];
-            v = sPc[j];
-            if (++j < je) ld_row<W>(sPk, j, b);
-        }
-        if (v != T(0) && keep_eval<W>(keep, k, to_f64(v))) {
-            if (kStore) {
-                store_key<W>(Ok, out + count, k);
-                Oc[out + count] = v;
-                if (s_hist) atomicAdd(&s_hist[mag_key<T>(v) >> 52], 1u);
-            }
-            ++count;
+            out.v[st] = v;
+            if (v != T(0) && keep_eval<W>(keep, out.k[st], to_f64(v))) out.keep |= 1u << st;
         }
     }
-    return count;
+    return i >= ie && j >= je;
 }
 
 template <int W, typename T>
@@ -770,8 +773,10 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
     __syncthreads();
     const uint32_t i0 = s_si[tid], j0 = s_sj[tid];
     const uint32_t ie = max(s_si[tid + 1], i0), je = max(s_sj[tid + 1], j0);
-    const uint32_t count =
-        merge_walk<W, T, false>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, A, keep, nullptr, nullptr, 0ull, nullptr);
+    WalkOut<W, T, ITEMS + 2> out;
+    if (!merge_walk<W, T, ITEMS + 2>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, A, keep, out))
+        raise_err(ctl, ERR_INTERNAL, 305);
+    const uint32_t count = __popc(out.keep);
     unsigned int total;
     unsigned int excl = block_exclusive_sum<kBlock>(count, s_warp, total);
     if (tid < 32) {
@@ -791,8 +796,16 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
     __syncthreads();
     const unsigned long long off = s_outoff;
     if (!PS_GUARD(ctl, off + total <= out_cap, 304)) return;
-    merge_walk<W, T, true>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, A, keep, Ok, Oc, off + excl,
-                           topn_hist ? s_hist : nullptr);
+    unsigned long long pos = off + excl;
+#pragma unroll
+    for (int st = 0; st < ITEMS + 2; ++st) {
+        if ((out.keep >> st) & 1u) {
+            store_key<W>(Ok, pos, out.k[st]);
+            Oc[pos] = out.v[st];
+            if (topn_hist) atomicAdd(&s_hist[mag_key<T>(out.v[st]) >> 52], 1u);
+            ++pos;
+        }
+    }
     if (topn_hist) {
         __syncthreads();
         for (int q = tid; q < kTopnHistBins; q += kBlock)
@@ -827,18 +840,25 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     *a.partners_out = m;
     if (m > a.p_cap) return cudaErrorMemoryAllocation;  // caller sized the partner buffers by n
     if (m > 0) {
-        // 2-3. level scans (batches of kMaxLevels), scatter on the last batch
+        // 2-3. level scans (batches of kMaxLevels; one batch of four covers every gate on at
+        // most two qubits), scatter on the last batch
         uint32_t stiles = (uint32_t)((m + kScanTile - 1) / kScanTile);
-        int nb = (a.levels->n + kMaxLevels - 1) / kMaxLevels;
+        const bool narrow = a.levels->n <= 4;
+        const int per = narrow ? 4 : kMaxLevels;
+        int nb = (a.levels->n + per - 1) / per;
         for (int b = 0; b < nb; ++b) {
             Levels lv{};
-            lv.n = min(kMaxLevels, a.levels->n - b * kMaxLevels);
-            for (int l = 0; l < lv.n; ++l) lv.rank[l] = a.levels->rank[b * kMaxLevels + l];
+            lv.n = min(per, a.levels->n - b * per);
+            for (int l = 0; l < lv.n; ++l) lv.rank[l] = a.levels->rank[b * per + l];
             cudaMemsetAsync(a.slots, 0, (size_t)stiles * sizeof(LevelSlot), st);
             cudaMemsetAsync(&ctl->tile_counter[1], 0, sizeof(unsigned int), st);
             a.prof->begin(K_FWD_LEVELS, (double)m * (2 + 4 + (b > 0 ? 4 : 0)), st);
-            k_fwd_levels<W><<<stiles, kBlock, 0, st>>>(a.idx, a.D, a.F, (uint32_t)m, a.Sk, a.n, lv, b > 0,
-                                                     reinterpret_cast<LevelSlot*>(a.slots), ctl);
+            if (narrow)
+                k_fwd_levels<W, 4><<<stiles, kBlock, 0, st>>>(a.idx, a.D, a.F, (uint32_t)m, a.Sk, a.n, lv, b > 0,
+                                                            reinterpret_cast<LevelSlot*>(a.slots), ctl);
+            else
+                k_fwd_levels<W, kMaxLevels><<<stiles, kBlock, 0, st>>>(a.idx, a.D, a.F, (uint32_t)m, a.Sk, a.n, lv,
+                                                                     b > 0, reinterpret_cast<LevelSlot*>(a.slots), ctl);
             a.prof->end(st);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
             cudaMemsetAsync(a.slots, 0, (size_t)stiles * sizeof(LevelSlot), st);
@@ -846,9 +866,14 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
             const bool last = b == nb - 1;
             a.prof->begin(K_BWD_LEVELS,
                           (double)m * (2 + 4 + (last ? 4 + 2.0 * (16 * W + sizeof(T)) : 4)), st);
-            k_bwd_levels<W, T><<<stiles, kBlock, 0, st>>>(a.idx, a.D, a.F, (uint32_t)m, a.Sk, a.Sc, a.n, lv, a.L,
-                                                        last, a.Pk, a.Pc,
-                                                        reinterpret_cast<LevelSlot*>(a.slots), ctl);
+            if (narrow)
+                k_bwd_levels<W, T, 4><<<stiles, kBlock, 0, st>>>(a.idx, a.D, a.F, (uint32_t)m, a.Sk, a.Sc, a.n, lv, a.L,
+                                                               last, a.Pk, a.Pc,
+                                                               reinterpret_cast<LevelSlot*>(a.slots), ctl);
+            else
+                k_bwd_levels<W, T, kMaxLevels><<<stiles, kBlock, 0, st>>>(
+                    a.idx, a.D, a.F, (uint32_t)m, a.Sk, a.Sc, a.n, lv, a.L, last, a.Pk, a.Pc,
+                    reinterpret_cast<LevelSlot*>(a.slots), ctl);
             a.prof->end(st);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
