@@ -637,52 +637,49 @@ __device__ __forceinline__ bool eq_regs(const uint64_t (&a)[2 * W], const uint64
     return d == 0;
 }
 
-// One thread's merge outputs, held in registers between the walk and the write-out.  A
-// thread's range holds at most ITEMS + 1 merged items (its start and end may each move by one
-// to keep an equal pair together), so ITEMS + 2 fixed slots cover it with static indexing.
-template <int W, typename T, int SLOTS>
-struct WalkOut {
-    uint64_t k[SLOTS][2 * W];
-    T v[SLOTS];
-    uint32_t keep;  // bit s: slot s holds a kept output
-};
-
 // Walk one thread's merge-path range with the two run heads held in registers (one shared
 // load per consumed item).  Own row first, partner second when their keys are equal, as the
-// reference's merge sums bucket-first.  Returns false if the range did not fit the slots.
-template <int W, typename T, int SLOTS>
-__device__ __forceinline__ bool merge_walk(const uint64_t* sSk, const T* sSc, const uint64_t* sPk, const T* sPc,
-                                           uint32_t i, uint32_t ie, uint32_t j, uint32_t je, const RotLayer<W>& L,
-                                           const AmpTab<T>& A, const KeepProg& keep, WalkOut<W, T, SLOTS>& out) {
-    out.keep = 0;
+// reference's merge sums bucket-first.  The first walk counts kept outputs; after the
+// tile's output offset is known the second walk (kStore) writes them straight to the store.
+template <int W, typename T, bool kStore>
+__device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc, const uint64_t* sPk, const T* sPc,
+                                               uint32_t i, uint32_t ie, uint32_t j, uint32_t je,
+                                               const RotLayer<W>& L, const AmpTab<T>& A, const KeepProg& keep,
+                                               uint64_t* __restrict__ Ok, T* __restrict__ Oc,
+                                               unsigned long long out, unsigned int* s_hist) {
+    uint32_t count = 0;
     uint64_t a[2 * W], b[2 * W];
     if (i < ie) ld_row<W>(sSk, i, a);
     if (j < je) ld_row<W>(sPk, j, b);
+    while (i < ie || j < je) {
+        const bool takeS = (j >= je) || (i < ie && le_regs<W>(a, b));
+        uint64_t k[2 * W];
+        T v;
+        if (takeS) {
 #pragma unroll
-    for (int st = 0; st < SLOTS; ++st) {
-        if (i < ie || j < je) {
-            const bool takeS = (j >= je) || (i < ie && le_regs<W>(a, b));
-            T v;
-            if (takeS) {
-#pragma unroll
-                for (int w = 0; w < 2 * W; ++w) out.k[st][w] = a[w];
-                v = own_coeff<W, T>(L, A, a, sSc[i]);
-                if (j < je && eq_regs<W>(a, b)) {
-                    v = add_rn(v, sPc[j]);
-                    if (++j < je) ld_row<W>(sPk, j, b);
-                }
-                if (++i < ie) ld_row<W>(sSk, i, a);
-            } else {
-#pragma unroll
-                for (int w = 0; w < 2 * W; ++w) out.k[st][w] = b[w];
-                v = sPc[j];
+            for (int w = 0; w < 2 * W; ++w) k[w] = a[w];
+            v = own_coeff<W, T>(L, A, a, sSc[i]);
+            if (j < je && eq_regs<W>(a, b)) {
+                v = add_rn(v, sPc[j]);
                 if (++j < je) ld_row<W>(sPk, j, b);
             }
-            out.v[st] = v;
-            if (v != T(0) && keep_eval<W>(keep, out.k[st], to_f64(v))) out.keep |= 1u << st;
+            if (++i < ie) ld_row<W>(sSk, i, a);
+        } else {
+#pragma unroll
+            for (int w = 0; w < 2 * W; ++w) k[w] = b[w];
+            v = sPc[j];
+            if (++j < je) ld_row<W>(sPk, j, b);
+        }
+        if (v != T(0) && keep_eval<W>(keep, k, to_f64(v))) {
+            if (kStore) {
+                store_key<W>(Ok, out + count, k);
+                Oc[out + count] = v;
+                if (s_hist) atomicAdd(&s_hist[mag_key<T>(v) >> 52], 1u);
+            }
+            ++count;
         }
     }
-    return i >= ie && j >= je;
+    return count;
 }
 
 template <int W, typename T>
@@ -773,10 +770,8 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
     __syncthreads();
     const uint32_t i0 = s_si[tid], j0 = s_sj[tid];
     const uint32_t ie = max(s_si[tid + 1], i0), je = max(s_sj[tid + 1], j0);
-    WalkOut<W, T, ITEMS + 2> out;
-    if (!merge_walk<W, T, ITEMS + 2>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, A, keep, out))
-        raise_err(ctl, ERR_INTERNAL, 305);
-    const uint32_t count = __popc(out.keep);
+    const uint32_t count =
+        merge_walk<W, T, false>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, A, keep, nullptr, nullptr, 0ull, nullptr);
     unsigned int total;
     unsigned int excl = block_exclusive_sum<kBlock>(count, s_warp, total);
     if (tid < 32) {
@@ -796,16 +791,8 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
     __syncthreads();
     const unsigned long long off = s_outoff;
     if (!PS_GUARD(ctl, off + total <= out_cap, 304)) return;
-    unsigned long long pos = off + excl;
-#pragma unroll
-    for (int st = 0; st < ITEMS + 2; ++st) {
-        if ((out.keep >> st) & 1u) {
-            store_key<W>(Ok, pos, out.k[st]);
-            Oc[pos] = out.v[st];
-            if (topn_hist) atomicAdd(&s_hist[mag_key<T>(out.v[st]) >> 52], 1u);
-            ++pos;
-        }
-    }
+    merge_walk<W, T, true>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, A, keep, Ok, Oc, off + excl,
+                           topn_hist ? s_hist : nullptr);
     if (topn_hist) {
         __syncthreads();
         for (int q = tid; q < kTopnHistBins; q += kBlock)
