@@ -204,26 +204,36 @@ def dist_setup(n_gpus):
     return world, rank, local
 
 
-def dist_max(v, world):
+def _reduce(v, world, op):
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def dist_max(v, world):
+    import torch.distributed as dist
+
+    return _reduce(v, world, dist.ReduceOp.MAX if world > 1 else None)
 
 
 def dist_sum(v, world):
-    if world == 1:
-        return v
-    import torch
     import torch.distributed as dist
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(v, world, dist.ReduceOp.SUM if world > 1 else None)
+
+
+def replica_throughput(terms: float, device_ms: float, world: int) -> tuple:
+    """Whole-job terms/s over independent replicas: every rank's terms over the slowest rank's
+    device time (weak scaling).  Returns (value, max_ms, all_terms)."""
+    max_ms = dist_max(device_ms, world)
+    all_terms = dist_sum(terms, world)
+    return all_terms / (max_ms * 1e-3), max_ms, all_terms
 
 
 def barrier(world):
@@ -300,9 +310,7 @@ def run_ours(args, world, rank, local):
     g.close()
     del g
 
-    max_ms = dist_max(dev_ms, world)
-    all_terms = dist_sum(terms, world)
-    value = all_terms / (max_ms * 1e-3)
+    value, max_ms, all_terms = replica_throughput(terms, dev_ms, world)
 
     # --- end to end through the C ABI with pinned host buffers ---------------------------------
     if args.no_e2e:

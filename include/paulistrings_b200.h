@@ -245,6 +245,16 @@ ps_status ps_expectation_device_noalloc(const uint64_t* keys, const void* coeffs
                                         uint64_t n, const uint64_t* axis_x, const uint64_t* axis_z,
                                         const uint64_t* negative, double* out, void* stream);
 
+/* Failure injection for tests (FaultPlan, crates/paulistrings/src/engine/gpu/partition.rs:33-45),
+ * host-side only.  PS_FAULT_OOM: after `arg` more device allocations of this handle succeed,
+ * the next one fails as if the device were out of memory.  PS_FAULT_STALL: the next layer's
+ * merge skips its first tile, so the following tile's output-offset wait sees a flag nothing
+ * sets and gives up after `arg` polls (0: the default limit), reporting PS_ERR_TIMEOUT; the
+ * limit stays in force for the handle.  PS_FAULT_NONE disarms.  Either way the layer fails and
+ * the store keeps the last completed layer. */
+typedef enum ps_fault_kind { PS_FAULT_NONE = 0, PS_FAULT_OOM = 1, PS_FAULT_STALL = 2 } ps_fault_kind;
+ps_status ps_inject_fault(ps_sum* sum, int32_t kind, uint64_t arg);
+
 /* Wait for the handle's stream.  PartitionStorage::settle. */
 ps_status ps_synchronize(ps_sum* sum);
 

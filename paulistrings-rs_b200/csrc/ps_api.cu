@@ -51,6 +51,8 @@ struct ps_sum {
     Buf up_x, up_z, up_c, up_k, up_v0, up_v1, up_c0, up_st;  // ingest / readout staging, grow-only
     LevelList* levels = nullptr;  // host scratch
     KernelProf prof;
+    long long fault_oom_after = -1;   // failure injection: allocations left before one fails
+    bool fault_stall = false;         // failure injection: next merge skips its first tile
     std::string err;
 };
 
@@ -82,6 +84,19 @@ cudaError_t ensure(Buf& b, size_t bytes) {
     }
     b.bytes = bytes;
     return cudaSuccess;
+}
+
+// ensure() through the handle, so an injected allocation failure can take its place.
+cudaError_t ensure(ps_sum* s, Buf& b, size_t bytes) {
+    if (b.bytes >= bytes && b.p) return cudaSuccess;
+    if (s->fault_oom_after >= 0) {
+        if (s->fault_oom_after == 0) {
+            s->fault_oom_after = -1;
+            return cudaErrorMemoryAllocation;
+        }
+        --s->fault_oom_after;
+    }
+    return ensure(b, bytes);
 }
 
 void release(Buf& b) {
@@ -509,8 +524,8 @@ struct Engine {
         uint64_t want = rows < 1024 ? 1024 : rows;
         // grow by 1.5x so a slowly growing sum does not reallocate every layer
         if (s->cap[which] && want < s->cap[which] + s->cap[which] / 2) want = s->cap[which] + s->cap[which] / 2;
-        cudaError_t e = ensure(s->keys[which], want * kKeyBytes);
-        if (e == cudaSuccess) e = ensure(s->coef[which], want * sizeof(T));
+        cudaError_t e = ensure(s, s->keys[which], want * kKeyBytes);
+        if (e == cudaSuccess) e = ensure(s, s->coef[which], want * sizeof(T));
         if (e != cudaSuccess) {
             release(s->keys[which]);
             release(s->coef[which]);
@@ -518,8 +533,8 @@ struct Engine {
             cudaGetLastError();
             // retry at the exact size
             want = rows < 1024 ? 1024 : rows;
-            e = ensure(s->keys[which], want * kKeyBytes);
-            if (e == cudaSuccess) e = ensure(s->coef[which], want * sizeof(T));
+            e = ensure(s, s->keys[which], want * kKeyBytes);
+            if (e == cudaSuccess) e = ensure(s, s->coef[which], want * sizeof(T));
             if (e != cudaSuccess) {
                 release(s->keys[which]);
                 release(s->coef[which]);
@@ -541,8 +556,8 @@ struct Engine {
             return PS_OK;
         }
         cudaError_t e = cudaSuccess;
-        if ((e = ensure(s->up_x, n * W * 8)) != cudaSuccess || (e = ensure(s->up_z, n * W * 8)) != cudaSuccess ||
-            (e = ensure(s->up_c, n * 8)) != cudaSuccess || (e = ensure(s->up_v0, n * 4)) != cudaSuccess ||
+        if ((e = ensure(s, s->up_x, n * W * 8)) != cudaSuccess || (e = ensure(s, s->up_z, n * W * 8)) != cudaSuccess ||
+            (e = ensure(s, s->up_c, n * 8)) != cudaSuccess || (e = ensure(s, s->up_v0, n * 4)) != cudaSuccess ||
             (e = reserve_store(s, spare, n)) != cudaSuccess)
             return cuda_fail(s, e, "upload: allocation");
         cudaMemcpyAsync(s->up_x.p, x, n * W * 8, cudaMemcpyHostToDevice, s->stream);
@@ -562,10 +577,10 @@ struct Engine {
         uint64_t out_n = n;
         if (!sorted) {
             const size_t tiles = (n + StoreOps<W, T>::sort_tile() - 1) / StoreOps<W, T>::sort_tile();
-            if ((e = ensure(s->up_k, 2 * n * kKeyBytes)) != cudaSuccess || (e = ensure(s->up_v1, n * 4)) != cudaSuccess ||
-                (e = ensure(s->up_c0, n * sizeof(T))) != cudaSuccess ||
-                (e = ensure(s->up_st, (n / 2048 + 2) * sizeof(unsigned long long))) != cudaSuccess ||
-                (e = ensure(s->sort_status, tiles * 256 * sizeof(unsigned int))) != cudaSuccess)
+            if ((e = ensure(s, s->up_k, 2 * n * kKeyBytes)) != cudaSuccess || (e = ensure(s, s->up_v1, n * 4)) != cudaSuccess ||
+                (e = ensure(s, s->up_c0, n * sizeof(T))) != cudaSuccess ||
+                (e = ensure(s, s->up_st, (n / 2048 + 2) * sizeof(unsigned long long))) != cudaSuccess ||
+                (e = ensure(s, s->sort_status, tiles * 256 * sizeof(unsigned int))) != cudaSuccess)
                 return cuda_fail(s, e, "upload: sort scratch");
             s->sort.status = static_cast<unsigned int*>(s->sort_status.p);
             uint64_t* k0 = (uint64_t*)s->up_k.p;
@@ -599,8 +614,8 @@ struct Engine {
         if (cap < s->n) return set_err(s, PS_ERR_INVALID, "download: capacity below the term count");
         if (s->n == 0) return PS_OK;
         cudaError_t e;
-        if ((e = ensure(s->up_x, s->n * W * 8)) != cudaSuccess || (e = ensure(s->up_z, s->n * W * 8)) != cudaSuccess ||
-            (e = ensure(s->up_c, s->n * 8)) != cudaSuccess)
+        if ((e = ensure(s, s->up_x, s->n * W * 8)) != cudaSuccess || (e = ensure(s, s->up_z, s->n * W * 8)) != cudaSuccess ||
+            (e = ensure(s, s->up_c, s->n * 8)) != cudaSuccess)
             return cuda_fail(s, e, "download: allocation");
         e = StoreOps<W, T>::unpack(K(s, s->cur), C(s, s->cur), s->n, (uint64_t*)s->up_x.p, (uint64_t*)s->up_z.p,
                                    (double*)s->up_c.p, s->sms, s->stream, &s->prof);
@@ -628,14 +643,14 @@ struct Engine {
         cudaError_t e = reserve_store(s, spare, out_rows);
         if (e != cudaSuccess) return cuda_fail(s, e, "apply: output store");
         const uint64_t tiles_hi = out_rows / kMinTileRows + 4;
-        if ((e = ensure(s->status, tiles_hi * sizeof(unsigned long long))) != cudaSuccess ||
-            (e = ensure(s->bounds, (tiles_hi + 2) * sizeof(ulonglong2))) != cudaSuccess)
+        if ((e = ensure(s, s->status, tiles_hi * sizeof(unsigned long long))) != cudaSuccess ||
+            (e = ensure(s, s->bounds, (tiles_hi + 2) * sizeof(ulonglong2))) != cudaSuccess)
             return cuda_fail(s, e, "apply: scratch");
         if (a.L.partners) {
-            if ((e = ensure(s->pk, n * kKeyBytes)) != cudaSuccess || (e = ensure(s->pc, n * sizeof(T))) != cudaSuccess ||
-                (e = ensure(s->idx, n * 4)) != cudaSuccess || (e = ensure(s->dv, n * 2)) != cudaSuccess ||
-                (e = ensure(s->fv, n * 4)) != cudaSuccess ||
-                (e = ensure(s->slots, (n / kScanTileRows + 4) * sizeof(LevelSlot))) != cudaSuccess)
+            if ((e = ensure(s, s->pk, n * kKeyBytes)) != cudaSuccess || (e = ensure(s, s->pc, n * sizeof(T))) != cudaSuccess ||
+                (e = ensure(s, s->idx, n * 4)) != cudaSuccess || (e = ensure(s, s->dv, n * 2)) != cudaSuccess ||
+                (e = ensure(s, s->fv, n * 4)) != cudaSuccess ||
+                (e = ensure(s, s->slots, (n / kScanTileRows + 4) * sizeof(LevelSlot))) != cudaSuccess)
                 return cuda_fail(s, e, "apply: partner scratch");
         }
         a.Sk = K(s, s->cur);
@@ -669,6 +684,8 @@ struct Engine {
             s->hist_ready = false;
         }
         a.topn_hist = fuse_topn ? (unsigned int*)s->hist.p : nullptr;
+        a.inject_stall = s->fault_stall ? 1 : 0;
+        s->fault_stall = false;
         e = launch_rotation_layer<W, T>(a, s->stream);
         s->prof.resolve();
         if (e != cudaSuccess) return cuda_fail(s, e, "apply: rotation layer");
@@ -709,8 +726,8 @@ struct Engine {
             }
             const int spare = 1 - s->cur;
             cudaError_t e = reserve_store(s, spare, p.n);
-            if (e == cudaSuccess) e = ensure(s->cand, s->n * sizeof(uint64_t));
-            if (e == cudaSuccess) e = ensure(s->status, (s->n / 4096 + 4) * sizeof(unsigned long long));
+            if (e == cudaSuccess) e = ensure(s, s->cand, s->n * sizeof(uint64_t));
+            if (e == cudaSuccess) e = ensure(s, s->status, (s->n / 4096 + 4) * sizeof(unsigned long long));
             if (e != cudaSuccess) {
                 if (use_hist) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
                 return cuda_fail(s, e, "topn: scratch");
@@ -734,8 +751,8 @@ struct Engine {
     }
 
     static ps_status expectation(ps_sum* s, const uint64_t* ax, const uint64_t* az, const uint64_t* neg, double* out) {
-        cudaError_t e = ensure(s->partial, kExpectBlocks * sizeof(double));
-        if (e == cudaSuccess) e = ensure(s->dout, sizeof(double));
+        cudaError_t e = ensure(s, s->partial, kExpectBlocks * sizeof(double));
+        if (e == cudaSuccess) e = ensure(s, s->dout, sizeof(double));
         if (e != cudaSuccess) return cuda_fail(s, e, "expectation: scratch");
         e = StoreOps<W, T>::expectation(K(s, s->cur), C(s, s->cur), s->n, ax, az, neg, (double*)s->partial.p,
                                         (double*)s->dout.p, s->sms, s->stream, &s->prof);
@@ -821,6 +838,10 @@ ps_status ps_create(int32_t device, int32_t num_qubits, int32_t dtype, ps_sum** 
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&s->ctl, sizeof(Ctl));
     if (e == cudaSuccess) e = cudaMemsetAsync(s->ctl, 0, sizeof(Ctl), s->stream);
+    if (e == cudaSuccess) {
+        static const unsigned long long limit = (unsigned long long)kSpinLimit;
+        e = cudaMemcpy(&s->ctl->spin_limit, &limit, sizeof(limit), cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess) e = cudaMallocHost(&s->hcount, 64 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMallocHost(&s->hout, 8 * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&s->sort.hist, 16 * W * 256 * sizeof(unsigned int));
@@ -1004,6 +1025,29 @@ ps_status ps_read_profile(ps_sum* s, ps_kernel_profile* out, int32_t cap, int32_
         out[i].timed_launches = s->prof.timed[i];
         out[i].total_ms = s->prof.ms[i];
         out[i].algorithmic_bytes = s->prof.bytes[i];
+    }
+    return PS_OK;
+}
+
+ps_status ps_inject_fault(ps_sum* s, int32_t kind, uint64_t arg) {
+    if (!s) return PS_ERR_INVALID;
+    DeviceGuard g(s->device);
+    switch (kind) {
+    case PS_FAULT_NONE:
+        s->fault_oom_after = -1;
+        s->fault_stall = false;
+        break;
+    case PS_FAULT_OOM:
+        s->fault_oom_after = (long long)arg;
+        break;
+    case PS_FAULT_STALL: {
+        s->fault_stall = true;
+        unsigned long long limit = arg ? arg : (unsigned long long)kSpinLimit;
+        cudaError_t e = cudaMemcpy(&s->ctl->spin_limit, &limit, sizeof(limit), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_fail(s, e, "inject_fault");
+        break;
+    }
+    default: return PS_ERR_INVALID;
     }
     return PS_OK;
 }

@@ -27,9 +27,11 @@ enum : uint32_t {
     ERR_INTERNAL = 8u     // an invariant of the layer pipeline failed
 };
 
-// Spin limit of every look-back / barrier wait.  With __nanosleep(64) between polls this
-// is well over a second, far beyond any legitimate wait, and still finite.
+// Default spin limit of every look-back / barrier wait (Ctl::spin_limit): a few seconds of
+// polling, far beyond any legitimate wait, and still finite.
 constexpr long long kSpinLimit = 1LL << 22;
+
+__device__ __forceinline__ long long spin_limit(const Ctl* ctl) { return (long long)ctl->spin_limit; }
 
 __device__ __forceinline__ void raise_err(Ctl* ctl, uint32_t bit, uint32_t info) {
     if ((atomicOr(&ctl->err, bit) & bit) == 0) atomicExch(&ctl->err_info, info);
@@ -105,7 +107,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, Ctl* ctl, uint32_t info) {
     long long spins = 0;
     while (!mbar_try_wait(bar, parity)) {
-        if (++spins > kSpinLimit) {
+        if (++spins > spin_limit(ctl)) {
             raise_err(ctl, ERR_TIMEOUT, info);
             return false;
         }
@@ -300,7 +302,7 @@ __device__ __forceinline__ unsigned long long lookback_sum_warp(const unsigned l
         const int first_inc = inc ? __ffs(inc) - 1 : 32;
         const unsigned int need = first_inc >= 31 ? 0xffffffffu : ((2u << first_inc) - 1u);
         if (empty & need) {
-            if (++spins > kSpinLimit) {
+            if (++spins > spin_limit(ctl)) {
                 if (lane == 0) raise_err(ctl, ERR_TIMEOUT, info);
                 return acc;
             }

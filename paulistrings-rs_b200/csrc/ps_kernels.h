@@ -14,6 +14,7 @@ struct Ctl {
     unsigned int err;              // ERR_* bits
     unsigned int err_info;         // id of the first check that failed
     unsigned long long aux[8];     // small per-pass values (TopN boundary, quota, ...)
+    unsigned long long spin_limit; // polls before a bounded device wait gives up
 };
 
 // Lowered keep program (postfix), KeepProgram in the reference's device path.
@@ -163,6 +164,7 @@ struct RotationArgs {
     uint64_t* out_count;
     KernelProf* prof;
     unsigned int* topn_hist;  // when set, the merge histograms key >> 52 of its outputs (2048 bins)
+    int inject_stall;         // failure injection: the merge skips its first tile
 };
 
 template <int W, typename T>

@@ -297,7 +297,7 @@ __device__ __forceinline__ void level_lookback(LevelSlot* slots, unsigned int ti
         const int first_inc = inc ? __ffs(inc) - 1 : 32;
         const unsigned int need = first_inc >= 31 ? 0xffffffffu : ((2u << first_inc) - 1u);
         if (empty & need) {
-            if (++spins > kSpinLimit) {
+            if (++spins > spin_limit(ctl)) {
                 if (lane == 0) raise_err(ctl, ERR_TIMEOUT, info);
                 break;
             }
@@ -883,7 +883,10 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     }
     // 5. merge
     cudaMemsetAsync(a.status, 0, (size_t)mtiles * sizeof(unsigned long long), st);
-    cudaMemsetAsync(&ctl->tile_counter[3], 0, sizeof(unsigned int), st);
+    // failure injection: start the dispenser at tile 1, so tile 0 never publishes and tile 1's
+    // bounded look-back gives up
+    cudaMemsetAsync(&ctl->tile_counter[3], a.inject_stall ? 1 : 0, 1, st);
+    cudaMemsetAsync(reinterpret_cast<unsigned char*>(&ctl->tile_counter[3]) + 1, 0, 3, st);
     size_t smem = MergeSmem<W, T>::bytes;
     a.prof->begin(K_MERGE, (double)(a.n + m) * (16 * W + sizeof(T)), st);
     k_merge<W, T><<<mtiles, kBlock, smem, st>>>(a.Sk, a.Sc, a.n, a.Pk, a.Pc, m, a.bounds, mtiles, a.L, a.keep,

@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(kThreads) k_sort_pass(const uint64_t* __restri
                 unsigned int s = ld_acquire_u32(status + (size_t)t * 256 + b);
                 unsigned int f = s & ~kSValMask;
                 if (f == 0) {
-                    if (++spins > kSpinLimit) {
+                    if (++spins > spin_limit(ctl)) {
                         raise_err(ctl, ERR_TIMEOUT, 501);
                         break;
                     }

@@ -49,8 +49,11 @@ EXPORTED = (
     "ps_set_profiling",
     "ps_read_profile",
     "ps_expectation_device_noalloc",
+    "ps_inject_fault",
     "ps_synchronize",
 )
+
+PS_FAULT_NONE, PS_FAULT_OOM, PS_FAULT_STALL = 0, 1, 2
 
 NOALLOC_MAX_TERMS = 1 << 30
 
@@ -190,6 +193,7 @@ def lib():
     L.ps_set_profiling.argtypes = [vp, i32]
     L.ps_read_profile.argtypes = [vp, P(KernelProfile), i32, P(i32)]
     L.ps_expectation_device_noalloc.argtypes = [vp, vp, i32, i32, u64, vp, vp, vp, vp, vp]
+    L.ps_inject_fault.argtypes = [vp, i32, u64]
     L.ps_synchronize.argtypes = [vp]
     for name in EXPORTED:
         fn = getattr(L, name)

@@ -1,0 +1,64 @@
+"""Failure handling without a GPU fault (needs a CUDA device).
+
+Failures are injected on the host through ``ps_inject_fault`` (the reference's FaultPlan):
+an allocation that reports out-of-memory, and a merge launch that skips its first tile so the
+next tile's output-offset wait polls a flag nothing sets until its (shortened) bounded limit.
+In both cases the call must fail with its status, the store must keep the last completed
+layer, and the handle must keep working.
+"""
+
+import numpy as np
+import pytest
+
+import paulistrings_b200 as ps
+from paulistrings_b200 import _lib, truncation, workloads
+from tests._util import assert_same_terms, oracle_arrays, oracle_channels, oracle_sum
+
+pytestmark = pytest.mark.gpu
+
+
+def _sum(num_qubits=32, count=20000, seed=9):
+    x, z, c = workloads.random_observable(num_qubits, count, seed=seed)
+    g = ps.GpuPauliSum(num_qubits)
+    g.upload(x, z, c)
+    return g, (x, z, c)
+
+
+def test_injected_oom_fails_the_layer_and_keeps_the_store():
+    g, _ = _sum()
+    before = g.download()
+    circ = workloads.random_pair_layers(32, 1, seed=4)
+    _lib.check(_lib.lib().ps_inject_fault(g._h, _lib.PS_FAULT_OOM, 0), g._h, "inject")
+    with pytest.raises(MemoryError):
+        g.propagate(circ, truncation.coeff(1e-12))
+    assert_same_terms(g.download(), before, what="after-oom")
+    # the handle still works, and matches the oracle from the same state
+    g.propagate(circ, truncation.coeff(1e-12))
+    o = oracle_sum(32, *before)
+    o.propagate(oracle_channels(circ), {"keep": [("coeff", 1e-12)]})
+    assert_same_terms(g.download(), oracle_arrays(o), what="after-recovery")
+
+
+def test_injected_stall_times_out_boundedly_and_keeps_the_store():
+    g, _ = _sum()
+    before = g.download()
+    circ = ps.Circuit(32)
+    circ.pauli_rotation("XY", [0, 1], 0.4)
+    _lib.check(_lib.lib().ps_inject_fault(g._h, _lib.PS_FAULT_STALL, 1 << 14), g._h, "inject")
+    with pytest.raises(_lib.PauliStringsError) as info:
+        g.propagate(circ, truncation.coeff(1e-12))
+    assert info.value.status == _lib.PS_ERR_TIMEOUT
+    assert_same_terms(g.download(), before, what="after-stall")
+    g.propagate(circ, truncation.coeff(1e-12))
+    o = oracle_sum(32, *before)
+    o.propagate(oracle_channels(circ), {"keep": [("coeff", 1e-12)]})
+    assert_same_terms(g.download(), oracle_arrays(o), what="after-stall-recovery")
+
+
+def test_injection_can_be_disarmed():
+    g, _ = _sum(count=2000)
+    _lib.check(_lib.lib().ps_inject_fault(g._h, _lib.PS_FAULT_OOM, 0), g._h, "inject")
+    _lib.check(_lib.lib().ps_inject_fault(g._h, _lib.PS_FAULT_NONE, 0), g._h, "disarm")
+    circ = workloads.random_pair_layers(32, 1, seed=2)
+    g.propagate(circ, truncation.coeff(1e-12))
+    assert len(g) > 2000
