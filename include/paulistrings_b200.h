@@ -247,7 +247,7 @@ ps_status ps_expectation_device_noalloc(const uint64_t* keys, const void* coeffs
 
 /* Failure injection for tests (FaultPlan, crates/paulistrings/src/engine/gpu/partition.rs:33-45),
  * host-side only.  PS_FAULT_OOM: after `arg` more device allocations of this handle succeed,
- * the next one fails as if the device were out of memory.  PS_FAULT_STALL: the next layer's
+ * every further one fails as if the device were out of memory, until PS_FAULT_NONE.  PS_FAULT_STALL: the next layer's
  * merge skips its first tile, so the following tile's output-offset wait sees a flag nothing
  * sets and gives up after `arg` polls (0: the default limit), reporting PS_ERR_TIMEOUT; the
  * limit stays in force for the handle.  PS_FAULT_NONE disarms.  Either way the layer fails and

@@ -51,7 +51,7 @@ struct ps_sum {
     Buf up_x, up_z, up_c, up_k, up_v0, up_v1, up_c0, up_st;  // ingest / readout staging, grow-only
     LevelList* levels = nullptr;  // host scratch
     KernelProf prof;
-    long long fault_oom_after = -1;   // failure injection: allocations left before one fails
+    long long fault_oom_after = -1;   // failure injection: allocations left before all fail
     bool fault_stall = false;         // failure injection: next merge skips its first tile
     std::string err;
 };
@@ -90,10 +90,7 @@ cudaError_t ensure(Buf& b, size_t bytes) {
 cudaError_t ensure(ps_sum* s, Buf& b, size_t bytes) {
     if (b.bytes >= bytes && b.p) return cudaSuccess;
     if (s->fault_oom_after >= 0) {
-        if (s->fault_oom_after == 0) {
-            s->fault_oom_after = -1;
-            return cudaErrorMemoryAllocation;
-        }
+        if (s->fault_oom_after == 0) return cudaErrorMemoryAllocation;  // until disarmed
         --s->fault_oom_after;
     }
     return ensure(b, bytes);

@@ -31,6 +31,7 @@ def test_injected_oom_fails_the_layer_and_keeps_the_store():
     _lib.check(_lib.lib().ps_inject_fault(g._h, _lib.PS_FAULT_OOM, 0), g._h, "inject")
     with pytest.raises(MemoryError):
         g.propagate(circ, truncation.coeff(1e-12))
+    _lib.check(_lib.lib().ps_inject_fault(g._h, _lib.PS_FAULT_NONE, 0), g._h, "disarm")
     assert_same_terms(g.download(), before, what="after-oom")
     # the handle still works, and matches the oracle from the same state
     g.propagate(circ, truncation.coeff(1e-12))
