@@ -161,8 +161,10 @@ class OracleSum:
             lib().pso_get(self._h, keys.ctypes.data, coeffs.ctypes.data)
         return keys, coeffs
 
-    def apply(self, channel, adjoint=False, policy=None, sorted_engine=False):
+    def apply(self, channel, adjoint=False, policy=None, sorted_engine=False, threads=None):
         arr = channel_array([channel])
+        if threads is not None:
+            lib().pso_set_threads(int(threads))
         pol = policy_struct(policy)
         fn = lib().pso_apply_channel_sorted if sorted_engine else lib().pso_apply_channel
         rc = fn(self._h, arr, int(bool(adjoint)), ctypes.byref(pol) if pol else None)

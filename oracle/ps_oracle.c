@@ -507,14 +507,38 @@ static void topn(pso_sum* s, uint64_t n) {
         double c = coef_at(s, i);
         m[i] = c * c;
     }
-    double* sorted = (double*)malloc(total * sizeof(double));
-    memcpy(sorted, m, total * sizeof(double));
-    qsort(sorted, total, sizeof(double), mag_desc_cmp);
-    double boundary = sorted[n - 1];
+    /* n-th largest |c|^2 by quickselect on a copy (select_nth_unstable, builtin.rs:107-111),
+     * NaN ordered below every number */
+    double* sel = (double*)malloc(total * sizeof(double));
+    memcpy(sel, m, total * sizeof(double));
+    size_t lo = 0, hi = total - 1, kth = (size_t)n - 1;
+    while (lo < hi) {
+        double pivot = sel[lo + (hi - lo) / 2];
+        size_t i = lo, j = hi;
+        while (i <= j) {
+            while (mag_desc_cmp(&sel[i], &pivot) < 0) ++i;
+            while (mag_desc_cmp(&sel[j], &pivot) > 0) --j;
+            if (i <= j) {
+                double t = sel[i];
+                sel[i] = sel[j];
+                sel[j] = t;
+                ++i;
+                if (j == 0) break;
+                --j;
+            }
+        }
+        if (kth <= j)
+            hi = j;
+        else if (kth >= i)
+            lo = i;
+        else
+            break;
+    }
+    double boundary = sel[kth];
+    free(sel);
     size_t above = 0;
-    for (size_t i = 0; i + 1 < n; ++i)
-        if (sorted[i] > boundary) ++above;
-    free(sorted);
+    for (size_t i = 0; i < total; ++i)
+        if (!isnan(m[i]) && (isnan(boundary) || m[i] > boundary)) ++above;
     size_t quota = (size_t)n - above;
     int K = 2 * s->W;
     size_t w = 0;
@@ -638,14 +662,288 @@ double pso_expectation(const pso_sum* s, const uint64_t* axis_x, const uint64_t*
 }
 
 /* ------------------------------------------------------------------------ */
-/* sorted-store engine for CPU timing (bucketed host engine's shape)         */
+/* sorted-store engine for CPU timing, in the reference host engine's shape:  */
+/* rotation scan, linear partner order, merge-join with keep_term, all       */
+/* parallel over chunks (crates/paulistrings/src/engine/bucketed.rs:376-490, */
+/* bucketed/rotation_layer.rs:159-229, bucketed/partner_order.rs:16-140).    */
+/* Same results as pso_apply_channel, bit for bit.                           */
 /* ------------------------------------------------------------------------ */
 
 static int g_threads = 0;
 void pso_set_threads(int threads) { g_threads = threads; }
 
+static int nthreads(void) {
+#ifdef _OPENMP
+    return g_threads > 0 ? g_threads : omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+/* first differing bit rank (0 = most significant) of two distinct keys */
+static unsigned div_rank(const uint64_t* a, const uint64_t* b, int W) {
+    for (int i = 0; i < 2 * W; ++i) {
+        uint64_t d = a[i] ^ b[i];
+        if (d) return 64u * (unsigned)i + (unsigned)__builtin_clzll(d);
+    }
+    return 0xFFFFFFFFu;
+}
+
+typedef struct {
+    int W, dtype;
+    size_t n, cap;
+    uint64_t* keys;
+    double* c64;
+    float* c32;
+} cols_t;
+
+static void cols_reserve(cols_t* c, size_t cap) {
+    if (cap <= c->cap) return;
+    c->keys = (uint64_t*)realloc(c->keys, cap * 2 * (size_t)c->W * 8);
+    if (c->dtype == PSO_F64)
+        c->c64 = (double*)realloc(c->c64, cap * sizeof(double));
+    else
+        c->c32 = (float*)realloc(c->c32, cap * sizeof(float));
+    c->cap = cap;
+}
+
+/* pattern amplitude of the own row (identity entry) and partner (generator entry) */
+static void rot_amps(const prepared_t* p, const uint64_t* k, int W, int dtype, double* a0, double* a1, float* f0,
+                     float* f1, int* emits) {
+    if (p->wide) {
+        int ac = anticommutes(k, p->gx, p->gz, W);
+        *emits = ac;
+        *a0 = ac ? p->cos64 : 1.0;
+        *f0 = ac ? p->cos32 : 1.0f;
+        if (ac) {
+            unsigned total = (1u + product_phase(k, p->gx, p->gz, W)) & 3u;
+            *a1 = (total & 2u) ? -p->sin64 : p->sin64;
+            *f1 = (total & 2u) ? -p->sin32 : p->sin32;
+        } else {
+            *a1 = 0.0;
+            *f1 = 0.0f;
+        }
+        return;
+    }
+    unsigned sp = support_bits(p, k, W);
+    *a0 = p->e[0].a64[sp];
+    *f0 = p->e[0].a32[sp];
+    if (p->num_entries > 1) {
+        *a1 = p->e[1].a64[sp];
+        *f1 = p->e[1].a32[sp];
+    } else {
+        *a1 = 0.0;
+        *f1 = 0.0f;
+    }
+    *emits = dtype == PSO_F64 ? (*a1 != 0.0) : (*f1 != 0.0f);
+}
+
 int pso_apply_channel_sorted(pso_sum* s, const pso_channel* ch, int adjoint, const pso_policy* policy) {
-    return pso_apply_channel(s, ch, adjoint, policy);
+    prepared_t p;
+    const int W = s->W, K = 2 * W;
+    if (prepare(ch, adjoint, W, s->nq, &p)) return -1;
+    const int rotation = p.wide || (p.num_entries == 2 && p.e[0].local_delta == 0) ||
+                         (p.num_entries == 1 && p.e[0].local_delta == 0);
+    if (!rotation) return pso_apply_channel(s, ch, adjoint, policy);  /* general tables: naive path */
+    const size_t n = s->n;
+    const int T = nthreads();
+    const uint64_t* gx = p.wide ? p.gx : p.e[p.num_entries > 1 ? 1 : 0].mx;
+    const uint64_t* gz = p.wide ? p.gz : p.e[p.num_entries > 1 ? 1 : 0].mz;
+
+    /* 1. scan: anticommuting rows, in row order, per chunk then concatenated */
+    size_t* cnt = (size_t*)calloc((size_t)T + 1, sizeof(size_t));
+    uint32_t* hit = (uint32_t*)malloc((n + 1) * sizeof(uint32_t));
+#pragma omp parallel num_threads(T)
+    {
+#ifdef _OPENMP
+        int t = omp_get_thread_num();
+#else
+        int t = 0;
+#endif
+        size_t lo = n * (size_t)t / (size_t)T, hi = n * (size_t)(t + 1) / (size_t)T, c = 0;
+        for (size_t i = lo; i < hi; ++i) {
+            double a0, a1;
+            float f0, f1;
+            int e;
+            rot_amps(&p, s->keys + i * K, W, s->dtype, &a0, &a1, &f0, &f1, &e);
+            c += (size_t)e;
+        }
+        cnt[t + 1] = c;
+#pragma omp barrier
+#pragma omp single
+        for (int q = 0; q < T; ++q) cnt[q + 1] += cnt[q];
+        size_t o = cnt[t];
+        for (size_t i = lo; i < hi; ++i) {
+            double a0, a1;
+            float f0, f1;
+            int e;
+            rot_amps(&p, s->keys + i * K, W, s->dtype, &a0, &a1, &f0, &f1, &e);
+            if (e) hit[o++] = (uint32_t)i;
+        }
+    }
+    const size_t m = cnt[T];
+    free(cnt);
+
+    /* 2. partner order: slot of each partner in key order of k ^ g (linear scans over the
+     * first-difference ranks; partner_order.rs:10-14) */
+    uint32_t levels[2 * 64 * PSO_MAX_W];
+    int nl = 0;
+    for (int wi = 0; wi < K; ++wi) {
+        uint64_t bits = wi < W ? gx[wi] : gz[wi - W];
+        while (bits) {
+            int b = 63 - __builtin_clzll(bits);
+            levels[nl++] = 64u * (unsigned)wi + (unsigned)(63 - b);
+            bits &= ~(1ull << b);
+        }
+    }
+    int64_t* shift = (int64_t*)calloc(m + 1, sizeof(int64_t));
+    uint32_t* dv = (uint32_t*)malloc((m + 1) * sizeof(uint32_t));
+    dv[0] = 0;
+#pragma omp parallel for num_threads(T) schedule(static)
+    for (size_t j = 1; j < m; ++j) dv[j] = div_rank(s->keys + (size_t)hit[j - 1] * K, s->keys + (size_t)hit[j] * K, W);
+    for (int l = 0; l < nl; ++l) {
+        const uint32_t L = levels[l];
+        size_t st = 0, sp = (size_t)-1;
+        for (size_t j = 0; j < m; ++j) {   /* forward: upper halves move down */
+            if (j == 0 || dv[j] < L) st = j;
+            if (j != 0 && dv[j] == L) sp = j;
+            if (sp != (size_t)-1 && sp > st) shift[j] -= (int64_t)(sp - st);
+        }
+        size_t e = m, q = m;
+        for (size_t jj = m; jj-- > 0;) {   /* backward: lower halves move up */
+            if (q < e) shift[jj] += (int64_t)(e - q);
+            if (jj != 0 && dv[jj] < L) e = jj;
+            if (jj != 0 && dv[jj] == L) q = jj;
+        }
+    }
+    cols_t P = {W, s->dtype, 0, 0, NULL, NULL, NULL};
+    cols_reserve(&P, m + 1);
+#pragma omp parallel for num_threads(T) schedule(static)
+    for (size_t j = 0; j < m; ++j) {
+        const size_t row = hit[j], d = (size_t)((int64_t)j + shift[j]);
+        const uint64_t* k = s->keys + row * K;
+        double a0, a1;
+        float f0, f1;
+        int e;
+        rot_amps(&p, k, W, s->dtype, &a0, &a1, &f0, &f1, &e);
+        for (int w = 0; w < W; ++w) {
+            P.keys[d * K + w] = k[w] ^ gx[w];
+            P.keys[d * K + W + w] = k[W + w] ^ gz[w];
+        }
+        if (s->dtype == PSO_F64)
+            P.c64[d] = s->c64[row] * a1;
+        else
+            P.c32[d] = s->c32[row] * f1;
+    }
+    P.n = m;
+    free(shift);
+    free(dv);
+    free(hit);
+
+    /* 3. merge-join own rows (scaled by a0) with the partners, own first on equal keys, keep
+     * on the sum, drop exact zeros; merge-path split across threads */
+    cols_t O = {W, s->dtype, 0, 0, NULL, NULL, NULL};
+    cols_reserve(&O, n + m + 1);
+    size_t* ocnt = (size_t*)calloc((size_t)T + 1, sizeof(size_t));
+    size_t* obase = (size_t*)calloc((size_t)T + 1, sizeof(size_t));
+#pragma omp parallel num_threads(T)
+    {
+#ifdef _OPENMP
+        int t = omp_get_thread_num();
+#else
+        int t = 0;
+#endif
+        size_t tot = n + m;
+        size_t d0 = tot * (size_t)t / (size_t)T, d1 = tot * (size_t)(t + 1) / (size_t)T;
+        size_t bnd[2][2];
+        for (int side = 0; side < 2; ++side) {
+            size_t dd = side ? d1 : d0;
+            size_t lo = dd > m ? dd - m : 0, hi = dd < n ? dd : n;
+            while (lo < hi) {
+                size_t mid = (lo + hi) / 2;
+                if (key_cmp(s->keys + mid * K, P.keys + (dd - 1 - mid) * K, W) <= 0)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            size_t i = lo, j = dd - lo;
+            if (i > 0 && j < m && key_cmp(s->keys + (i - 1) * K, P.keys + j * K, W) == 0) ++j;
+            bnd[side][0] = i;
+            bnd[side][1] = j;
+        }
+        size_t i = bnd[0][0], j = bnd[0][1], ie = bnd[1][0], je = bnd[1][1];
+        /* thread-local output, then one copy at the thread's offset */
+        size_t cap = (ie - i) + (je > j ? je - j : 0) + 1;
+        uint64_t* lk = (uint64_t*)malloc(cap * K * 8);
+        double* l64 = (double*)malloc(cap * sizeof(double));
+        float* l32 = (float*)malloc(cap * sizeof(float));
+        size_t c = 0;
+        while (i < ie || j < je) {
+            int takeS = (j >= je) || (i < ie && key_cmp(s->keys + i * K, P.keys + j * K, W) <= 0);
+            const uint64_t* k;
+            double v64 = 0.0;
+            float v32 = 0.0f;
+            if (takeS) {
+                k = s->keys + i * K;
+                double a0, a1;
+                float f0, f1;
+                int e;
+                rot_amps(&p, k, W, s->dtype, &a0, &a1, &f0, &f1, &e);
+                v64 = s->dtype == PSO_F64 ? s->c64[i] * a0 : 0.0;
+                v32 = s->dtype == PSO_F32 ? s->c32[i] * f0 : 0.0f;
+                if (j < je && key_cmp(k, P.keys + j * K, W) == 0) {
+                    if (s->dtype == PSO_F64)
+                        v64 = v64 + P.c64[j];
+                    else
+                        v32 = v32 + P.c32[j];
+                    ++j;
+                }
+                ++i;
+            } else {
+                k = P.keys + j * K;
+                v64 = s->dtype == PSO_F64 ? P.c64[j] : 0.0;
+                v32 = s->dtype == PSO_F32 ? P.c32[j] : 0.0f;
+                ++j;
+            }
+            double v = s->dtype == PSO_F64 ? v64 : (double)v32;
+            if (v != 0.0 && keep_eval(policy, k, W, v)) {
+                memcpy(lk + c * K, k, (size_t)K * 8);
+                l64[c] = v64;
+                l32[c] = v32;
+                ++c;
+            }
+        }
+        ocnt[t + 1] = c;
+#pragma omp barrier
+#pragma omp single
+        for (int q = 0; q < T; ++q) obase[q + 1] = obase[q] + ocnt[q + 1];
+        size_t o = obase[t];
+        memcpy(O.keys + o * K, lk, c * K * 8);
+        if (s->dtype == PSO_F64)
+            memcpy(O.c64 + o, l64, c * sizeof(double));
+        else
+            memcpy(O.c32 + o, l32, c * sizeof(float));
+        free(lk);
+        free(l64);
+        free(l32);
+    }
+    O.n = obase[T];
+    free(ocnt);
+    free(obase);
+    free(P.keys);
+    free(P.c64);
+    free(P.c32);
+    /* swap in */
+    free(s->keys);
+    free(s->c64);
+    free(s->c32);
+    s->keys = O.keys;
+    s->c64 = O.c64;
+    s->c32 = O.c32;
+    s->n = O.n;
+    s->cap = O.cap;
+    pso_finalize_layer(s, policy);
+    return 0;
 }
 
 int pso_propagate_sorted(pso_sum* s, const pso_channel* chans, size_t num_channels,
