@@ -88,18 +88,39 @@ typedef struct ps_policy {
     ps_pass passes[PS_MAX_PASSES];
 } ps_policy;
 
-/* ---- channels (the Channel plug-in's built-ins, crates/paulistrings-py/src/circuit.rs:269-321) */
+/* ---- channels (the Channel plug-in's built-ins, crates/paulistrings-py/src/circuit.rs:232-345,
+ * crates/paulistrings/src/channel/ptm/{clifford,unitary,noise}.rs) */
 typedef enum ps_channel_kind {
-    PS_CH_PAULI_ROTATION = 1, /* exp(-i param P / 2), P = paulis[j] ('X','Y','Z') on qubits[j] */
-    PS_CH_DEPOLARIZING = 2    /* one qubit, param = p: X, Y, Z scaled by 1 - 4p/3 (ptm/noise.rs:12-16) */
+    PS_CH_PAULI_ROTATION = 1,    /* exp(-i param P / 2), P = paulis[j] ('X','Y','Z') on qubits[j] */
+    PS_CH_DEPOLARIZING = 2,      /* one qubit, param = p: X, Y, Z scaled by 1 - 4p/3 (ptm/noise.rs:12-16) */
+    PS_CH_HADAMARD = 3,          /* X -> Z, Z -> X, Y -> -Y */
+    PS_CH_PHASE = 4,             /* S: X -> Y, Y -> -X */
+    PS_CH_PHASE_DAGGER = 5,      /* S^dagger: X -> -Y, Y -> X */
+    PS_CH_PAULI_X = 6,
+    PS_CH_PAULI_Y = 7,
+    PS_CH_PAULI_Z = 8,
+    PS_CH_CNOT = 9,              /* qubits[0] control, qubits[1] target */
+    PS_CH_CZ = 10,
+    PS_CH_SWAP = 11,
+    PS_CH_UNITARY = 12,          /* matrix: 2^k x 2^k complex, row-major, re/im interleaved, qubits[0] the
+                                    more significant tensor factor; k = num_support in {1, 2} */
+    PS_CH_DEPHASING = 13,        /* param = p: X, Y scaled by 1 - 2p */
+    PS_CH_PAULI_CHANNEL = 14,    /* params = (px, py, pz) */
+    PS_CH_DEPOLARIZING_2Q = 15,  /* two qubits, param = p: every non-identity Pauli scaled by 1 - 16p/15 */
+    PS_CH_AMPLITUDE_DAMPING = 16 /* param = gamma */
 } ps_channel_kind;
 
 typedef struct ps_channel {
     int32_t kind;             /* ps_channel_kind */
     int32_t num_support;
     const uint32_t* qubits;
-    const char* paulis;       /* num_support characters; ignored for depolarizing */
+    const char* paulis;       /* PS_CH_PAULI_ROTATION: num_support characters */
     double param;
+    const double* matrix;     /* PS_CH_UNITARY only */
+    double params[3];         /* PS_CH_PAULI_CHANNEL only */
+    int32_t adjoint;          /* nonzero: the channel's adjoint (PtmChannel::adjoint, ptm.rs:126-149;
+                                 a rotation's negated angle), composed with the layer direction */
+    int32_t reserved;
 } ps_channel;
 
 /* ---- prepared per-layer table (Prepared, crates/paulistrings/src/channel/prepared.rs:345-350) */
@@ -133,7 +154,7 @@ typedef struct ps_table {
 typedef enum ps_layer_path {
     PS_PATH_RESCALE = 1,      /* key-preserving rescale + keep */
     PS_PATH_ROTATION = 2,     /* partner reorder + merge-path join */
-    PS_PATH_SORT = 3          /* branch records + radix sort + segmented dedup */
+    PS_PATH_SORT = 3          /* general table: branch records + radix sort + segmented dedup */
 } ps_layer_path;
 
 typedef struct ps_layer_stats {
@@ -257,6 +278,14 @@ ps_status ps_inject_fault(ps_sum* sum, int32_t kind, uint64_t arg);
 
 /* Wait for the handle's stream.  PartitionStorage::settle. */
 ps_status ps_synchronize(ps_sum* sum);
+
+/* Sum each output key's contributions on the sort path (general tables, three or more
+ * contributions per key) with TwoSum compensation: the rounding error of every addition is
+ * carried and added back once at the end of the run.  Off by default, which adds in plain
+ * arithmetic in the order of the reference's layer.  No counterpart in the reference; meant
+ * for PS_F32 sums, where it keeps dense-table layers close to a float64 run.  The rotation and
+ * rescale paths add at most two contributions per key, where compensation changes nothing. */
+ps_status ps_set_compensated_sums(ps_sum* sum, int32_t enabled);
 
 #ifdef __cplusplus
 }

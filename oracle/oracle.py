@@ -3,9 +3,12 @@
 TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()`` and
 ``bench.py``'s CPU-baseline leg, as the checker.  The product package never imports it.
 
-Channels are ``(kind, paulis, qubits, param)`` tuples: kind ``"rotation"``
-(``exp(-i param P / 2)``, ``paulis`` one of ``XYZ`` per qubit) or ``"depolarize"``
-(single qubit, ``param = p``).  Policies are ``{"keep": [...postfix nodes...],
+Channels are ``(kind, paulis, qubits, param[, extra])`` tuples: kind ``"rotation"``
+(``exp(-i param P / 2)``, ``paulis`` one of ``XYZ`` per qubit), ``"depolarize"`` (single
+qubit, ``param = p``), the Cliffords ``"h" "s" "sdg" "x" "y" "z" "cnot" "cz" "swap"``,
+``"unitary"`` (``extra["matrix"]``: 2^k x 2^k complex), ``"dephase"``, ``"pauli_channel"``
+(``extra["params"] = (px, py, pz)``), ``"depolarize2"`` and ``"amplitude_damping"``;
+``extra["adjoint"]`` applies the channel's adjoint.  Policies are ``{"keep": [...postfix nodes...],
 "passes": [("topn", n), ...]}`` with nodes ``("coeff", eps)``, ``("weight", k)``,
 ``("and",)``, ``("or",)``, ``("true",)``.
 """
@@ -25,7 +28,9 @@ LIB_PATH = HERE / "_build" / "libps_oracle.so"
 F64, F32 = 0, 1
 _KEEP = {"true": 0, "coeff": 1, "weight": 2, "and": 3, "or": 4}
 _PASS = {"topn": 1}
-_KIND = {"rotation": 1, "depolarize": 2}
+_KIND = {"rotation": 1, "depolarize": 2, "h": 3, "s": 4, "sdg": 5, "x": 6, "y": 7, "z": 8, "cnot": 9,
+         "cz": 10, "swap": 11, "unitary": 12, "dephase": 13, "pauli_channel": 14, "depolarize2": 15,
+         "amplitude_damping": 16}
 
 
 class _Policy(ctypes.Structure):
@@ -47,6 +52,9 @@ class _Channel(ctypes.Structure):
         ("qubits", ctypes.c_uint32 * 64),
         ("paulis", ctypes.c_char * 64),
         ("param", ctypes.c_double),
+        ("params", ctypes.c_double * 3),
+        ("matrix", ctypes.c_double * 32),
+        ("adjoint", ctypes.c_int32),
     ]
 
 
@@ -81,6 +89,8 @@ def lib():
         L.pso_expectation.restype = ctypes.c_double
         L.pso_expectation.argtypes = [vp, vp, vp, vp]
         L.pso_set_threads.argtypes = [ctypes.c_int]
+        L.pso_prepare_table.argtypes = [ctypes.POINTER(_Channel), ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp,
+                                        vp, vp, vp]
         _lib = L
     return _lib
 
@@ -108,7 +118,9 @@ def policy_struct(policy) -> _Policy | None:
 
 def channel_array(channels):
     arr = (_Channel * max(1, len(channels)))()
-    for i, (kind, paulis, qubits, param) in enumerate(channels):
+    for i, ch in enumerate(channels):
+        kind, paulis, qubits, param = ch[:4]
+        extra = ch[4] if len(ch) > 4 else {}
         c = arr[i]
         c.kind = _KIND[kind]
         c.num_support = len(qubits)
@@ -116,7 +128,35 @@ def channel_array(channels):
             c.qubits[j] = int(q)
         c.paulis = (paulis or "").encode()
         c.param = float(param)
+        for j, v in enumerate(extra.get("params", ())):
+            c.params[j] = float(v)
+        if "matrix" in extra:
+            u = np.asarray(extra["matrix"], dtype=np.complex128).reshape(-1)
+            for j, v in enumerate(u):
+                c.matrix[2 * j] = float(v.real)
+                c.matrix[2 * j + 1] = float(v.imag)
+        c.adjoint = 1 if extra.get("adjoint") else 0
     return arr
+
+
+def prepare_table(channel, num_qubits: int, adjoint: bool = False):
+    """The oracle's prepared table of one channel: ``None`` for a wide rotation, else
+    ``(qubits, [(local_delta, amplitudes[16]), ...])``; ``ValueError`` when declined."""
+    arr = channel_array([channel])
+    W = width_for(num_qubits)
+    wide, k, ne = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+    q = (ctypes.c_uint32 * 2)()
+    deltas = (ctypes.c_uint32 * 16)()
+    amps = (ctypes.c_double * 256)()
+    rc = lib().pso_prepare_table(arr, int(bool(adjoint)), W, num_qubits, ctypes.addressof(wide), ctypes.addressof(k),
+                                 ctypes.addressof(q), ctypes.addressof(ne), ctypes.addressof(deltas),
+                                 ctypes.addressof(amps))
+    if rc:
+        raise ValueError(f"oracle declined channel {channel}")
+    if wide.value:
+        return None
+    ents = [(int(deltas[e]), [float(amps[16 * e + s]) for s in range(16)]) for e in range(ne.value)]
+    return tuple(int(q[j]) for j in range(k.value)), ents
 
 
 def width_for(num_qubits: int) -> int:

@@ -358,8 +358,276 @@ static int build_generator(const pso_channel* ch, int W, int nq, uint64_t* gx, u
     return 0;
 }
 
+/* ------------------------------------------------------------------------ */
+/* PTM channels: ptm.rs, ptm/clifford.rs, ptm/unitary.rs, ptm/noise.rs       */
+/* ------------------------------------------------------------------------ */
+
+/* num-complex 0.4 arithmetic: (a+bi)(c+di) = (ac-bd) + (ad+bc)i, parts rounded once */
+typedef struct {
+    double re, im;
+} cplx;
+
+static cplx cx(double re, double im) {
+    cplx v;
+    v.re = re;
+    v.im = im;
+    return v;
+}
+static cplx cx_mul(cplx a, cplx b) { return cx(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+static cplx cx_add(cplx a, cplx b) { return cx(a.re + b.re, a.im + b.im); }
+static int cx_zero(cplx a) { return a.re == 0.0 && a.im == 0.0; }
+/* a / (c + 0i): ((a.re c + a.im 0) / (c c + 0 0), (a.im c - a.re 0) / (c c + 0 0)) */
+static cplx cx_div_real(cplx a, double c) {
+    double nrm = c * c + 0.0 * 0.0;
+    return cx((a.re * c + a.im * 0.0) / nrm, (a.im * c - a.re * 0.0) / nrm);
+}
+
+/* pauli_matrix (unitary.rs:82-90), I, X, Z, Y index order */
+static void pauli_2x2(int idx, cplx* m) {
+    cplx o = cx(1, 0), z = cx(0, 0), mo = cx(-1, 0), i = cx(0, 1), mi = cx(0, -1);
+    cplx t[4][4] = {{o, z, z, o}, {z, o, o, z}, {o, z, z, mo}, {z, mi, i, z}};
+    for (int q = 0; q < 4; ++q) m[q] = t[idx][q];
+}
+
+/* matmul (unitary.rs:92-106): zero a[i][k] skipped, sums from zero in k order */
+static void cx_matmul(int N, const cplx* a, const cplx* b, cplx* out) {
+    for (int q = 0; q < N * N; ++q) out[q] = cx(0, 0);
+    for (int i = 0; i < N; ++i)
+        for (int k = 0; k < N; ++k) {
+            cplx aik = a[i * N + k];
+            if (cx_zero(aik)) continue;
+            for (int j = 0; j < N; ++j) out[i * N + j] = cx_add(out[i * N + j], cx_mul(aik, b[k * N + j]));
+        }
+}
+
+/* the 2^k x 2^k matrix of local Pauli s; kron(P(s & 3), P(s >> 2)) for k = 2 (unitary.rs:37, 116-121) */
+static void local_pauli_matrix(int k, int s, cplx* m) {
+    cplx a[4], b[4];
+    if (k == 1) {
+        pauli_2x2(s, m);
+        return;
+    }
+    pauli_2x2(s & 3, a);
+    pauli_2x2(s >> 2, b);
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) m[r * 4 + c] = cx_mul(a[(r / 2) * 2 + c / 2], b[(r % 2) * 2 + c % 2]);
+}
+
+/* unitary_1q / unitary_2q (unitary.rs:13-53): assert_unitary (1e-10, NaN fails), then
+ * ptm[s][t] = clean(tr(P_t . U P_s U^dagger) / 2^k), clean snapping parts below 1e-12. */
+static int unitary_ptm(int k, const double* mat, cplx ptm[16][16]) {
+    int d = 1 << k, dim = 1 << (2 * k);
+    cplx U[16], Ud[16], prod[16];
+    for (int r = 0; r < d; ++r)
+        for (int c = 0; c < d; ++c) U[r * d + c] = cx(mat[2 * (r * d + c)], mat[2 * (r * d + c) + 1]);
+    for (int r = 0; r < d; ++r)
+        for (int c = 0; c < d; ++c) Ud[r * d + c] = cx(U[c * d + r].re, -U[c * d + r].im);
+    cx_matmul(d, Ud, U, prod);
+    double largest = 0.0;
+    for (int r = 0; r < d; ++r)
+        for (int c = 0; c < d; ++c) {
+            double dr = prod[r * d + c].re - (r == c ? 1.0 : 0.0), di = prod[r * d + c].im;
+            double e = hypot(dr, di);
+            if (e > largest || isnan(e)) largest = e;
+        }
+    if (!(largest <= 1e-10)) return -1;
+    for (int s = 0; s < dim; ++s) {
+        cplx Ps[16], t1[16], conj[16];
+        local_pauli_matrix(k, s, Ps);
+        cx_matmul(d, U, Ps, t1);
+        cx_matmul(d, t1, Ud, conj);
+        for (int t = 0; t < dim; ++t) {
+            cplx Pt[16], m[16], tr = cx(0, 0);
+            local_pauli_matrix(k, t, Pt);
+            cx_matmul(d, Pt, conj, m);
+            for (int i = 0; i < d; ++i) tr = cx_add(tr, m[i * d + i]);
+            cplx v = cx_div_real(tr, (double)d);
+            if (fabs(v.re) < 1e-12) v.re = 0.0;
+            if (fabs(v.im) < 1e-12) v.im = 0.0;
+            ptm[s][t] = v;
+        }
+    }
+    return 0;
+}
+
+/* clifford_2q (clifford.rs:83-111): the signed permutation multiplied out from the images of
+ * X0, Z0, X1, Z1 (packed x0 | z0 << 1 | x1 << 2 | z1 << 3), one i per input Y. */
+static void clifford_2q_table(const unsigned images[4], cplx ptm[16][16]) {
+    for (int index = 0; index < 16; ++index) {
+        uint64_t prod[2] = {0, 0}; /* one-word key on qubits 0 and 1 */
+        unsigned phase = 0;
+        for (int g = 0; g < 4; ++g) {
+            if (!((index >> g) & 1)) continue;
+            unsigned im = images[g];
+            uint64_t ox = (uint64_t)(im & 1u) | ((uint64_t)((im >> 2) & 1u) << 1);
+            uint64_t oz = (uint64_t)((im >> 1) & 1u) | ((uint64_t)((im >> 3) & 1u) << 1);
+            phase += product_phase(prod, &ox, &oz, 1);
+            prod[0] ^= ox;
+            prod[1] ^= oz;
+        }
+        unsigned y_count = (unsigned)(((index & 1) & ((index >> 1) & 1)) + (((index >> 2) & 1) & ((index >> 3) & 1)));
+        phase = (phase + y_count) & 3u;
+        unsigned t = (unsigned)((prod[0] & 1u) | ((prod[1] & 1u) << 1) | (((prod[0] >> 1) & 1u) << 2) |
+                                (((prod[1] >> 1) & 1u) << 3));
+        ptm[index][t] = cx(phase == 2u ? -1.0 : 1.0, 0.0);
+    }
+}
+
+static void signed_perm_1q(const unsigned image[4], unsigned negated, cplx ptm[16][16]) {
+    for (int s = 0; s < 4; ++s) ptm[s][image[s]] = cx(((negated >> s) & 1u) ? -1.0 : 1.0, 0.0);
+}
+
+static int in_unit(double v) { return v >= 0.0 && v <= 1.0; }
+
+/* The constructor-order PTM of a named channel (k support qubits); -1 when the
+ * constructor would panic. */
+static int named_ptm(const pso_channel* ch, int* k_out, cplx ptm[16][16]) {
+    for (int a = 0; a < 16; ++a)
+        for (int b = 0; b < 16; ++b) ptm[a][b] = cx(0, 0);
+    static const unsigned H[4] = {0, 2, 1, 3}, S[4] = {0, 3, 2, 1}, ID[4] = {0, 1, 2, 3};
+    /* packed generator images: pack(x0, z0, x1, z1) = x0 | z0 << 1 | x1 << 2 | z1 << 3 */
+    static const unsigned CNOT[4] = {1u | 4u, 2u, 4u, 2u | 8u};
+    static const unsigned CZ[4] = {1u | 8u, 2u, 2u | 4u, 8u};
+    static const unsigned SWAP[4] = {4u, 8u, 1u, 2u};
+    int k = 1;
+    switch (ch->kind) {
+    case PSO_CH_DEPOLARIZE: {
+        if (!in_unit(ch->param)) return -1;
+        double sc = 1.0 - 4.0 * ch->param / 3.0;
+        ptm[0][0] = cx(1, 0);
+        for (int q = 1; q < 4; ++q) ptm[q][q] = cx(sc, 0);
+        break;
+    }
+    case PSO_CH_HADAMARD: signed_perm_1q(H, 0x8u, ptm); break;
+    case PSO_CH_PHASE: signed_perm_1q(S, 0x8u, ptm); break;
+    case PSO_CH_PHASE_DAGGER: {
+        /* phase_gate(q).adjoint(): the inverse signed permutation (ptm.rs:128-137) */
+        unsigned inv[4], neg = 0;
+        for (unsigned s = 0; s < 4; ++s) {
+            inv[S[s]] = s;
+            neg |= ((0x8u >> s) & 1u) << S[s];
+        }
+        signed_perm_1q(inv, neg, ptm);
+        break;
+    }
+    case PSO_CH_PAULI_X: signed_perm_1q(ID, 0xCu, ptm); break;
+    case PSO_CH_PAULI_Y: signed_perm_1q(ID, 0x6u, ptm); break;
+    case PSO_CH_PAULI_Z: signed_perm_1q(ID, 0xAu, ptm); break;
+    case PSO_CH_CNOT: k = 2; clifford_2q_table(CNOT, ptm); break;
+    case PSO_CH_CZ: k = 2; clifford_2q_table(CZ, ptm); break;
+    case PSO_CH_SWAP: k = 2; clifford_2q_table(SWAP, ptm); break;
+    case PSO_CH_UNITARY:
+        k = ch->num_support;
+        if (k != 1 && k != 2) return -1;
+        if (unitary_ptm(k, ch->matrix, ptm)) return -1;
+        break;
+    case PSO_CH_DEPHASING: {
+        if (!in_unit(ch->param)) return -1;
+        double sc = 1.0 - 2.0 * ch->param;
+        ptm[0][0] = cx(1, 0);
+        ptm[1][1] = cx(sc, 0);
+        ptm[2][2] = cx(1, 0);
+        ptm[3][3] = cx(sc, 0);
+        break;
+    }
+    case PSO_CH_PAULI_CHANNEL: {
+        double px = ch->params[0], py = ch->params[1], pz = ch->params[2];
+        if (!in_unit(px) || !in_unit(py) || !in_unit(pz) || !(px + py + pz <= 1.0)) return -1;
+        ptm[0][0] = cx(1, 0);
+        ptm[1][1] = cx(1.0 - 2.0 * (py + pz), 0);
+        ptm[2][2] = cx(1.0 - 2.0 * (px + py), 0);
+        ptm[3][3] = cx(1.0 - 2.0 * (px + pz), 0);
+        break;
+    }
+    case PSO_CH_DEPOLARIZING_2Q: {
+        if (!in_unit(ch->param)) return -1;
+        k = 2;
+        double sc = 1.0 - 16.0 * ch->param / 15.0;
+        for (int q = 0; q < 16; ++q) ptm[q][q] = cx(q ? sc : 1.0, 0);
+        break;
+    }
+    case PSO_CH_AMPLITUDE_DAMPING: {
+        double g = ch->param;
+        if (!in_unit(g)) return -1;
+        double tr = sqrt(1.0 - g);
+        ptm[0][0] = cx(1, 0);
+        ptm[0][2] = cx(g, 0);
+        ptm[1][1] = cx(tr, 0);
+        ptm[2][2] = cx(1.0 - g, 0);
+        ptm[3][3] = cx(tr, 0);
+        break;
+    }
+    default: return -1;
+    }
+    *k_out = k;
+    return 0;
+}
+
+/* push_deltas (prepared.rs:257-281) then convert to the real type (prepared.rs:214-233):
+ * one entry per local delta the table reaches, ascending; an imaginary part above 1e-12
+ * declines the table. */
+static int push_table(prepared_t* p, cplx table[16][16], int W) {
+    int dim = 1 << (2 * p->k);
+    int has[16] = {0};
+    for (int s = 0; s < dim; ++s)
+        for (int t = 0; t < dim; ++t)
+            if (!cx_zero(table[s][t])) has[s ^ t] = 1;
+    for (int d = 0; d < dim; ++d) {
+        if (!has[d]) continue;
+        entry_t* e = &p->e[p->num_entries++];
+        e->local_delta = (unsigned)d;
+        lift(p, (unsigned)d, e->mx, e->mz, W);
+        for (int s = 0; s < dim; ++s) {
+            cplx a = table[s][s ^ d];
+            if (!(fabs(a.im) <= 1e-12)) return -1;
+            e->a64[s] = a.re;
+            e->a32[s] = (float)a.re;
+        }
+    }
+    return 0;
+}
+
+/* RotationLayer::of Clifford residue rule (bucketed/rotation_layer.rs:101-122): on a
+ * rotation-shaped table whose identity amplitudes are rounding residues of the generator
+ * amplitudes, strings move instead of splitting. */
+static void clifford_residue(prepared_t* p) {
+    if (p->num_entries != 2 || p->e[0].local_delta != 0) return;
+    int dim = 1 << (2 * p->k);
+    entry_t* e0 = &p->e[0];
+    entry_t* e1 = &p->e[1];
+    unsigned delta = e1->local_delta;
+    const double eps = 2.220446049250313e-16;
+    for (int prec = 0; prec < 2; ++prec) {
+        int clifford = 1, shaped = 1;
+        for (int s = 0; s < dim; ++s) {
+            double a0 = prec ? (double)e0->a32[s] : e0->a64[s];
+            double a1 = prec ? (double)e1->a32[s] : e1->a64[s];
+            double b1 = prec ? (double)e1->a32[s ^ delta] : e1->a64[s ^ delta];
+            if (a1 == 0.0) {
+                if (a0 != 1.0) shaped = 0;
+            } else {
+                if (b1 == 0.0) shaped = 0;
+                clifford &= (a0 * a0 <= eps * eps * (a1 * a1));
+            }
+        }
+        if (shaped && clifford) {
+            for (int s = 0; s < dim; ++s) {
+                if ((prec ? (double)e1->a32[s] : e1->a64[s]) == 0.0) continue;
+                if (prec)
+                    e0->a32[s] = 0.0f;
+                else
+                    e0->a64[s] = 0.0;
+            }
+        }
+    }
+}
+
 static int prepare(const pso_channel* ch, int adjoint, int W, int nq, prepared_t* p) {
     memset(p, 0, sizeof(*p));
+    adjoint = (adjoint != 0) ^ (ch->adjoint != 0);
+    cplx table[16][16];
+    for (int a = 0; a < 16; ++a)
+        for (int b = 0; b < 16; ++b) table[a][b] = cx(0, 0);
     if (ch->kind == PSO_CH_ROTATION) {
         uint64_t gx[PSO_MAX_W], gz[PSO_MAX_W];
         if (build_generator(ch, W, nq, gx, gz)) return -1;
@@ -390,17 +658,15 @@ static int prepare(const pso_channel* ch, int adjoint, int W, int nq, prepared_t
         }
         p->k = k;
         int dim = 1 << (2 * k);
-        double table[16][16];
-        memset(table, 0, sizeof(table));
         /* probe_table: apply on each local basis Pauli with coefficient 1 */
         for (int s = 0; s < dim; ++s) {
             uint64_t key[2 * PSO_MAX_W];
             lift(p, (unsigned)s, key, key + W, W);
             if (!anticommutes(key, gx, gz, W)) {
-                table[s][s] += 1.0;
+                table[s][s].re += 1.0;
                 continue;
             }
-            table[s][s] += 1.0 * cs;
+            table[s][s].re += 1.0 * cs;
             unsigned total = (1u + product_phase(key, gx, gz, W)) & 3u;
             double sgn = (total & 2u) ? -1.0 : 1.0; /* real mul_phase: even phase only */
             uint64_t out[2 * PSO_MAX_W];
@@ -409,76 +675,56 @@ static int prepare(const pso_channel* ch, int adjoint, int W, int nq, prepared_t
                 out[W + i] = key[W + i] ^ gz[i];
             }
             unsigned t = support_bits(p, out, W);
-            table[s][t] += sgn * sn;
+            table[s][t].re += sgn * sn;
         }
-        /* push_deltas (prepared.rs:257-281): one entry per realized delta, ascending */
-        int has[16] = {0};
+    } else {
+        /* a PtmChannel: transfer_matrix (ptm.rs:248-263), transposed for the adjoint and
+         * reordered to ascending-qubit local indices */
+        cplx ptm[16][16];
+        int k = 0;
+        if (named_ptm(ch, &k, ptm)) return -1;
+        if (ch->num_support != k) return -1;
+        for (int j = 0; j < k; ++j)
+            if ((int)ch->qubits[j] >= nq) return -1;
+        if (k == 2 && ch->qubits[0] == ch->qubits[1]) return -1;
+        int reversed = k == 2 && ch->qubits[0] > ch->qubits[1];
+        p->k = k;
+        p->q[0] = reversed ? ch->qubits[1] : ch->qubits[0];
+        p->q[1] = k == 2 ? (reversed ? ch->qubits[0] : ch->qubits[1]) : 0;
+        int dim = 1 << (2 * k);
         for (int s = 0; s < dim; ++s)
-            for (int t = 0; t < dim; ++t)
-                if (table[s][t] != 0.0) has[s ^ t] = 1;
-        for (int d = 0; d < dim; ++d) {
-            if (!has[d]) continue;
-            entry_t* e = &p->e[p->num_entries++];
-            e->local_delta = (unsigned)d;
-            lift(p, (unsigned)d, e->mx, e->mz, W);
-            for (int s = 0; s < dim; ++s) {
-                e->a64[s] = table[s][s ^ d];
-                e->a32[s] = (float)e->a64[s];
-            }
-        }
-        /* RotationLayer::of Clifford residue rule (bucketed/rotation_layer.rs:101-122):
-         * on a rotation-shaped table whose identity amplitudes are rounding residues of the
-         * generator amplitudes, strings move instead of splitting. */
-        if (p->num_entries == 2 && p->e[0].local_delta == 0) {
-            entry_t* e0 = &p->e[0];
-            entry_t* e1 = &p->e[1];
-            unsigned delta = e1->local_delta;
-            const double eps = 2.220446049250313e-16;
-            for (int prec = 0; prec < 2; ++prec) {
-                int clifford = 1, shaped = 1;
-                for (int s = 0; s < dim; ++s) {
-                    double a0 = prec ? (double)e0->a32[s] : e0->a64[s];
-                    double a1 = prec ? (double)e1->a32[s] : e1->a64[s];
-                    double b1 = prec ? (double)e1->a32[s ^ delta] : e1->a64[s ^ delta];
-                    if (a1 == 0.0) {
-                        if (a0 != 1.0) shaped = 0;
-                    } else {
-                        if (b1 == 0.0) shaped = 0;
-                        clifford &= (a0 * a0 <= eps * eps * (a1 * a1));
-                    }
+            for (int t = 0; t < dim; ++t) {
+                if (cx_zero(ptm[s][t])) continue;
+                int row = adjoint ? t : s, col = adjoint ? s : t;
+                if (reversed) {
+                    row = ((row & 3) << 2) | (row >> 2);
+                    col = ((col & 3) << 2) | (col >> 2);
                 }
-                if (shaped && clifford) {
-                    for (int s = 0; s < dim; ++s) {
-                        if ((prec ? (double)e1->a32[s] : e1->a64[s]) == 0.0) continue;
-                        if (prec)
-                            e0->a32[s] = 0.0f;
-                        else
-                            e0->a64[s] = 0.0;
-                    }
-                }
+                table[row][col] = cx_add(table[row][col], ptm[s][t]);
             }
-        }
-        return 0;
     }
-    if (ch->kind == PSO_CH_DEPOLARIZE) {
-        if (ch->num_support != 1 || (int)ch->qubits[0] >= nq) return -1;
-        double pr = ch->param;
-        if (!(pr >= 0.0 && pr <= 1.0)) return -1;
-        double scale = 1.0 - 4.0 * pr / 3.0;
-        p->k = 1;
-        p->q[0] = ch->qubits[0];
-        p->num_entries = 1;
-        entry_t* e = &p->e[0];
-        memset(e->mx, 0, sizeof(e->mx));
-        memset(e->mz, 0, sizeof(e->mz));
-        double diag[4] = {1.0, scale, scale, scale};
-        for (int s = 0; s < 4; ++s) {
-            e->a64[s] = diag[s];
-            e->a32[s] = (float)diag[s];
-        }
-        return 0;
+    if (push_table(p, table, W)) return -1;
+    clifford_residue(p);
+    return 0;
+}
+
+/* The prepared table of one channel, for comparing table builders: wide rotations report
+ * wide = 1 and nothing else; local tables their support, entries (ascending local delta) and
+ * float64 amplitudes amps[16 * e + s]. */
+int pso_prepare_table(const pso_channel* ch, int adjoint, int W, int nq, int* wide, int* k, uint32_t* qubits,
+                      int* num_entries, uint32_t* deltas, double* amps) {
+    prepared_t p;
+    if (W < 1 || W > PSO_MAX_W || prepare(ch, adjoint, W, nq, &p)) return -1;
+    *wide = p.wide;
+    *k = p.k;
+    qubits[0] = p.q[0];
+    qubits[1] = p.q[1];
+    *num_entries = p.num_entries;
+    for (int e = 0; e < p.num_entries; ++e) {
+        deltas[e] = p.e[e].local_delta;
+        for (int s = 0; s < 16; ++s) amps[16 * e + s] = p.e[e].a64[s];
     }
-    return -1;
+    return 0;
 }
 
 /* ------------------------------------------------------------------------ */

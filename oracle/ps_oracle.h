@@ -11,7 +11,11 @@
  *   real mul_phase      crates/paulistrings/src/coefficient.rs:107-114
  *   rotation apply      crates/paulistrings/src/channel/rotation.rs:43-77
  *   local table probe   crates/paulistrings/src/channel/prepared.rs:214-281, 401-493
- *   depolarizing scale  crates/paulistrings/src/channel/ptm/noise.rs:12-16
+ *   PTM channels        crates/paulistrings/src/channel/ptm.rs:126-149 (adjoint), 248-263
+ *                       (transfer_matrix), ptm/clifford.rs:10-111, ptm/unitary.rs:13-127,
+ *                       ptm/noise.rs:7-80; complex arithmetic as num-complex 0.4
+ *                       (mul, add, division by (d, 0)); real conversion with |im| <= 1e-12
+ *                       (coefficient.rs:20, 97-99)
  *   naive layer         crates/paulistrings/src/test_support/oracle.rs:21-54
  *   threshold / weight  crates/paulistrings/src/truncation/builtin.rs:28-59
  *   TopN (+NaN, ties)   crates/paulistrings/src/truncation/builtin.rs:73-129, 210-239
@@ -59,9 +63,23 @@ typedef struct pso_policy {
     uint64_t pass_n[4];
 } pso_policy;
 
-/* channel kinds */
+/* channel kinds (same numbers as the product's C ABI) */
 #define PSO_CH_ROTATION 1     /* exp(-i theta P / 2); paulis[j] in "XYZ" on qubits[j] */
 #define PSO_CH_DEPOLARIZE 2   /* single-qubit depolarizing, param = p */
+#define PSO_CH_HADAMARD 3
+#define PSO_CH_PHASE 4
+#define PSO_CH_PHASE_DAGGER 5
+#define PSO_CH_PAULI_X 6
+#define PSO_CH_PAULI_Y 7
+#define PSO_CH_PAULI_Z 8
+#define PSO_CH_CNOT 9         /* qubits[0] control */
+#define PSO_CH_CZ 10
+#define PSO_CH_SWAP 11
+#define PSO_CH_UNITARY 12     /* matrix: 2^k x 2^k complex row-major, re/im interleaved */
+#define PSO_CH_DEPHASING 13
+#define PSO_CH_PAULI_CHANNEL 14 /* params = px, py, pz */
+#define PSO_CH_DEPOLARIZING_2Q 15
+#define PSO_CH_AMPLITUDE_DAMPING 16
 
 typedef struct pso_channel {
     int32_t kind;
@@ -69,6 +87,9 @@ typedef struct pso_channel {
     uint32_t qubits[64];
     char paulis[64];
     double param;
+    double params[3];
+    double matrix[32];
+    int32_t adjoint;          /* the channel's own adjoint, composed with the layer direction */
 } pso_channel;
 
 typedef struct pso_sum pso_sum;
@@ -86,6 +107,11 @@ void pso_get(const pso_sum* s, uint64_t* keys, double* coeffs);
 /* One channel layer (naive: emit, hash-accumulate, keep on sums, drop exact zeros, sort)
  * followed by the policy's layer passes.  adjoint != 0 applies the adjoint channel. */
 int pso_apply_channel(pso_sum* s, const pso_channel* ch, int adjoint, const pso_policy* policy);
+/* The prepared table of one channel (support, entries ascending by local delta, float64
+ * amplitudes amps[16 * e + s]); wide rotations set *wide only.  -1 when the channel is
+ * declined. */
+int pso_prepare_table(const pso_channel* ch, int adjoint, int W, int nq, int* wide, int* k, uint32_t* qubits,
+                      int* num_entries, uint32_t* deltas, double* amps);
 /* The policy's layer passes alone. */
 void pso_finalize_layer(pso_sum* s, const pso_policy* policy);
 /* The whole circuit; direction 0 = forward, 1 = heisenberg (reverse order, adjoint channels).

@@ -5,6 +5,7 @@
 // and the handle flips to the spare only when every kernel of the layer finished without
 // a device-side error, so a failed layer leaves the last completed layer in place
 // (crates/paulistrings/src/engine/gpu/driver.rs:44).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -46,6 +47,7 @@ struct ps_sum {
     Buf pk, pc;
     Buf idx, dv, fv, slots, status, bounds, hist, cand, partial, dout;
     bool hist_ready = false;  // hist holds the TopN digit-1 histogram of the current store
+    bool compensated = false; // sort-path dedup sums runs with TwoSum compensation
     SortScratch sort{};
     Buf sort_status;
     Buf up_x, up_z, up_c, up_k, up_v0, up_v1, up_c0, up_st;  // ingest / readout staging, grow-only
@@ -281,6 +283,202 @@ void push_deltas(ps_table& t, const double (&table)[16][16], int W) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// PTM channels (crates/paulistrings/src/channel/ptm.rs:248-263, ptm/clifford.rs,
+// ptm/unitary.rs, ptm/noise.rs).  Local index per qubit: x | z << 1 (I 0, X 1, Z 2, Y 3);
+// the constructor's first qubit in the low two bits.  ptm[s][t]: input s -> output t in the
+// Schroedinger map; the adjoint reads the transpose.
+// ---------------------------------------------------------------------------
+struct Cx {
+    double re, im;
+};
+inline Cx cmul(Cx a, Cx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+inline Cx cadd(Cx a, Cx b) { return {a.re + b.re, a.im + b.im}; }
+
+// Pauli matrix of local index (I, X, Z, Y order), 2x2
+void pauli_mat(int idx, Cx (&m)[2][2]) {
+    const Cx z{0, 0}, o{1, 0}, mo{-1, 0}, i{0, 1}, mi{0, -1};
+    switch (idx) {
+    case 0: m[0][0] = o; m[0][1] = z; m[1][0] = z; m[1][1] = o; break;
+    case 1: m[0][0] = z; m[0][1] = o; m[1][0] = o; m[1][1] = z; break;
+    case 2: m[0][0] = o; m[0][1] = z; m[1][0] = z; m[1][1] = mo; break;
+    default: m[0][0] = z; m[0][1] = mi; m[1][0] = i; m[1][1] = z; break;
+    }
+}
+
+// P_s as a 2^k x 2^k matrix; for k = 2, kron(P(s & 3), P(s >> 2)), the first qubit the more
+// significant tensor factor (ptm/unitary.rs:42)
+void local_pauli(int k, int s, Cx (&m)[4][4]) {
+    Cx a[2][2], b[2][2];
+    if (k == 1) {
+        pauli_mat(s, a);
+        for (int r = 0; r < 2; ++r)
+            for (int c = 0; c < 2; ++c) m[r][c] = a[r][c];
+        return;
+    }
+    pauli_mat(s & 3, a);
+    pauli_mat(s >> 2, b);
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) m[r][c] = cmul(a[r / 2][c / 2], b[r % 2][c % 2]);
+}
+
+// ptm[s][t] = tr(P_t U P_s U^dagger) / 2^k, parts within 1e-12 of zero snapped to zero
+// (ptm/unitary.rs:13-53, 123-127); false if U is not unitary to 1e-10 or an entry is complex.
+bool unitary_ptm(int k, const double* mat, double (&ptm)[16][16], std::string& why) {
+    const int d = 1 << k, dim = 1 << (2 * k);
+    Cx U[4][4], Ud[4][4];
+    for (int r = 0; r < d; ++r)
+        for (int c = 0; c < d; ++c) {
+            U[r][c] = {mat[2 * (r * d + c)], mat[2 * (r * d + c) + 1]};
+            if (!std::isfinite(U[r][c].re) || !std::isfinite(U[r][c].im)) {
+                why = "unitary: non-finite entry";
+                return false;
+            }
+        }
+    for (int r = 0; r < d; ++r)
+        for (int c = 0; c < d; ++c) Ud[r][c] = {U[c][r].re, -U[c][r].im};
+    double dev = 0.0;
+    for (int r = 0; r < d; ++r)
+        for (int c = 0; c < d; ++c) {
+            Cx acc{0, 0};
+            for (int q = 0; q < d; ++q) acc = cadd(acc, cmul(Ud[r][q], U[q][c]));
+            acc.re -= (r == c) ? 1.0 : 0.0;
+            dev = std::max(dev, std::hypot(acc.re, acc.im));
+        }
+    if (!(dev <= 1e-10)) {
+        why = "unitary: the matrix is not unitary to 1e-10";
+        return false;
+    }
+    for (int s = 0; s < dim; ++s) {
+        Cx Ps[4][4], T1[4][4], C[4][4];
+        local_pauli(k, s, Ps);
+        for (int r = 0; r < d; ++r)
+            for (int c = 0; c < d; ++c) {
+                Cx acc{0, 0};
+                for (int q = 0; q < d; ++q) acc = cadd(acc, cmul(U[r][q], Ps[q][c]));
+                T1[r][c] = acc;
+            }
+        for (int r = 0; r < d; ++r)
+            for (int c = 0; c < d; ++c) {
+                Cx acc{0, 0};
+                for (int q = 0; q < d; ++q) acc = cadd(acc, cmul(T1[r][q], Ud[q][c]));
+                C[r][c] = acc;
+            }
+        for (int t = 0; t < dim; ++t) {
+            Cx Pt[4][4];
+            local_pauli(k, t, Pt);
+            Cx tr{0, 0};
+            for (int r = 0; r < d; ++r)
+                for (int q = 0; q < d; ++q) tr = cadd(tr, cmul(Pt[r][q], C[q][r]));
+            double re = tr.re / d, im = tr.im / d;
+            if (std::fabs(re) < 1e-12) re = 0.0;
+            if (std::fabs(im) < 1e-12) im = 0.0;
+            if (!(std::fabs(im) <= 1e-12)) {  // Coefficient::from_complex64, coefficient.rs:97-99
+                why = "unitary: complex transfer-matrix entry (a real coefficient type needs a real PTM)";
+                return false;
+            }
+            ptm[s][t] = re;
+        }
+    }
+    return true;
+}
+
+// The named PTM channels as ptm[s][t] in constructor order; k = support size.
+bool named_ptm(const ps_channel* ch, int& k, double (&ptm)[16][16], std::string& why) {
+    std::memset(ptm, 0, sizeof ptm);
+    auto signed_perm_1q = [&](const int (&image)[4], unsigned negated) {
+        k = 1;
+        for (int s = 0; s < 4; ++s) ptm[s][image[s]] = ((negated >> s) & 1u) ? -1.0 : 1.0;
+    };
+    auto prob = [&](double v, const char* name) {
+        if (!(v >= 0.0 && v <= 1.0)) {
+            why = std::string(name) + " must lie in [0, 1]";
+            return false;
+        }
+        return true;
+    };
+    static const double kCnot[32] = {1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 0,
+                                     0, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 0, 1, 0, 0, 0};
+    static const double kCz[32] = {1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 0,
+                                   0, 0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, -1, 0};
+    static const double kSwap[32] = {1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0,
+                                     0, 0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 0};
+    switch (ch->kind) {
+    case PS_CH_HADAMARD: signed_perm_1q({0, 2, 1, 3}, 0b1000u); return true;
+    case PS_CH_PHASE: signed_perm_1q({0, 3, 2, 1}, 0b1000u); return true;
+    case PS_CH_PHASE_DAGGER: {  // the transpose of S
+        signed_perm_1q({0, 3, 2, 1}, 0b1000u);
+        double t[16][16];
+        std::memcpy(t, ptm, sizeof t);
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b) ptm[a][b] = t[b][a];
+        return true;
+    }
+    case PS_CH_PAULI_X: signed_perm_1q({0, 1, 2, 3}, 0b1100u); return true;
+    case PS_CH_PAULI_Y: signed_perm_1q({0, 1, 2, 3}, 0b0110u); return true;
+    case PS_CH_PAULI_Z: signed_perm_1q({0, 1, 2, 3}, 0b1010u); return true;
+    case PS_CH_CNOT: k = 2; return unitary_ptm(2, kCnot, ptm, why);
+    case PS_CH_CZ: k = 2; return unitary_ptm(2, kCz, ptm, why);
+    case PS_CH_SWAP: k = 2; return unitary_ptm(2, kSwap, ptm, why);
+    case PS_CH_UNITARY:
+        k = ch->num_support;
+        if (k != 1 && k != 2) {
+            why = "unitary: one or two qubits";
+            return false;
+        }
+        if (!ch->matrix) {
+            why = "unitary: missing matrix";
+            return false;
+        }
+        return unitary_ptm(k, ch->matrix, ptm, why);
+    case PS_CH_DEPHASING: {
+        if (!prob(ch->param, "dephasing: p")) return false;
+        k = 1;
+        const double sc = 1.0 - 2.0 * ch->param;
+        ptm[0][0] = 1.0;
+        ptm[1][1] = sc;
+        ptm[2][2] = 1.0;
+        ptm[3][3] = sc;
+        return true;
+    }
+    case PS_CH_PAULI_CHANNEL: {
+        const double px = ch->params[0], py = ch->params[1], pz = ch->params[2];
+        if (!prob(px, "pauli_channel: px") || !prob(py, "pauli_channel: py") || !prob(pz, "pauli_channel: pz"))
+            return false;
+        if (!(px + py + pz <= 1.0)) {
+            why = "pauli_channel: px + py + pz must be at most 1";
+            return false;
+        }
+        k = 1;
+        ptm[0][0] = 1.0;
+        ptm[1][1] = 1.0 - 2.0 * (py + pz);
+        ptm[2][2] = 1.0 - 2.0 * (px + py);
+        ptm[3][3] = 1.0 - 2.0 * (px + pz);
+        return true;
+    }
+    case PS_CH_DEPOLARIZING_2Q: {
+        if (!prob(ch->param, "depolarizing_2q: p")) return false;
+        k = 2;
+        const double sc = 1.0 - 16.0 * ch->param / 15.0;
+        for (int q = 0; q < 16; ++q) ptm[q][q] = q ? sc : 1.0;
+        return true;
+    }
+    case PS_CH_AMPLITUDE_DAMPING: {
+        const double g = ch->param;
+        if (!prob(g, "amplitude_damping: gamma")) return false;
+        k = 1;
+        const double tr = std::sqrt(1.0 - g);
+        ptm[0][0] = 1.0;
+        ptm[0][2] = g;
+        ptm[1][1] = tr;
+        ptm[2][2] = 1.0 - g;
+        ptm[3][3] = tr;
+        return true;
+    }
+    default: why = "unknown channel kind"; return false;
+    }
+}
+
 ps_status build_table(int nq, const ps_channel* ch, int adjoint, ps_table* out, std::string& why) {
     const int W = width_for(nq);
     if (!W) {
@@ -293,6 +491,7 @@ ps_status build_table(int nq, const ps_channel* ch, int adjoint, ps_table* out, 
         why = "channel: bad support";
         return PS_ERR_INVALID;
     }
+    adjoint = (adjoint != 0) != (ch->adjoint != 0);
     if (ch->kind == PS_CH_PAULI_ROTATION) {
         if (ch->num_support && !ch->paulis) {
             why = "pauli_rotation: missing Pauli labels";
@@ -400,6 +599,43 @@ ps_status build_table(int nq, const ps_channel* ch, int adjoint, ps_table* out, 
         push_deltas(*out, table, W);
         return PS_OK;
     }
+    if (ch->kind >= PS_CH_HADAMARD && ch->kind <= PS_CH_AMPLITUDE_DAMPING) {
+        double ptm[16][16];
+        int k = 0;
+        if (!named_ptm(ch, k, ptm, why)) return PS_ERR_INVALID;
+        if (ch->num_support != k) {
+            why = "channel: expected " + std::to_string(k) + " qubit(s)";
+            return PS_ERR_INVALID;
+        }
+        for (int j = 0; j < k; ++j)
+            if ((int)ch->qubits[j] >= nq) {
+                why = "channel: qubit outside the register";
+                return PS_ERR_INVALID;
+            }
+        if (k == 2 && ch->qubits[0] == ch->qubits[1]) {
+            why = "channel: the two qubits must differ";
+            return PS_ERR_INVALID;
+        }
+        // transfer_matrix (ptm.rs:248-263): transposed for the adjoint, reordered to
+        // ascending-qubit local indices
+        const bool reversed = k == 2 && ch->qubits[0] > ch->qubits[1];
+        auto reorder = [&](int idx) { return reversed ? (((idx & 3) << 2) | (idx >> 2)) : idx; };
+        double table[16][16];
+        std::memset(table, 0, sizeof table);
+        const int dim = 1 << (2 * k);
+        for (int a = 0; a < dim; ++a)
+            for (int b = 0; b < dim; ++b) {
+                if (ptm[a][b] == 0.0) continue;
+                const int row = adjoint ? b : a, col = adjoint ? a : b;
+                table[reorder(row)][reorder(col)] += ptm[a][b];
+            }
+        out->mode = PS_TABLE_LOCAL;
+        out->k = k;
+        out->qubits[0] = reversed ? ch->qubits[1] : ch->qubits[0];
+        out->qubits[1] = k == 2 ? (reversed ? ch->qubits[0] : ch->qubits[1]) : 0;
+        push_deltas(*out, table, W);
+        return PS_OK;
+    }
     why = "unknown channel kind";
     return PS_ERR_UNSUPPORTED;
 }
@@ -407,10 +643,19 @@ ps_status build_table(int nq, const ps_channel* ch, int adjoint, ps_table* out, 
 // ---------------------------------------------------------------------------
 // table -> device layer
 // ---------------------------------------------------------------------------
+// Rotation-shaped tables run on the partner path: the identity entry scales every term in
+// place and one more entry (delta g) sends some terms to k ^ g, so every output key gets at
+// most two contributions and their order cannot change the sum.  The reference takes the
+// tables RotationLayer::of accepts (crates/paulistrings/src/engine/bucketed/rotation_layer.rs:
+// 101-140) this way; this path also takes the two-entry tables that rule declines only because
+// a non-emitting pattern is scaled (Hadamard's Y -> -Y) or a partner is one-sided (amplitude
+// damping's Z -> I), which are rotation-shaped in the sense above.  Every other local table
+// sets *general and runs on the sort path.
 template <int W, typename T>
-ps_status to_rot_layer(const ps_table& t, RotLayer<W>& L, LevelList& lv, std::string& why) {
+ps_status to_rot_layer(const ps_table& t, RotLayer<W>& L, LevelList& lv, std::string& why, bool* general) {
     std::memset(&L, 0, sizeof L);
     lv.n = 0;
+    *general = false;
     uint64_t dx[W] = {0}, dz[W] = {0};
     if (t.mode == PS_TABLE_ROTATION) {
         L.wide = 1;
@@ -447,20 +692,18 @@ ps_status to_rot_layer(const ps_table& t, RotLayer<W>& L, LevelList& lv, std::st
         } else if (t.num_entries == 2 && t.entries[0].local_delta == 0) {
             const ps_table_entry &e0 = t.entries[0], &e1 = t.entries[1];
             const unsigned delta = e1.local_delta;
-            // RotationLayer::of (bucketed/rotation_layer.rs:101-140), per coefficient type
+            // RotationLayer::of's shape test (bucketed/rotation_layer.rs:101-140), per
+            // coefficient type; its Clifford residue rule applies only to the tables it accepts
+            bool ref_shaped = true;
             for (int s = 0; s < dim; ++s) {
                 T a0 = (T)e0.amplitude[s], a1 = (T)e1.amplitude[s];
                 if (a1 == T(0)) {
-                    if (a0 != T(1)) {
-                        why = "table: not rotation-shaped (general tables run on the sort path)";
-                        return PS_ERR_UNSUPPORTED;
-                    }
+                    if (a0 != T(1)) ref_shaped = false;
                 } else if ((T)e1.amplitude[s ^ delta] == T(0)) {
-                    why = "table: not rotation-shaped";
-                    return PS_ERR_UNSUPPORTED;
+                    ref_shaped = false;
                 }
             }
-            bool clifford = true;
+            bool clifford = ref_shaped;
             const double eps = 2.220446049250313e-16;
             for (int s = 0; s < dim; ++s) {
                 double a0 = (double)(T)e0.amplitude[s], a1 = (double)(T)e1.amplitude[s];
@@ -481,8 +724,8 @@ ps_status to_rot_layer(const ps_table& t, RotLayer<W>& L, LevelList& lv, std::st
                 L.a1f[s] = (float)a1;
             }
         } else {
-            why = "table: general local tables (Clifford permutations, dense PTMs) are not on the device path";
-            return PS_ERR_UNSUPPORTED;
+            *general = true;
+            return PS_OK;
         }
     } else {
         why = "table: unknown mode";
@@ -507,6 +750,37 @@ ps_status to_rot_layer(const ps_table& t, RotLayer<W>& L, LevelList& lv, std::st
         }
     }
     return PS_OK;
+}
+
+// A local table as per-pattern record lists (ascending entry order, zero amplitudes in the
+// coefficient type skipped, as DeltaEntry::emit skips them).
+template <int W, typename T>
+void to_gen_layer(const ps_table& t, GenLayer<W, T>& G) {
+    std::memset(&G, 0, sizeof G);
+    for (int j = 0; j < 2; ++j) {
+        uint32_t q = t.k ? t.qubits[j < t.k ? j : 0] : 0;
+        G.qw[j] = (int)(q / 64);
+        G.qb[j] = (int)(q % 64);
+    }
+    G.pattern_mask = (1u << (2 * t.k)) - 1u;
+    G.num_entries = t.num_entries;
+    for (int e = 0; e < t.num_entries; ++e)
+        for (int w = 0; w < W; ++w) {
+            G.mx[e][w] = t.entries[e].mask_x[w];
+            G.mz[e][w] = t.entries[e].mask_z[w];
+        }
+    const int dim = 1 << (2 * t.k);
+    for (int s = 0; s < dim; ++s) {
+        int c = 0;
+        for (int e = 0; e < t.num_entries; ++e) {
+            const T a = (T)t.entries[e].amplitude[s];
+            if (a == T(0)) continue;
+            G.ent[s][c] = (uint8_t)e;
+            G.amp[s][c] = a;
+            ++c;
+        }
+        G.cnt[s] = (uint8_t)c;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -631,8 +905,10 @@ struct Engine {
         if (ps != PS_OK) return set_err(s, ps, why);
         RotationArgs<W, T> a;
         std::memset(&a, 0, sizeof a);
-        ps = to_rot_layer<W, T>(t, a.L, *s->levels, why);
+        bool general = false;
+        ps = to_rot_layer<W, T>(t, a.L, *s->levels, why, &general);
         if (ps != PS_OK) return set_err(s, ps, why);
+        if (general) return apply_general(s, t, keep, policy, stats);
         const uint64_t n = s->n;
         if (n >= (1ull << 31) - 1) return set_err(s, PS_ERR_UNSUPPORTED, "apply: at most 2^31 - 2 terms");
         const int spare = 1 - s->cur;
@@ -698,6 +974,70 @@ struct Engine {
             stats->terms_out = out_n;
             stats->terms_after_passes = out_n;
             stats->path = a.L.partners ? PS_PATH_ROTATION : PS_PATH_RESCALE;
+        }
+        s->cur = spare;
+        s->n = out_n;
+        return PS_OK;
+    }
+
+    // The sort path: branch records, LSD radix sort of (key, record index), run-summing dedup
+    // with the keep program (apply_layer_body's general tables, engine/gpu/layer.rs:614-763).
+    static ps_status apply_general(ps_sum* s, const ps_table& t, const KeepProg& keep, const ps_policy* policy,
+                                   ps_layer_stats* stats) {
+        (void)policy;
+        GenLayer<W, T> G;
+        to_gen_layer<W, T>(t, G);
+        const uint64_t n = s->n;
+        if (s->hist_ready) {
+            cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+            s->hist_ready = false;
+        }
+        uint64_t m = 0;
+        cudaError_t e = GeneralOps<W, T>::count(K(s, s->cur), n, G, s->ctl, s->hcount, &m, s->sms, s->stream, &s->prof);
+        s->prof.resolve();
+        if (e != cudaSuccess) return cuda_fail(s, e, "apply: record count");
+        if (m >= (1ull << 32) - 1)
+            return set_err(s, PS_ERR_UNSUPPORTED, "apply: a general layer emits at most 2^32 - 2 records");
+        const int spare = 1 - s->cur;
+        uint64_t out_n = 0;
+        if (m) {
+            const size_t sort_tiles = (m + StoreOps<W, T>::sort_tile() - 1) / StoreOps<W, T>::sort_tile();
+            const size_t branch_tiles = (n + GeneralOps<W, T>::branch_tile() - 1) / GeneralOps<W, T>::branch_tile();
+            if ((e = reserve_store(s, spare, m)) != cudaSuccess || (e = ensure(s, s->up_k, 2 * m * kKeyBytes)) != cudaSuccess ||
+                (e = ensure(s, s->up_v0, m * 4)) != cudaSuccess || (e = ensure(s, s->up_v1, m * 4)) != cudaSuccess ||
+                (e = ensure(s, s->up_c0, m * sizeof(T))) != cudaSuccess ||
+                (e = ensure(s, s->up_st, (m / 2048 + 2) * sizeof(unsigned long long))) != cudaSuccess ||
+                (e = ensure(s, s->status, (branch_tiles + 2) * sizeof(unsigned long long))) != cudaSuccess ||
+                (e = ensure(s, s->sort_status, sort_tiles * 256 * sizeof(unsigned int))) != cudaSuccess)
+                return cuda_fail(s, e, "apply: sort-path scratch");
+            s->sort.status = static_cast<unsigned int*>(s->sort_status.p);
+            uint64_t* k0 = (uint64_t*)s->up_k.p;
+            uint64_t* k1 = k0 + m * 2 * W;
+            uint32_t* v0 = (uint32_t*)s->up_v0.p;
+            uint32_t* v1 = (uint32_t*)s->up_v1.p;
+            T* rc = (T*)s->up_c0.p;
+            e = GeneralOps<W, T>::branch(K(s, s->cur), C(s, s->cur), n, G, k0, v0, rc, m,
+                                         (unsigned long long*)s->status.p, s->ctl, s->stream, &s->prof);
+            if (e != cudaSuccess) return cuda_fail(s, e, "apply: branch");
+            bool alt = false;
+            e = StoreOps<W, T>::sort_pairs(k0, v0, k1, v1, m, s->sort, s->ctl, s->sms, s->stream, alt, &s->prof);
+            if (e != cudaSuccess) return cuda_fail(s, e, "apply: sort");
+            ps_status fs = check_device_flags(s, "apply");
+            if (fs != PS_OK) return fs;
+            e = StoreOps<W, T>::dedup(alt ? k1 : k0, alt ? v1 : v0, rc, m, keep, s->compensated, K(s, spare),
+                                      C(s, spare), (unsigned long long*)s->up_st.p, s->ctl, s->hcount, &out_n,
+                                      s->stream, &s->prof);
+            s->prof.resolve();
+            if (e != cudaSuccess) return cuda_fail(s, e, "apply: dedup");
+            fs = check_device_flags(s, "apply");
+            if (fs != PS_OK) return fs;
+        }
+        if (stats) {
+            stats->terms_in = n;
+            stats->partners = m > n ? m - n : 0;
+            stats->terms_out = out_n;
+            stats->terms_after_passes = out_n;
+            stats->path = PS_PATH_SORT;
         }
         s->cur = spare;
         s->n = out_n;
@@ -1011,7 +1351,7 @@ ps_status ps_read_profile(ps_sum* s, ps_kernel_profile* out, int32_t cap, int32_
     static const char* kNames[K_NUM_KERNELS] = {"k_classify",     "k_fwd_levels", "k_bwd_levels", "k_partition",
                                                 "k_merge",        "k_topn_hist",  "k_topn_step",  "k_topn_compact",
                                                 "k_pack",         "k_sort_hist",  "k_sort_pass",  "k_dedup",
-                                                "k_unpack",       "k_expect"};
+                                                "k_unpack",       "k_expect",     "k_gen_count",  "k_gen_branch"};
     DeviceGuard g(s->device);
     s->prof.resolve();
     *count = K_NUM_KERNELS;
@@ -1054,6 +1394,12 @@ ps_status ps_synchronize(ps_sum* s) {
     DeviceGuard g(s->device);
     cudaError_t e = cudaStreamSynchronize(s->stream);
     return e == cudaSuccess ? PS_OK : cuda_fail(s, e, "synchronize");
+}
+
+ps_status ps_set_compensated_sums(ps_sum* s, int32_t enabled) {
+    if (!s) return PS_ERR_INVALID;
+    s->compensated = enabled != 0;
+    return PS_OK;
 }
 
 }  // extern "C"

@@ -60,6 +60,21 @@ struct RotLayer {
     float cos32, sin32;
 };
 
+// Device form of a general local table (LocalPtm with any entries), per input support
+// pattern s: the records it emits, in ascending entry order (DeltaEntry::emit,
+// crates/paulistrings/src/channel/prepared.rs:50-68).
+template <int W, typename T>
+struct GenLayer {
+    int32_t qw[2], qb[2];     // support qubit j lives in word qw[j], bit qb[j]
+    uint32_t pattern_mask;    // (1 << 2k) - 1
+    int32_t num_entries;
+    uint64_t mx[16][W];       // entry e: x / z XOR masks
+    uint64_t mz[16][W];
+    uint8_t cnt[16];          // records emitted by pattern s
+    uint8_t ent[16][16];      // entry of record j of pattern s
+    T amp[16][16];            // amplitude of record j of pattern s
+};
+
 // Kernel ids of the per-kernel profile.
 enum KernelId : int {
     K_CLASSIFY = 0,
@@ -76,6 +91,8 @@ enum KernelId : int {
     K_DEDUP,
     K_UNPACK,
     K_EXPECT,
+    K_GEN_COUNT,
+    K_GEN_BRANCH,
     K_NUM_KERNELS
 };
 
@@ -171,6 +188,19 @@ template <int W, typename T>
 cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st);
 template <int W, typename T>
 cudaError_t configure_rotation_kernels();
+
+// General-table layer (branch records for the sort path).
+template <int W, typename T>
+struct GeneralOps {
+    // records the layer emits (synchronizes)
+    static cudaError_t count(const uint64_t* keys, uint64_t n, const GenLayer<W, T>& G, Ctl* ctl,
+                             unsigned long long* host_count, uint64_t* m, int sms, cudaStream_t st, KernelProf* prof);
+    // records (key ^ mask, c * amplitude, own index) in (term, entry) order; status >= tiles words
+    static cudaError_t branch(const uint64_t* keys, const T* coef, uint64_t n, const GenLayer<W, T>& G,
+                              uint64_t* rkeys, uint32_t* rvals, T* rcoef, uint64_t m_cap,
+                              unsigned long long* status, Ctl* ctl, cudaStream_t st, KernelProf* prof);
+    static size_t branch_tile();
+};
 
 // One scan tile's look-back slot: flag 1 = agg valid, 2 = inc (prefix combined with agg) valid.
 struct LevelSlot {

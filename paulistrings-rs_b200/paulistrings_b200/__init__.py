@@ -8,7 +8,7 @@ behind the C ABI in ``include/paulistrings_b200.h``.
 
 from . import truncation
 from ._lib import PauliStringsError, device_count
-from .circuit import Circuit, Depolarizing, PauliRotation, gates, noise
+from .circuit import Circuit, Depolarizing, PauliRotation, PtmChannel, gates, noise
 from .sum import (
     GpuPauliSum,
     PauliSum,
@@ -35,6 +35,7 @@ __all__ = [
     "Depolarizing",
     "GpuPauliSum",
     "PauliRotation",
+    "PtmChannel",
     "PauliStringsError",
     "PauliSum",
     "PropagationStats",

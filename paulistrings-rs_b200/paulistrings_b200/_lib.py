@@ -25,7 +25,9 @@ PS_F64, PS_F32 = 0, 1
 PS_FORWARD, PS_HEISENBERG = 0, 1
 PS_KEEP_TRUE, PS_KEEP_COEFF, PS_KEEP_WEIGHT, PS_KEEP_AND, PS_KEEP_OR = range(5)
 PS_PASS_NONE, PS_PASS_TOPN = 0, 1
-PS_CH_PAULI_ROTATION, PS_CH_DEPOLARIZING = 1, 2
+(PS_CH_PAULI_ROTATION, PS_CH_DEPOLARIZING, PS_CH_HADAMARD, PS_CH_PHASE, PS_CH_PHASE_DAGGER, PS_CH_PAULI_X,
+ PS_CH_PAULI_Y, PS_CH_PAULI_Z, PS_CH_CNOT, PS_CH_CZ, PS_CH_SWAP, PS_CH_UNITARY, PS_CH_DEPHASING,
+ PS_CH_PAULI_CHANNEL, PS_CH_DEPOLARIZING_2Q, PS_CH_AMPLITUDE_DAMPING) = range(1, 17)
 PS_TABLE_LOCAL, PS_TABLE_ROTATION = 1, 2
 PS_PATH_RESCALE, PS_PATH_ROTATION, PS_PATH_SORT = 1, 2, 3
 
@@ -51,6 +53,7 @@ EXPORTED = (
     "ps_expectation_device_noalloc",
     "ps_inject_fault",
     "ps_synchronize",
+    "ps_set_compensated_sums",
 )
 
 PS_FAULT_NONE, PS_FAULT_OOM, PS_FAULT_STALL = 0, 1, 2
@@ -82,6 +85,10 @@ class Channel(ctypes.Structure):
         ("qubits", ctypes.POINTER(ctypes.c_uint32)),
         ("paulis", ctypes.c_char_p),
         ("param", ctypes.c_double),
+        ("matrix", ctypes.POINTER(ctypes.c_double)),
+        ("params", ctypes.c_double * 3),
+        ("adjoint", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 

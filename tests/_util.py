@@ -9,7 +9,7 @@ import numpy as np
 
 from oracle.oracle import OracleSum
 from paulistrings_b200 import _lib
-from paulistrings_b200.circuit import Circuit, Depolarizing, PauliRotation
+from paulistrings_b200.circuit import Circuit, Depolarizing, PauliRotation, PtmChannel
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 
@@ -33,9 +33,23 @@ def oracle_channels(circuit: Circuit):
             out.append(("rotation", ch.paulis, list(ch.qubits), ch.theta))
         elif isinstance(ch, Depolarizing):
             out.append(("depolarize", "", [ch.qubit], ch.p))
+        elif isinstance(ch, PtmChannel):
+            extra = {"adjoint": ch.is_adjoint, "params": ch.params}
+            if ch.matrix is not None:
+                flat = np.asarray(ch.matrix)
+                extra["matrix"] = flat[0::2] + 1j * flat[1::2]
+            out.append((_PTM_NAMES[ch.kind], "", list(ch.qubits), ch.param, extra))
         else:
             raise TypeError(ch)
     return out
+
+
+_PTM_NAMES = {_lib.PS_CH_HADAMARD: "h", _lib.PS_CH_PHASE: "s", _lib.PS_CH_PHASE_DAGGER: "sdg",
+              _lib.PS_CH_PAULI_X: "x", _lib.PS_CH_PAULI_Y: "y", _lib.PS_CH_PAULI_Z: "z",
+              _lib.PS_CH_CNOT: "cnot", _lib.PS_CH_CZ: "cz", _lib.PS_CH_SWAP: "swap",
+              _lib.PS_CH_UNITARY: "unitary", _lib.PS_CH_DEPHASING: "dephase",
+              _lib.PS_CH_PAULI_CHANNEL: "pauli_channel", _lib.PS_CH_DEPOLARIZING_2Q: "depolarize2",
+              _lib.PS_CH_AMPLITUDE_DAMPING: "amplitude_damping"}
 
 
 def oracle_policy(policy):
