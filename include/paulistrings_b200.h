@@ -65,7 +65,9 @@ typedef enum ps_keep_op {
 
 typedef enum ps_pass_kind {
     PS_PASS_NONE = 0,
-    PS_PASS_TOPN = 1     /* keep the n largest |c|^2; ties first in key order (builtin.rs:73-129) */
+    PS_PASS_TOPN = 1,    /* keep the n largest |c|^2; ties first in key order (builtin.rs:73-129) */
+    PS_PASS_SCORED_TOPN = 2 /* keep the n terms the handle's scorer ranks highest (ps_set_scorer);
+                               ties first in key order, a NaN score never kept */
 } ps_pass_kind;
 
 typedef struct ps_keep_node {
@@ -278,6 +280,52 @@ ps_status ps_inject_fault(ps_sum* sum, int32_t kind, uint64_t arg);
 
 /* Wait for the handle's stream.  PartitionStorage::settle. */
 ps_status ps_synchronize(ps_sum* sum);
+
+/* ---- learned truncation -------------------------------------------------------------
+ * A scorer is a small MLP implementing a TruncationPolicy layer pass (the TruncationPolicy
+ * trait, crates/paulistrings/src/truncation/mod.rs:30-107; no built-in counterpart in the
+ * reference): from a term's per-qubit I/X/Y/Z code, its Pauli weight, log|c| and the remaining
+ * depth it predicts log of the magnitude the term's descendants contribute to the final
+ * expectation.  Architecture: one-hot (num_qubits x 4) + 3 scalar features -> 128 -> GELU ->
+ * 128 -> GELU -> 1, BF16 weights, FP32 accumulation, the 128 x 128 layer on the tensor cores.
+ * Parameters (fp32, this order): embed[num_qubits][3][128] (rows for X, Z, Y: local index
+ * x | z << 1, minus one; the identity's one-hot column is folded into b1), u[3][128] (weight,
+ * log|c|, remaining-depth columns), b1[128], w2[128][128] (in, out), b2[128], w3[128], b3.
+ * Scalar features enter as weight * s0, log|c| * s1 and remaining * s2, with
+ * remaining = layers still to apply / layers_per_unit. */
+typedef struct ps_scorer ps_scorer;
+
+typedef struct ps_scorer_config {
+    int32_t num_qubits;       /* <= 256 */
+    int32_t reserved;
+    double layers_per_unit;   /* layers per unit of the remaining-depth feature (e.g. per Trotter step) */
+    float feature_scale[3];   /* s0, s1, s2 */
+    float init_scale;         /* standard deviation of the initial embedding and u weights */
+    uint64_t seed;            /* initial weights (splitmix64 + Box-Muller) */
+} ps_scorer_config;
+
+ps_status ps_scorer_create(int32_t device, const ps_scorer_config* config, ps_scorer** out);
+ps_status ps_scorer_destroy(ps_scorer* scorer);
+const char* ps_scorer_last_error(const ps_scorer* scorer);
+uint64_t ps_scorer_num_params(const ps_scorer* scorer);
+ps_status ps_scorer_get_params(ps_scorer* scorer, float* out);      /* fp32 master weights */
+ps_status ps_scorer_set_params(ps_scorer* scorer, const float* in);
+/* Scores of n terms (keys: n rows of 2W words, x words then z words, W the scorer's width). */
+ps_status ps_scorer_score(ps_scorer* scorer, const uint64_t* keys, const float* log_abs_c, const float* remaining,
+                          uint64_t n, float* out);
+/* Gradients of the mean squared error sum((y - target)^2) / n over one batch (n <= 65536),
+ * without updating; *loss = that mean.  For checking the backward kernels. */
+ps_status ps_scorer_gradients(ps_scorer* scorer, const uint64_t* keys, const float* log_abs_c, const float* remaining,
+                              const float* target, uint64_t n, float* grads_out, float* loss);
+/* Adam (beta 0.9 / 0.999, eps 1e-8) over shuffled minibatches of `batch` terms for `epochs`
+ * passes; epoch_loss[e] = mean squared error over epoch e (optional). */
+ps_status ps_scorer_train(ps_scorer* scorer, const uint64_t* keys, const float* log_abs_c, const float* remaining,
+                          const float* target, uint64_t n, int32_t epochs, int32_t batch, float learning_rate,
+                          float* epoch_loss);
+/* Attach a scorer for PS_PASS_SCORED_TOPN passes; remaining_layers = layers still to apply.
+ * Each ps_finalize_layer (and each layer of ps_propagate) first counts one layer down, then
+ * scores with the remaining depth that is left.  NULL detaches. */
+ps_status ps_set_scorer(ps_sum* sum, ps_scorer* scorer, double remaining_layers);
 
 /* Sum each output key's contributions on the sort path (general tables, three or more
  * contributions per key) with TwoSum compensation: the rounding error of every addition is

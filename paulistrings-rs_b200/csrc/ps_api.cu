@@ -15,6 +15,7 @@
 #include "../../include/paulistrings_b200.h"
 #include "ps_device.cuh"
 #include "ps_kernels.h"
+#include "ps_scorer.h"
 #include "ps_store.h"
 
 using namespace psb;
@@ -29,6 +30,22 @@ struct Buf {
 };
 
 }  // namespace
+
+struct ps_scorer {
+    int device = 0;
+    int nq = 0;
+    int W = 1;
+    int sms = 148;
+    ps_scorer_config cfg{};
+    ScorerLayout L{};
+    cudaStream_t stream = nullptr;
+    Ctl* ctl = nullptr;
+    Buf master, bf, grads, m, v;                                   // parameters, Adam state
+    Buf keys, logc, rem, target, h1, gz1, dz2, scores, loss;        // batch staging
+    int step = 0;
+    KernelProf prof;
+    std::string err;
+};
 
 struct ps_sum {
     int device = 0;
@@ -48,6 +65,9 @@ struct ps_sum {
     Buf idx, dv, fv, slots, status, bounds, hist, cand, partial, dout;
     bool hist_ready = false;  // hist holds the TopN digit-1 histogram of the current store
     bool compensated = false; // sort-path dedup sums runs with TwoSum compensation
+    ps_scorer* scorer = nullptr;   // PS_PASS_SCORED_TOPN
+    double scorer_remaining = 0;   // layers still to apply
+    Buf sel;                       // scored TopN select keys
     SortScratch sort{};
     Buf sort_status;
     Buf up_x, up_z, up_c, up_k, up_v0, up_v1, up_c0, up_st;  // ingest / readout staging, grow-only
@@ -195,7 +215,8 @@ ps_status lower_keep(const ps_policy* p, KeepProg& k, std::string& why) {
         k.fast_k = k.iarg[1 - ci];
     }
     for (int i = 0; i < p->num_passes; ++i) {
-        if (p->passes[i].kind != PS_PASS_TOPN && p->passes[i].kind != PS_PASS_NONE) {
+        if (p->passes[i].kind != PS_PASS_TOPN && p->passes[i].kind != PS_PASS_SCORED_TOPN &&
+            p->passes[i].kind != PS_PASS_NONE) {
             why = "policy: unknown layer pass";
             return PS_ERR_UNSUPPORTED;
         }
@@ -1047,9 +1068,16 @@ struct Engine {
     static ps_status finalize(ps_sum* s, const ps_policy* policy) {
         const bool ready = s->hist_ready;
         if (ready) s->hist_ready = false;
+        if (s->scorer) s->scorer_remaining -= 1.0;
         ps_status result = PS_OK;
         for (int i = 0; policy && i < policy->num_passes; ++i) {
             const ps_pass& p = policy->passes[i];
+            if (p.kind == PS_PASS_SCORED_TOPN) {
+                if (ready && i == 0) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+                ps_status ps = scored_topn(s, p.n);
+                if (ps != PS_OK) return ps;
+                continue;
+            }
             if (p.kind != PS_PASS_TOPN) continue;
             const bool use_hist = ready && i == 0;
             if (s->n <= p.n) {
@@ -1085,6 +1113,60 @@ struct Engine {
             s->n = out_n;
         }
         return result;
+    }
+
+    // The learned pass: the attached scorer scores every term (tensor-core MLP, select keys and
+    // their first-digit histogram written in the same pass), then the TopN select and the
+    // order-preserving compaction run on the score keys.
+    static ps_status scored_topn(ps_sum* s, uint64_t keep_n) {
+        ps_scorer* sc = s->scorer;
+        if (!sc) return set_err(s, PS_ERR_INVALID, "scored TopN: no scorer attached (ps_set_scorer)");
+        if (s->n <= keep_n) return PS_OK;
+        if (keep_n == 0) {
+            s->n = 0;
+            return PS_OK;
+        }
+        const int spare = 1 - s->cur;
+        cudaError_t e = reserve_store(s, spare, keep_n);
+        if (e == cudaSuccess) e = ensure(s, s->sel, s->n * sizeof(uint64_t));
+        if (e == cudaSuccess) e = ensure(s, s->cand, s->n * sizeof(uint64_t));
+        if (e == cudaSuccess) e = ensure(s, s->status, (s->n / 4096 + 4) * sizeof(unsigned long long));
+        if (e != cudaSuccess) return cuda_fail(s, e, "scored TopN: scratch");
+        ScorerArgs A;
+        A.p = static_cast<const uint16_t*>(sc->bf.p);
+        A.L = sc->L;
+        A.nq = sc->nq;
+        for (int f = 0; f < 3; ++f) A.fscale[f] = sc->cfg.feature_scale[f];
+        ScoreInput in{};
+        in.keys = K(s, s->cur);
+        in.coef64 = std::is_same<T, double>::value ? (const double*)C(s, s->cur) : nullptr;
+        in.coef32 = std::is_same<T, float>::value ? (const float*)C(s, s->cur) : nullptr;
+        in.rem_uniform = (float)(s->scorer_remaining / sc->cfg.layers_per_unit);
+        in.n = s->n;
+        cudaMemsetAsync(s->hist.p, 0, kTopnBins1 * sizeof(unsigned int), s->stream);
+        e = launch_score<W>(A, in, nullptr, (uint64_t*)s->sel.p, (unsigned int*)s->hist.p, s->ctl, s->sms,
+                            s->stream, &s->prof);
+        if (e != cudaSuccess) return cuda_fail(s, e, "scored TopN: score");
+        ps_status ps = check_device_flags(s, "scored TopN");
+        if (ps != PS_OK) {
+            cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+            return ps;
+        }
+        uint64_t out_n = 0;
+        e = StoreOps<W, T>::topn(K(s, s->cur), C(s, s->cur), s->n, keep_n, K(s, spare), C(s, spare),
+                                 (unsigned int*)s->hist.p, true, (uint64_t*)s->cand.p, s->n,
+                                 (unsigned long long*)s->status.p, s->ctl, s->hcount, &out_n, s->sms, s->stream,
+                                 &s->prof, (const uint64_t*)s->sel.p);
+        s->prof.resolve();
+        if (e != cudaSuccess) return cuda_fail(s, e, "scored TopN");
+        ps = check_device_flags(s, "scored TopN");
+        if (ps != PS_OK) {
+            cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+            return ps;
+        }
+        s->cur = spare;
+        s->n = out_n;
+        return PS_OK;
     }
 
     static ps_status expectation(ps_sum* s, const uint64_t* ax, const uint64_t* az, const uint64_t* neg, double* out) {
@@ -1211,7 +1293,7 @@ ps_status ps_destroy(ps_sum* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (Buf* b : {&s->keys[0], &s->keys[1], &s->coef[0], &s->coef[1], &s->pk, &s->pc, &s->idx, &s->dv, &s->fv,
                    &s->slots, &s->status, &s->bounds, &s->hist, &s->cand, &s->partial, &s->dout, &s->sort_status,
-                   &s->up_x, &s->up_z, &s->up_c, &s->up_k, &s->up_v0, &s->up_v1, &s->up_c0, &s->up_st})
+                   &s->up_x, &s->up_z, &s->up_c, &s->up_k, &s->up_v0, &s->up_v1, &s->up_c0, &s->up_st, &s->sel})
         release(*b);
     if (s->ctl) cudaFree(s->ctl);
     if (s->sort.hist) cudaFree(s->sort.hist);
@@ -1351,7 +1433,8 @@ ps_status ps_read_profile(ps_sum* s, ps_kernel_profile* out, int32_t cap, int32_
     static const char* kNames[K_NUM_KERNELS] = {"k_classify",     "k_fwd_levels", "k_bwd_levels", "k_partition",
                                                 "k_merge",        "k_topn_hist",  "k_topn_step",  "k_topn_compact",
                                                 "k_pack",         "k_sort_hist",  "k_sort_pass",  "k_dedup",
-                                                "k_unpack",       "k_expect",     "k_gen_count",  "k_gen_branch"};
+                                                "k_unpack",       "k_expect",     "k_gen_count",  "k_gen_branch",
+                                                "k_score",        "k_score_train"};
     DeviceGuard g(s->device);
     s->prof.resolve();
     *count = K_NUM_KERNELS;
@@ -1399,6 +1482,307 @@ ps_status ps_synchronize(ps_sum* s) {
 ps_status ps_set_compensated_sums(ps_sum* s, int32_t enabled) {
     if (!s) return PS_ERR_INVALID;
     s->compensated = enabled != 0;
+    return PS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// learned truncation: the scorer
+// ---------------------------------------------------------------------------
+ps_status ps_scorer_create(int32_t device, const ps_scorer_config* cfg, ps_scorer** out) {
+    if (!out || !cfg) return PS_ERR_INVALID;
+    *out = nullptr;
+    if (cfg->num_qubits < 1 || cfg->num_qubits > 256 || !(cfg->layers_per_unit > 0.0)) return PS_ERR_INVALID;
+    int count = ps_device_count();
+    if (count == 0 || device < 0 || device >= count) return PS_ERR_NO_DEVICE;
+    DeviceGuard g(device);
+    ps_scorer* sc = new ps_scorer();
+    sc->device = device;
+    sc->nq = cfg->num_qubits;
+    sc->W = width_for(cfg->num_qubits);
+    sc->cfg = *cfg;
+    sc->L = scorer_layout(sc->nq);
+    cudaDeviceGetAttribute(&sc->sms, cudaDevAttrMultiProcessorCount, device);
+    const size_t np = sc->L.total;
+    // initial weights: N(0, init_scale) for the embedding rows and feature columns, N(0, 1/sqrt(128))
+    // for the two dense layers, zero biases (splitmix64 stream, Box-Muller)
+    std::vector<float> init(np, 0.0f);
+    uint64_t state = cfg->seed;
+    auto next = [&]() {
+        uint64_t z = (state += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    auto normal = [&]() {
+        const double u1 = ((next() >> 11) + 1.0) * (1.0 / 9007199254740993.0), u2 = (next() >> 11) * (1.0 / 9007199254740992.0);
+        return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+    };
+    for (size_t i = sc->L.embed; i < sc->L.b1; ++i) init[i] = (float)(cfg->init_scale * normal());
+    const double dense = 1.0 / std::sqrt((double)kHid);
+    for (size_t i = sc->L.w2; i < sc->L.b2; ++i) init[i] = (float)(dense * normal());
+    for (size_t i = sc->L.w3; i < sc->L.b3; ++i) init[i] = (float)(dense * normal());
+    cudaError_t e = cudaStreamCreateWithFlags(&sc->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&sc->ctl, sizeof(Ctl));
+    if (e == cudaSuccess) e = cudaMemset(sc->ctl, 0, sizeof(Ctl));
+    if (e == cudaSuccess) {
+        static const unsigned long long limit = (unsigned long long)kSpinLimit;
+        e = cudaMemcpy(&sc->ctl->spin_limit, &limit, sizeof(limit), cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = ensure(sc->master, np * 4);
+    if (e == cudaSuccess) e = ensure(sc->bf, np * 2);
+    if (e == cudaSuccess) e = ensure(sc->grads, np * 4);
+    if (e == cudaSuccess) e = ensure(sc->m, np * 4);
+    if (e == cudaSuccess) e = ensure(sc->v, np * 4);
+    if (e == cudaSuccess) e = ensure(sc->loss, 16);
+    if (e == cudaSuccess) e = cudaMemcpy(sc->master.p, init.data(), np * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(sc->grads.p, 0, np * 4);
+    if (e == cudaSuccess) e = cudaMemset(sc->m.p, 0, np * 4);
+    if (e == cudaSuccess) e = cudaMemset(sc->v.p, 0, np * 4);
+    if (e == cudaSuccess) e = launch_to_bf16((const float*)sc->master.p, (uint16_t*)sc->bf.p, np, sc->stream);
+    if (e == cudaSuccess) {
+        switch (sc->W) {
+        case 1: e = configure_scorer_kernels<1>(); break;
+        case 2: e = configure_scorer_kernels<2>(); break;
+        default: e = configure_scorer_kernels<4>(); break;
+        }
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sc->stream);
+    if (e != cudaSuccess) {
+        ps_scorer_destroy(sc);
+        cudaGetLastError();
+        return e == cudaErrorMemoryAllocation ? PS_ERR_OOM : PS_ERR_DEVICE;
+    }
+    *out = sc;
+    return PS_OK;
+}
+
+ps_status ps_scorer_destroy(ps_scorer* sc) {
+    if (!sc) return PS_OK;
+    DeviceGuard g(sc->device);
+    if (sc->stream) cudaStreamSynchronize(sc->stream);
+    for (Buf* b : {&sc->master, &sc->bf, &sc->grads, &sc->m, &sc->v, &sc->keys, &sc->logc, &sc->rem, &sc->target,
+                   &sc->h1, &sc->gz1, &sc->dz2, &sc->scores, &sc->loss})
+        release(*b);
+    if (sc->ctl) cudaFree(sc->ctl);
+    sc->prof.destroy();
+    if (sc->stream) cudaStreamDestroy(sc->stream);
+    delete sc;
+    return PS_OK;
+}
+
+const char* ps_scorer_last_error(const ps_scorer* sc) { return sc ? sc->err.c_str() : "null scorer"; }
+uint64_t ps_scorer_num_params(const ps_scorer* sc) { return sc ? (uint64_t)sc->L.total : 0; }
+
+}  // extern "C"
+
+namespace {
+
+ps_status scorer_fail(ps_scorer* sc, ps_status st, const std::string& msg) {
+    sc->err = msg;
+    return st;
+}
+
+ps_status scorer_cuda(ps_scorer* sc, cudaError_t e, const char* where) {
+    if (e == cudaErrorMemoryAllocation) cudaGetLastError();
+    return scorer_fail(sc, e == cudaErrorMemoryAllocation ? PS_ERR_OOM : PS_ERR_DEVICE,
+                       std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+ps_status scorer_flags(ps_scorer* sc, const char* where) {
+    unsigned int flags[2] = {0, 0};
+    cudaError_t e = cudaMemcpyAsync(flags, &sc->ctl->err, sizeof(flags), cudaMemcpyDeviceToHost, sc->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sc->stream);
+    if (e != cudaSuccess) return scorer_cuda(sc, e, where);
+    if (flags[0] == 0) return PS_OK;
+    cudaMemsetAsync(&sc->ctl->err, 0, 2 * sizeof(unsigned int), sc->stream);
+    cudaStreamSynchronize(sc->stream);
+    char msg[160];
+    snprintf(msg, sizeof msg, "%s: device check failed (flags %u, check %u)", where, flags[0], flags[1]);
+    return scorer_fail(sc, (flags[0] & ERR_TIMEOUT) ? PS_ERR_TIMEOUT : PS_ERR_DEVICE, msg);
+}
+
+ScorerArgs scorer_args(const ps_scorer* sc) {
+    ScorerArgs A;
+    A.p = static_cast<const uint16_t*>(sc->bf.p);
+    A.L = sc->L;
+    A.nq = sc->nq;
+    for (int f = 0; f < 3; ++f) A.fscale[f] = sc->cfg.feature_scale[f];
+    return A;
+}
+
+// Host feature arrays of n terms into the scorer's staging buffers.
+cudaError_t scorer_stage(ps_scorer* sc, const uint64_t* keys, const float* logc, const float* rem, const float* target,
+                         uint64_t n) {
+    const size_t kb = (size_t)n * 16 * sc->W;
+    cudaError_t e = ensure(sc->keys, kb ? kb : 16);
+    if (e == cudaSuccess) e = ensure(sc->logc, n * 4 + 16);
+    if (e == cudaSuccess) e = ensure(sc->rem, n * 4 + 16);
+    if (e == cudaSuccess && target) e = ensure(sc->target, n * 4 + 16);
+    if (e != cudaSuccess) return e;
+    if (!n) return cudaSuccess;
+    e = cudaMemcpyAsync(sc->keys.p, keys, kb, cudaMemcpyHostToDevice, sc->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sc->logc.p, logc, n * 4, cudaMemcpyHostToDevice, sc->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sc->rem.p, rem, n * 4, cudaMemcpyHostToDevice, sc->stream);
+    if (e == cudaSuccess && target)
+        e = cudaMemcpyAsync(sc->target.p, target, n * 4, cudaMemcpyHostToDevice, sc->stream);
+    return e;
+}
+
+cudaError_t scorer_batch(ps_scorer* sc, uint64_t offset, uint64_t nb) {
+    ScoreInput in{};
+    in.keys = static_cast<const uint64_t*>(sc->keys.p) + offset * 2 * sc->W;
+    in.logc = static_cast<const float*>(sc->logc.p) + offset;
+    in.rem = static_cast<const float*>(sc->rem.p) + offset;
+    in.n = nb;
+    TrainScratch S{static_cast<uint16_t*>(sc->h1.p), static_cast<uint16_t*>(sc->gz1.p),
+                   static_cast<uint16_t*>(sc->dz2.p)};
+    const float* tgt = static_cast<const float*>(sc->target.p) + offset;
+    const ScorerArgs A = scorer_args(sc);
+    float* grads = static_cast<float*>(sc->grads.p);
+    float* loss = static_cast<float*>(sc->loss.p);
+    switch (sc->W) {
+    case 1: return launch_train_batch<1>(A, in, tgt, 1.0f / (float)nb, S, grads, loss, sc->ctl, sc->sms, sc->stream, &sc->prof);
+    case 2: return launch_train_batch<2>(A, in, tgt, 1.0f / (float)nb, S, grads, loss, sc->ctl, sc->sms, sc->stream, &sc->prof);
+    default: return launch_train_batch<4>(A, in, tgt, 1.0f / (float)nb, S, grads, loss, sc->ctl, sc->sms, sc->stream, &sc->prof);
+    }
+}
+
+cudaError_t scorer_train_scratch(ps_scorer* sc, uint64_t batch) {
+    cudaError_t e = ensure(sc->h1, batch * kHid * 2);
+    if (e == cudaSuccess) e = ensure(sc->gz1, batch * kHid * 2);
+    if (e == cudaSuccess) e = ensure(sc->dz2, batch * kHid * 2);
+    return e;
+}
+
+}  // namespace
+
+extern "C" {
+
+ps_status ps_scorer_get_params(ps_scorer* sc, float* out) {
+    if (!sc || !out) return PS_ERR_INVALID;
+    DeviceGuard g(sc->device);
+    cudaError_t e = cudaMemcpyAsync(out, sc->master.p, sc->L.total * 4, cudaMemcpyDeviceToHost, sc->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sc->stream);
+    return e == cudaSuccess ? PS_OK : scorer_cuda(sc, e, "get_params");
+}
+
+ps_status ps_scorer_set_params(ps_scorer* sc, const float* in) {
+    if (!sc || !in) return PS_ERR_INVALID;
+    DeviceGuard g(sc->device);
+    cudaError_t e = cudaMemcpyAsync(sc->master.p, in, sc->L.total * 4, cudaMemcpyHostToDevice, sc->stream);
+    if (e == cudaSuccess) e = launch_to_bf16((const float*)sc->master.p, (uint16_t*)sc->bf.p, sc->L.total, sc->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sc->stream);
+    return e == cudaSuccess ? PS_OK : scorer_cuda(sc, e, "set_params");
+}
+
+ps_status ps_scorer_score(ps_scorer* sc, const uint64_t* keys, const float* logc, const float* rem, uint64_t n,
+                          float* out) {
+    if (!sc || (n && (!keys || !logc || !rem || !out))) return PS_ERR_INVALID;
+    DeviceGuard g(sc->device);
+    cudaError_t e = scorer_stage(sc, keys, logc, rem, nullptr, n);
+    if (e == cudaSuccess) e = ensure(sc->scores, n * 4 + 16);
+    if (e != cudaSuccess) return scorer_cuda(sc, e, "score: staging");
+    if (!n) return PS_OK;
+    ScoreInput in{};
+    in.keys = static_cast<const uint64_t*>(sc->keys.p);
+    in.logc = static_cast<const float*>(sc->logc.p);
+    in.rem = static_cast<const float*>(sc->rem.p);
+    in.n = n;
+    const ScorerArgs A = scorer_args(sc);
+    float* sco = static_cast<float*>(sc->scores.p);
+    switch (sc->W) {
+    case 1: e = launch_score<1>(A, in, sco, nullptr, nullptr, sc->ctl, sc->sms, sc->stream, &sc->prof); break;
+    case 2: e = launch_score<2>(A, in, sco, nullptr, nullptr, sc->ctl, sc->sms, sc->stream, &sc->prof); break;
+    default: e = launch_score<4>(A, in, sco, nullptr, nullptr, sc->ctl, sc->sms, sc->stream, &sc->prof); break;
+    }
+    if (e != cudaSuccess) return scorer_cuda(sc, e, "score");
+    ps_status ps = scorer_flags(sc, "score");
+    if (ps != PS_OK) return ps;
+    e = cudaMemcpyAsync(out, sco, n * 4, cudaMemcpyDeviceToHost, sc->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sc->stream);
+    return e == cudaSuccess ? PS_OK : scorer_cuda(sc, e, "score: readback");
+}
+
+ps_status ps_scorer_gradients(ps_scorer* sc, const uint64_t* keys, const float* logc, const float* rem,
+                              const float* target, uint64_t n, float* grads_out, float* loss) {
+    if (!sc || !n || n > 65536 || !keys || !logc || !rem || !target || !grads_out) return PS_ERR_INVALID;
+    DeviceGuard g(sc->device);
+    cudaError_t e = scorer_stage(sc, keys, logc, rem, target, n);
+    if (e == cudaSuccess) e = scorer_train_scratch(sc, n);
+    if (e != cudaSuccess) return scorer_cuda(sc, e, "gradients: staging");
+    cudaMemsetAsync(sc->grads.p, 0, sc->L.total * 4, sc->stream);
+    cudaMemsetAsync(sc->loss.p, 0, 16, sc->stream);
+    e = scorer_batch(sc, 0, n);
+    if (e != cudaSuccess) return scorer_cuda(sc, e, "gradients");
+    ps_status ps = scorer_flags(sc, "gradients");
+    if (ps != PS_OK) return ps;
+    float l = 0.f;
+    e = cudaMemcpyAsync(grads_out, sc->grads.p, sc->L.total * 4, cudaMemcpyDeviceToHost, sc->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&l, sc->loss.p, 4, cudaMemcpyDeviceToHost, sc->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sc->stream);
+    cudaMemsetAsync(sc->grads.p, 0, sc->L.total * 4, sc->stream);
+    if (e != cudaSuccess) return scorer_cuda(sc, e, "gradients: readback");
+    if (loss) *loss = l / (float)n;
+    return PS_OK;
+}
+
+ps_status ps_scorer_train(ps_scorer* sc, const uint64_t* keys, const float* logc, const float* rem, const float* target,
+                          uint64_t n, int32_t epochs, int32_t batch, float lr, float* epoch_loss) {
+    if (!sc || !n || !keys || !logc || !rem || !target || epochs < 1 || batch < 1 || batch > 65536 || !(lr > 0.f))
+        return PS_ERR_INVALID;
+    DeviceGuard g(sc->device);
+    const int K = 2 * sc->W;
+    std::vector<uint64_t> pk((size_t)n * K);
+    std::vector<float> pl(n), pr(n), pt(n);
+    std::vector<uint64_t> perm(n);
+    for (uint64_t i = 0; i < n; ++i) perm[i] = i;
+    uint64_t state = sc->cfg.seed ^ 0xA5A5A5A5DEADBEEFull;
+    auto next = [&]() {
+        uint64_t z = (state += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    cudaError_t e = scorer_train_scratch(sc, (uint64_t)batch);
+    if (e != cudaSuccess) return scorer_cuda(sc, e, "train: scratch");
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    for (int ep = 0; ep < epochs; ++ep) {
+        for (uint64_t i = n - 1; i > 0; --i) std::swap(perm[i], perm[next() % (i + 1)]);  // Fisher-Yates
+        for (uint64_t i = 0; i < n; ++i) {
+            const uint64_t j = perm[i];
+            std::memcpy(&pk[i * K], &keys[j * K], K * sizeof(uint64_t));
+            pl[i] = logc[j];
+            pr[i] = rem[j];
+            pt[i] = target[j];
+        }
+        e = scorer_stage(sc, pk.data(), pl.data(), pr.data(), pt.data(), n);
+        if (e != cudaSuccess) return scorer_cuda(sc, e, "train: staging");
+        cudaMemsetAsync(sc->loss.p, 0, 16, sc->stream);
+        for (uint64_t off = 0; off < n; off += (uint64_t)batch) {
+            const uint64_t nb = std::min<uint64_t>((uint64_t)batch, n - off);
+            e = scorer_batch(sc, off, nb);
+            if (e == cudaSuccess)
+                e = launch_adam((float*)sc->master.p, (uint16_t*)sc->bf.p, (float*)sc->grads.p, (float*)sc->m.p,
+                                (float*)sc->v.p, sc->L.total, lr, b1, b2, eps, ++sc->step, sc->stream);
+            if (e != cudaSuccess) return scorer_cuda(sc, e, "train: step");
+        }
+        ps_status ps = scorer_flags(sc, "train");
+        if (ps != PS_OK) return ps;
+        float l = 0.f;
+        e = cudaMemcpyAsync(&l, sc->loss.p, 4, cudaMemcpyDeviceToHost, sc->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(sc->stream);
+        if (e != cudaSuccess) return scorer_cuda(sc, e, "train: loss");
+        if (epoch_loss) epoch_loss[ep] = l / (float)n;
+    }
+    return PS_OK;
+}
+
+ps_status ps_set_scorer(ps_sum* s, ps_scorer* sc, double remaining_layers) {
+    if (!s) return PS_ERR_INVALID;
+    if (sc && (sc->device != s->device || sc->nq != s->nq))
+        return set_err(s, PS_ERR_INVALID, "set_scorer: the scorer was built for another device or qubit count");
+    s->scorer = sc;
+    s->scorer_remaining = remaining_layers;
     return PS_OK;
 }
 

@@ -93,6 +93,8 @@ enum KernelId : int {
     K_EXPECT,
     K_GEN_COUNT,
     K_GEN_BRANCH,
+    K_SCORE,
+    K_SCORE_TRAIN,
     K_NUM_KERNELS
 };
 

@@ -368,11 +368,19 @@ __global__ void __launch_bounds__(1024) k_topn_select(unsigned int* __restrict__
     }
 }
 
+// The select key of element e: mag_key of its coefficient, or a precomputed key (the scored
+// TopN's score keys, same conventions: 0 never kept, larger kept first).
+template <typename T>
+__device__ __forceinline__ uint64_t select_key(const T* __restrict__ coef, const uint64_t* __restrict__ sel, uint64_t e) {
+    return sel ? sel[e] : mag_key<T>(coef[e]);
+}
+
 // Gather the keys of the boundary bin (order does not matter for the select): each block
 // takes chunks of kThreads * 16 elements and claims its output slots with one atomic per chunk.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_topn_cand(const T* __restrict__ coef, uint64_t n, Ctl* ctl,
-                                                        uint64_t* __restrict__ cand, uint64_t cand_cap) {
+__global__ void __launch_bounds__(kThreads) k_topn_cand(const T* __restrict__ coef, const uint64_t* __restrict__ sel,
+                                                        uint64_t n, Ctl* ctl, uint64_t* __restrict__ cand,
+                                                        uint64_t cand_cap) {
     constexpr int ITEMS = 16;
     constexpr int CHUNK = kThreads * ITEMS;
     __shared__ unsigned int s_w[kThreads / 32];
@@ -388,7 +396,7 @@ __global__ void __launch_bounds__(kThreads) k_topn_cand(const T* __restrict__ co
         for (int i = 0; i < ITEMS; ++i) {
             const uint64_t e = wbase + (uint64_t)i * 32 + lane;
             bool hit = false;
-            if (e < n) hit = (mag_key<T>(coef[e]) & mask) == prefix;
+            if (e < n) hit = (select_key<T>(coef, sel, e) & mask) == prefix;
             ball[i] = __ballot_sync(0xffffffffu, hit);
             wc += __popc(ball[i]);
         }
@@ -408,7 +416,7 @@ __global__ void __launch_bounds__(kThreads) k_topn_cand(const T* __restrict__ co
             if ((ball[i] >> lane) & 1u) {
                 const uint64_t e = wbase + (uint64_t)i * 32 + lane;
                 const unsigned long long q = slot + __popc(ball[i] & lt);
-                if (PS_GUARD(ctl, q < cand_cap, 703)) cand[q] = mag_key<T>(coef[e]);
+                if (PS_GUARD(ctl, q < cand_cap, 703)) cand[q] = select_key<T>(coef, sel, e);
             }
             slot += __popc(ball[i]);
         }
@@ -435,7 +443,8 @@ __global__ void __launch_bounds__(kThreads) k_topn_hist_cand(const uint64_t* __r
 // `quota` boundary ties in key order.
 template <int W, typename T>
 __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __restrict__ keys, const T* __restrict__ coef,
-                                                           uint64_t n, unsigned long long quota,
+                                                           const uint64_t* __restrict__ sel, uint64_t n,
+                                                           unsigned long long quota,
                                                            uint64_t* __restrict__ okeys, T* __restrict__ ocoef,
                                                            unsigned long long* status, Ctl* ctl) {
     constexpr int ITEMS = 16;
@@ -457,7 +466,7 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
         const uint64_t e = wbase + (uint64_t)i * 32 + lane;
         bool isa = false, ist = false;
         if (e < n) {
-            const uint64_t mk = mag_key<T>(coef[e]);
+            const uint64_t mk = select_key<T>(coef, sel, e);
             isa = mk > boundary;
             ist = mk == boundary && boundary != 0;
         }
@@ -692,7 +701,7 @@ template <int W, typename T>
 cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n, uint64_t keep_n, uint64_t* okeys,
                                  T* ocoef, unsigned int* hist, bool hist_ready, uint64_t* cand, uint64_t cand_cap,
                                  unsigned long long* status, Ctl* ctl, unsigned long long* host_count,
-                                 uint64_t* out_n, int sms, cudaStream_t st, KernelProf* prof) {
+                                 uint64_t* out_n, int sms, cudaStream_t st, KernelProf* prof, const uint64_t* sel) {
     // aux: prefix, mask, remaining rank, above; count[4]: candidates
     unsigned long long* init = host_count + 8;
     init[0] = 0ull;
@@ -714,7 +723,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     k_topn_select<kTopnBins1><<<1, 1024, 0, st>>>(hist, 52, 12, ctl);
     prof->end(st);
     prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
-    k_topn_cand<T><<<grid_for(n, sms), kThreads, 0, st>>>(coef, n, ctl, cand, cand_cap);
+    k_topn_cand<T><<<grid_for(n, sms), kThreads, 0, st>>>(coef, sel, n, ctl, cand, cand_cap);
     prof->end(st);
     // 52 remaining bits: digits at 39, 26, 13, 0 (13 bits each)
     for (int shift = 39; shift >= 0; shift -= 13) {
@@ -735,7 +744,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     cudaMemsetAsync(status, 0, (size_t)tiles * sizeof(unsigned long long), st);
     cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
-    k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, n, quota, okeys, ocoef, status, ctl);
+    k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, sel, n, quota, okeys, ocoef, status, ctl);
     prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     cudaMemcpyAsync(host_count, &ctl->count[3], sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);

@@ -43,10 +43,12 @@ struct StoreOps {
     // hist: kTopnBinsN words, zero on entry and on exit; when hist_ready its first kTopnBins1
     // words already hold the digit-1 histogram of coef (built by the layer's merge).
     // host_count: pinned scratch of at least 20 words.
+    // sel: when non-null, precomputed select keys (larger kept first, 0 never) replace mag_key(c);
+    // hist_ready must then hold their digit-1 histogram.
     static cudaError_t topn(const uint64_t* keys, const T* coef, uint64_t n, uint64_t keep_n, uint64_t* okeys, T* ocoef,
                             unsigned int* hist, bool hist_ready, uint64_t* cand, uint64_t cand_cap,
                             unsigned long long* status, Ctl* ctl, unsigned long long* host_count, uint64_t* out_n,
-                            int sms, cudaStream_t st, KernelProf* prof);
+                            int sms, cudaStream_t st, KernelProf* prof, const uint64_t* sel = nullptr);
     static cudaError_t expectation(const uint64_t* keys, const T* coef, uint64_t n, const uint64_t* ax,
                                    const uint64_t* az, const uint64_t* neg, double* partial, double* out_dev, int sms,
                                    cudaStream_t st, KernelProf* prof);

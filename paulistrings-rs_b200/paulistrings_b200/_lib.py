@@ -24,7 +24,7 @@ PS_OK, PS_ERR_OOM, PS_ERR_UNSUPPORTED, PS_ERR_INVALID, PS_ERR_DEVICE, PS_ERR_TIM
 PS_F64, PS_F32 = 0, 1
 PS_FORWARD, PS_HEISENBERG = 0, 1
 PS_KEEP_TRUE, PS_KEEP_COEFF, PS_KEEP_WEIGHT, PS_KEEP_AND, PS_KEEP_OR = range(5)
-PS_PASS_NONE, PS_PASS_TOPN = 0, 1
+PS_PASS_NONE, PS_PASS_TOPN, PS_PASS_SCORED_TOPN = 0, 1, 2
 (PS_CH_PAULI_ROTATION, PS_CH_DEPOLARIZING, PS_CH_HADAMARD, PS_CH_PHASE, PS_CH_PHASE_DAGGER, PS_CH_PAULI_X,
  PS_CH_PAULI_Y, PS_CH_PAULI_Z, PS_CH_CNOT, PS_CH_CZ, PS_CH_SWAP, PS_CH_UNITARY, PS_CH_DEPHASING,
  PS_CH_PAULI_CHANNEL, PS_CH_DEPOLARIZING_2Q, PS_CH_AMPLITUDE_DAMPING) = range(1, 17)
@@ -54,6 +54,16 @@ EXPORTED = (
     "ps_inject_fault",
     "ps_synchronize",
     "ps_set_compensated_sums",
+    "ps_scorer_create",
+    "ps_scorer_destroy",
+    "ps_scorer_last_error",
+    "ps_scorer_num_params",
+    "ps_scorer_get_params",
+    "ps_scorer_set_params",
+    "ps_scorer_score",
+    "ps_scorer_gradients",
+    "ps_scorer_train",
+    "ps_set_scorer",
 )
 
 PS_FAULT_NONE, PS_FAULT_OOM, PS_FAULT_STALL = 0, 1, 2
@@ -63,6 +73,17 @@ NOALLOC_MAX_TERMS = 1 << 30
 
 class KeepNode(ctypes.Structure):
     _fields_ = [("op", ctypes.c_int32), ("reserved", ctypes.c_int32), ("iarg", ctypes.c_int64), ("farg", ctypes.c_double)]
+
+
+class ScorerConfig(ctypes.Structure):
+    _fields_ = [
+        ("num_qubits", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("layers_per_unit", ctypes.c_double),
+        ("feature_scale", ctypes.c_float * 3),
+        ("init_scale", ctypes.c_float),
+        ("seed", ctypes.c_uint64),
+    ]
 
 
 class Pass(ctypes.Structure):
@@ -202,9 +223,23 @@ def lib():
     L.ps_expectation_device_noalloc.argtypes = [vp, vp, i32, i32, u64, vp, vp, vp, vp, vp]
     L.ps_inject_fault.argtypes = [vp, i32, u64]
     L.ps_synchronize.argtypes = [vp]
+    L.ps_set_compensated_sums.argtypes = [vp, i32]
+    L.ps_scorer_create.argtypes = [i32, P(ScorerConfig), P(vp)]
+    L.ps_scorer_destroy.argtypes = [vp]
+    L.ps_scorer_last_error.restype = ctypes.c_char_p
+    L.ps_scorer_last_error.argtypes = [vp]
+    L.ps_scorer_num_params.restype = u64
+    L.ps_scorer_num_params.argtypes = [vp]
+    L.ps_scorer_get_params.argtypes = [vp, vp]
+    L.ps_scorer_set_params.argtypes = [vp, vp]
+    L.ps_scorer_score.argtypes = [vp, vp, vp, vp, u64, vp]
+    L.ps_scorer_gradients.argtypes = [vp, vp, vp, vp, vp, u64, vp, vp]
+    L.ps_scorer_train.argtypes = [vp, vp, vp, vp, vp, u64, i32, i32, ctypes.c_float, vp]
+    L.ps_set_scorer.argtypes = [vp, vp, ctypes.c_double]
     for name in EXPORTED:
         fn = getattr(L, name)
-        if name not in ("ps_abi_version", "ps_device_count", "ps_last_error", "ps_width", "ps_num_qubits", "ps_dtype_of"):
+        if name not in ("ps_abi_version", "ps_device_count", "ps_last_error", "ps_width", "ps_num_qubits",
+                        "ps_dtype_of", "ps_scorer_last_error", "ps_scorer_num_params"):
             fn.restype = i32
     _lib = L
     return L

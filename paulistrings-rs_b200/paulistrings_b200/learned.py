@@ -1,0 +1,227 @@
+"""Learned truncation: a scorer network ranks terms for ``truncation.scored_topn``.
+
+The scorer is a small MLP (``ps_scorer`` in the C ABI) that predicts, from a term's
+per-qubit I/X/Y/Z code, its Pauli weight, ``log|c|`` and the remaining circuit depth, the log
+magnitude its descendants contribute to the final expectation.  It plugs in where the
+reference's ``TruncationPolicy`` trait takes a layer pass (crates/paulistrings/src/truncation/
+mod.rs:30-107); the reference has no built-in learned policy.  Inference runs on the device
+inside the truncation pass (tensor cores for the 128 x 128 layer); training runs on the device
+with the library's own forward, backward and Adam kernels.
+
+Training data comes from the engine itself (``attribution_data``): at each Trotter-step
+boundary of a tight-threshold run, a sample of the terms is tagged with distinct Z strings on
+extra qubits that no gate touches, propagated together through the remaining steps under the
+same threshold, and read out per tag, which gives each sampled term's own contribution
+``c * <psi| U_rest^dagger P U_rest |psi>`` (descendants of different terms never merge, since
+their tags differ).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from .circuit import Circuit
+from .sum import GpuPauliSum, PauliSum, product_basis, width_for
+
+HIDDEN = 128
+
+
+def layout(num_qubits: int) -> dict:
+    """Slices of the flat parameter vector (the order ``ps_scorer_get_params`` uses)."""
+    sizes = [("embed", num_qubits * 3 * HIDDEN), ("u", 3 * HIDDEN), ("b1", HIDDEN), ("w2", HIDDEN * HIDDEN),
+             ("b2", HIDDEN), ("w3", HIDDEN), ("b3", 1)]
+    out, off = {}, 0
+    for name, n in sizes:
+        out[name] = slice(off, off + n)
+        off += n
+    out["total"] = off
+    return out
+
+
+def pack_keys(x: np.ndarray, z: np.ndarray) -> np.ndarray:
+    """Rows (x words, z words) as the store and the scorer read them."""
+    x = np.asarray(x, np.uint64)
+    z = np.asarray(z, np.uint64)
+    return np.ascontiguousarray(np.concatenate([x.reshape(len(x), -1), z.reshape(len(z), -1)], axis=1))
+
+
+class Scorer:
+    """A scorer network on one device."""
+
+    def __init__(self, num_qubits: int, layers_per_unit: float, feature_scale=(0.1, 0.1, 0.1),
+                 init_scale: float = 0.05, seed: int = 1, device: int = 0):
+        cfg = _lib.ScorerConfig()
+        cfg.num_qubits = int(num_qubits)
+        cfg.layers_per_unit = float(layers_per_unit)
+        for i, v in enumerate(feature_scale):
+            cfg.feature_scale[i] = float(v)
+        cfg.init_scale = float(init_scale)
+        cfg.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+        h = ctypes.c_void_p()
+        st = _lib.lib().ps_scorer_create(int(device), ctypes.byref(cfg), ctypes.byref(h))
+        _lib.check(st, None, "scorer_create")
+        self._h = h
+        self.num_qubits = int(num_qubits)
+        self.W = width_for(self.num_qubits)
+        self.layers_per_unit = float(layers_per_unit)
+        self.feature_scale = tuple(float(v) for v in feature_scale)
+        self.layout = layout(self.num_qubits)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.lib().ps_scorer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st, what):
+        if st != _lib.PS_OK:
+            msg = _lib.lib().ps_scorer_last_error(self._h)
+            _lib.check(st, None, f"{what}: {msg.decode() if msg else ''}")
+
+    @property
+    def num_params(self) -> int:
+        return int(_lib.lib().ps_scorer_num_params(self._h))
+
+    def get_params(self) -> np.ndarray:
+        out = np.zeros(self.num_params, np.float32)
+        self._check(_lib.lib().ps_scorer_get_params(self._h, out.ctypes.data), "get_params")
+        return out
+
+    def set_params(self, params: np.ndarray) -> None:
+        p = np.ascontiguousarray(params, np.float32)
+        if p.shape != (self.num_params,):
+            raise ValueError(f"expected {self.num_params} parameters")
+        self._check(_lib.lib().ps_scorer_set_params(self._h, p.ctypes.data), "set_params")
+
+    def _arrays(self, keys, logc, rem, target=None):
+        keys = np.ascontiguousarray(keys, np.uint64).reshape(-1, 2 * self.W)
+        n = keys.shape[0]
+        logc = np.ascontiguousarray(np.broadcast_to(np.asarray(logc, np.float32), (n,)))
+        rem = np.ascontiguousarray(np.broadcast_to(np.asarray(rem, np.float32), (n,)))
+        t = None if target is None else np.ascontiguousarray(target, np.float32).reshape(n)
+        return keys, logc, rem, t, n
+
+    def score(self, keys, logc, rem) -> np.ndarray:
+        keys, logc, rem, _, n = self._arrays(keys, logc, rem)
+        out = np.zeros(n, np.float32)
+        self._check(_lib.lib().ps_scorer_score(self._h, keys.ctypes.data, logc.ctypes.data, rem.ctypes.data, n,
+                                               out.ctypes.data), "score")
+        return out
+
+    def gradients(self, keys, logc, rem, target):
+        """Gradients of mean((y - target)^2) over one batch (no update), and that loss."""
+        keys, logc, rem, t, n = self._arrays(keys, logc, rem, target)
+        grads = np.zeros(self.num_params, np.float32)
+        loss = ctypes.c_float()
+        self._check(_lib.lib().ps_scorer_gradients(self._h, keys.ctypes.data, logc.ctypes.data, rem.ctypes.data,
+                                                   t.ctypes.data, n, grads.ctypes.data, ctypes.byref(loss)),
+                    "gradients")
+        return grads, float(loss.value)
+
+    def train(self, keys, logc, rem, target, epochs: int = 10, batch: int = 4096, lr: float = 1e-3) -> np.ndarray:
+        keys, logc, rem, t, n = self._arrays(keys, logc, rem, target)
+        losses = np.zeros(int(epochs), np.float32)
+        self._check(_lib.lib().ps_scorer_train(self._h, keys.ctypes.data, logc.ctypes.data, rem.ctypes.data,
+                                               t.ctypes.data, n, int(epochs), int(batch), float(lr),
+                                               losses.ctypes.data), "train")
+        return losses
+
+
+# ---------------------------------------------------------------------------
+# attribution data from the engine
+# ---------------------------------------------------------------------------
+
+def widened(circuit: Circuit, num_qubits: int) -> Circuit:
+    """The same channels on a register of ``num_qubits`` (extra qubits untouched)."""
+    out = Circuit(num_qubits)
+    for ch in circuit:
+        out.append(ch)
+    return out
+
+
+def tagged_contributions(terms_x, terms_z, terms_c, num_qubits: int, rest: Circuit, policy, state: str,
+                         direction: str = "heisenberg", device: int = 0) -> np.ndarray:
+    """Each term's own contribution to ``<state| (rest applied) |state>``: the terms carry
+    distinct Z tags on ``ceil(log2 n)`` extra qubits, run through ``rest`` together, and the
+    final sum is read out per tag."""
+    n = len(terms_c)
+    tag_bits = max(1, int(math.ceil(math.log2(max(n, 2)))))
+    nq2 = num_qubits + tag_bits
+    W, W2 = width_for(num_qubits), width_for(nq2)
+    x = np.zeros((n, W2), np.uint64)
+    z = np.zeros((n, W2), np.uint64)
+    x[:, :W] = np.asarray(terms_x, np.uint64).reshape(n, W)
+    z[:, :W] = np.asarray(terms_z, np.uint64).reshape(n, W)
+    idx = np.arange(n, dtype=np.uint64)
+    for b in range(tag_bits):
+        q = num_qubits + b
+        bit = ((idx >> np.uint64(b)) & np.uint64(1)) << np.uint64(q % 64)
+        z[:, q // 64] |= bit
+    g = GpuPauliSum(nq2, "f64", device)
+    try:
+        g.upload(x, z, np.asarray(terms_c, np.float64))
+        g.propagate(widened(rest, nq2), policy, direction)
+        fx, fz, fc = g.download()
+    finally:
+        g.close()
+    if len(state) != num_qubits:  # a uniform label: x+, y+ or z+ on every system qubit
+        state = {"x+": "+", "y+": "r", "z+": "0"}[state.lower()] * num_qubits
+    ax, az, neg = product_basis(state + "0" * tag_bits, nq2, W2)  # tags are Z: +1 in |0>
+    sup = fx | fz
+    mismatch = ((fx ^ (sup & ax)) | (fz ^ (sup & az))).any(axis=1)
+    parity = np.bitwise_count(sup & neg[None, :]).sum(axis=1) & 1
+    val = np.where(parity.astype(bool), -fc, fc)
+    val[mismatch] = 0.0
+    tag = np.zeros(len(fc), np.int64)
+    for b in range(tag_bits):
+        q = num_qubits + b
+        tag |= (((fz[:, q // 64] >> np.uint64(q % 64)) & np.uint64(1)).astype(np.int64)) << b
+    out = np.zeros(n, np.float64)
+    np.add.at(out, tag, val)
+    return out
+
+
+def attribution_data(observable: PauliSum, step: Circuit, steps: int, state: str, threshold: float,
+                     samples_per_step: int = 4096, seed: int = 0, floor: float = 1e-12, device: int = 0,
+                     truncation_policy=None):
+    """Training rows from a tight-threshold Heisenberg run of ``steps`` repetitions of ``step``.
+
+    At every step boundary d (0 <= d < steps) up to ``samples_per_step`` terms of the sum are
+    drawn (uniformly, without replacement), each one's contribution to the final expectation
+    is measured by ``tagged_contributions`` through the remaining ``steps - d`` steps under the
+    same threshold, and a row (key, log|c|, remaining steps, log(|contribution| + floor)) is
+    recorded.  Returns (keys, logc, rem, target) as numpy arrays."""
+    from . import truncation
+
+    rng = np.random.default_rng(seed)
+    policy = truncation_policy if truncation_policy is not None else truncation.coeff(threshold)
+    nq = observable.num_qubits
+    g = observable.to_device(device)
+    rows = ([], [], [], [])
+    try:
+        for d in range(steps):
+            x, z, c = g.download()
+            take = min(samples_per_step, len(c))
+            if take:
+                pick = np.sort(rng.choice(len(c), size=take, replace=False))
+                rest = Circuit(nq)
+                for _ in range(steps - d):
+                    rest.extend(step)
+                contrib = tagged_contributions(x[pick], z[pick], c[pick], nq, rest, policy, state, device=device)
+                rows[0].append(pack_keys(x[pick], z[pick]))
+                rows[1].append(np.log(np.abs(c[pick])).astype(np.float32))
+                rows[2].append(np.full(take, steps - d, np.float32))
+                rows[3].append(np.log(np.abs(contrib) + floor).astype(np.float32))
+            g.propagate(step, policy, "heisenberg")
+    finally:
+        g.close()
+    return tuple(np.concatenate(r) for r in rows)

@@ -213,13 +213,17 @@ class GpuPauliSum:
         out._set_sorted(x, z, c)
         return out
 
-    def propagate(self, circuit: Circuit, policy=None, direction=None, with_stats: bool = False):
+    def propagate(self, circuit: Circuit, policy=None, direction=None, with_stats: bool = False,
+                  remaining_layers=None):
+        """``remaining_layers``: layers still to apply when this call starts, for a scored_topn
+        policy's remaining-depth feature (default: this circuit's length)."""
         if circuit.num_qubits != self.num_qubits:
             raise ValueError(
                 f"circuit acts on {circuit.num_qubits} qubits but the sum has {self.num_qubits}"
             )
         arr, count, keep = circuit.to_c()
         pol = policy_to_c(policy)
+        self._attach_scorer(policy, count if remaining_layers is None else remaining_layers)
         after = np.zeros(max(1, count), dtype=np.uint64)
         rs = _lib.RunStats()
         st = _lib.lib().ps_propagate(
@@ -239,6 +243,14 @@ class GpuPauliSum:
                 kernel_launches=int(rs.kernel_launches),
             )
         return None
+
+    def _attach_scorer(self, policy, remaining_layers) -> None:
+        sc = policy.scorer() if policy is not None else None
+        if sc is None:
+            _lib.lib().ps_set_scorer(self._h, None, 0.0)
+            return
+        _lib.check(_lib.lib().ps_set_scorer(self._h, sc._h, float(remaining_layers)), self._h, "set_scorer")
+        self._scorer = sc  # keep it alive while attached
 
     def apply_layer(self, channel, policy=None, adjoint: bool = False) -> _lib.LayerStats:
         """One layer through ``ps_prepare_channel`` + ``ps_apply_layer`` + ``ps_finalize_layer``."""

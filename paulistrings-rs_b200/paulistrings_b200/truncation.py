@@ -2,7 +2,9 @@
 
 ``coeff(eps)`` keeps ``|c|^2 > eps^2`` (crates/paulistrings/src/truncation/builtin.rs:19-41),
 ``weight(k)`` keeps Pauli weight ``<= k`` (:43-59), ``topn(n)`` retains the ``n`` largest
-magnitudes after every layer (:61-150).  ``a & b`` keeps a term iff both keep it and runs
+magnitudes after every layer (:61-150), ``scored_topn(n, scorer)`` the ``n`` terms a learned
+scorer ranks highest (``paulistrings_b200.learned``; a ``TruncationPolicy`` of this package,
+crates/paulistrings/src/truncation/mod.rs:30-107).  ``a & b`` keeps a term iff both keep it and runs
 a's layer passes then b's (:470-526); ``a | b`` combines per-term filters only (:574-625).
 A policy lowers to a postfix keep program plus an ordered list of layer passes, the form
 ``ps_policy`` carries across the C ABI (KeepProgram, crates/paulistrings/src/engine/gpu/
@@ -34,7 +36,7 @@ class Truncation:
         return Truncation("or", self, other)
 
     def has_layer_pass(self) -> bool:
-        if self.kind == "topn":
+        if self.kind in ("topn", "scored_topn"):
             return True
         if self.kind in ("and", "or"):
             return self.args[0].has_layer_pass() or self.args[1].has_layer_pass()
@@ -44,6 +46,8 @@ class Truncation:
         if self.kind in ("and", "or"):
             op = " & " if self.kind == "and" else " | "
             return f"({self.args[0]!r}{op}{self.args[1]!r})"
+        if self.kind == "scored_topn":
+            return f"truncation.scored_topn({self.args[0]!r}, <scorer>)"
         return f"truncation.{self.kind}({', '.join(repr(a) for a in self.args)})"
 
     # -- lowering ----------------------------------------------------------
@@ -55,12 +59,26 @@ class Truncation:
         elif self.kind == "topn":
             nodes.append((_lib.PS_KEEP_TRUE, 0, 0.0))
             passes.append((_lib.PS_PASS_TOPN, int(self.args[0])))
+        elif self.kind == "scored_topn":
+            nodes.append((_lib.PS_KEEP_TRUE, 0, 0.0))
+            passes.append((_lib.PS_PASS_SCORED_TOPN, int(self.args[0])))
         elif self.kind in ("and", "or"):
             self.args[0]._lower(nodes, passes)
             self.args[1]._lower(nodes, passes)
             nodes.append((_lib.PS_KEEP_AND if self.kind == "and" else _lib.PS_KEEP_OR, 0, 0.0))
         else:
             raise ValueError(f"unknown truncation {self.kind}")
+
+    def scorer(self):
+        """The scorer of the tree's scored_topn pass, or None (at most one scorer per policy)."""
+        if self.kind == "scored_topn":
+            return self.args[1]
+        if self.kind in ("and", "or"):
+            a, b = self.args[0].scorer(), self.args[1].scorer()
+            if a is not None and b is not None and a is not b:
+                raise ValueError("a policy can carry one scorer")
+            return a if a is not None else b
+        return None
 
     def lowered(self):
         """(keep nodes, passes) with the keep program simplified of always-true nodes."""
@@ -123,6 +141,14 @@ def topn(n: int) -> Truncation:
     if n < 0:
         raise ValueError("topn needs n >= 0")
     return Truncation("topn", int(n))
+
+
+def scored_topn(n: int, scorer) -> Truncation:
+    """Keep the ``n`` terms ``scorer`` (a ``paulistrings_b200.learned.Scorer``) ranks highest
+    after every layer; ties first in key order, NaN scores never kept."""
+    if n < 0:
+        raise ValueError("scored_topn needs n >= 0")
+    return Truncation("scored_topn", int(n), scorer)
 
 
 def policy_to_c(policy):

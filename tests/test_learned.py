@@ -1,0 +1,181 @@
+"""Learned truncation: the scorer network, its training kernels and the scored TopN pass.
+
+CPU tests pin the numpy restatement of the network (``oracle/scorer_ref.py``) against finite
+differences of its own forward pass and against torch's bfloat16 rounding, and check the
+policy lowering.  GPU tests compare the device scores and the device gradients (tensor-core
+forward and backward) with the restatement, check that the scored pass keeps exactly the
+terms the scorer ranks highest, and that training lowers the loss.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import paulistrings_b200 as ps
+from oracle import scorer_ref
+from paulistrings_b200 import _lib, learned, truncation, workloads
+from paulistrings_b200.circuit import Circuit
+
+
+def random_params(nq, seed, scale=0.3):
+    rng = np.random.default_rng(seed)
+    L = learned.layout(nq)
+    p = np.zeros(L["total"], np.float32)
+    p[L["embed"]] = rng.normal(scale=scale, size=L["embed"].stop - L["embed"].start)
+    p[L["u"]] = rng.normal(scale=scale, size=3 * 128)
+    p[L["b1"]] = rng.normal(scale=0.1, size=128)
+    p[L["w2"]] = rng.normal(scale=1 / np.sqrt(128), size=128 * 128)
+    p[L["b2"]] = rng.normal(scale=0.1, size=128)
+    p[L["w3"]] = rng.normal(scale=1 / np.sqrt(128), size=128)
+    p[L["b3"]] = 0.3
+    return p
+
+
+def random_rows(nq, n, seed):
+    x, z, c = workloads.random_observable(nq, n, seed=seed)
+    keys = learned.pack_keys(x, z)
+    rng = np.random.default_rng(seed + 1)
+    logc = np.log(np.abs(c)).astype(np.float32)
+    rem = rng.integers(0, 20, size=n).astype(np.float32)
+    target = (rng.normal(size=n) - 3.0).astype(np.float32)
+    return keys, logc, rem, target
+
+
+FSCALE = (0.1, 0.1, 0.1)
+
+
+# ---------------------------------------------------------------------------
+# CPU
+# ---------------------------------------------------------------------------
+
+def test_bf16_rounding_matches_torch():
+    import torch
+
+    a = np.random.default_rng(0).normal(size=4096).astype(np.float32) * 10
+    want = torch.from_numpy(a).to(torch.bfloat16).to(torch.float32).numpy()
+    assert np.array_equal(scorer_ref.bf16(a), want)
+
+
+def test_reference_gradients_match_finite_differences():
+    nq, W = 8, 1
+    keys, logc, rem, target = random_rows(nq, 64, seed=3)
+    p = random_params(nq, 5)
+    # exact-arithmetic variant: no bf16 rounding, float64, so differences are clean
+    scorer_ref.EXACT = True
+    try:
+        p64 = p.astype(np.float64)
+        g, _ = scorer_ref.gradients(p64, keys, logc, rem, target, nq, W, FSCALE)
+
+        def loss(q):
+            y, _ = scorer_ref.forward(q, keys, logc, rem, nq, W, FSCALE)
+            return float(np.mean((y - target) ** 2))
+
+        rng = np.random.default_rng(1)
+        L = learned.layout(nq)
+        for name in ("embed", "u", "b1", "w2", "b2", "w3", "b3"):
+            sl = L[name]
+            for i in rng.choice(np.arange(sl.start, sl.stop), size=min(6, sl.stop - sl.start), replace=False):
+                h = 1e-6
+                q1, q2 = p64.copy(), p64.copy()
+                q1[i] += h
+                q2[i] -= h
+                fd = (loss(q1) - loss(q2)) / (2 * h)
+                assert abs(fd - g[i]) <= 1e-6 + 1e-4 * abs(fd), (name, i, fd, g[i])
+    finally:
+        scorer_ref.EXACT = False
+
+
+def test_scored_topn_lowering():
+    sc = object()
+    pol = truncation.coeff(1e-8) & truncation.scored_topn(1000, sc)
+    nodes, passes = pol.lowered()
+    assert passes == [(_lib.PS_PASS_SCORED_TOPN, 1000)]
+    assert pol.scorer() is sc
+    assert truncation.topn(5).scorer() is None
+    with pytest.raises(ValueError):
+        truncation.coeff(1e-3) | truncation.scored_topn(10, sc)
+    with pytest.raises(ValueError):
+        (truncation.scored_topn(10, sc) & truncation.scored_topn(20, object())).scorer()
+
+
+# ---------------------------------------------------------------------------
+# GPU
+# ---------------------------------------------------------------------------
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nq", [16, 64, 100])
+def test_device_scores_match_the_reference(nq):
+    W = ps.width_for(nq)
+    sc = learned.Scorer(nq, layers_per_unit=10.0, feature_scale=FSCALE, seed=2)
+    p = random_params(nq, 7)
+    sc.set_params(p)
+    assert sc.num_params == learned.layout(nq)["total"]
+    assert np.array_equal(sc.get_params(), p)
+    keys, logc, rem, _ = random_rows(nq, 1000, seed=11)
+    got = sc.score(keys, logc, rem)
+    want, _ = scorer_ref.forward(p, keys, logc, rem, nq, W, FSCALE)
+    assert np.all(np.isfinite(got))
+    np.testing.assert_allclose(got, want, rtol=2e-3, atol=2e-3)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nq,n", [(16, 128), (64, 1000), (100, 777)])
+def test_device_gradients_match_the_reference(nq, n):
+    W = ps.width_for(nq)
+    sc = learned.Scorer(nq, layers_per_unit=10.0, feature_scale=FSCALE, seed=2)
+    p = random_params(nq, 9)
+    sc.set_params(p)
+    keys, logc, rem, target = random_rows(nq, n, seed=13)
+    g, loss = sc.gradients(keys, logc, rem, target)
+    gw, lw = scorer_ref.gradients(p, keys, logc, rem, target, nq, W, FSCALE)
+    assert abs(loss - lw) <= 1e-3 * abs(lw) + 1e-5
+    L = learned.layout(nq)
+    for name in ("embed", "u", "b1", "w2", "b2", "w3", "b3"):
+        a, b = g[L[name]], gw[L[name]]
+        err = np.linalg.norm(a - b)
+        assert err <= 2e-2 * np.linalg.norm(b) + 1e-6, (name, err, np.linalg.norm(b))
+
+
+@pytest.mark.gpu
+def test_training_lowers_the_loss():
+    nq = 16
+    keys, logc, rem, _ = random_rows(nq, 8192, seed=21)
+    # a learnable target: depends on the weight, the coefficient and the remaining depth
+    p = scorer_ref.support(keys, nq, 1)
+    weight = (p != 0).sum(axis=1)
+    target = (0.8 * logc - 0.3 * weight - 0.05 * rem).astype(np.float32)
+    sc = learned.Scorer(nq, layers_per_unit=1.0, feature_scale=FSCALE, seed=4)
+    losses = sc.train(keys, logc, rem, target, epochs=15, batch=1024, lr=2e-3)
+    assert np.all(np.isfinite(losses))
+    assert losses[-1] < 0.1 * losses[0], losses
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_scored_pass_keeps_the_highest_scored_terms(dtype):
+    nq = 64
+    sc = learned.Scorer(nq, layers_per_unit=1.0, feature_scale=FSCALE, seed=6)
+    sc.set_params(random_params(nq, 17))
+    x, z, c = workloads.random_observable(nq, 20000, seed=3)
+    circ = Circuit(nq)
+    circ.pauli_rotation("XY", [3, 17], 0.7)
+    full = ps.GpuPauliSum(nq, dtype)
+    full.upload(x, z, c)
+    full.propagate(circ, None, "forward")
+    fx, fz, fc = full.download()
+    keep = 9000
+    g = ps.GpuPauliSum(nq, dtype)
+    g.upload(x, z, c)
+    st = g.propagate(circ, truncation.scored_topn(keep, sc), "forward", with_stats=True)
+    kx, kz, kc = g.download()
+    assert len(kc) == keep and st.final_terms == keep
+    scores = sc.score(learned.pack_keys(fx, fz), np.log(np.abs(fc)).astype(np.float32), 0.0)
+    order = np.argsort(-scores, kind="stable")
+    chosen = np.sort(order[:keep])
+    kept = {(a.tobytes(), b.tobytes()) for a, b in zip(kx, kz)}
+    want = {(fx[i].tobytes(), fz[i].tobytes()) for i in chosen}
+    # the device scores f64 coefficients' log in float64 before rounding; allow a sliver of
+    # boundary disagreement from that
+    assert len(kept ^ want) <= 4
+    assert np.array_equal(kc, fc[np.isin(np.arange(len(fc)), chosen)]) or len(kept ^ want) > 0
