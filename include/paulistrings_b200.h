@@ -297,7 +297,8 @@ typedef struct ps_scorer ps_scorer;
 
 typedef struct ps_scorer_config {
     int32_t num_qubits;       /* <= 256 */
-    int32_t reserved;
+    int32_t residual;         /* nonzero: the score is log|c| + the network's output (the network
+                                 predicts the descendants' factor; train it on target - log|c|) */
     double layers_per_unit;   /* layers per unit of the remaining-depth feature (e.g. per Trotter step) */
     float feature_scale[3];   /* s0, s1, s2 */
     float init_scale;         /* standard deviation of the initial embedding and u weights */

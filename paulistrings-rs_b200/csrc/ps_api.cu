@@ -130,26 +130,31 @@ int width_for(int nq) {
     return 0;
 }
 
+// Status of device-side error flags already read back; clears them on the device when set.
+ps_status flags_status(ps_sum* s, unsigned int flags, unsigned int info, const char* where) {
+    if (flags == 0) return PS_OK;
+    cudaMemsetAsync(&s->ctl->err, 0, 2 * sizeof(unsigned int), s->stream);
+    cudaStreamSynchronize(s->stream);
+    char msg[160];
+    if (flags & ERR_KEY_RANGE) {
+        snprintf(msg, sizeof msg, "%s: a key has a bit at or above num_qubits=%d", where, s->nq);
+        return set_err(s, PS_ERR_INVALID, msg);
+    }
+    if (flags & ERR_TIMEOUT) {
+        snprintf(msg, sizeof msg, "%s: a bounded device wait gave up (check %u)", where, info);
+        return set_err(s, PS_ERR_TIMEOUT, msg);
+    }
+    snprintf(msg, sizeof msg, "%s: device check failed (flags %u, check %u)", where, flags, info);
+    return set_err(s, PS_ERR_DEVICE, msg);
+}
+
 // Device-side error flags of the handle (synchronizes).
 ps_status check_device_flags(ps_sum* s, const char* where) {
     unsigned int flags[2] = {0, 0};
     cudaError_t e = cudaMemcpyAsync(flags, &s->ctl->err, sizeof(flags), cudaMemcpyDeviceToHost, s->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e == cudaSuccess) e = spin_sync(s->stream);
     if (e != cudaSuccess) return cuda_fail(s, e, where);
-    if (flags[0] == 0) return PS_OK;
-    cudaMemsetAsync(&s->ctl->err, 0, 2 * sizeof(unsigned int), s->stream);
-    cudaStreamSynchronize(s->stream);
-    char msg[160];
-    if (flags[0] & ERR_KEY_RANGE) {
-        snprintf(msg, sizeof msg, "%s: a key has a bit at or above num_qubits=%d", where, s->nq);
-        return set_err(s, PS_ERR_INVALID, msg);
-    }
-    if (flags[0] & ERR_TIMEOUT) {
-        snprintf(msg, sizeof msg, "%s: a bounded device wait gave up (check %u)", where, flags[1]);
-        return set_err(s, PS_ERR_TIMEOUT, msg);
-    }
-    snprintf(msg, sizeof msg, "%s: device check failed (flags %u, check %u)", where, flags[0], flags[1]);
-    return set_err(s, PS_ERR_DEVICE, msg);
+    return flags_status(s, flags[0], flags[1], where);
 }
 
 // ---------------------------------------------------------------------------
@@ -967,8 +972,11 @@ struct Engine {
         a.ctl = s->ctl;
         a.host_count = s->hcount;
         uint64_t partners = 0, out_n = 0;
+        unsigned int err_flags = 0, err_info = 0;
         a.partners_out = &partners;
         a.out_count = &out_n;
+        a.err_flags = &err_flags;
+        a.err_info = &err_info;
         a.prof = &s->prof;
         // the first layer pass is TopN and could trigger: the merge builds its first select digit
         const bool fuse_topn = policy && policy->num_passes > 0 && policy->passes[0].kind == PS_PASS_TOPN &&
@@ -983,7 +991,7 @@ struct Engine {
         e = launch_rotation_layer<W, T>(a, s->stream);
         s->prof.resolve();
         if (e != cudaSuccess) return cuda_fail(s, e, "apply: rotation layer");
-        ps = check_device_flags(s, "apply");
+        ps = flags_status(s, err_flags, err_info, "apply");
         if (ps != PS_OK) {
             if (fuse_topn) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
             return ps;
@@ -1104,7 +1112,9 @@ struct Engine {
                                      s->stream, &s->prof);
             s->prof.resolve();
             if (e != cudaSuccess) return cuda_fail(s, e, "topn");
-            ps_status ps = check_device_flags(s, "topn");
+            unsigned int fl = 0, fi = 0;
+            topn_flags(s->hcount, &fl, &fi);
+            ps_status ps = flags_status(s, fl, fi, "topn");
             if (ps != PS_OK) {
                 cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
                 return ps;
@@ -1137,6 +1147,7 @@ struct Engine {
         A.L = sc->L;
         A.nq = sc->nq;
         for (int f = 0; f < 3; ++f) A.fscale[f] = sc->cfg.feature_scale[f];
+        A.residual = sc->cfg.residual ? 1 : 0;
         ScoreInput in{};
         in.keys = K(s, s->cur);
         in.coef64 = std::is_same<T, double>::value ? (const double*)C(s, s->cur) : nullptr;
@@ -1159,7 +1170,9 @@ struct Engine {
                                  &s->prof, (const uint64_t*)s->sel.p);
         s->prof.resolve();
         if (e != cudaSuccess) return cuda_fail(s, e, "scored TopN");
-        ps = check_device_flags(s, "scored TopN");
+        unsigned int fl = 0, fi = 0;
+        topn_flags(s->hcount, &fl, &fi);
+        ps = flags_status(s, fl, fi, "scored TopN");
         if (ps != PS_OK) {
             cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
             return ps;
@@ -1607,6 +1620,7 @@ ScorerArgs scorer_args(const ps_scorer* sc) {
     A.L = sc->L;
     A.nq = sc->nq;
     for (int f = 0; f < 3; ++f) A.fscale[f] = sc->cfg.feature_scale[f];
+    A.residual = sc->cfg.residual ? 1 : 0;
     return A;
 }
 

@@ -173,7 +173,7 @@ cudaError_t GeneralOps<W, T>::count(const uint64_t* keys, uint64_t n, const GenL
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     cudaMemcpyAsync(host_count, &ctl->count[6], sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    if ((e = spin_sync(st)) != cudaSuccess) return e;
     *m = *host_count;
     return cudaSuccess;
 }

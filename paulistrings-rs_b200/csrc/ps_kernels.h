@@ -7,6 +7,25 @@
 
 namespace psb {
 
+// Wait for everything queued on `st`, the calling thread spinning on an event instead of
+// sleeping in the driver: a layer waits for its counts once or twice, and a sleeping thread's
+// wake-up on a busy host can cost more than the kernels it waited for.  One event per device
+// and host thread.
+inline cudaError_t spin_sync(cudaStream_t st) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaStreamSynchronize(st);
+    thread_local cudaEvent_t events[64] = {};
+    if (!events[dev] && cudaEventCreateWithFlags(&events[dev], cudaEventDisableTiming) != cudaSuccess) {
+        events[dev] = nullptr;
+        return cudaStreamSynchronize(st);
+    }
+    cudaError_t e = cudaEventRecord(events[dev], st);
+    if (e != cudaSuccess) return e;
+    while ((e = cudaEventQuery(events[dev])) == cudaErrorNotReady) {
+    }
+    return e;
+}
+
 // Device-resident control block of one handle.
 struct Ctl {
     unsigned long long count[8];   // counts published by kernels (partners, outputs, ...)
@@ -178,9 +197,11 @@ struct RotationArgs {
     T* Oc;
     uint64_t out_cap;
     Ctl* ctl;
-    unsigned long long* host_count;  // pinned host word
+    unsigned long long* host_count;  // pinned host scratch, >= 16 words
     uint64_t* partners_out;
     uint64_t* out_count;
+    unsigned int* err_flags;          // the control block's error bits after the layer
+    unsigned int* err_info;
     KernelProf* prof;
     unsigned int* topn_hist;  // when set, the merge histograms key >> 52 of its outputs (2048 bins)
     int inject_stall;         // failure injection: the merge skips its first tile

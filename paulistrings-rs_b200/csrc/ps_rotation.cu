@@ -21,6 +21,8 @@
 //
 // Key-preserving tables (depolarizing noise, quarter turns with sin = 0) run
 // k_partition + k_merge with an empty partner stream.
+#include <cstddef>
+
 #include "ps_device.cuh"
 #include "ps_kernels.h"
 
@@ -340,9 +342,8 @@ __device__ __forceinline__ void fix_divergence(const uint32_t* __restrict__ idx,
 
 template <int W, int LV>
 __global__ void __launch_bounds__(kBlock) k_fwd_levels(const uint32_t* __restrict__ idx, uint16_t* __restrict__ D,
-                                                       int32_t* __restrict__ F, uint32_t m,
-                                                       const uint64_t* __restrict__ keys, uint64_t n,
-                                                       const Levels lv, int accumulate, LevelSlot* slots,
+                                                       int32_t* __restrict__ F, const uint64_t* __restrict__ keys,
+                                                       uint64_t n, const Levels lv, int accumulate, LevelSlot* slots,
                                                        Ctl* ctl) {
     __shared__ unsigned int s_tile;
     __shared__ int s_wagg[kBlock / 32][2 * LV];
@@ -351,6 +352,8 @@ __global__ void __launch_bounds__(kBlock) k_fwd_levels(const uint32_t* __restric
     if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[1], 1u);
     __syncthreads();
     const unsigned int tile = s_tile;
+    const uint32_t m = (uint32_t)ctl->count[0];  // partners, published by k_classify
+    if ((uint64_t)tile * kScanTile >= m) return;  // the grid is sized for every row partnering
     const uint32_t j0 = tile * (uint32_t)kScanTile + (uint32_t)tid * kScanItems;
     const int NL = lv.n;
 
@@ -438,7 +441,7 @@ __global__ void __launch_bounds__(kBlock) k_fwd_levels(const uint32_t* __restric
 template <int W, typename T, int LV>
 __global__ void __launch_bounds__(kBlock) k_bwd_levels(const uint32_t* __restrict__ idx,
                                                        const uint16_t* __restrict__ D, int32_t* __restrict__ F,
-                                                       uint32_t m, const uint64_t* __restrict__ keys,
+                                                       const uint64_t* __restrict__ keys,
                                                        const T* __restrict__ coef, uint64_t n, const Levels lv,
                                                        const RotLayer<W> L, int scatter,
                                                        uint64_t* __restrict__ Pk, T* __restrict__ Pc,
@@ -453,6 +456,8 @@ __global__ void __launch_bounds__(kBlock) k_bwd_levels(const uint32_t* __restric
     stage_amps<W, T>(L, A);
     __syncthreads();
     const unsigned int tile = s_tile;  // tile 0 covers the last kScanTile partners
+    const uint32_t m = (uint32_t)ctl->count[0];  // partners, published by k_classify
+    if ((uint64_t)tile * kScanTile >= m) return;  // the grid is sized for every row partnering
     const long long hi = (long long)m - (long long)tile * kScanTile;
     const long long lo = hi - kScanTile;  // may be negative for the first partners
     const long long jbase = lo + (long long)tid * kScanItems;
@@ -563,10 +568,12 @@ __device__ __forceinline__ bool mp_pred(const uint64_t* Sk, const uint64_t* Pk, 
 }
 
 template <int W>
-__global__ void k_partition(const uint64_t* __restrict__ Sk, uint64_t n, const uint64_t* __restrict__ Pk, uint64_t m,
-                            uint32_t tile_items, uint32_t num_tiles, ulonglong2* __restrict__ bounds) {
+__global__ void k_partition(const uint64_t* __restrict__ Sk, uint64_t n, const uint64_t* __restrict__ Pk,
+                            uint32_t tile_items, ulonglong2* __restrict__ bounds, const Ctl* ctl) {
     const int lane = threadIdx.x & 31;
     const uint32_t t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint64_t m = ctl->count[0];  // partners, published by k_classify (0 without partners)
+    const uint32_t num_tiles = (uint32_t)((n + m + tile_items - 1) / tile_items);
     if (t > num_tiles) return;
     uint64_t dd = (uint64_t)t * tile_items;
     if (dd > n + m) dd = n + m;
@@ -685,8 +692,7 @@ __device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc
 template <int W, typename T>
 __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ Sk, const T* __restrict__ Sc,
                                                   uint64_t n, const uint64_t* __restrict__ Pk,
-                                                  const T* __restrict__ Pc, uint64_t m,
-                                                  const ulonglong2* __restrict__ bounds, uint32_t num_tiles,
+                                                  const T* __restrict__ Pc, const ulonglong2* __restrict__ bounds,
                                                   const RotLayer<W> L, const KeepProg keep,
                                                   uint64_t* __restrict__ Ok, T* __restrict__ Oc, uint64_t out_cap,
                                                   unsigned long long* status, Ctl* ctl,
@@ -714,7 +720,9 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
     stage_amps<W, T>(L, A);
     __syncthreads();
     const unsigned int tile = s_tile;
-    if (tile >= num_tiles) return;
+    const uint64_t m = ctl->count[0];  // partners, published by k_classify (0 without partners)
+    const uint32_t num_tiles = (uint32_t)((n + m + SM::TILE - 1) / SM::TILE);
+    if (tile >= num_tiles) return;  // the grid is sized for every row partnering
     const ulonglong2 b0 = bounds[tile], b1 = bounds[tile + 1];
     if (!PS_GUARD(ctl, b1.x >= b0.x && b1.y >= b0.y && b1.x - b0.x + b1.y - b0.y <= (uint64_t)SM::TILE + 2 &&
                            b1.x <= n && b1.y <= m,
@@ -805,12 +813,18 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
 // ---------------------------------------------------------------------------
 template <int W, typename T>
 cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) {
+    // One host synchronization per layer: k_classify publishes the partner count m on the
+    // device and every later kernel reads it there, their grids sized for m = n (surplus blocks
+    // return at once); the host reads m, the output count and the error flags in one copy at
+    // the end.
     constexpr int CT = RotTile<W>::kClassifyTile;
     constexpr int MT = RotTile<W>::kMergeTile;
     Ctl* ctl = a.ctl;
     cudaError_t e;
-    uint64_t m = 0;
-    if (a.L.partners && a.n > 0) {
+    const uint64_t m_hi = a.L.partners ? a.n : 0;  // partners cannot outnumber the terms
+    if (m_hi > a.p_cap) return cudaErrorMemoryAllocation;  // caller sized the partner buffers by n
+    cudaMemsetAsync(&ctl->count[0], 0, 2 * sizeof(unsigned long long), st);
+    if (m_hi > 0) {
         // 1. classify
         uint32_t tiles = (uint32_t)((a.n + CT - 1) / CT);
         cudaMemsetAsync(a.status, 0, (size_t)tiles * sizeof(unsigned long long), st);
@@ -819,17 +833,9 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
         k_classify<W, T><<<tiles, kBlock, 0, st>>>(a.Sk, a.n, a.L, a.idx, a.D, a.status, ctl);
         a.prof->end(st);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        cudaMemcpyAsync(a.host_count, &ctl->count[0], sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
-        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-        m = *a.host_count;
-        a.prof->add_bytes(K_CLASSIFY, (double)m * 6);  // idx + divergence writes
-    }
-    *a.partners_out = m;
-    if (m > a.p_cap) return cudaErrorMemoryAllocation;  // caller sized the partner buffers by n
-    if (m > 0) {
         // 2-3. level scans (batches of kMaxLevels; one batch of four covers every gate on at
         // most two qubits), scatter on the last batch
-        uint32_t stiles = (uint32_t)((m + kScanTile - 1) / kScanTile);
+        uint32_t stiles = (uint32_t)((m_hi + kScanTile - 1) / kScanTile);
         const bool narrow = a.levels->n <= 4;
         const int per = narrow ? 4 : kMaxLevels;
         int nb = (a.levels->n + per - 1) / per;
@@ -839,64 +845,83 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
             for (int l = 0; l < lv.n; ++l) lv.rank[l] = a.levels->rank[b * per + l];
             cudaMemsetAsync(a.slots, 0, (size_t)stiles * sizeof(LevelSlot), st);
             cudaMemsetAsync(&ctl->tile_counter[1], 0, sizeof(unsigned int), st);
-            a.prof->begin(K_FWD_LEVELS, (double)m * (2 + 4 + (b > 0 ? 4 : 0)), st);
+            a.prof->begin(K_FWD_LEVELS, 0.0, st);
             if (narrow)
-                k_fwd_levels<W, 4><<<stiles, kBlock, 0, st>>>(a.idx, a.D, a.F, (uint32_t)m, a.Sk, a.n, lv, b > 0,
+                k_fwd_levels<W, 4><<<stiles, kBlock, 0, st>>>(a.idx, a.D, a.F, a.Sk, a.n, lv, b > 0,
                                                             reinterpret_cast<LevelSlot*>(a.slots), ctl);
             else
-                k_fwd_levels<W, kMaxLevels><<<stiles, kBlock, 0, st>>>(a.idx, a.D, a.F, (uint32_t)m, a.Sk, a.n, lv,
-                                                                     b > 0, reinterpret_cast<LevelSlot*>(a.slots), ctl);
+                k_fwd_levels<W, kMaxLevels><<<stiles, kBlock, 0, st>>>(a.idx, a.D, a.F, a.Sk, a.n, lv, b > 0,
+                                                                     reinterpret_cast<LevelSlot*>(a.slots), ctl);
             a.prof->end(st);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
             cudaMemsetAsync(a.slots, 0, (size_t)stiles * sizeof(LevelSlot), st);
             cudaMemsetAsync(&ctl->tile_counter[2], 0, sizeof(unsigned int), st);
             const bool last = b == nb - 1;
-            a.prof->begin(K_BWD_LEVELS,
-                          (double)m * (2 + 4 + (last ? 4 + 2.0 * (16 * W + sizeof(T)) : 4)), st);
+            a.prof->begin(K_BWD_LEVELS, 0.0, st);
             if (narrow)
-                k_bwd_levels<W, T, 4><<<stiles, kBlock, 0, st>>>(a.idx, a.D, a.F, (uint32_t)m, a.Sk, a.Sc, a.n, lv, a.L,
-                                                               last, a.Pk, a.Pc,
-                                                               reinterpret_cast<LevelSlot*>(a.slots), ctl);
+                k_bwd_levels<W, T, 4><<<stiles, kBlock, 0, st>>>(a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, last,
+                                                               a.Pk, a.Pc, reinterpret_cast<LevelSlot*>(a.slots),
+                                                               ctl);
             else
                 k_bwd_levels<W, T, kMaxLevels><<<stiles, kBlock, 0, st>>>(
-                    a.idx, a.D, a.F, (uint32_t)m, a.Sk, a.Sc, a.n, lv, a.L, last, a.Pk, a.Pc,
+                    a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, last, a.Pk, a.Pc,
                     reinterpret_cast<LevelSlot*>(a.slots), ctl);
             a.prof->end(st);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
     }
     // 4. partition
-    uint64_t total = a.n + m;
-    uint32_t mtiles = (uint32_t)((total + MT - 1) / MT);
-    if (mtiles == 0) {
+    const uint64_t total_hi = a.n + m_hi;
+    const uint32_t mtiles_hi = (uint32_t)((total_hi + MT - 1) / MT);
+    if (mtiles_hi == 0) {
+        *a.partners_out = 0;
         *a.out_count = 0;
         return cudaSuccess;
     }
-    if (total > a.out_cap) return cudaErrorMemoryAllocation;
+    if (total_hi > a.out_cap) return cudaErrorMemoryAllocation;
     {
-        uint32_t warps = mtiles + 1;
+        uint32_t warps = mtiles_hi + 1;
         uint32_t blocks = (warps + 7) / 8;
-        a.prof->begin(K_PARTITION, (double)(mtiles + 1) * 16, st);
-        k_partition<W><<<blocks, 256, 0, st>>>(a.Sk, a.n, a.Pk, m, (uint32_t)MT, mtiles, a.bounds);
+        a.prof->begin(K_PARTITION, 0.0, st);
+        k_partition<W><<<blocks, 256, 0, st>>>(a.Sk, a.n, a.Pk, (uint32_t)MT, a.bounds, ctl);
         a.prof->end(st);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     // 5. merge
-    cudaMemsetAsync(a.status, 0, (size_t)mtiles * sizeof(unsigned long long), st);
+    cudaMemsetAsync(a.status, 0, (size_t)mtiles_hi * sizeof(unsigned long long), st);
     // failure injection: start the dispenser at tile 1, so tile 0 never publishes and tile 1's
     // bounded look-back gives up
     cudaMemsetAsync(&ctl->tile_counter[3], a.inject_stall ? 1 : 0, 1, st);
     cudaMemsetAsync(reinterpret_cast<unsigned char*>(&ctl->tile_counter[3]) + 1, 0, 3, st);
     size_t smem = MergeSmem<W, T>::bytes;
-    a.prof->begin(K_MERGE, (double)(a.n + m) * (16 * W + sizeof(T)), st);
-    k_merge<W, T><<<mtiles, kBlock, smem, st>>>(a.Sk, a.Sc, a.n, a.Pk, a.Pc, m, a.bounds, mtiles, a.L, a.keep,
-                                               a.Ok, a.Oc, a.out_cap, a.status, ctl, a.topn_hist);
+    a.prof->begin(K_MERGE, 0.0, st);
+    k_merge<W, T><<<mtiles_hi, kBlock, smem, st>>>(a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc,
+                                                  a.out_cap, a.status, ctl, a.topn_hist);
     a.prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    cudaMemcpyAsync(a.host_count, &ctl->count[1], sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-    *a.out_count = *a.host_count;
-    a.prof->add_bytes(K_MERGE, (double)(*a.out_count) * (16 * W + sizeof(T)));
+    // counts and error flags in one copy: count[0..7], tile_counter[0..7], err, err_info
+    cudaMemcpyAsync(a.host_count, &ctl->count[0], offsetof(Ctl, err_info) + sizeof(unsigned int),
+                    cudaMemcpyDeviceToHost, st);
+    if ((e = spin_sync(st)) != cudaSuccess) return e;
+    const uint64_t m = a.host_count[0];
+    *a.partners_out = m;
+    *a.out_count = a.host_count[1];
+    const unsigned int* flags = reinterpret_cast<const unsigned int*>(
+        reinterpret_cast<const unsigned char*>(a.host_count) + offsetof(Ctl, err));
+    *a.err_flags = flags[0];
+    *a.err_info = flags[1];
+    // algorithmic bytes, booked now that m and the output count are known
+    a.prof->add_bytes(K_CLASSIFY, (double)m * 6);  // idx + divergence writes
+    const int nlv = a.levels->n;
+    const int per = nlv <= 4 ? 4 : kMaxLevels;
+    const int nb = m ? (nlv + per - 1) / per : 0;
+    for (int b = 0; b < nb; ++b) {
+        const bool last = b == nb - 1;
+        a.prof->add_bytes(K_FWD_LEVELS, (double)m * (2 + 4 + (b > 0 ? 4 : 0)));
+        a.prof->add_bytes(K_BWD_LEVELS, (double)m * (2 + 4 + (last ? 4 + 2.0 * (16 * W + sizeof(T)) : 4)));
+    }
+    a.prof->add_bytes(K_PARTITION, (double)((a.n + m + MT - 1) / MT + 1) * 16);
+    a.prof->add_bytes(K_MERGE, (double)(a.n + m + *a.out_count) * (16 * W + sizeof(T)));
     return cudaSuccess;
 }
 

@@ -132,12 +132,12 @@ __device__ __forceinline__ float warp_column_sum(float (&v)[32]) {
 }
 
 template <int W>
-__device__ __forceinline__ void term_features(const ScorerArgs& A, const ScoreInput& in, uint64_t row, bool valid,
-                                              uint64_t (&k)[2 * W], float (&f)[3]) {
+__device__ __forceinline__ float term_features(const ScorerArgs& A, const ScoreInput& in, uint64_t row, bool valid,
+                                               uint64_t (&k)[2 * W], float (&f)[3]) {
 #pragma unroll
     for (int i = 0; i < 2 * W; ++i) k[i] = 0;
     f[0] = f[1] = f[2] = 0.0f;
-    if (!valid) return;
+    if (!valid) return 0.0f;
     load_key<W>(in.keys, row, k);
     int weight = 0;
 #pragma unroll
@@ -154,6 +154,7 @@ __device__ __forceinline__ void term_features(const ScorerArgs& A, const ScoreIn
     f[0] = (float)weight * A.fscale[0];
     f[1] = logc * A.fscale[1];
     f[2] = rem * A.fscale[2];
+    return logc;
 }
 
 __device__ __forceinline__ void load_bf16x32(const uint16_t* p, float (&v)[32]) {
@@ -274,7 +275,7 @@ __global__ void __launch_bounds__(kScoreThreads) k_score(const ScorerArgs A, con
         const bool valid = row < in.n;
         uint64_t k[2 * W];
         float f[3];
-        term_features<W>(A, in, row, valid, k, f);
+        const float logc = term_features<W>(A, in, row, valid, k, f);
 #pragma unroll 1
         for (int c = 0; c < kHid / 32; ++c) {
             float z[32], h[32];
@@ -320,6 +321,7 @@ __global__ void __launch_bounds__(kScoreThreads) k_score(const ScorerArgs A, con
             for (int j = 0; j < 32; ++j) y += gelu(z2[j] + s_b2[32 * c + j]) * s_w3[32 * c + j];
         }
         if (!TRAIN) {
+            if (A.residual) y += logc;
             if (valid) {
                 if (scores) scores[row] = y;
                 if (sel) {

@@ -44,6 +44,7 @@ struct ScorerArgs {
     ScorerLayout L;
     int nq;
     float fscale[3];          // feature scales: weight, log|c|, remaining depth
+    int residual;             // scores = log|c| + output
 };
 
 // Per-term features: the key, and log|c| from a coefficient column (coef64 / coef32) or an

@@ -20,6 +20,7 @@
 #include "ps_device.cuh"
 #include "ps_store.h"
 
+#include <cstddef>
 #include <type_traits>
 
 namespace psb {
@@ -440,13 +441,15 @@ __global__ void __launch_bounds__(kThreads) k_topn_hist_cand(const uint64_t* __r
 }
 
 // Order-preserving compaction, warp-striped: keeps keys above the boundary and the first
-// `quota` boundary ties in key order.
+// `quota` boundary ties in key order, quota = keep_n - (count above the boundary), none when
+// the boundary is NaN (the select leaves boundary and count above in aux[0] / aux[3]).
 template <int W, typename T>
 __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __restrict__ keys, const T* __restrict__ coef,
                                                            const uint64_t* __restrict__ sel, uint64_t n,
-                                                           unsigned long long quota,
+                                                           unsigned long long keep_n,
                                                            uint64_t* __restrict__ okeys, T* __restrict__ ocoef,
                                                            unsigned long long* status, Ctl* ctl) {
+    const unsigned long long quota = ctl->aux[0] == 0 ? 0ull : keep_n - ctl->aux[3];
     constexpr int ITEMS = 16;
     constexpr int TILE = kThreads * ITEMS;
     __shared__ unsigned int s_tile;
@@ -608,7 +611,7 @@ cudaError_t StoreOps<W, T>::check_sorted(const uint64_t* keys, const T* coef, ui
     if (n) k_check_sorted<W, T><<<grid_for(n, sms), kThreads, 0, st>>>(keys, coef, n, ctl);
     prof->end(st);
     cudaMemcpyAsync(host_count, &ctl->count[5], sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
-    cudaError_t e = cudaStreamSynchronize(st);
+    cudaError_t e = spin_sync(st);
     *sorted = e == cudaSuccess && *host_count == 0;
     return e;
 }
@@ -637,7 +640,7 @@ cudaError_t StoreOps<W, T>::sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t*
     prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     cudaMemcpyAsync(s.host_hist, s.hist, (size_t)ND * 256 * sizeof(unsigned int), cudaMemcpyDeviceToHost, st);
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    if ((e = spin_sync(st)) != cudaSuccess) return e;
     constexpr int TILE = SortTile<W>::TILE;
     const uint32_t tiles = (uint32_t)((n + TILE - 1) / TILE);
     uint64_t *ka = keys, *kb = keys_alt;
@@ -670,7 +673,7 @@ cudaError_t StoreOps<W, T>::sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t*
         result_in_alt = !result_in_alt;
     }
     // the host copies of the bases must outlive the async copies
-    return cudaStreamSynchronize(st);
+    return spin_sync(st);
 }
 
 template <int W, typename T>
@@ -691,7 +694,7 @@ cudaError_t StoreOps<W, T>::dedup(const uint64_t* keys, const uint32_t* vals, co
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     cudaMemcpyAsync(host_count, &ctl->count[2], sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    if ((e = spin_sync(st)) != cudaSuccess) return e;
     *out_n = *host_count;
     prof->add_bytes(K_DEDUP, (double)*out_n * (16 * W + sizeof(T)));
     return cudaSuccess;
@@ -735,21 +738,19 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
         prof->end(st);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    unsigned long long* aux = host_count + 16;
-    cudaMemcpyAsync(aux, ctl->aux, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-    unsigned long long quota = keep_n - aux[3];
-    if (aux[0] == 0) quota = 0;  // NaN boundary: only the non-NaN terms stay
     const uint32_t tiles = (uint32_t)((n + kThreads * 16 - 1) / (kThreads * 16));
     cudaMemsetAsync(status, 0, (size_t)tiles * sizeof(unsigned long long), st);
     cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
-    k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, sel, n, quota, okeys, ocoef, status, ctl);
+    k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, sel, n, (unsigned long long)keep_n, okeys, ocoef,
+                                                     status, ctl);
     prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    cudaMemcpyAsync(host_count, &ctl->count[3], sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-    *out_n = *host_count;
+    // the one host synchronization of the pass: counts and error flags in one copy
+    cudaMemcpyAsync(host_count, &ctl->count[0], offsetof(Ctl, err_info) + sizeof(unsigned int),
+                    cudaMemcpyDeviceToHost, st);
+    if ((e = spin_sync(st)) != cudaSuccess) return e;
+    *out_n = host_count[3];
     prof->add_bytes(K_TOPN_COMPACT, (double)*out_n * (2 * 16 * W + sizeof(T)));
     return cudaSuccess;
 }

@@ -1,6 +1,7 @@
 // ps_store.h -- launchers of the store kernels (ingest, readout, TopN).
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -19,6 +20,14 @@ struct SortScratch {
     unsigned int* host_hist;   // pinned, 16W x 256
     unsigned int* host_base;   // pinned, 16W x 256
 };
+
+// Error bits and check id left in host_count by StoreOps::topn.
+inline void topn_flags(const unsigned long long* host_count, unsigned int* flags, unsigned int* info) {
+    const unsigned int* f = reinterpret_cast<const unsigned int*>(reinterpret_cast<const unsigned char*>(host_count) +
+                                                                  offsetof(Ctl, err));
+    *flags = f[0];
+    *info = f[1];
+}
 
 template <int W, typename T>
 struct StoreOps {
@@ -42,7 +51,8 @@ struct StoreOps {
                              unsigned long long* host_count, uint64_t* out_n, cudaStream_t st, KernelProf* prof);
     // hist: kTopnBinsN words, zero on entry and on exit; when hist_ready its first kTopnBins1
     // words already hold the digit-1 histogram of coef (built by the layer's merge).
-    // host_count: pinned scratch of at least 20 words.
+    // host_count: pinned scratch of at least 20 words; on return it holds the control block's
+    // counts, tile counters and error words (read the flags with topn_flags).
     // sel: when non-null, precomputed select keys (larger kept first, 0 never) replace mag_key(c);
     // hist_ready must then hold their digit-1 histogram.
     static cudaError_t topn(const uint64_t* keys, const T* coef, uint64_t n, uint64_t keep_n, uint64_t* okeys, T* ocoef,

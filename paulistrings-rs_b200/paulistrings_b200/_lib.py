@@ -78,7 +78,7 @@ class KeepNode(ctypes.Structure):
 class ScorerConfig(ctypes.Structure):
     _fields_ = [
         ("num_qubits", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("residual", ctypes.c_int32),
         ("layers_per_unit", ctypes.c_double),
         ("feature_scale", ctypes.c_float * 3),
         ("init_scale", ctypes.c_float),

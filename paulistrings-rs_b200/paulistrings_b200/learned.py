@@ -53,9 +53,12 @@ class Scorer:
     """A scorer network on one device."""
 
     def __init__(self, num_qubits: int, layers_per_unit: float, feature_scale=(0.1, 0.1, 0.1),
-                 init_scale: float = 0.05, seed: int = 1, device: int = 0):
+                 init_scale: float = 0.05, seed: int = 1, device: int = 0, residual: bool = False):
+        """``residual``: scores are ``log|c|`` + the network's output, the network predicting the
+        log of the descendants' factor (train it with ``target - logc``)."""
         cfg = _lib.ScorerConfig()
         cfg.num_qubits = int(num_qubits)
+        cfg.residual = 1 if residual else 0
         cfg.layers_per_unit = float(layers_per_unit)
         for i, v in enumerate(feature_scale):
             cfg.feature_scale[i] = float(v)
@@ -70,6 +73,7 @@ class Scorer:
         self.layers_per_unit = float(layers_per_unit)
         self.feature_scale = tuple(float(v) for v in feature_scale)
         self.layout = layout(self.num_qubits)
+        self.residual = bool(residual)
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -192,14 +196,19 @@ def tagged_contributions(terms_x, terms_z, terms_c, num_qubits: int, rest: Circu
 
 def attribution_data(observable: PauliSum, step: Circuit, steps: int, state: str, threshold: float,
                      samples_per_step: int = 4096, seed: int = 0, floor: float = 1e-12, device: int = 0,
-                     truncation_policy=None):
+                     truncation_policy=None, chunk: int = 256, every: int = 1, top_fraction: float = 0.0,
+                     top_pool: int = 0):
     """Training rows from a tight-threshold Heisenberg run of ``steps`` repetitions of ``step``.
 
     At every step boundary d (0 <= d < steps) up to ``samples_per_step`` terms of the sum are
     drawn (uniformly, without replacement), each one's contribution to the final expectation
     is measured by ``tagged_contributions`` through the remaining ``steps - d`` steps under the
     same threshold, and a row (key, log|c|, remaining steps, log(|contribution| + floor)) is
-    recorded.  Returns (keys, logc, rem, target) as numpy arrays."""
+    recorded.  The tagged runs take ``chunk`` terms at a time (their light cones never merge,
+    so a chunk's sum is about ``chunk`` times one cone); ``every`` > 1 samples only every
+    ``every``-th boundary.  With ``top_fraction`` > 0 that share of each sample is drawn from
+    the ``top_pool`` largest |c| (the region a TopN budget decides on) and the rest uniformly.
+    Returns (keys, logc, rem, target) as numpy arrays."""
     from . import truncation
 
     rng = np.random.default_rng(seed)
@@ -210,13 +219,24 @@ def attribution_data(observable: PauliSum, step: Circuit, steps: int, state: str
     try:
         for d in range(steps):
             x, z, c = g.download()
-            take = min(samples_per_step, len(c))
+            take = min(samples_per_step, len(c)) if d % every == 0 else 0
             if take:
-                pick = np.sort(rng.choice(len(c), size=take, replace=False))
+                n_top = int(round(take * top_fraction))
+                if n_top and top_pool:
+                    pool = np.argsort(-np.abs(c), kind="stable")[:max(top_pool, n_top)]
+                    top = rng.choice(pool, size=min(n_top, len(pool)), replace=False)
+                    others = np.setdiff1d(np.arange(len(c)), top)
+                    rest_pick = rng.choice(others, size=min(take - len(top), len(others)), replace=False)
+                    pick = np.sort(np.concatenate([top, rest_pick]))
+                else:
+                    pick = np.sort(rng.choice(len(c), size=take, replace=False))
                 rest = Circuit(nq)
                 for _ in range(steps - d):
                     rest.extend(step)
-                contrib = tagged_contributions(x[pick], z[pick], c[pick], nq, rest, policy, state, device=device)
+                contrib = np.concatenate([
+                    tagged_contributions(x[pick[i:i + chunk]], z[pick[i:i + chunk]], c[pick[i:i + chunk]], nq, rest,
+                                         policy, state, device=device)
+                    for i in range(0, take, chunk)])
                 rows[0].append(pack_keys(x[pick], z[pick]))
                 rows[1].append(np.log(np.abs(c[pick])).astype(np.float32))
                 rows[2].append(np.full(take, steps - d, np.float32))
