@@ -66,8 +66,11 @@ typedef enum ps_keep_op {
 typedef enum ps_pass_kind {
     PS_PASS_NONE = 0,
     PS_PASS_TOPN = 1,    /* keep the n largest |c|^2; ties first in key order (builtin.rs:73-129) */
-    PS_PASS_SCORED_TOPN = 2 /* keep the n terms the handle's scorer ranks highest (ps_set_scorer);
+    PS_PASS_SCORED_TOPN = 2, /* keep the n terms the handle's scorer ranks highest (ps_set_scorer);
                                ties first in key order, a NaN score never kept */
+    PS_PASS_APPROX_TOPN = 3  /* ApproxTopN (builtin.rs:240-468): every octave of |c|^2 above the
+                               boundary octave kept whole, then the first of the boundary octave
+                               in key order up to n in all; a NaN never kept */
 } ps_pass_kind;
 
 typedef struct ps_keep_node {

@@ -27,7 +27,7 @@ LIB_PATH = HERE / "_build" / "libps_oracle.so"
 
 F64, F32 = 0, 1
 _KEEP = {"true": 0, "coeff": 1, "weight": 2, "and": 3, "or": 4}
-_PASS = {"topn": 1}
+_PASS = {"topn": 1, "approx_topn": 3}
 _KIND = {"rotation": 1, "depolarize": 2, "h": 3, "s": 4, "sdg": 5, "x": 6, "y": 7, "z": 8, "cnot": 9,
          "cz": 10, "swap": 11, "unitary": 12, "dephase": 13, "pauli_channel": 14, "depolarize2": 15,
          "amplitude_damping": 16}

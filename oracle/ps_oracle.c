@@ -813,10 +813,71 @@ static void topn(pso_sum* s, uint64_t n) {
     free(m);
 }
 
+/* ApproxTopN (builtin.rs:240-468): octave = bits(|c|^2) >> 52, the histogram counting NaN in
+ * the top bin; walk from the top, the first octave that overflows n is the boundary; keep
+ * every non-NaN term above it and its first `quota` non-NaN terms in store (key) order. */
+static void approx_topn(pso_sum* s, uint64_t n) {
+    if (s->n <= n) return;
+    if (n == 0) {
+        s->n = 0;
+        return;
+    }
+    static uint64_t hist[2048];
+    memset(hist, 0, sizeof hist);
+    size_t total = s->n;
+    unsigned* oct = (unsigned*)malloc(total * sizeof(unsigned));
+    unsigned char* nan = (unsigned char*)malloc(total);
+    for (size_t i = 0; i < total; ++i) {
+        double c = coef_at(s, i);
+        double m = c * c;
+        uint64_t bits;
+        memcpy(&bits, &m, 8);
+        nan[i] = (unsigned char)isnan(m);
+        oct[i] = nan[i] ? 2047u : (unsigned)(bits >> 52);
+        hist[oct[i]]++;
+    }
+    uint64_t above = 0;
+    unsigned bin = 0;
+    for (int b = 2047; b >= 0; --b) {
+        if (above + hist[b] > n) {
+            bin = (unsigned)b;
+            break;
+        }
+        above += hist[b];
+    }
+    uint64_t quota = n - above;
+    int K = 2 * s->W;
+    size_t w = 0;
+    for (size_t i = 0; i < total; ++i) {
+        int keep = 0;
+        if (!nan[i]) {
+            if (oct[i] > bin)
+                keep = 1;
+            else if (oct[i] == bin && quota > 0) {
+                keep = 1;
+                --quota;
+            }
+        }
+        if (!keep) continue;
+        if (w != i) {
+            memmove(s->keys + w * K, s->keys + i * K, (size_t)K * 8);
+            if (s->dtype == PSO_F64)
+                s->c64[w] = s->c64[i];
+            else
+                s->c32[w] = s->c32[i];
+        }
+        ++w;
+    }
+    s->n = w;
+    free(oct);
+    free(nan);
+}
+
 void pso_finalize_layer(pso_sum* s, const pso_policy* policy) {
     if (!policy) return;
     for (int i = 0; i < policy->num_passes; ++i) {
         if (policy->pass_kind[i] == PSO_PASS_TOPN) topn(s, policy->pass_n[i]);
+        if (policy->pass_kind[i] == PSO_PASS_APPROX_TOPN) approx_topn(s, policy->pass_n[i]);
     }
 }
 

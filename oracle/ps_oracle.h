@@ -19,6 +19,8 @@
  *   naive layer         crates/paulistrings/src/test_support/oracle.rs:21-54
  *   threshold / weight  crates/paulistrings/src/truncation/builtin.rs:28-59
  *   TopN (+NaN, ties)   crates/paulistrings/src/truncation/builtin.rs:73-129, 210-239
+ *   ApproxTopN          crates/paulistrings/src/truncation/builtin.rs:240-468 (octave histogram
+ *                       with NaN in the top bin, edge walk from the top, boundary quota)
  *   And / Or            crates/paulistrings/src/truncation/builtin.rs:479-526, 604-625
  *   Heisenberg order    crates/paulistrings/src/engine/driver.rs:349-352
  *   product readout     crates/paulistrings/src/readout/product_state.rs:84-101
@@ -52,6 +54,7 @@ extern "C" {
 
 /* layer passes */
 #define PSO_PASS_TOPN 1    /* n = retained count */
+#define PSO_PASS_APPROX_TOPN 3 /* ApproxTopN: octave cut, n = retained count */
 
 typedef struct pso_policy {
     int32_t num_nodes;

@@ -64,6 +64,8 @@ struct ps_sum {
     Buf pk, pc;
     Buf idx, dv, fv, slots, status, bounds, hist, cand, partial, dout;
     bool hist_ready = false;  // hist holds the TopN digit-1 histogram of the current store
+    int hist_kind = 0;        // ... of that pass kind: PS_PASS_TOPN or PS_PASS_APPROX_TOPN
+    unsigned int* hhist = nullptr;  // pinned, kTopnBins1 words
     bool compensated = false; // sort-path dedup sums runs with TwoSum compensation
     ps_scorer* scorer = nullptr;   // PS_PASS_SCORED_TOPN
     double scorer_remaining = 0;   // layers still to apply
@@ -221,7 +223,7 @@ ps_status lower_keep(const ps_policy* p, KeepProg& k, std::string& why) {
     }
     for (int i = 0; i < p->num_passes; ++i) {
         if (p->passes[i].kind != PS_PASS_TOPN && p->passes[i].kind != PS_PASS_SCORED_TOPN &&
-            p->passes[i].kind != PS_PASS_NONE) {
+            p->passes[i].kind != PS_PASS_APPROX_TOPN && p->passes[i].kind != PS_PASS_NONE) {
             why = "policy: unknown layer pass";
             return PS_ERR_UNSUPPORTED;
         }
@@ -978,9 +980,12 @@ struct Engine {
         a.err_flags = &err_flags;
         a.err_info = &err_info;
         a.prof = &s->prof;
-        // the first layer pass is TopN and could trigger: the merge builds its first select digit
-        const bool fuse_topn = policy && policy->num_passes > 0 && policy->passes[0].kind == PS_PASS_TOPN &&
+        // the first layer pass is TopN (or ApproxTopN) and could trigger: the merge builds its
+        // first select digit (the octave histogram)
+        const int first_pass = policy && policy->num_passes > 0 ? policy->passes[0].kind : PS_PASS_NONE;
+        const bool fuse_topn = (first_pass == PS_PASS_TOPN || first_pass == PS_PASS_APPROX_TOPN) &&
                                out_rows > policy->passes[0].n;
+        a.topn_hist_octave = first_pass == PS_PASS_APPROX_TOPN ? 1 : 0;
         if (s->hist_ready) {
             cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
             s->hist_ready = false;
@@ -997,6 +1002,7 @@ struct Engine {
             return ps;
         }
         s->hist_ready = fuse_topn;
+        s->hist_kind = first_pass;
         if (stats) {
             stats->terms_in = n;
             stats->partners = partners;
@@ -1074,7 +1080,7 @@ struct Engine {
     }
 
     static ps_status finalize(ps_sum* s, const ps_policy* policy) {
-        const bool ready = s->hist_ready;
+        bool ready = s->hist_ready;
         if (ready) s->hist_ready = false;
         if (s->scorer) s->scorer_remaining -= 1.0;
         ps_status result = PS_OK;
@@ -1086,7 +1092,17 @@ struct Engine {
                 if (ps != PS_OK) return ps;
                 continue;
             }
+            if (p.kind == PS_PASS_APPROX_TOPN) {
+                ps_status ps = approx_topn(s, p.n, ready && i == 0 && s->hist_kind == PS_PASS_APPROX_TOPN,
+                                           ready && i == 0);
+                if (ps != PS_OK) return ps;
+                continue;
+            }
             if (p.kind != PS_PASS_TOPN) continue;
+            if (ready && i == 0 && s->hist_kind != PS_PASS_TOPN) {  // a histogram of another pass kind
+                cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+                ready = false;
+            }
             const bool use_hist = ready && i == 0;
             if (s->n <= p.n) {
                 if (use_hist) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
@@ -1123,6 +1139,42 @@ struct Engine {
             s->n = out_n;
         }
         return result;
+    }
+
+    // ApproxTopN: the octave histogram (fused into the layer's merge when use_hist), the edge
+    // walk on the host, one compaction.  held: the hist buffer holds some histogram to clear.
+    static ps_status approx_topn(ps_sum* s, uint64_t keep_n, bool use_hist, bool held) {
+        if (held && !use_hist) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+        if (s->n <= keep_n) {
+            if (use_hist) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+            return PS_OK;
+        }
+        if (keep_n == 0) {
+            if (use_hist) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+            s->n = 0;
+            return PS_OK;
+        }
+        const int spare = 1 - s->cur;
+        cudaError_t e = reserve_store(s, spare, keep_n);
+        if (e == cudaSuccess) e = ensure(s, s->status, (s->n / 4096 + 4) * sizeof(unsigned long long));
+        if (e != cudaSuccess) {
+            if (use_hist) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+            return cuda_fail(s, e, "approx TopN: scratch");
+        }
+        uint64_t out_n = 0;
+        e = StoreOps<W, T>::approx_topn(K(s, s->cur), C(s, s->cur), s->n, keep_n, K(s, spare), C(s, spare),
+                                        (unsigned int*)s->hist.p, use_hist, s->hhist,
+                                        (unsigned long long*)s->status.p, s->ctl, s->hcount, &out_n, s->sms,
+                                        s->stream, &s->prof);
+        s->prof.resolve();
+        if (e != cudaSuccess) return cuda_fail(s, e, "approx TopN");
+        unsigned int fl = 0, fi = 0;
+        topn_flags(s->hcount, &fl, &fi);
+        ps_status ps = flags_status(s, fl, fi, "approx TopN");
+        if (ps != PS_OK) return ps;
+        s->cur = spare;
+        s->n = out_n;
+        return PS_OK;
     }
 
     // The learned pass: the attached scorer scores every term (tensor-core MLP, select keys and
@@ -1276,6 +1328,7 @@ ps_status ps_create(int32_t device, int32_t num_qubits, int32_t dtype, ps_sum** 
     }
     if (e == cudaSuccess) e = cudaMallocHost(&s->hcount, 64 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMallocHost(&s->hout, 8 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->hhist, kTopnBins1 * sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMalloc(&s->sort.hist, 16 * W * 256 * sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMalloc(&s->sort.base, 16 * W * 256 * sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMallocHost(&s->sort.host_hist, 16 * W * 256 * sizeof(unsigned int));
@@ -1315,6 +1368,7 @@ ps_status ps_destroy(ps_sum* s) {
     if (s->sort.host_base) cudaFreeHost(s->sort.host_base);
     if (s->hcount) cudaFreeHost(s->hcount);
     if (s->hout) cudaFreeHost(s->hout);
+    if (s->hhist) cudaFreeHost(s->hhist);
     s->prof.destroy();
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s->levels;

@@ -226,6 +226,25 @@ __device__ __forceinline__ uint64_t mag_key(T c) {
     return (uint64_t)__double_as_longlong(m) + 1ull;
 }
 
+// ApproxTopN's octave of |c|^2: the exponent field of its f64 pattern, NaN counted in the top
+// bin as the reference's histogram counts it (crates/paulistrings/src/truncation/builtin.rs:264-293).
+template <typename T>
+__device__ __forceinline__ uint32_t octave_bin(T c) {
+    const double v = to_f64(c);
+    const double m = __dmul_rn(v, v);
+    if (isnan(m)) return 2047u;
+    return (uint32_t)((uint64_t)__double_as_longlong(m) >> 52);
+}
+
+// Select key of the octave: 0 for NaN (never kept), else octave + 1.
+template <typename T>
+__device__ __forceinline__ uint64_t octave_key(T c) {
+    const double v = to_f64(c);
+    const double m = __dmul_rn(v, v);
+    if (isnan(m)) return 0ull;
+    return ((uint64_t)__double_as_longlong(m) >> 52) + 1ull;
+}
+
 // Knuth TwoSum: s + e == a + b exactly.
 template <typename T>
 __device__ __forceinline__ void two_sum(T a, T b, T& s, T& e) {

@@ -204,6 +204,7 @@ struct RotationArgs {
     unsigned int* err_info;
     KernelProf* prof;
     unsigned int* topn_hist;  // when set, the merge histograms key >> 52 of its outputs (2048 bins)
+    int topn_hist_octave;     // ... or, when nonzero, their octave of |c|^2 (ApproxTopN)
     int inject_stall;         // failure injection: the merge skips its first tile
 };
 

@@ -376,6 +376,27 @@ __device__ __forceinline__ uint64_t select_key(const T* __restrict__ coef, const
     return sel ? sel[e] : mag_key<T>(coef[e]);
 }
 
+// The compaction's key: 0 mag_key, 1 precomputed, 2 ApproxTopN's octave key.
+template <typename T>
+__device__ __forceinline__ uint64_t compact_key(const T* __restrict__ coef, const uint64_t* __restrict__ sel, int mode,
+                                                uint64_t e) {
+    return mode == 2 ? octave_key<T>(coef[e]) : select_key<T>(coef, sel, e);
+}
+
+// ApproxTopN's octave histogram of |c|^2 (2048 bins, NaN in the top one).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_octave_hist(const T* __restrict__ coef, uint64_t n,
+                                                          unsigned int* __restrict__ hist) {
+    __shared__ unsigned int sh[kTopnBins1];
+    for (int i = threadIdx.x; i < kTopnBins1; i += kThreads) sh[i] = 0;
+    __syncthreads();
+    for (uint64_t i = blockIdx.x * (uint64_t)kThreads + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kThreads)
+        atomicAdd(&sh[octave_bin<T>(coef[i])], 1u);
+    __syncthreads();
+    for (int i = threadIdx.x; i < kTopnBins1; i += kThreads)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
 // Gather the keys of the boundary bin (order does not matter for the select): each block
 // takes chunks of kThreads * 16 elements and claims its output slots with one atomic per chunk.
 template <typename T>
@@ -445,8 +466,8 @@ __global__ void __launch_bounds__(kThreads) k_topn_hist_cand(const uint64_t* __r
 // the boundary is NaN (the select leaves boundary and count above in aux[0] / aux[3]).
 template <int W, typename T>
 __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __restrict__ keys, const T* __restrict__ coef,
-                                                           const uint64_t* __restrict__ sel, uint64_t n,
-                                                           unsigned long long keep_n,
+                                                           const uint64_t* __restrict__ sel, int key_mode,
+                                                           uint64_t n, unsigned long long keep_n,
                                                            uint64_t* __restrict__ okeys, T* __restrict__ ocoef,
                                                            unsigned long long* status, Ctl* ctl) {
     const unsigned long long quota = ctl->aux[0] == 0 ? 0ull : keep_n - ctl->aux[3];
@@ -469,7 +490,7 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
         const uint64_t e = wbase + (uint64_t)i * 32 + lane;
         bool isa = false, ist = false;
         if (e < n) {
-            const uint64_t mk = select_key<T>(coef, sel, e);
+            const uint64_t mk = compact_key<T>(coef, sel, key_mode, e);
             isa = mk > boundary;
             ist = mk == boundary && boundary != 0;
         }
@@ -742,11 +763,65 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     cudaMemsetAsync(status, 0, (size_t)tiles * sizeof(unsigned long long), st);
     cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
-    k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, sel, n, (unsigned long long)keep_n, okeys, ocoef,
-                                                     status, ctl);
+    k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, sel, sel ? 1 : 0, n, (unsigned long long)keep_n,
+                                                     okeys, ocoef, status, ctl);
     prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // the one host synchronization of the pass: counts and error flags in one copy
+    cudaMemcpyAsync(host_count, &ctl->count[0], offsetof(Ctl, err_info) + sizeof(unsigned int),
+                    cudaMemcpyDeviceToHost, st);
+    if ((e = spin_sync(st)) != cudaSuccess) return e;
+    *out_n = host_count[3];
+    prof->add_bytes(K_TOPN_COMPACT, (double)*out_n * (2 * 16 * W + sizeof(T)));
+    return cudaSuccess;
+}
+
+template <int W, typename T>
+cudaError_t StoreOps<W, T>::approx_topn(const uint64_t* keys, const T* coef, uint64_t n, uint64_t keep_n,
+                                        uint64_t* okeys, T* ocoef, unsigned int* hist, bool hist_ready,
+                                        unsigned int* host_hist, unsigned long long* status, Ctl* ctl,
+                                        unsigned long long* host_count, uint64_t* out_n, int sms, cudaStream_t st,
+                                        KernelProf* prof) {
+    // octave_edge (crates/paulistrings/src/truncation/builtin.rs:312-353): walk the octaves from
+    // the top; the first whose population overflows keep_n is the boundary, cut by a quota
+    cudaError_t e;
+    if (!hist_ready) {
+        prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
+        k_octave_hist<T><<<grid_for(n, sms), kThreads, 0, st>>>(coef, n, hist);
+        prof->end(st);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    cudaMemcpyAsync(host_hist, hist, kTopnBins1 * sizeof(unsigned int), cudaMemcpyDeviceToHost, st);
+    cudaMemsetAsync(hist, 0, kTopnBins1 * sizeof(unsigned int), st);
+    if ((e = spin_sync(st)) != cudaSuccess) return e;
+    unsigned long long above = 0, bin = 0;
+    bool found = false;
+    for (int b = kTopnBins1 - 1; b >= 0; --b) {
+        if (above + host_hist[b] > keep_n) {
+            bin = (unsigned long long)b;
+            found = true;
+            break;
+        }
+        above += host_hist[b];
+    }
+    if (!found) {  // cannot happen for n > keep_n; keep everything rather than guess
+        *out_n = n;
+        return cudaErrorInvalidValue;
+    }
+    unsigned long long* init = host_count + 8;
+    init[0] = bin + 1;  // octave keys are octave + 1
+    init[1] = 0;
+    init[2] = 0;
+    init[3] = above;
+    cudaMemcpyAsync(ctl->aux, init, 4 * sizeof(unsigned long long), cudaMemcpyHostToDevice, st);
+    const uint32_t tiles = (uint32_t)((n + kThreads * 16 - 1) / (kThreads * 16));
+    cudaMemsetAsync(status, 0, (size_t)tiles * sizeof(unsigned long long), st);
+    cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
+    prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
+    k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, nullptr, 2, n, (unsigned long long)keep_n, okeys,
+                                                     ocoef, status, ctl);
+    prof->end(st);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     cudaMemcpyAsync(host_count, &ctl->count[0], offsetof(Ctl, err_info) + sizeof(unsigned int),
                     cudaMemcpyDeviceToHost, st);
     if ((e = spin_sync(st)) != cudaSuccess) return e;

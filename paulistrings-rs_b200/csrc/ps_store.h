@@ -59,6 +59,14 @@ struct StoreOps {
                             unsigned int* hist, bool hist_ready, uint64_t* cand, uint64_t cand_cap,
                             unsigned long long* status, Ctl* ctl, unsigned long long* host_count, uint64_t* out_n,
                             int sms, cudaStream_t st, KernelProf* prof, const uint64_t* sel = nullptr);
+    // ApproxTopN (crates/paulistrings/src/truncation/builtin.rs:240-468): every octave of |c|^2
+    // above the boundary octave kept, then the first quota boundary terms in key order.
+    // hist: 2048 words, zero on entry and exit, holding the octave histogram when hist_ready;
+    // host_hist: pinned, 2048 words.
+    static cudaError_t approx_topn(const uint64_t* keys, const T* coef, uint64_t n, uint64_t keep_n, uint64_t* okeys,
+                                   T* ocoef, unsigned int* hist, bool hist_ready, unsigned int* host_hist,
+                                   unsigned long long* status, Ctl* ctl, unsigned long long* host_count,
+                                   uint64_t* out_n, int sms, cudaStream_t st, KernelProf* prof);
     static cudaError_t expectation(const uint64_t* keys, const T* coef, uint64_t n, const uint64_t* ax,
                                    const uint64_t* az, const uint64_t* neg, double* partial, double* out_dev, int sms,
                                    cudaStream_t st, KernelProf* prof);

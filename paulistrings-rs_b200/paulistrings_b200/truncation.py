@@ -2,7 +2,8 @@
 
 ``coeff(eps)`` keeps ``|c|^2 > eps^2`` (crates/paulistrings/src/truncation/builtin.rs:19-41),
 ``weight(k)`` keeps Pauli weight ``<= k`` (:43-59), ``topn(n)`` retains the ``n`` largest
-magnitudes after every layer (:61-150), ``scored_topn(n, scorer)`` the ``n`` terms a learned
+magnitudes after every layer (:61-150), ``approx_topn(n)`` cuts at an octave of |c|^2 instead
+(:240-468), ``scored_topn(n, scorer)`` the ``n`` terms a learned
 scorer ranks highest (``paulistrings_b200.learned``; a ``TruncationPolicy`` of this package,
 crates/paulistrings/src/truncation/mod.rs:30-107).  ``a & b`` keeps a term iff both keep it and runs
 a's layer passes then b's (:470-526); ``a | b`` combines per-term filters only (:574-625).
@@ -36,7 +37,7 @@ class Truncation:
         return Truncation("or", self, other)
 
     def has_layer_pass(self) -> bool:
-        if self.kind in ("topn", "scored_topn"):
+        if self.kind in ("topn", "scored_topn", "approx_topn"):
             return True
         if self.kind in ("and", "or"):
             return self.args[0].has_layer_pass() or self.args[1].has_layer_pass()
@@ -62,6 +63,9 @@ class Truncation:
         elif self.kind == "scored_topn":
             nodes.append((_lib.PS_KEEP_TRUE, 0, 0.0))
             passes.append((_lib.PS_PASS_SCORED_TOPN, int(self.args[0])))
+        elif self.kind == "approx_topn":
+            nodes.append((_lib.PS_KEEP_TRUE, 0, 0.0))
+            passes.append((_lib.PS_PASS_APPROX_TOPN, int(self.args[0])))
         elif self.kind in ("and", "or"):
             self.args[0]._lower(nodes, passes)
             self.args[1]._lower(nodes, passes)
@@ -141,6 +145,15 @@ def topn(n: int) -> Truncation:
     if n < 0:
         raise ValueError("topn needs n >= 0")
     return Truncation("topn", int(n))
+
+
+def approx_topn(n: int) -> Truncation:
+    """ApproxTopN (crates/paulistrings/src/truncation/builtin.rs:240-468): retain ``n`` terms,
+    cutting at an octave of ``|c|^2`` — every octave that fits whole from the top, then the
+    first terms of the boundary octave in key order; NaN never kept."""
+    if n < 0:
+        raise ValueError("approx_topn needs n >= 0")
+    return Truncation("approx_topn", int(n))
 
 
 def scored_topn(n: int, scorer) -> Truncation:

@@ -67,7 +67,8 @@ def oracle_policy(policy):
             keep.append((nm, iarg))
         else:
             keep.append((nm,))
-    return {"keep": keep, "passes": [("topn", n) for kind, n in passes if kind == _lib.PS_PASS_TOPN]}
+    names = {_lib.PS_PASS_TOPN: "topn", _lib.PS_PASS_APPROX_TOPN: "approx_topn"}
+    return {"keep": keep, "passes": [(names[kind], n) for kind, n in passes if kind in names]}
 
 
 def oracle_sum(num_qubits, x, z, c, dtype="f64") -> OracleSum:
