@@ -68,9 +68,15 @@ typedef enum ps_pass_kind {
     PS_PASS_TOPN = 1,    /* keep the n largest |c|^2; ties first in key order (builtin.rs:73-129) */
     PS_PASS_SCORED_TOPN = 2, /* keep the n terms the handle's scorer ranks highest (ps_set_scorer);
                                ties first in key order, a NaN score never kept */
-    PS_PASS_APPROX_TOPN = 3  /* ApproxTopN (builtin.rs:240-468): every octave of |c|^2 above the
+    PS_PASS_APPROX_TOPN = 3, /* ApproxTopN (builtin.rs:240-468): every octave of |c|^2 above the
                                boundary octave kept whole, then the first of the boundary octave
                                in key order up to n in all; a NaN never kept */
+    PS_PASS_COLLAPSE_SAMPLE = 4 /* CollapseSample (collapse_sample.rs:1-240): above n terms, `samples`
+                               systematic draws in proportion to |c| (one uniform from the
+                               xoshiro256++ stream keyed (seed, call)); a drawn term keeps
+                               sign(c) * multiplicity * sum|c| / samples.  Stretches accumulate in
+                               key order per block of 1024 terms, as the reference accumulates
+                               per bucket (target_bucket_len 1024). */
 } ps_pass_kind;
 
 typedef struct ps_keep_node {
@@ -83,7 +89,11 @@ typedef struct ps_keep_node {
 typedef struct ps_pass {
     int32_t kind;        /* ps_pass_kind */
     int32_t reserved;
-    uint64_t n;
+    uint64_t n;          /* TopN / ApproxTopN / scored: terms kept; CollapseSample: the cache */
+    uint64_t samples;    /* CollapseSample: draws per collapse (>= 1) */
+    uint64_t seed;       /* CollapseSample: trajectory seed */
+    uint64_t call;       /* CollapseSample: pass index of the first layer; ps_propagate's layer
+                            i uses call + i, as the reference's policy counts its passes */
 } ps_pass;
 
 typedef struct ps_policy {
@@ -178,6 +188,7 @@ typedef struct ps_run_stats {
     uint64_t total_terms_in;  /* sum over layers of terms_in */
     uint64_t kernel_launches; /* kernels this call launched */
     double device_ms;         /* CUDA-event time of the whole run */
+    uint64_t collapses;       /* CollapseSample collapses performed */
 } ps_run_stats;
 
 /* Per-kernel profile (the phase-timing counters, crates/paulistrings/src/engine/stats.rs:12 and

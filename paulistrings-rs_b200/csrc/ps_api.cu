@@ -65,6 +65,10 @@ struct ps_sum {
     Buf idx, dv, fv, slots, status, bounds, hist, cand, partial, dout;
     bool hist_ready = false;  // hist holds the TopN digit-1 histogram of the current store
     int hist_kind = 0;        // ... of that pass kind: PS_PASS_TOPN or PS_PASS_APPROX_TOPN
+    bool hist_window = false; // ... binned in the TopN window starting at hist_base
+    uint64_t hist_base = 0;
+    bool topn_window = false; // the next TopN histogram may use the window at topn_base, centred
+    uint64_t topn_base = 0;   // on the last boundary (the boundary moves little between layers)
     unsigned int* hhist = nullptr;  // pinned, kTopnBins1 words
     bool compensated = false; // sort-path dedup sums runs with TwoSum compensation
     ps_scorer* scorer = nullptr;   // PS_PASS_SCORED_TOPN
@@ -985,7 +989,9 @@ struct Engine {
         const int first_pass = policy && policy->num_passes > 0 ? policy->passes[0].kind : PS_PASS_NONE;
         const bool fuse_topn = (first_pass == PS_PASS_TOPN || first_pass == PS_PASS_APPROX_TOPN) &&
                                out_rows > policy->passes[0].n;
-        a.topn_hist_octave = first_pass == PS_PASS_APPROX_TOPN ? 1 : 0;
+        const bool window = first_pass == PS_PASS_TOPN && s->topn_window;
+        a.topn_hist_mode = first_pass == PS_PASS_APPROX_TOPN ? 1 : (window ? 2 : 0);
+        a.topn_hist_base = window ? s->topn_base : 0;
         if (s->hist_ready) {
             cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
             s->hist_ready = false;
@@ -1003,6 +1009,8 @@ struct Engine {
         }
         s->hist_ready = fuse_topn;
         s->hist_kind = first_pass;
+        s->hist_window = fuse_topn && window;
+        s->hist_base = a.topn_hist_base;
         if (stats) {
             stats->terms_in = n;
             stats->partners = partners;
@@ -1115,25 +1123,39 @@ struct Engine {
             }
             const int spare = 1 - s->cur;
             cudaError_t e = reserve_store(s, spare, p.n);
-            if (e == cudaSuccess) e = ensure(s, s->cand, s->n * sizeof(uint64_t));
+            if (e == cudaSuccess) e = ensure(s, s->cand, topn_cand_words(s->n, s->sms) * sizeof(uint64_t));
             if (e == cudaSuccess) e = ensure(s, s->status, (s->n / 4096 + 4) * sizeof(unsigned long long));
             if (e != cudaSuccess) {
                 if (use_hist) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
                 return cuda_fail(s, e, "topn: scratch");
             }
             uint64_t out_n = 0;
-            e = StoreOps<W, T>::topn(K(s, s->cur), C(s, s->cur), s->n, p.n, K(s, spare), C(s, spare),
-                                     (unsigned int*)s->hist.p, use_hist, (uint64_t*)s->cand.p, s->n,
-                                     (unsigned long long*)s->status.p, s->ctl, s->hcount, &out_n, s->sms,
-                                     s->stream, &s->prof);
-            s->prof.resolve();
-            if (e != cudaSuccess) return cuda_fail(s, e, "topn");
-            unsigned int fl = 0, fi = 0;
-            topn_flags(s->hcount, &fl, &fi);
-            ps_status ps = flags_status(s, fl, fi, "topn");
-            if (ps != PS_OK) {
-                cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
-                return ps;
+            // a histogram binned in the window around the last boundary selects in 1/16 octaves
+            // (few candidates); when the boundary left the window, the pass reruns in full range
+            const bool window = use_hist && s->hist_window;
+            for (int attempt = 0; attempt < 2; ++attempt) {
+                const bool win = window && attempt == 0;
+                e = StoreOps<W, T>::topn(K(s, s->cur), C(s, s->cur), s->n, p.n, K(s, spare), C(s, spare),
+                                         (unsigned int*)s->hist.p, use_hist && attempt == 0, (uint64_t*)s->cand.p,
+                                         topn_cand_words(s->n, s->sms), (unsigned long long*)s->status.p, s->ctl,
+                                         s->hcount, &out_n, s->sms,
+                                         s->stream, &s->prof, nullptr, win, win ? s->hist_base : 0);
+                s->prof.resolve();
+                if (e != cudaSuccess) return cuda_fail(s, e, "topn");
+                unsigned int fl = 0, fi = 0;
+                topn_flags(s->hcount, &fl, &fi);
+                ps_status ps = flags_status(s, fl, fi, "topn");
+                if (ps != PS_OK) {
+                    cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+                    return ps;
+                }
+                if (!(win && topn_window_missed(s->hcount))) {
+                    const uint64_t boundary = topn_boundary(s->hcount, win ? s->hist_base : 0);
+                    const uint64_t half = 1024ull << 48;
+                    s->topn_window = boundary != 0;
+                    s->topn_base = boundary > half ? boundary - half : 0;
+                    break;
+                }
             }
             s->cur = spare;
             s->n = out_n;
@@ -1191,7 +1213,7 @@ struct Engine {
         const int spare = 1 - s->cur;
         cudaError_t e = reserve_store(s, spare, keep_n);
         if (e == cudaSuccess) e = ensure(s, s->sel, s->n * sizeof(uint64_t));
-        if (e == cudaSuccess) e = ensure(s, s->cand, s->n * sizeof(uint64_t));
+        if (e == cudaSuccess) e = ensure(s, s->cand, topn_cand_words(s->n, s->sms) * sizeof(uint64_t));
         if (e == cudaSuccess) e = ensure(s, s->status, (s->n / 4096 + 4) * sizeof(unsigned long long));
         if (e != cudaSuccess) return cuda_fail(s, e, "scored TopN: scratch");
         ScorerArgs A;
@@ -1217,7 +1239,7 @@ struct Engine {
         }
         uint64_t out_n = 0;
         e = StoreOps<W, T>::topn(K(s, s->cur), C(s, s->cur), s->n, keep_n, K(s, spare), C(s, spare),
-                                 (unsigned int*)s->hist.p, true, (uint64_t*)s->cand.p, s->n,
+                                 (unsigned int*)s->hist.p, true, (uint64_t*)s->cand.p, topn_cand_words(s->n, s->sms),
                                  (unsigned long long*)s->status.p, s->ctl, s->hcount, &out_n, s->sms, s->stream,
                                  &s->prof, (const uint64_t*)s->sel.p);
         s->prof.resolve();

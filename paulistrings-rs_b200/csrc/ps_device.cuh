@@ -226,6 +226,14 @@ __device__ __forceinline__ uint64_t mag_key(T c) {
     return (uint64_t)__double_as_longlong(m) + 1ull;
 }
 
+// TopN's first select digit, windowed: 2048 bins of 2^48 select-key units (1/16 of an octave
+// of |c|^2) starting at `base`; keys below the window land in bin 0, above it in bin 2047.
+__device__ __forceinline__ uint64_t window_key(uint64_t mk, uint64_t base) {
+    if (mk < base) return 0ull;
+    const uint64_t d = mk - base;
+    return d > ((1ull << 59) - 1) ? ((1ull << 59) - 1) : d;
+}
+
 // ApproxTopN's octave of |c|^2: the exponent field of its f64 pattern, NaN counted in the top
 // bin as the reference's histogram counts it (crates/paulistrings/src/truncation/builtin.rs:264-293).
 template <typename T>
@@ -244,6 +252,17 @@ __device__ __forceinline__ uint64_t octave_key(T c) {
     if (isnan(m)) return 0ull;
     return ((uint64_t)__double_as_longlong(m) >> 52) + 1ull;
 }
+
+// A coefficient's bit pattern in a 64-bit word and back, so a loop can issue all of its loads
+// before it uses any of them.
+__device__ __forceinline__ uint64_t raw_bits(double v) { return (uint64_t)__double_as_longlong(v); }
+__device__ __forceinline__ uint64_t raw_bits(float v) { return (uint64_t)__float_as_uint(v); }
+template <typename T>
+__device__ __forceinline__ T from_raw(uint64_t r);
+template <>
+__device__ __forceinline__ double from_raw<double>(uint64_t r) { return __longlong_as_double((long long)r); }
+template <>
+__device__ __forceinline__ float from_raw<float>(uint64_t r) { return __uint_as_float((uint32_t)r); }
 
 // Knuth TwoSum: s + e == a + b exactly.
 template <typename T>

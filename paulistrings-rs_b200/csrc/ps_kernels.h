@@ -203,8 +203,9 @@ struct RotationArgs {
     unsigned int* err_flags;          // the control block's error bits after the layer
     unsigned int* err_info;
     KernelProf* prof;
-    unsigned int* topn_hist;  // when set, the merge histograms key >> 52 of its outputs (2048 bins)
-    int topn_hist_octave;     // ... or, when nonzero, their octave of |c|^2 (ApproxTopN)
+    unsigned int* topn_hist;  // when set, the merge histograms its outputs into 2048 bins:
+    int topn_hist_mode;       // 0 select key >> 52, 1 octave of |c|^2 (ApproxTopN),
+    uint64_t topn_hist_base;  // 2 window_key(select key, topn_hist_base) >> 48
     int inject_stall;         // failure injection: the merge skips its first tile
 };
 

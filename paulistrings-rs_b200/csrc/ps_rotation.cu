@@ -653,7 +653,8 @@ __device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc
                                                uint32_t i, uint32_t ie, uint32_t j, uint32_t je,
                                                const RotLayer<W>& L, const AmpTab<T>& A, const KeepProg& keep,
                                                uint64_t* __restrict__ Ok, T* __restrict__ Oc,
-                                               unsigned long long out, unsigned int* s_hist, int hist_octave) {
+                                               unsigned long long out, unsigned int* s_hist, int hist_mode,
+                                               uint64_t hist_base) {
     uint32_t count = 0;
     uint64_t a[2 * W], b[2 * W];
     if (i < ie) ld_row<W>(sSk, i, a);
@@ -681,7 +682,16 @@ __device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc
             if (kStore) {
                 store_key<W>(Ok, out + count, k);
                 Oc[out + count] = v;
-                if (s_hist) atomicAdd(&s_hist[hist_octave ? octave_bin<T>(v) : (uint32_t)(mag_key<T>(v) >> 52)], 1u);
+                if (s_hist) {
+                    uint32_t bin;
+                    if (hist_mode == 1)
+                        bin = octave_bin<T>(v);
+                    else if (hist_mode == 2)
+                        bin = (uint32_t)(window_key(mag_key<T>(v), hist_base) >> 48);
+                    else
+                        bin = (uint32_t)(mag_key<T>(v) >> 52);
+                    atomicAdd(&s_hist[bin], 1u);
+                }
             }
             ++count;
         }
@@ -696,7 +706,8 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
                                                   const RotLayer<W> L, const KeepProg keep,
                                                   uint64_t* __restrict__ Ok, T* __restrict__ Oc, uint64_t out_cap,
                                                   unsigned long long* status, Ctl* ctl,
-                                                  unsigned int* __restrict__ topn_hist, int hist_octave) {
+                                                  unsigned int* __restrict__ topn_hist, int hist_mode,
+                                                  uint64_t hist_base) {
     using SM = MergeSmem<W, T>;
     constexpr int ITEMS = RotTile<W>::kMergeItems;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -779,7 +790,8 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
     const uint32_t i0 = s_si[tid], j0 = s_sj[tid];
     const uint32_t ie = max(s_si[tid + 1], i0), je = max(s_sj[tid + 1], j0);
     const uint32_t count =
-        merge_walk<W, T, false>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, A, keep, nullptr, nullptr, 0ull, nullptr, 0);
+        merge_walk<W, T, false>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, A, keep, nullptr, nullptr, 0ull, nullptr, 0,
+                                0ull);
     unsigned int total;
     unsigned int excl = block_exclusive_sum<kBlock>(count, s_warp, total);
     if (tid < 32) {
@@ -800,7 +812,7 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
     const unsigned long long off = s_outoff;
     if (!PS_GUARD(ctl, off + total <= out_cap, 304)) return;
     merge_walk<W, T, true>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, A, keep, Ok, Oc, off + excl,
-                           topn_hist ? s_hist : nullptr, hist_octave);
+                           topn_hist ? s_hist : nullptr, hist_mode, hist_base);
     if (topn_hist) {
         __syncthreads();
         for (int q = tid; q < kTopnHistBins; q += kBlock)
@@ -896,7 +908,8 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     size_t smem = MergeSmem<W, T>::bytes;
     a.prof->begin(K_MERGE, 0.0, st);
     k_merge<W, T><<<mtiles_hi, kBlock, smem, st>>>(a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc,
-                                                  a.out_cap, a.status, ctl, a.topn_hist, a.topn_hist_octave);
+                                                  a.out_cap, a.status, ctl, a.topn_hist, a.topn_hist_mode,
+                                                  a.topn_hist_base);
     a.prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // counts and error flags in one copy: count[0..7], tile_counter[0..7], err, err_info

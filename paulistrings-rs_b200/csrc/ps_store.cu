@@ -398,11 +398,14 @@ __global__ void __launch_bounds__(kThreads) k_octave_hist(const T* __restrict__ 
 }
 
 // Gather the keys of the boundary bin (order does not matter for the select): each block
-// takes chunks of kThreads * 16 elements and claims its output slots with one atomic per chunk.
+// takes chunks of kThreads * 16 elements and appends their candidates to its own segment of
+// the candidate buffer (seg_cap keys, room for every element of the block's chunks), so no
+// counter is shared between blocks; seg_count[block] receives the segment's length.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_topn_cand(const T* __restrict__ coef, const uint64_t* __restrict__ sel,
-                                                        uint64_t n, Ctl* ctl, uint64_t* __restrict__ cand,
-                                                        uint64_t cand_cap) {
+                                                        int window, uint64_t base, uint64_t n, Ctl* ctl,
+                                                        uint64_t* __restrict__ cand, uint64_t cand_cap,
+                                                        uint64_t seg_cap, unsigned int* __restrict__ seg_count) {
     constexpr int ITEMS = 16;
     constexpr int CHUNK = kThreads * ITEMS;
     __shared__ unsigned int s_w[kThreads / 32];
@@ -410,15 +413,31 @@ __global__ void __launch_bounds__(kThreads) k_topn_cand(const T* __restrict__ co
     const uint64_t prefix = ctl->aux[0], mask = ctl->aux[1];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned int lt = (1u << lane) - 1u;
+    if (window && blockIdx.x == 0 && tid == 0) {
+        const uint64_t bin = prefix >> 48;
+        if (bin == 0 || bin == 2047) ctl->aux[5] = 1;  // the boundary left the window: retry in full range
+    }
+    if (tid == 0) s_base = 0;
+    __syncthreads();
     for (uint64_t c0 = (uint64_t)blockIdx.x * CHUNK; c0 < n; c0 += (uint64_t)gridDim.x * CHUNK) {
         const uint64_t wbase = c0 + (uint64_t)warp * 32 * ITEMS;
+        // every load of the chunk first, then the keys and ballots
+        uint64_t key[ITEMS];
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            const uint64_t e = wbase + (uint64_t)i * 32 + lane;
+            key[i] = e < n ? (sel ? sel[e] : raw_bits(coef[e])) : 0ull;
+        }
         unsigned int ball[ITEMS];
         unsigned int wc = 0;
 #pragma unroll
         for (int i = 0; i < ITEMS; ++i) {
             const uint64_t e = wbase + (uint64_t)i * 32 + lane;
-            bool hit = false;
-            if (e < n) hit = (select_key<T>(coef, sel, e) & mask) == prefix;
+            if (!sel) {
+                const uint64_t mk = mag_key<T>(from_raw<T>(key[i]));
+                key[i] = window ? window_key(mk, base) : mk;
+            }
+            const bool hit = e < n && (key[i] & mask) == prefix;
             ball[i] = __ballot_sync(0xffffffffu, hit);
             wc += __popc(ball[i]);
         }
@@ -430,31 +449,39 @@ __global__ void __launch_bounds__(kThreads) k_topn_cand(const T* __restrict__ co
             wx += w < warp ? s_w[w] : 0u;
             tot += s_w[w];
         }
-        if (tid == 0) s_base = tot ? atomicAdd(&ctl->count[4], (unsigned long long)tot) : 0ull;
+        // this block's own segment of the candidate buffer: no counter shared between blocks
+        const unsigned long long seg_used = s_base;
         __syncthreads();
-        unsigned long long slot = s_base + wx;
+        if (tid == 0) s_base = seg_used + tot;
+        unsigned long long slot = (uint64_t)blockIdx.x * seg_cap + seg_used + wx;
 #pragma unroll
         for (int i = 0; i < ITEMS; ++i) {
             if ((ball[i] >> lane) & 1u) {
-                const uint64_t e = wbase + (uint64_t)i * 32 + lane;
                 const unsigned long long q = slot + __popc(ball[i] & lt);
-                if (PS_GUARD(ctl, q < cand_cap, 703)) cand[q] = select_key<T>(coef, sel, e);
+                if (PS_GUARD(ctl, q < cand_cap, 703)) cand[q] = key[i];
             }
             slot += __popc(ball[i]);
         }
         __syncthreads();
     }
+    if (tid == 0) seg_count[blockIdx.x] = (unsigned int)s_base;
 }
 
 __global__ void __launch_bounds__(kThreads) k_topn_hist_cand(const uint64_t* __restrict__ cand, Ctl* ctl, int shift,
-                                                             unsigned int* __restrict__ hist) {
+                                                             unsigned int* __restrict__ hist, uint64_t seg_cap,
+                                                             const unsigned int* __restrict__ seg_count,
+                                                             unsigned int nseg) {
     __shared__ unsigned int sh[kTopnBinsN];
     for (int i = threadIdx.x; i < kTopnBinsN; i += kThreads) sh[i] = 0;
     __syncthreads();
-    const uint64_t prefix = ctl->aux[0], mask = ctl->aux[1], m = ctl->count[4];
-    for (uint64_t i = blockIdx.x * (uint64_t)kThreads + threadIdx.x; i < m; i += (uint64_t)gridDim.x * kThreads) {
-        uint64_t mk = cand[i];
-        if ((mk & mask) == prefix) atomicAdd(&sh[(mk >> shift) & (kTopnBinsN - 1)], 1u);
+    const uint64_t prefix = ctl->aux[0], mask = ctl->aux[1];
+    for (unsigned int g = blockIdx.x; g < nseg; g += gridDim.x) {
+        const uint64_t* seg = cand + (uint64_t)g * seg_cap;
+        const unsigned int len = seg_count[g];
+        for (unsigned int i = threadIdx.x; i < len; i += kThreads) {
+            const uint64_t mk = seg[i];
+            if ((mk & mask) == prefix) atomicAdd(&sh[(mk >> shift) & (kTopnBinsN - 1)], 1u);
+        }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < kTopnBinsN; i += kThreads)
@@ -467,7 +494,7 @@ __global__ void __launch_bounds__(kThreads) k_topn_hist_cand(const uint64_t* __r
 template <int W, typename T>
 __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __restrict__ keys, const T* __restrict__ coef,
                                                            const uint64_t* __restrict__ sel, int key_mode,
-                                                           uint64_t n, unsigned long long keep_n,
+                                                           uint64_t base, uint64_t n, unsigned long long keep_n,
                                                            uint64_t* __restrict__ okeys, T* __restrict__ ocoef,
                                                            unsigned long long* status, Ctl* ctl) {
     const unsigned long long quota = ctl->aux[0] == 0 ? 0ull : keep_n - ctl->aux[3];
@@ -481,7 +508,7 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
     if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[6], 1u);
     __syncthreads();
     const unsigned int tile = s_tile;
-    const uint64_t boundary = ctl->aux[0];
+    const uint64_t boundary = ctl->aux[0] == 0 ? 0ull : ctl->aux[0] + base;  // a windowed select's key back in full range
     const uint64_t wbase = (uint64_t)tile * TILE + (uint64_t)warp * 32 * ITEMS;
     unsigned int ba[ITEMS], bt[ITEMS];
     unsigned int wa = 0, wt = 0;
@@ -612,6 +639,17 @@ static inline unsigned int grid_for(uint64_t n, int sms) {
     return (unsigned int)(blocks ? blocks : 1);
 }
 
+// Keys per block segment of the TopN candidate buffer: every element of the block's chunks.
+static inline uint64_t topn_seg_cap(uint64_t n, int sms) {
+    const uint64_t g = grid_for(n, sms), nchunks = (n + kThreads * 16 - 1) / (kThreads * 16);
+    return (nchunks + g - 1) / g * (kThreads * 16);
+}
+
+uint64_t topn_cand_words(uint64_t n, int sms) {
+    const uint64_t g = grid_for(n, sms);
+    return topn_seg_cap(n, sms) * g + (g + 1) / 2;
+}
+
 template <int W, typename T>
 cudaError_t StoreOps<W, T>::pack(const uint64_t* x, const uint64_t* z, const double* c, uint64_t n, uint32_t nq,
                                  uint64_t* keys, T* coef, uint32_t* vals, Ctl* ctl, int sms, cudaStream_t st,
@@ -725,15 +763,24 @@ template <int W, typename T>
 cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n, uint64_t keep_n, uint64_t* okeys,
                                  T* ocoef, unsigned int* hist, bool hist_ready, uint64_t* cand, uint64_t cand_cap,
                                  unsigned long long* status, Ctl* ctl, unsigned long long* host_count,
-                                 uint64_t* out_n, int sms, cudaStream_t st, KernelProf* prof, const uint64_t* sel) {
-    // aux: prefix, mask, remaining rank, above; count[4]: candidates
+                                 uint64_t* out_n, int sms, cudaStream_t st, KernelProf* prof, const uint64_t* sel,
+                                 bool window, uint64_t base) {
+    // aux: prefix, mask, remaining rank, above, -, window miss; count[4]: candidates
+    window = window && hist_ready && !sel;
+    if (!window) base = 0;
     unsigned long long* init = host_count + 8;
     init[0] = 0ull;
     init[1] = 0ull;
     init[2] = (unsigned long long)keep_n;
     init[3] = 0ull;
-    cudaMemcpyAsync(ctl->aux, init, 4 * sizeof(unsigned long long), cudaMemcpyHostToDevice, st);
-    cudaMemsetAsync(&ctl->count[4], 0, sizeof(unsigned long long), st);
+    init[4] = 0ull;
+    init[5] = 0ull;
+    cudaMemcpyAsync(ctl->aux, init, 6 * sizeof(unsigned long long), cudaMemcpyHostToDevice, st);
+    const unsigned int cgrid = grid_for(n, sms);
+    const uint64_t seg_cap = topn_seg_cap(n, sms);
+    const uint64_t key_cap = seg_cap * cgrid;  // segments, then the segment lengths
+    if (key_cap + (cgrid + 1) / 2 > cand_cap) return cudaErrorInvalidValue;  // sized by topn_cand_words
+    unsigned int* seg_count = reinterpret_cast<unsigned int*>(cand + key_cap);
     cudaError_t e;
     if (!hist_ready) {
         cudaMemsetAsync(hist, 0, kTopnBins1 * sizeof(unsigned int), st);
@@ -743,16 +790,20 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
                                                             n, hist);
         prof->end(st);
     }
+    // digit 1: the select key's top 12 bits (key >> 52), or in a window the bin of 2^48 units;
+    // then 13-bit digits down to bit 0 (a window's last digit overlaps bits already fixed)
     prof->begin(K_TOPN_STEP, kTopnBins1 * 8.0, st);
-    k_topn_select<kTopnBins1><<<1, 1024, 0, st>>>(hist, 52, 12, ctl);
+    k_topn_select<kTopnBins1><<<1, 1024, 0, st>>>(hist, window ? 48 : 52, window ? 11 : 12, ctl);
     prof->end(st);
     prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
-    k_topn_cand<T><<<grid_for(n, sms), kThreads, 0, st>>>(coef, sel, n, ctl, cand, cand_cap);
+    k_topn_cand<T><<<cgrid, kThreads, 0, st>>>(coef, sel, window ? 1 : 0, base, n, ctl, cand, key_cap, seg_cap,
+                                              seg_count);
     prof->end(st);
-    // 52 remaining bits: digits at 39, 26, 13, 0 (13 bits each)
-    for (int shift = 39; shift >= 0; shift -= 13) {
+    static const int kShifts[2][4] = {{39, 26, 13, 0}, {35, 22, 9, 0}};
+    for (int d = 0; d < 4; ++d) {
+        const int shift = kShifts[window ? 1 : 0][d];
         prof->begin(K_TOPN_HIST, 0.0, st);
-        k_topn_hist_cand<<<2 * sms, kThreads, 0, st>>>(cand, ctl, shift, hist);
+        k_topn_hist_cand<<<2 * sms, kThreads, 0, st>>>(cand, ctl, shift, hist, seg_cap, seg_count, cgrid);
         prof->end(st);
         prof->begin(K_TOPN_STEP, kTopnBinsN * 8.0, st);
         k_topn_select<kTopnBinsN><<<1, 1024, 0, st>>>(hist, shift, 13, ctl);
@@ -763,13 +814,12 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     cudaMemsetAsync(status, 0, (size_t)tiles * sizeof(unsigned long long), st);
     cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
-    k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, sel, sel ? 1 : 0, n, (unsigned long long)keep_n,
-                                                     okeys, ocoef, status, ctl);
+    k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, sel, sel ? 1 : 0, base, n,
+                                                     (unsigned long long)keep_n, okeys, ocoef, status, ctl);
     prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    // the one host synchronization of the pass: counts and error flags in one copy
-    cudaMemcpyAsync(host_count, &ctl->count[0], offsetof(Ctl, err_info) + sizeof(unsigned int),
-                    cudaMemcpyDeviceToHost, st);
+    // the one host synchronization of the pass: counts, error flags and the select's aux words
+    cudaMemcpyAsync(host_count, &ctl->count[0], offsetof(Ctl, spin_limit), cudaMemcpyDeviceToHost, st);
     if ((e = spin_sync(st)) != cudaSuccess) return e;
     *out_n = host_count[3];
     prof->add_bytes(K_TOPN_COMPACT, (double)*out_n * (2 * 16 * W + sizeof(T)));
@@ -818,8 +868,8 @@ cudaError_t StoreOps<W, T>::approx_topn(const uint64_t* keys, const T* coef, uin
     cudaMemsetAsync(status, 0, (size_t)tiles * sizeof(unsigned long long), st);
     cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
-    k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, nullptr, 2, n, (unsigned long long)keep_n, okeys,
-                                                     ocoef, status, ctl);
+    k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, nullptr, 2, 0ull, n, (unsigned long long)keep_n,
+                                                     okeys, ocoef, status, ctl);
     prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     cudaMemcpyAsync(host_count, &ctl->count[0], offsetof(Ctl, err_info) + sizeof(unsigned int),

@@ -21,6 +21,22 @@ struct SortScratch {
     unsigned int* host_base;   // pinned, 16W x 256
 };
 
+// 64-bit words the TopN candidate buffer needs for n terms (block segments and their lengths).
+uint64_t topn_cand_words(uint64_t n, int sms);
+
+// The select's boundary (full-range select key) and whether a windowed select missed, from
+// the aux words StoreOps::topn leaves in host_count.
+inline uint64_t topn_boundary(const unsigned long long* host_count, uint64_t base) {
+    const unsigned long long* aux = reinterpret_cast<const unsigned long long*>(
+        reinterpret_cast<const unsigned char*>(host_count) + offsetof(Ctl, aux));
+    return aux[0] == 0 ? 0 : aux[0] + base;
+}
+inline bool topn_window_missed(const unsigned long long* host_count) {
+    const unsigned long long* aux = reinterpret_cast<const unsigned long long*>(
+        reinterpret_cast<const unsigned char*>(host_count) + offsetof(Ctl, aux));
+    return aux[5] != 0;
+}
+
 // Error bits and check id left in host_count by StoreOps::topn.
 inline void topn_flags(const unsigned long long* host_count, unsigned int* flags, unsigned int* info) {
     const unsigned int* f = reinterpret_cast<const unsigned int*>(reinterpret_cast<const unsigned char*>(host_count) +
@@ -58,7 +74,8 @@ struct StoreOps {
     static cudaError_t topn(const uint64_t* keys, const T* coef, uint64_t n, uint64_t keep_n, uint64_t* okeys, T* ocoef,
                             unsigned int* hist, bool hist_ready, uint64_t* cand, uint64_t cand_cap,
                             unsigned long long* status, Ctl* ctl, unsigned long long* host_count, uint64_t* out_n,
-                            int sms, cudaStream_t st, KernelProf* prof, const uint64_t* sel = nullptr);
+                            int sms, cudaStream_t st, KernelProf* prof, const uint64_t* sel = nullptr,
+                            bool window = false, uint64_t base = 0);
     // ApproxTopN (crates/paulistrings/src/truncation/builtin.rs:240-468): every octave of |c|^2
     // above the boundary octave kept, then the first quota boundary terms in key order.
     // hist: 2048 words, zero on entry and exit, holding the octave histogram when hist_ready;

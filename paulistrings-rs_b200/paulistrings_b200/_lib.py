@@ -24,7 +24,7 @@ PS_OK, PS_ERR_OOM, PS_ERR_UNSUPPORTED, PS_ERR_INVALID, PS_ERR_DEVICE, PS_ERR_TIM
 PS_F64, PS_F32 = 0, 1
 PS_FORWARD, PS_HEISENBERG = 0, 1
 PS_KEEP_TRUE, PS_KEEP_COEFF, PS_KEEP_WEIGHT, PS_KEEP_AND, PS_KEEP_OR = range(5)
-PS_PASS_NONE, PS_PASS_TOPN, PS_PASS_SCORED_TOPN, PS_PASS_APPROX_TOPN = 0, 1, 2, 3
+PS_PASS_NONE, PS_PASS_TOPN, PS_PASS_SCORED_TOPN, PS_PASS_APPROX_TOPN, PS_PASS_COLLAPSE_SAMPLE = 0, 1, 2, 3, 4
 (PS_CH_PAULI_ROTATION, PS_CH_DEPOLARIZING, PS_CH_HADAMARD, PS_CH_PHASE, PS_CH_PHASE_DAGGER, PS_CH_PAULI_X,
  PS_CH_PAULI_Y, PS_CH_PAULI_Z, PS_CH_CNOT, PS_CH_CZ, PS_CH_SWAP, PS_CH_UNITARY, PS_CH_DEPHASING,
  PS_CH_PAULI_CHANNEL, PS_CH_DEPOLARIZING_2Q, PS_CH_AMPLITUDE_DAMPING) = range(1, 17)
@@ -87,7 +87,8 @@ class ScorerConfig(ctypes.Structure):
 
 
 class Pass(ctypes.Structure):
-    _fields_ = [("kind", ctypes.c_int32), ("reserved", ctypes.c_int32), ("n", ctypes.c_uint64)]
+    _fields_ = [("kind", ctypes.c_int32), ("reserved", ctypes.c_int32), ("n", ctypes.c_uint64),
+                ("samples", ctypes.c_uint64), ("seed", ctypes.c_uint64), ("call", ctypes.c_uint64)]
 
 
 class Policy(ctypes.Structure):
@@ -157,6 +158,7 @@ class RunStats(ctypes.Structure):
         ("total_terms_in", ctypes.c_uint64),
         ("kernel_launches", ctypes.c_uint64),
         ("device_ms", ctypes.c_double),
+        ("collapses", ctypes.c_uint64),
     ]
 
 

@@ -245,3 +245,30 @@ def attribution_data(observable: PauliSum, step: Circuit, steps: int, state: str
     finally:
         g.close()
     return tuple(np.concatenate(r) for r in rows)
+
+
+def _score_benchmark(log2_terms: int = 22, num_qubits: int = 64) -> None:
+    """Score 2^log2_terms terms (the 65,536-term random observable of the bench, tiled) with a
+    fresh residual scorer through ``ps_scorer_score``: three warm-up calls, then one timed."""
+    import time
+
+    from . import workloads
+
+    x, z, c = workloads.random_observable(num_qubits, 1 << 16, seed=3)
+    reps = max(1, (1 << log2_terms) // len(c))
+    keys = np.tile(pack_keys(x, z), (reps, 1))
+    logc = np.tile(np.log(np.abs(c)).astype(np.float32), reps)
+    rem = np.full(len(logc), 5.0, np.float32)
+    sc = Scorer(num_qubits, layers_per_unit=96, seed=1, residual=True)
+    for _ in range(3):
+        sc.score(keys, logc, rem)
+    t0 = time.perf_counter()
+    s = sc.score(keys, logc, rem)
+    dt = time.perf_counter() - t0
+    print(f"scored {len(s)} terms, finite {bool(np.all(np.isfinite(s)))}, {dt * 1e3:.2f} ms with host copies")
+
+
+if __name__ == "__main__":
+    import sys
+
+    _score_benchmark(int(sys.argv[1]) if len(sys.argv) > 1 else 22)
