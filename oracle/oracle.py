@@ -27,7 +27,7 @@ LIB_PATH = HERE / "_build" / "libps_oracle.so"
 
 F64, F32 = 0, 1
 _KEEP = {"true": 0, "coeff": 1, "weight": 2, "and": 3, "or": 4}
-_PASS = {"topn": 1, "approx_topn": 3}
+_PASS = {"topn": 1, "approx_topn": 3, "collapse_sample": 4}
 _KIND = {"rotation": 1, "depolarize": 2, "h": 3, "s": 4, "sdg": 5, "x": 6, "y": 7, "z": 8, "cnot": 9,
          "cz": 10, "swap": 11, "unitary": 12, "dephase": 13, "pauli_channel": 14, "depolarize2": 15,
          "amplitude_damping": 16}
@@ -42,6 +42,9 @@ class _Policy(ctypes.Structure):
         ("num_passes", ctypes.c_int32),
         ("pass_kind", ctypes.c_int32 * 4),
         ("pass_n", ctypes.c_uint64 * 4),
+        ("pass_samples", ctypes.c_uint64 * 4),
+        ("pass_seed", ctypes.c_uint64 * 4),
+        ("pass_call", ctypes.c_uint64 * 4),
     ]
 
 
@@ -89,6 +92,13 @@ def lib():
         L.pso_expectation.restype = ctypes.c_double
         L.pso_expectation.argtypes = [vp, vp, vp, vp]
         L.pso_set_threads.argtypes = [ctypes.c_int]
+        L.pso_collapses.restype = ctypes.c_uint64
+        L.pso_collapses.argtypes = []
+        L.pso_splitmix64_first.restype = ctypes.c_uint64
+        L.pso_splitmix64_first.argtypes = [ctypes.c_uint64]
+        L.pso_xoshiro_two.argtypes = [vp, vp]
+        L.pso_keyed_uniform.restype = ctypes.c_double
+        L.pso_keyed_uniform.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
         L.pso_prepare_table.argtypes = [ctypes.POINTER(_Channel), ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp,
                                         vp, vp, vp]
         _lib = L
@@ -110,10 +120,17 @@ def policy_struct(policy) -> _Policy | None:
             p.iarg[i] = int(node[1])
     passes = policy.get("passes", [])
     p.num_passes = len(passes)
-    for i, (kind, n) in enumerate(passes):
-        p.pass_kind[i] = _PASS[kind]
-        p.pass_n[i] = int(n)
+    for i, ps_ in enumerate(passes):
+        p.pass_kind[i] = _PASS[ps_[0]]
+        p.pass_n[i] = int(ps_[1])
+        if len(ps_) > 2:  # collapse_sample: (kind, cache, samples, seed, call)
+            p.pass_samples[i], p.pass_seed[i], p.pass_call[i] = int(ps_[2]), int(ps_[3]), int(ps_[4])
     return p
+
+
+def collapses() -> int:
+    """CollapseSample collapses the oracle performed in this process."""
+    return int(lib().pso_collapses())
 
 
 def channel_array(channels):

@@ -873,11 +873,138 @@ static void approx_topn(pso_sum* s, uint64_t n) {
     free(nan);
 }
 
+/* rng.rs: splitmix64 absorbs the key words, seeds xoshiro256++; uniform() is the first
+ * output's top 53 bits scaled by 2^-53. */
+static uint64_t rng_mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+static uint64_t rng_splitmix(uint64_t* state) {
+    *state += 0x9E3779B97F4A7C15ull;
+    return rng_mix64(*state);
+}
+static uint64_t rng_rotl(uint64_t x, int r) { return (x << r) | (x >> (64 - r)); }
+static double keyed_uniform(uint64_t seed, uint64_t call) {
+    uint64_t key[2] = {seed, call};
+    uint64_t absorbed = 2;
+    for (int i = 0; i < 2; ++i) {
+        uint64_t t = absorbed ^ key[i];
+        absorbed = rng_splitmix(&t);
+    }
+    uint64_t st[4];
+    for (int i = 0; i < 4; ++i) st[i] = rng_splitmix(&absorbed);
+    if (!(st[0] | st[1] | st[2] | st[3])) st[0] = 1;
+    uint64_t out = rng_rotl(st[0] + st[3], 23) + st[0];
+    return (double)(out >> 11) * (1.0 / 9007199254740992.0);
+}
+
+/* Test hooks for the stream: splitmix64's first output from `state`, xoshiro256++'s first two
+ * outputs from `st`, and the keyed uniform. */
+uint64_t pso_splitmix64_first(uint64_t state) { return rng_splitmix(&state); }
+void pso_xoshiro_two(const uint64_t* st_in, uint64_t* out) {
+    uint64_t st[4] = {st_in[0], st_in[1], st_in[2], st_in[3]};
+    for (int k = 0; k < 2; ++k) {
+        out[k] = rng_rotl(st[0] + st[3], 23) + st[0];
+        uint64_t t = st[1] << 17;
+        st[2] ^= st[0];
+        st[3] ^= st[1];
+        st[1] ^= st[2];
+        st[0] ^= st[3];
+        st[2] ^= t;
+        st[3] = rng_rotl(st[3], 45);
+    }
+}
+double pso_keyed_uniform(uint64_t seed, uint64_t call) { return keyed_uniform(seed, call); }
+
+static uint64_t g_call_offset = 0; /* pso_propagate's layer index, added to the policy's call */
+static uint64_t g_collapses = 0;
+uint64_t pso_collapses(void) { return g_collapses; }
+
+/* CollapseSample (collapse_sample.rs:80-172): the store's |c| end to end in key order, each
+ * 1024-term block's start the left-to-right sum of the blocks before it and each boundary the
+ * block start plus a running sum from 0.0; points (u + k) * h, h = sum / samples; a term holding
+ * m points keeps (c / |c|) * (m * h). */
+static void collapse_sample(pso_sum* s, uint64_t cache, uint64_t samples, uint64_t seed, uint64_t call) {
+    size_t n = s->n;
+    if (n <= cache || samples == 0) return;
+    size_t nb = (n + 1023) / 1024;
+    double* starts = (double*)malloc((nb + 1) * sizeof(double));
+    double prefix = 0.0;
+    for (size_t b = 0; b < nb; ++b) {
+        size_t lo = b * 1024, hi = lo + 1024 < n ? lo + 1024 : n;
+        double norm = 0.0;
+        for (size_t i = lo; i < hi; ++i) norm = norm + fabs(coef_at(s, i));
+        starts[b] = prefix;
+        prefix = prefix + norm;
+    }
+    starts[nb] = prefix;
+    double total = prefix;
+    if (!(total > 0.0 && total <= 1.7976931348623157e308)) { /* assert_drawable */
+        free(starts);
+        return;
+    }
+    double u = keyed_uniform(seed, call), step = total / (double)samples;
+    uint64_t* first = (uint64_t*)malloc((nb + 1) * sizeof(uint64_t));
+    for (size_t b = 0; b <= nb; ++b) { /* SystematicPoints::below */
+        double boundary = starts[b];
+        if (boundary >= total) {
+            first[b] = samples;
+            continue;
+        }
+        uint64_t lo = 0, hi = samples;
+        while (lo < hi) {
+            uint64_t mid = lo + (hi - lo) / 2;
+            if ((u + (double)mid) * step < boundary)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        first[b] = lo;
+    }
+    int K = 2 * s->W;
+    size_t w = 0;
+    for (size_t b = 0; b < nb; ++b) {
+        size_t lo = b * 1024, hi = lo + 1024 < n ? lo + 1024 : n;
+        uint64_t next = first[b], end = first[b + 1];
+        double running = 0.0;
+        for (size_t i = lo; i < hi; ++i) {
+            if (next == end) continue;
+            double c = coef_at(s, i);
+            double mag = fabs(c);
+            running = running + mag;
+            double boundary = 0.0 + (starts[b] + running);
+            uint64_t stop = end;
+            if (boundary < total) {
+                stop = next;
+                while (stop < end && (u + (double)stop) * step < boundary) ++stop;
+            }
+            uint64_t m = stop - next;
+            next = stop;
+            if (!m) continue;
+            double v = (c / mag) * ((double)m * step);
+            memmove(s->keys + w * K, s->keys + i * K, (size_t)K * 8);
+            if (s->dtype == PSO_F64)
+                s->c64[w] = v;
+            else
+                s->c32[w] = (float)v;
+            ++w;
+        }
+    }
+    s->n = w;
+    ++g_collapses;
+    free(first);
+    free(starts);
+}
+
 void pso_finalize_layer(pso_sum* s, const pso_policy* policy) {
     if (!policy) return;
     for (int i = 0; i < policy->num_passes; ++i) {
         if (policy->pass_kind[i] == PSO_PASS_TOPN) topn(s, policy->pass_n[i]);
         if (policy->pass_kind[i] == PSO_PASS_APPROX_TOPN) approx_topn(s, policy->pass_n[i]);
+        if (policy->pass_kind[i] == PSO_PASS_COLLAPSE_SAMPLE)
+            collapse_sample(s, policy->pass_n[i], policy->pass_samples[i], policy->pass_seed[i],
+                            policy->pass_call[i] + g_call_offset);
     }
 }
 
@@ -941,7 +1068,10 @@ int pso_propagate(pso_sum* s, const pso_channel* chans, size_t num_channels, con
                   int direction, uint64_t* terms_after) {
     for (size_t li = 0; li < num_channels; ++li) {
         size_t ci = direction ? num_channels - 1 - li : li;
-        if (pso_apply_channel(s, &chans[ci], direction, policy)) return -1;
+        g_call_offset = li;
+        int rc = pso_apply_channel(s, &chans[ci], direction, policy);
+        g_call_offset = 0;
+        if (rc) return -1;
         if (terms_after) terms_after[li] = s->n;
     }
     return 0;
@@ -1257,7 +1387,10 @@ int pso_propagate_sorted(pso_sum* s, const pso_channel* chans, size_t num_channe
                          const pso_policy* policy, int direction, uint64_t* terms_after) {
     for (size_t li = 0; li < num_channels; ++li) {
         size_t ci = direction ? num_channels - 1 - li : li;
-        if (pso_apply_channel_sorted(s, &chans[ci], direction, policy)) return -1;
+        g_call_offset = li;
+        int rc = pso_apply_channel_sorted(s, &chans[ci], direction, policy);
+        g_call_offset = 0;
+        if (rc) return -1;
         if (terms_after) terms_after[li] = s->n;
     }
     return 0;

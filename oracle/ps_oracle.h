@@ -21,6 +21,9 @@
  *   TopN (+NaN, ties)   crates/paulistrings/src/truncation/builtin.rs:73-129, 210-239
  *   ApproxTopN          crates/paulistrings/src/truncation/builtin.rs:240-468 (octave histogram
  *                       with NaN in the top bin, edge walk from the top, boundary quota)
+ *   CollapseSample      crates/paulistrings/src/truncation/collapse_sample.rs:1-240 and the
+ *                       key-addressed stream of crates/paulistrings/src/rng.rs:1-62; stretches
+ *                       accumulated per 1024-term block of the store (the reference's buckets)
  *   And / Or            crates/paulistrings/src/truncation/builtin.rs:479-526, 604-625
  *   Heisenberg order    crates/paulistrings/src/engine/driver.rs:349-352
  *   product readout     crates/paulistrings/src/readout/product_state.rs:84-101
@@ -55,6 +58,7 @@ extern "C" {
 /* layer passes */
 #define PSO_PASS_TOPN 1    /* n = retained count */
 #define PSO_PASS_APPROX_TOPN 3 /* ApproxTopN: octave cut, n = retained count */
+#define PSO_PASS_COLLAPSE_SAMPLE 4 /* CollapseSample: above n terms, systematic resample by |c| */
 
 typedef struct pso_policy {
     int32_t num_nodes;
@@ -64,6 +68,9 @@ typedef struct pso_policy {
     int32_t num_passes;
     int32_t pass_kind[4];
     uint64_t pass_n[4];
+    uint64_t pass_samples[4];  /* CollapseSample: draws per collapse */
+    uint64_t pass_seed[4];     /* CollapseSample: trajectory seed */
+    uint64_t pass_call[4];     /* CollapseSample: pass index of the first layer */
 } pso_policy;
 
 /* channel kinds (same numbers as the product's C ABI) */
@@ -115,6 +122,12 @@ int pso_apply_channel(pso_sum* s, const pso_channel* ch, int adjoint, const pso_
  * declined. */
 int pso_prepare_table(const pso_channel* ch, int adjoint, int W, int nq, int* wide, int* k, uint32_t* qubits,
                       int* num_entries, uint32_t* deltas, double* amps);
+/* Test hooks of the key-addressed stream (rng.rs). */
+uint64_t pso_splitmix64_first(uint64_t state);
+void pso_xoshiro_two(const uint64_t* state4, uint64_t* out2);
+double pso_keyed_uniform(uint64_t seed, uint64_t call);
+/* CollapseSample collapses performed by this process so far. */
+uint64_t pso_collapses(void);
 /* The policy's layer passes alone. */
 void pso_finalize_layer(pso_sum* s, const pso_policy* policy);
 /* The whole circuit; direction 0 = forward, 1 = heisenberg (reverse order, adjoint channels).

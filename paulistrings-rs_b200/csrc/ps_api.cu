@@ -71,6 +71,12 @@ struct ps_sum {
     uint64_t topn_base = 0;   // on the last boundary (the boundary moves little between layers)
     unsigned int* hhist = nullptr;  // pinned, kTopnBins1 words
     bool compensated = false; // sort-path dedup sums runs with TwoSum compensation
+    uint64_t pass_call = 0;        // CollapseSample: added to the policy's call (ps_propagate's layer)
+    uint64_t collapses = 0;        // CollapseSample collapses performed
+    Buf cnorms, cfirst;            // CollapseSample block sums / first points
+    double* hnorms = nullptr;      // pinned, hnorms_cap doubles
+    uint64_t* hfirst = nullptr;    // pinned, hfirst_cap words
+    size_t hnorms_cap = 0, hfirst_cap = 0;
     ps_scorer* scorer = nullptr;   // PS_PASS_SCORED_TOPN
     double scorer_remaining = 0;   // layers still to apply
     Buf sel;                       // scored TopN select keys
@@ -226,8 +232,13 @@ ps_status lower_keep(const ps_policy* p, KeepProg& k, std::string& why) {
         k.fast_k = k.iarg[1 - ci];
     }
     for (int i = 0; i < p->num_passes; ++i) {
+        if (p->passes[i].kind == PS_PASS_COLLAPSE_SAMPLE && p->passes[i].samples == 0) {
+            why = "policy: CollapseSample needs at least one sample";
+            return PS_ERR_INVALID;
+        }
         if (p->passes[i].kind != PS_PASS_TOPN && p->passes[i].kind != PS_PASS_SCORED_TOPN &&
-            p->passes[i].kind != PS_PASS_APPROX_TOPN && p->passes[i].kind != PS_PASS_NONE) {
+            p->passes[i].kind != PS_PASS_APPROX_TOPN && p->passes[i].kind != PS_PASS_COLLAPSE_SAMPLE &&
+            p->passes[i].kind != PS_PASS_NONE) {
             why = "policy: unknown layer pass";
             return PS_ERR_UNSUPPORTED;
         }
@@ -1100,6 +1111,12 @@ struct Engine {
                 if (ps != PS_OK) return ps;
                 continue;
             }
+            if (p.kind == PS_PASS_COLLAPSE_SAMPLE) {
+                if (ready && i == 0) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+                ps_status ps = collapse(s, p.n, p.samples, p.seed, p.call + s->pass_call);
+                if (ps != PS_OK) return ps;
+                continue;
+            }
             if (p.kind == PS_PASS_APPROX_TOPN) {
                 ps_status ps = approx_topn(s, p.n, ready && i == 0 && s->hist_kind == PS_PASS_APPROX_TOPN,
                                            ready && i == 0);
@@ -1161,6 +1178,53 @@ struct Engine {
             s->n = out_n;
         }
         return result;
+    }
+
+    // CollapseSample: above `cache` terms, a systematic resample of `samples` points.
+    static ps_status collapse(ps_sum* s, uint64_t cache, uint64_t samples, uint64_t seed, uint64_t call) {
+        if (s->n <= cache) return PS_OK;
+        const uint64_t n = s->n, nb = (n + 1023) / 1024;
+        const int spare = 1 - s->cur;
+        cudaError_t e = reserve_store(s, spare, n);
+        if (e == cudaSuccess) e = ensure(s, s->cnorms, 2 * (nb + 1) * sizeof(double));
+        if (e == cudaSuccess) e = ensure(s, s->cfirst, (nb + 1) * sizeof(uint64_t));
+        if (e == cudaSuccess) e = ensure(s, s->idx, n * sizeof(uint32_t));
+        if (e == cudaSuccess) e = ensure(s, s->status, (n / 4096 + 4) * sizeof(unsigned long long));
+        if (e == cudaSuccess && s->hnorms_cap < 2 * (nb + 1)) {
+            if (s->hnorms) cudaFreeHost(s->hnorms);
+            s->hnorms = nullptr;
+            s->hnorms_cap = 0;
+            e = cudaMallocHost(&s->hnorms, 2 * (nb + 1) * sizeof(double));
+            if (e == cudaSuccess) s->hnorms_cap = 2 * (nb + 1);
+        }
+        if (e == cudaSuccess && s->hfirst_cap < nb + 1) {
+            if (s->hfirst) cudaFreeHost(s->hfirst);
+            s->hfirst = nullptr;
+            s->hfirst_cap = 0;
+            e = cudaMallocHost(&s->hfirst, (nb + 1) * sizeof(uint64_t));
+            if (e == cudaSuccess) s->hfirst_cap = nb + 1;
+        }
+        if (e != cudaSuccess) return cuda_fail(s, e, "CollapseSample: scratch");
+        uint64_t out_n = 0;
+        bool drawable = true;
+        e = StoreOps<W, T>::collapse_sample(K(s, s->cur), C(s, s->cur), n, samples, seed, call, K(s, spare),
+                                            C(s, spare), (double*)s->cnorms.p, s->hnorms, (uint64_t*)s->cfirst.p,
+                                            s->hfirst, (uint32_t*)s->idx.p, (unsigned long long*)s->status.p,
+                                            s->ctl, s->hcount, &out_n, &drawable, s->stream, &s->prof);
+        s->prof.resolve();
+        if (e != cudaSuccess) return cuda_fail(s, e, "CollapseSample");
+        if (!drawable)
+            return set_err(s, PS_ERR_INVALID,
+                           "CollapseSample: cannot draw by |c| from " + std::to_string(n) +
+                               " terms whose sum of |c| is zero or not finite");
+        unsigned int fl = 0, fi = 0;
+        topn_flags(s->hcount, &fl, &fi);
+        ps_status ps = flags_status(s, fl, fi, "CollapseSample");
+        if (ps != PS_OK) return ps;
+        s->cur = spare;
+        s->n = out_n;
+        ++s->collapses;
+        return PS_OK;
     }
 
     // ApproxTopN: the octave histogram (fused into the layer's merge when use_hist), the edge
@@ -1381,7 +1445,8 @@ ps_status ps_destroy(ps_sum* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (Buf* b : {&s->keys[0], &s->keys[1], &s->coef[0], &s->coef[1], &s->pk, &s->pc, &s->idx, &s->dv, &s->fv,
                    &s->slots, &s->status, &s->bounds, &s->hist, &s->cand, &s->partial, &s->dout, &s->sort_status,
-                   &s->up_x, &s->up_z, &s->up_c, &s->up_k, &s->up_v0, &s->up_v1, &s->up_c0, &s->up_st, &s->sel})
+                   &s->up_x, &s->up_z, &s->up_c, &s->up_k, &s->up_v0, &s->up_v1, &s->up_c0, &s->up_st, &s->sel,
+                   &s->cnorms, &s->cfirst})
         release(*b);
     if (s->ctl) cudaFree(s->ctl);
     if (s->sort.hist) cudaFree(s->sort.hist);
@@ -1391,6 +1456,8 @@ ps_status ps_destroy(ps_sum* s) {
     if (s->hcount) cudaFreeHost(s->hcount);
     if (s->hout) cudaFreeHost(s->hout);
     if (s->hhist) cudaFreeHost(s->hhist);
+    if (s->hnorms) cudaFreeHost(s->hnorms);
+    if (s->hfirst) cudaFreeHost(s->hfirst);
     s->prof.destroy();
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s->levels;
@@ -1474,11 +1541,14 @@ ps_status ps_propagate(ps_sum* s, const ps_channel* channels, uint64_t num_chann
     rs.peak_terms = s->n;
     unsigned long long launches0 = 0;
     for (int i = 0; i < K_NUM_KERNELS; ++i) launches0 += s->prof.launches[i];
+    const uint64_t collapses0 = s->collapses;
     for (uint64_t li = 0; li < num_channels; ++li) {
         ps_layer_stats ls;
         rs.total_terms_in += s->n;
         ps = ps_apply_layer(s, &tables[li], policy, &ls);
+        s->pass_call = li;  // CollapseSample's pass index of this layer
         if (ps == PS_OK) ps = ps_finalize_layer(s, policy);
+        s->pass_call = 0;
         if (ps != PS_OK) {
             s->err = "layer " + std::to_string(li) + ": " + s->err;
             break;
@@ -1498,6 +1568,7 @@ ps_status ps_propagate(ps_sum* s, const ps_channel* channels, uint64_t num_chann
     unsigned long long launches1 = 0;
     for (int i = 0; i < K_NUM_KERNELS; ++i) launches1 += s->prof.launches[i];
     rs.kernel_launches = launches1 - launches0;
+    rs.collapses = s->collapses - collapses0;
     if (stats) *stats = rs;
     return ps;
 }

@@ -580,6 +580,130 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
 }
 
 // ---------------------------------------------------------------------------
+// CollapseSample (crates/paulistrings/src/truncation/collapse_sample.rs): the terms' |c| laid
+// end to end in key order, stretch boundaries accumulated per block of kCollapseBlock terms
+// (the block's start plus a running sum from 0.0, as the reference accumulates per bucket),
+// samples systematic points (u + k) * h; a term holding m points keeps sign(c) * m * h.
+// ---------------------------------------------------------------------------
+constexpr uint64_t kCollapseBlock = 1024;
+
+// One thread per block: the block's sum of |c|, left to right from 0.0.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_collapse_norms(const T* __restrict__ coef, uint64_t n,
+                                                             double* __restrict__ norms) {
+    const uint64_t b = blockIdx.x * (uint64_t)kThreads + threadIdx.x;
+    const uint64_t lo = b * kCollapseBlock;
+    if (lo >= n) return;
+    const uint64_t hi = lo + kCollapseBlock < n ? lo + kCollapseBlock : n;
+    double sum = 0.0;
+    for (uint64_t i = lo; i < hi; ++i) sum = add_rn(sum, fabs(to_f64(coef[i])));
+    norms[b] = sum;
+}
+
+// One thread per block: each term's multiplicity, walking the block's points from first[b]
+// (systematic_resample, collapse_sample.rs:144-172).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_collapse_mult(const T* __restrict__ coef, uint64_t n,
+                                                            const double* __restrict__ starts,
+                                                            const uint64_t* __restrict__ first, double u,
+                                                            uint64_t samples, double total,
+                                                            uint32_t* __restrict__ mult) {
+    const uint64_t b = blockIdx.x * (uint64_t)kThreads + threadIdx.x;
+    const uint64_t lo = b * kCollapseBlock;
+    if (lo >= n) return;
+    const uint64_t hi = lo + kCollapseBlock < n ? lo + kCollapseBlock : n;
+    const double start = starts[b], step = total / (double)samples;
+    uint64_t next = first[b];
+    const uint64_t end = first[b + 1];
+    double running = 0.0;
+    for (uint64_t i = lo; i < hi; ++i) {
+        if (next == end) {
+            mult[i] = 0;
+            continue;
+        }
+        running = add_rn(running, fabs(to_f64(coef[i])));
+        const double boundary = add_rn(0.0, add_rn(start, running));
+        uint64_t stop = end;
+        if (boundary < total) {
+            stop = next;
+            while (stop < end && mul_rn(add_rn(u, (double)stop), step) < boundary) ++stop;
+        }
+        mult[i] = (uint32_t)(stop - next);
+        next = stop;
+    }
+}
+
+// Order-preserving compaction of the drawn terms, coefficient sign(c) * m * h (in f64, then T).
+template <int W, typename T>
+__global__ void __launch_bounds__(kThreads) k_collapse_compact(const uint64_t* __restrict__ keys,
+                                                               const T* __restrict__ coef,
+                                                               const uint32_t* __restrict__ mult, uint64_t n,
+                                                               double step, uint64_t* __restrict__ okeys,
+                                                               T* __restrict__ ocoef, unsigned long long* status,
+                                                               Ctl* ctl) {
+    constexpr int ITEMS = 16;
+    constexpr int TILE = kThreads * ITEMS;
+    __shared__ unsigned int s_tile;
+    __shared__ unsigned int s_w[kThreads / 32];
+    __shared__ unsigned long long s_off;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned int lt = (1u << lane) - 1u;
+    if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[6], 1u);
+    __syncthreads();
+    const unsigned int tile = s_tile;
+    const uint64_t wbase = (uint64_t)tile * TILE + (uint64_t)warp * 32 * ITEMS;
+    unsigned int ball[ITEMS];
+    unsigned int wc = 0;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const uint64_t e = wbase + (uint64_t)i * 32 + lane;
+        ball[i] = __ballot_sync(0xffffffffu, e < n && mult[e] > 0);
+        wc += __popc(ball[i]);
+    }
+    if (lane == 0) s_w[warp] = wc;
+    __syncthreads();
+    unsigned int wx = 0, tot = 0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) {
+        wx += w < warp ? s_w[w] : 0u;
+        tot += s_w[w];
+    }
+    if (tid < 32) {
+        unsigned long long p = 0;
+        if (tile == 0) {
+            if (tid == 0) st_release_u64(status + tile, kFlagInc | (unsigned long long)tot);
+        } else {
+            if (tid == 0) st_release_u64(status + tile, kFlagAgg | (unsigned long long)tot);
+            p = lookback_sum_warp(status, tile, ctl, 721);
+            if (tid == 0) st_release_u64(status + tile, kFlagInc | (p + tot));
+        }
+        if (tid == 0) {
+            s_off = p;
+            if ((uint64_t)(tile + 1) * TILE >= n) ctl->count[3] = p + tot;
+        }
+    }
+    __syncthreads();
+    unsigned long long o = s_off + wx;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        if ((ball[i] >> lane) & 1u) {
+            const uint64_t e = wbase + (uint64_t)i * 32 + lane;
+            const unsigned long long pos = o + __popc(ball[i] & lt);
+            const double c = to_f64(coef[e]);
+            const double weight = mul_rn((double)mult[e], step);
+            const double v = mul_rn(c / fabs(c), weight);  // drawn(), collapse_sample.rs:136-140
+            uint64_t k[2 * W];
+            load_key<W>(keys, e, k);
+            if (PS_GUARD(ctl, pos < n, 722)) {
+                store_key<W>(okeys, pos, k);
+                ocoef[pos] = (T)v;
+            }
+        }
+        o += __popc(ball[i]);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // expectation in a product state
 // ---------------------------------------------------------------------------
 template <int W>
@@ -877,6 +1001,94 @@ cudaError_t StoreOps<W, T>::approx_topn(const uint64_t* keys, const T* coef, uin
     if ((e = spin_sync(st)) != cudaSuccess) return e;
     *out_n = host_count[3];
     prof->add_bytes(K_TOPN_COMPACT, (double)*out_n * (2 * 16 * W + sizeof(T)));
+    return cudaSuccess;
+}
+
+// The key-addressed stream of rng.rs: splitmix64 absorbs the key words, seeds xoshiro256++,
+// and uniform() is the first output's top 53 bits (crates/paulistrings/src/rng.rs:1-62).
+static uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+static uint64_t splitmix64(uint64_t& state) {
+    state += 0x9E3779B97F4A7C15ull;
+    return mix64(state);
+}
+static double keyed_uniform(uint64_t k0, uint64_t k1) {
+    const uint64_t key[2] = {k0, k1};
+    uint64_t absorbed = 2;
+    for (uint64_t w : key) {
+        uint64_t t = absorbed ^ w;
+        absorbed = splitmix64(t);
+    }
+    uint64_t st[4];
+    for (auto& w : st) w = splitmix64(absorbed);
+    if (!(st[0] | st[1] | st[2] | st[3])) st[0] = 1;
+    auto rotl = [](uint64_t x, int r) { return (x << r) | (x >> (64 - r)); };
+    const uint64_t out = rotl(st[0] + st[3], 23) + st[0];
+    return (double)(out >> 11) * (1.0 / 9007199254740992.0);
+}
+
+template <int W, typename T>
+cudaError_t StoreOps<W, T>::collapse_sample(const uint64_t* keys, const T* coef, uint64_t n, uint64_t samples,
+                                            uint64_t seed, uint64_t call, uint64_t* okeys, T* ocoef,
+                                            double* norms, double* host_norms, uint64_t* first,
+                                            uint64_t* host_first, uint32_t* mult, unsigned long long* status,
+                                            Ctl* ctl, unsigned long long* host_count, uint64_t* out_n,
+                                            bool* drawable, cudaStream_t st, KernelProf* prof) {
+    const uint64_t nb = (n + kCollapseBlock - 1) / kCollapseBlock;
+    const unsigned int grid = (unsigned int)((nb + kThreads - 1) / kThreads);
+    cudaError_t e;
+    prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
+    k_collapse_norms<T><<<grid, kThreads, 0, st>>>(coef, n, norms);
+    prof->end(st);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    cudaMemcpyAsync(host_norms, norms, nb * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if ((e = spin_sync(st)) != cudaSuccess) return e;
+    // the blocks' starts, left to right from 0.0, and sum |c| (systematic_resample's `starts`)
+    double* starts = host_norms + nb + 1;
+    double prefix = 0.0;
+    for (uint64_t b = 0; b < nb; ++b) {
+        starts[b] = prefix;
+        prefix += host_norms[b];
+    }
+    starts[nb] = prefix;
+    const double total = prefix;
+    *drawable = total > 0.0 && total <= 1.7976931348623157e308;  // assert_drawable: positive and finite
+    if (!*drawable) return cudaSuccess;
+    const double u = keyed_uniform(seed, call), step = total / (double)samples;
+    auto below = [&](double boundary) {  // SystematicPoints::below
+        if (boundary >= total) return samples;
+        uint64_t lo = 0, hi = samples;
+        while (lo < hi) {
+            const uint64_t mid = lo + (hi - lo) / 2;
+            if ((u + (double)mid) * step < boundary)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        return lo;
+    };
+    for (uint64_t b = 0; b <= nb; ++b) host_first[b] = below(starts[b]);
+    double* dstarts = norms + nb + 1;
+    cudaMemcpyAsync(dstarts, starts, (nb + 1) * sizeof(double), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(first, host_first, (nb + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st);
+    prof->begin(K_TOPN_STEP, (double)n * (sizeof(T) + 4), st);
+    k_collapse_mult<T><<<grid, kThreads, 0, st>>>(coef, n, dstarts, first, u, samples, total, mult);
+    prof->end(st);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const uint32_t tiles = (uint32_t)((n + kThreads * 16 - 1) / (kThreads * 16));
+    cudaMemsetAsync(status, 0, (size_t)tiles * sizeof(unsigned long long), st);
+    cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
+    prof->begin(K_TOPN_COMPACT, (double)n * (4 + sizeof(T)), st);
+    k_collapse_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, mult, n, step, okeys, ocoef, status, ctl);
+    prof->end(st);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    cudaMemcpyAsync(host_count, &ctl->count[0], offsetof(Ctl, err_info) + sizeof(unsigned int),
+                    cudaMemcpyDeviceToHost, st);
+    if ((e = spin_sync(st)) != cudaSuccess) return e;
+    *out_n = host_count[3];
     return cudaSuccess;
 }
 

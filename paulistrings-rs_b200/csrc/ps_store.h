@@ -84,6 +84,15 @@ struct StoreOps {
                                    T* ocoef, unsigned int* hist, bool hist_ready, unsigned int* host_hist,
                                    unsigned long long* status, Ctl* ctl, unsigned long long* host_count,
                                    uint64_t* out_n, int sms, cudaStream_t st, KernelProf* prof);
+    // CollapseSample's draw of `samples` points (the caller decides that n exceeds the cache).
+    // norms: device, 2 * (blocks + 1) doubles; host_norms: pinned, 2 * (blocks + 1); first /
+    // host_first: blocks + 1 words; mult: n words; blocks = ceil(n / 1024).  *drawable false
+    // (nothing written) when sum |c| is zero or not finite.
+    static cudaError_t collapse_sample(const uint64_t* keys, const T* coef, uint64_t n, uint64_t samples,
+                                       uint64_t seed, uint64_t call, uint64_t* okeys, T* ocoef, double* norms,
+                                       double* host_norms, uint64_t* first, uint64_t* host_first, uint32_t* mult,
+                                       unsigned long long* status, Ctl* ctl, unsigned long long* host_count,
+                                       uint64_t* out_n, bool* drawable, cudaStream_t st, KernelProf* prof);
     static cudaError_t expectation(const uint64_t* keys, const T* coef, uint64_t n, const uint64_t* ax,
                                    const uint64_t* az, const uint64_t* neg, double* partial, double* out_dev, int sms,
                                    cudaStream_t st, KernelProf* prof);

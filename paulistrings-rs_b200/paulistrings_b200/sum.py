@@ -123,6 +123,7 @@ class PropagationStats:
     device_ms: float = 0.0
     total_terms_in: int = 0
     kernel_launches: int = 0
+    collapses: int = 0
 
 
 class GpuPauliSum:
@@ -231,6 +232,10 @@ class GpuPauliSum:
             after.ctypes.data, ctypes.byref(rs),
         )
         del keep
+        if policy is not None:  # the CollapseSample pass counters live in the policy
+            for state in policy.collapse_states():
+                state["calls"] += int(rs.layers)
+                state["collapses"] += int(rs.collapses)
         _lib.check(st, self._h, "propagate")
         if with_stats:
             return PropagationStats(
@@ -241,6 +246,7 @@ class GpuPauliSum:
                 device_ms=float(rs.device_ms),
                 total_terms_in=int(rs.total_terms_in),
                 kernel_launches=int(rs.kernel_launches),
+                collapses=int(rs.collapses),
             )
         return None
 
@@ -268,6 +274,9 @@ class GpuPauliSum:
         polp = ctypes.byref(pol) if pol is not None else None
         _lib.check(L.ps_apply_layer(self._h, ctypes.byref(table), polp, ctypes.byref(stats)), self._h, "apply_layer")
         _lib.check(L.ps_finalize_layer(self._h, polp), self._h, "finalize_layer")
+        if policy is not None:
+            for state in policy.collapse_states():
+                state["calls"] += 1
         return stats
 
     def expectation(self, state: str = "z+") -> float:

@@ -3,7 +3,8 @@
 ``coeff(eps)`` keeps ``|c|^2 > eps^2`` (crates/paulistrings/src/truncation/builtin.rs:19-41),
 ``weight(k)`` keeps Pauli weight ``<= k`` (:43-59), ``topn(n)`` retains the ``n`` largest
 magnitudes after every layer (:61-150), ``approx_topn(n)`` cuts at an octave of |c|^2 instead
-(:240-468), ``scored_topn(n, scorer)`` the ``n`` terms a learned
+(:240-468), ``collapse_sample(cache, samples, seed)`` resamples by |c| above a cache
+(collapse_sample.rs), ``scored_topn(n, scorer)`` the ``n`` terms a learned
 scorer ranks highest (``paulistrings_b200.learned``; a ``TruncationPolicy`` of this package,
 crates/paulistrings/src/truncation/mod.rs:30-107).  ``a & b`` keeps a term iff both keep it and runs
 a's layer passes then b's (:470-526); ``a | b`` combines per-term filters only (:574-625).
@@ -37,7 +38,7 @@ class Truncation:
         return Truncation("or", self, other)
 
     def has_layer_pass(self) -> bool:
-        if self.kind in ("topn", "scored_topn", "approx_topn"):
+        if self.kind in ("topn", "scored_topn", "approx_topn", "collapse_sample"):
             return True
         if self.kind in ("and", "or"):
             return self.args[0].has_layer_pass() or self.args[1].has_layer_pass()
@@ -49,6 +50,8 @@ class Truncation:
             return f"({self.args[0]!r}{op}{self.args[1]!r})"
         if self.kind == "scored_topn":
             return f"truncation.scored_topn({self.args[0]!r}, <scorer>)"
+        if self.kind == "collapse_sample":
+            return f"truncation.collapse_sample({self.args[0]!r}, {self.args[1]!r}, {self.args[2]!r})"
         return f"truncation.{self.kind}({', '.join(repr(a) for a in self.args)})"
 
     # -- lowering ----------------------------------------------------------
@@ -66,6 +69,11 @@ class Truncation:
         elif self.kind == "approx_topn":
             nodes.append((_lib.PS_KEEP_TRUE, 0, 0.0))
             passes.append((_lib.PS_PASS_APPROX_TOPN, int(self.args[0])))
+        elif self.kind == "collapse_sample":
+            nodes.append((_lib.PS_KEEP_TRUE, 0, 0.0))
+            state = self.args[3]
+            passes.append((_lib.PS_PASS_COLLAPSE_SAMPLE, int(self.args[0]), int(self.args[1]), int(self.args[2]),
+                           int(state["calls"])))
         elif self.kind in ("and", "or"):
             self.args[0]._lower(nodes, passes)
             self.args[1]._lower(nodes, passes)
@@ -105,10 +113,20 @@ class Truncation:
             p.nodes[i].iarg = iarg
             p.nodes[i].farg = farg
         p.num_passes = len(passes)
-        for i, (kind, n) in enumerate(passes):
-            p.passes[i].kind = kind
-            p.passes[i].n = n
+        for i, ps_ in enumerate(passes):
+            p.passes[i].kind = ps_[0]
+            p.passes[i].n = ps_[1]
+            if len(ps_) > 2:
+                p.passes[i].samples, p.passes[i].seed, p.passes[i].call = ps_[2], ps_[3], ps_[4]
         return p
+
+    def collapse_states(self):
+        """The pass counters of the tree's CollapseSample passes (advanced after each run)."""
+        if self.kind == "collapse_sample":
+            return [self.args[3]]
+        if self.kind in ("and", "or"):
+            return self.args[0].collapse_states() + self.args[1].collapse_states()
+        return []
 
 
 def _simplify(nodes: list) -> list:
@@ -154,6 +172,31 @@ def approx_topn(n: int) -> Truncation:
     if n < 0:
         raise ValueError("approx_topn needs n >= 0")
     return Truncation("approx_topn", int(n))
+
+
+class CollapseSample(Truncation):
+    """CollapseSample (crates/paulistrings/src/truncation/collapse_sample.rs): whenever the sum holds
+    more than ``cache`` terms after a layer, ``samples`` systematic draws in proportion to |c|
+    replace it — an unbiased estimate.  One seed is one trajectory: the uniform of the k-th layer
+    pass is a function of (seed, k), and the pass counter lives in the policy, so reusing a policy
+    continues its sequence."""
+
+    def __init__(self, cache: int, samples: int, seed: int):
+        if samples < 1:
+            raise ValueError("CollapseSample: samples must be at least 1")
+        super().__init__("collapse_sample", int(cache), int(samples), int(seed) & 0xFFFFFFFFFFFFFFFF,
+                         {"calls": 0, "collapses": 0})
+
+    @property
+    def calls(self) -> int:
+        return self.args[3]["calls"]
+
+    def collapses(self) -> int:
+        return self.args[3]["collapses"]
+
+
+def collapse_sample(cache: int, samples: int, seed: int) -> CollapseSample:
+    return CollapseSample(cache, samples, seed)
 
 
 def scored_topn(n: int, scorer) -> Truncation:

@@ -67,8 +67,9 @@ def oracle_policy(policy):
             keep.append((nm, iarg))
         else:
             keep.append((nm,))
-    names = {_lib.PS_PASS_TOPN: "topn", _lib.PS_PASS_APPROX_TOPN: "approx_topn"}
-    return {"keep": keep, "passes": [(names[kind], n) for kind, n in passes if kind in names]}
+    names = {_lib.PS_PASS_TOPN: "topn", _lib.PS_PASS_APPROX_TOPN: "approx_topn",
+             _lib.PS_PASS_COLLAPSE_SAMPLE: "collapse_sample"}
+    return {"keep": keep, "passes": [(names[p[0]],) + tuple(p[1:]) for p in passes if p[0] in names]}
 
 
 def oracle_sum(num_qubits, x, z, c, dtype="f64") -> OracleSum:
