@@ -435,6 +435,64 @@ def finish(args, world, rank, value, max_ms, launches, prof, dev_ms, clocks, sta
     print(json.dumps(line))
 
 
+def precision_report(args):
+    """The precision form of the workload (random layers + depolarizing noise p = 1e-3 on every
+    qubit after each layer), run in float64 and in float32 with compensated sums: one JSON line
+    with the <O> error on |0...0> and the largest coefficient error over the strings both runs
+    kept.  Not the headline metric; a report for the f32 form."""
+    import numpy as np
+    import torch
+
+    import paulistrings_b200 as ps
+    from paulistrings_b200 import _lib, truncation, workloads
+
+    seed = SEED
+    policy = truncation.topn(args.term_cap) & truncation.coeff(EPS)
+    layers = layer_circuits(seed)[: args.precision_layers]
+    for c in layers:
+        c.depolarize(1e-3, range(NUM_QUBITS))
+    x0, z0, c0 = workloads.random_observable(NUM_QUBITS, 65536, seed + 1)
+    out = {}
+    for dtype in ("f64", "f32"):
+        g = ps.GpuPauliSum(NUM_QUBITS, dtype)
+        if dtype == "f32":
+            _lib.check(_lib.lib().ps_set_compensated_sums(g._h, 1), g._h, "compensated")
+        g.upload(x0, z0, c0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for c in layers:
+            g.propagate(c, policy, "heisenberg")
+        torch.cuda.synchronize()
+        secs = time.perf_counter() - t0
+        out[dtype] = (g.expectation("z+"), g.download(), secs)
+        g.close()
+    e64, (x64, z64, c64), s64 = out["f64"]
+    e32, (x32, z32, c32), s32 = out["f32"]
+    k64 = torch.from_numpy(np.concatenate([x64, z64], axis=1).view(np.int64)).cuda()
+    k32 = torch.from_numpy(np.concatenate([x32, z32], axis=1).view(np.int64)).cuda()
+    _, inv = torch.unique(torch.cat([k64, k32]), dim=0, return_inverse=True)
+    m = int(inv.max().item()) + 1
+    a = torch.full((m,), float("nan"), dtype=torch.float64, device="cuda")
+    b = torch.full((m,), float("nan"), dtype=torch.float64, device="cuda")
+    a[inv[: len(c64)]] = torch.from_numpy(c64).cuda()
+    b[inv[len(c64):]] = torch.from_numpy(c32.astype(np.float64)).cuda()
+    both = ~torch.isnan(a) & ~torch.isnan(b)
+    diff = (a - b)[both].abs()
+    line = {
+        "report": "precision (f32 with compensated sums vs f64)",
+        "config": {"workload": "random two-qubit rotation layers + depolarizing p=1e-3 on every qubit after each "
+                               "layer, 64 qubits, 65,536-term random observable, Heisenberg, "
+                               f"TopN({args.term_cap}) & coeff(1e-10)", "layers": len(layers)},
+        "expectation_f64": e64, "expectation_f32": e32,
+        "abs_error": abs(e32 - e64), "rel_error": abs(e32 - e64) / abs(e64) if e64 else None,
+        "terms_f64": int(len(c64)), "terms_f32": int(len(c32)), "common_terms": int(both.sum().item()),
+        "max_coeff_abs_error_common": float(diff.max().item()) if diff.numel() else 0.0,
+        "max_abs_coeff_f64": float(np.max(np.abs(c64))) if len(c64) else 0.0,
+        "seconds": {"f64": round(s64, 3), "f32": round(s32, 3)},
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -445,9 +503,15 @@ def main():
     ap.add_argument("--term-cap", type=int, default=TERM_CAP,
                     help="TopN cap; smaller values give the small cases profiled under ncu")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--precision-report", action="store_true",
+                    help="print the f32-vs-f64 precision report of the noisy workload instead of the bench line")
+    ap.add_argument("--precision-layers", type=int, default=LAYERS)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
+    if args.precision_report:
+        precision_report(args)
+        return
     world, rank, local = dist_setup(args.gpus)
     try:
         if args.impl == "reference":
