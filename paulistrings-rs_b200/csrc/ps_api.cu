@@ -87,6 +87,13 @@ struct ps_sum {
     KernelProf prof;
     long long fault_oom_after = -1;   // failure injection: allocations left before all fail
     bool fault_stall = false;         // failure injection: next merge skips its first tile
+    // Slotted store: the last merge left each tile's rows at the start of a fixed slot of
+    // slot_rows rows (n = the slots' span, live_n = rows in them) for the TopN pass that follows
+    // to compact; every other reader compacts it first (Engine::densify).
+    bool slotted = false;
+    uint64_t live_n = 0;
+    uint32_t slot_rows = 0;
+    Buf slot_count;
     std::string err;
 };
 
@@ -867,6 +874,7 @@ struct Engine {
         const int spare = 1 - s->cur;
         if (n == 0) {
             s->n = 0;
+            s->slotted = false;
             return PS_OK;
         }
         cudaError_t e = cudaSuccess;
@@ -916,6 +924,7 @@ struct Engine {
         }
         s->cur = spare;
         s->n = out_n;
+        s->slotted = false;
         if (s->hist_ready) {
             cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
             s->hist_ready = false;
@@ -923,7 +932,38 @@ struct Engine {
         return PS_OK;
     }
 
+    // Compact a slotted store into the spare buffer (a no-op on a dense store).
+    static ps_status densify(ps_sum* s, const char* what) {
+        if (!s->slotted) return PS_OK;
+        const int spare = 1 - s->cur;
+        cudaError_t e = reserve_store(s, spare, s->live_n);
+        if (e == cudaSuccess) e = ensure(s, s->status, (s->n / 4096 + 4) * sizeof(unsigned long long));
+        if (e != cudaSuccess) return cuda_fail(s, e, what);
+        uint64_t out_n = 0;
+        e = StoreOps<W, T>::densify(K(s, s->cur), C(s, s->cur), s->n, slot_map(s), K(s, spare), C(s, spare),
+                                    (unsigned long long*)s->status.p, s->ctl, s->hcount, &out_n, s->stream, &s->prof);
+        s->prof.resolve();
+        if (e != cudaSuccess) return cuda_fail(s, e, what);
+        unsigned int fl = 0, fi = 0;
+        topn_flags(s->hcount, &fl, &fi);
+        ps_status ps = flags_status(s, fl, fi, what);
+        if (ps != PS_OK) return ps;
+        if (out_n != s->live_n) return set_err(s, PS_ERR_DEVICE, std::string(what) + ": slotted store lost rows");
+        s->cur = spare;
+        s->n = out_n;
+        s->slotted = false;
+        return PS_OK;
+    }
+
+    static SlotMap slot_map(const ps_sum* s) {
+        return s->slotted ? SlotMap{(const unsigned int*)s->slot_count.p, s->slot_rows} : SlotMap{nullptr, 0u};
+    }
+
     static ps_status download(ps_sum* s, uint64_t* x, uint64_t* z, double* c, uint64_t cap, uint64_t* nout) {
+        {
+            ps_status ps = densify(s, "download");
+            if (ps != PS_OK) return ps;
+        }
         if (nout) *nout = s->n;
         if (cap < s->n) return set_err(s, PS_ERR_INVALID, "download: capacity below the term count");
         if (s->n == 0) return PS_OK;
@@ -946,6 +986,7 @@ struct Engine {
         std::string why;
         ps_status ps = lower_keep(policy, keep, why);
         if (ps != PS_OK) return set_err(s, ps, why);
+        if ((ps = densify(s, "apply")) != PS_OK) return ps;
         RotationArgs<W, T> a;
         std::memset(&a, 0, sizeof a);
         bool general = false;
@@ -956,7 +997,16 @@ struct Engine {
         if (n >= (1ull << 31) - 1) return set_err(s, PS_ERR_UNSUPPORTED, "apply: at most 2^31 - 2 terms");
         const int spare = 1 - s->cur;
         const uint64_t out_rows = a.L.partners ? 2 * n : n;
-        cudaError_t e = reserve_store(s, spare, out_rows);
+        // the first layer pass is TopN (or ApproxTopN) and could trigger: the merge builds its
+        // first select digit (the octave histogram); before plain TopN the merge writes slots
+        const int first_pass = policy && policy->num_passes > 0 ? policy->passes[0].kind : PS_PASS_NONE;
+        const bool fuse_topn = (first_pass == PS_PASS_TOPN || first_pass == PS_PASS_APPROX_TOPN) &&
+                               out_rows > policy->passes[0].n;
+        const bool slotted = fuse_topn && first_pass == PS_PASS_TOPN && !s->fault_stall;
+        const uint64_t span_rows = merge_span_rows<W>(out_rows);
+        cudaError_t e = reserve_store(s, spare, slotted ? span_rows : out_rows);
+        if (e == cudaSuccess && slotted)
+            e = ensure(s, s->slot_count, (span_rows / merge_slot_rows<W>() + 1) * sizeof(unsigned int));
         if (e != cudaSuccess) return cuda_fail(s, e, "apply: output store");
         const uint64_t tiles_hi = out_rows / kMinTileRows + 4;
         if ((e = ensure(s, s->status, tiles_hi * sizeof(unsigned long long))) != cudaSuccess ||
@@ -995,11 +1045,6 @@ struct Engine {
         a.err_flags = &err_flags;
         a.err_info = &err_info;
         a.prof = &s->prof;
-        // the first layer pass is TopN (or ApproxTopN) and could trigger: the merge builds its
-        // first select digit (the octave histogram)
-        const int first_pass = policy && policy->num_passes > 0 ? policy->passes[0].kind : PS_PASS_NONE;
-        const bool fuse_topn = (first_pass == PS_PASS_TOPN || first_pass == PS_PASS_APPROX_TOPN) &&
-                               out_rows > policy->passes[0].n;
         const bool window = first_pass == PS_PASS_TOPN && s->topn_window;
         a.topn_hist_mode = first_pass == PS_PASS_APPROX_TOPN ? 1 : (window ? 2 : 0);
         a.topn_hist_base = window ? s->topn_base : 0;
@@ -1010,6 +1055,9 @@ struct Engine {
         a.topn_hist = fuse_topn ? (unsigned int*)s->hist.p : nullptr;
         a.inject_stall = s->fault_stall ? 1 : 0;
         s->fault_stall = false;
+        uint64_t span = 0;
+        a.slot_count = slotted ? (unsigned int*)s->slot_count.p : nullptr;
+        a.span_out = &span;
         e = launch_rotation_layer<W, T>(a, s->stream);
         s->prof.resolve();
         if (e != cudaSuccess) return cuda_fail(s, e, "apply: rotation layer");
@@ -1030,7 +1078,10 @@ struct Engine {
             stats->path = a.L.partners ? PS_PATH_ROTATION : PS_PATH_RESCALE;
         }
         s->cur = spare;
-        s->n = out_n;
+        s->n = slotted ? span : out_n;
+        s->slotted = slotted;
+        s->live_n = out_n;
+        s->slot_rows = slotted ? merge_slot_rows<W>() : 0u;
         return PS_OK;
     }
 
@@ -1099,6 +1150,10 @@ struct Engine {
     }
 
     static ps_status finalize(ps_sum* s, const ps_policy* policy) {
+        if (!(policy && policy->num_passes > 0 && policy->passes[0].kind == PS_PASS_TOPN)) {
+            ps_status ps = densify(s, "finalize");
+            if (ps != PS_OK) return ps;
+        }
         bool ready = s->hist_ready;
         if (ready) s->hist_ready = false;
         if (s->scorer) s->scorer_remaining -= 1.0;
@@ -1129,13 +1184,16 @@ struct Engine {
                 ready = false;
             }
             const bool use_hist = ready && i == 0;
-            if (s->n <= p.n) {
+            if ((s->slotted ? s->live_n : s->n) <= p.n) {
                 if (use_hist) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+                ps_status ps = densify(s, "topn");
+                if (ps != PS_OK) return ps;
                 continue;
             }
             if (p.n == 0) {
                 if (use_hist) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
                 s->n = 0;
+                s->slotted = false;
                 continue;
             }
             const int spare = 1 - s->cur;
@@ -1156,7 +1214,7 @@ struct Engine {
                                          (unsigned int*)s->hist.p, use_hist && attempt == 0, (uint64_t*)s->cand.p,
                                          topn_cand_words(s->n, s->sms), (unsigned long long*)s->status.p, s->ctl,
                                          s->hcount, &out_n, s->sms,
-                                         s->stream, &s->prof, nullptr, win, win ? s->hist_base : 0);
+                                         s->stream, &s->prof, nullptr, win, win ? s->hist_base : 0, slot_map(s));
                 s->prof.resolve();
                 if (e != cudaSuccess) return cuda_fail(s, e, "topn");
                 unsigned int fl = 0, fi = 0;
@@ -1176,6 +1234,7 @@ struct Engine {
             }
             s->cur = spare;
             s->n = out_n;
+            s->slotted = false;
         }
         return result;
     }
@@ -1321,6 +1380,10 @@ struct Engine {
     }
 
     static ps_status expectation(ps_sum* s, const uint64_t* ax, const uint64_t* az, const uint64_t* neg, double* out) {
+        {
+            ps_status ps = densify(s, "expectation");
+            if (ps != PS_OK) return ps;
+        }
         cudaError_t e = ensure(s, s->partial, kExpectBlocks * sizeof(double));
         if (e == cudaSuccess) e = ensure(s, s->dout, sizeof(double));
         if (e != cudaSuccess) return cuda_fail(s, e, "expectation: scratch");
@@ -1446,7 +1509,7 @@ ps_status ps_destroy(ps_sum* s) {
     for (Buf* b : {&s->keys[0], &s->keys[1], &s->coef[0], &s->coef[1], &s->pk, &s->pc, &s->idx, &s->dv, &s->fv,
                    &s->slots, &s->status, &s->bounds, &s->hist, &s->cand, &s->partial, &s->dout, &s->sort_status,
                    &s->up_x, &s->up_z, &s->up_c, &s->up_k, &s->up_v0, &s->up_v1, &s->up_c0, &s->up_st, &s->sel,
-                   &s->cnorms, &s->cfirst})
+                   &s->cnorms, &s->cfirst, &s->slot_count})
         release(*b);
     if (s->ctl) cudaFree(s->ctl);
     if (s->sort.hist) cudaFree(s->sort.hist);
@@ -1479,7 +1542,7 @@ ps_status ps_upload(ps_sum* s, const uint64_t* x, const uint64_t* z, const doubl
 
 ps_status ps_len(ps_sum* s, uint64_t* n) {
     if (!s || !n) return PS_ERR_INVALID;
-    *n = s->n;
+    *n = s->slotted ? s->live_n : s->n;
     return PS_OK;
 }
 

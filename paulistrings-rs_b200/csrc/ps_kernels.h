@@ -176,6 +176,14 @@ struct KernelProf {
     }
 };
 
+// A slotted store: row e is live when e % rows < count[e / rows] (tile e / rows of a slotted
+// merge wrote count[e / rows] rows at the start of its slot).  count == nullptr: every row
+// below n is live (a dense store).
+struct SlotMap {
+    const unsigned int* count;
+    uint32_t rows;
+};
+
 template <int W, typename T>
 struct RotationArgs {
     const uint64_t* Sk;          // sorted store keys (n rows of 2W words)
@@ -207,7 +215,18 @@ struct RotationArgs {
     int topn_hist_mode;       // 0 select key >> 52, 1 octave of |c|^2 (ApproxTopN),
     uint64_t topn_hist_base;  // 2 window_key(select key, topn_hist_base) >> 48
     int inject_stall;         // failure injection: the merge skips its first tile
+    unsigned int* slot_count; // when set, the merge writes tile t at rows t * merge_slot_rows<W>()
+                              // and its row count to slot_count[t], with no look-back (slotted
+                              // output, compacted by the TopN pass that follows); >= merge tiles
+    uint64_t* span_out;       // slotted output: rows its slots span
 };
+
+// Rows of one merge tile's output slot, and the rows a slotted merge of at most `rows_in`
+// input rows (own rows plus partners) can span.
+template <int W>
+uint32_t merge_slot_rows();
+template <int W>
+uint64_t merge_span_rows(uint64_t rows_in);
 
 template <int W, typename T>
 cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st);

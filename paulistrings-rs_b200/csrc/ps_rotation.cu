@@ -644,59 +644,46 @@ __device__ __forceinline__ bool eq_regs(const uint64_t (&a)[2 * W], const uint64
     return d == 0;
 }
 
-// Walk one thread's merge-path range with the two run heads held in registers (one shared
-// load per consumed item).  Own row first, partner second when their keys are equal, as the
-// reference's merge sums bucket-first.  The first walk counts kept outputs; after the
-// tile's output offset is known the second walk (kStore) writes them straight to the store.
-template <int W, typename T, bool kStore>
+// Walk one thread's merge-path range once, with the two run heads held in registers (one
+// shared load per consumed item).  Own row first, partner second when their keys are equal, as
+// the reference's merge sums bucket-first.  A range holds at most ITEMS + 1 rows and an equal
+// pair is consumed in one step, so STEPS = ITEMS + 1 unrolled steps cover it (the caller checks
+// that nothing is left).  Step s leaves its output in ok[s] / ov[s] and sets bit s of the
+// returned mask when the output is kept (nonzero and passing the keep program).
+template <int W, typename T, int STEPS>
 __device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc, const uint64_t* sPk, const T* sPc,
-                                               uint32_t i, uint32_t ie, uint32_t j, uint32_t je,
+                                               uint32_t& i, uint32_t ie, uint32_t& j, uint32_t je,
                                                const RotLayer<W>& L, const AmpTab<T>& A, const KeepProg& keep,
-                                               uint64_t* __restrict__ Ok, T* __restrict__ Oc,
-                                               unsigned long long out, unsigned int* s_hist, int hist_mode,
-                                               uint64_t hist_base) {
-    uint32_t count = 0;
+                                               uint64_t (&ok)[STEPS][2 * W], T (&ov)[STEPS]) {
+    uint32_t mask = 0;
     uint64_t a[2 * W], b[2 * W];
     if (i < ie) ld_row<W>(sSk, i, a);
     if (j < je) ld_row<W>(sPk, j, b);
-    while (i < ie || j < je) {
-        const bool takeS = (j >= je) || (i < ie && le_regs<W>(a, b));
-        uint64_t k[2 * W];
-        T v;
-        if (takeS) {
 #pragma unroll
-            for (int w = 0; w < 2 * W; ++w) k[w] = a[w];
-            v = own_coeff<W, T>(L, A, a, sSc[i]);
-            if (j < je && eq_regs<W>(a, b)) {
-                v = add_rn(v, sPc[j]);
+    for (int s = 0; s < STEPS; ++s) {
+        if (i < ie || j < je) {
+            const bool takeS = (j >= je) || (i < ie && le_regs<W>(a, b));
+            T v;
+            if (takeS) {
+#pragma unroll
+                for (int w = 0; w < 2 * W; ++w) ok[s][w] = a[w];
+                v = own_coeff<W, T>(L, A, a, sSc[i]);
+                if (j < je && eq_regs<W>(a, b)) {
+                    v = add_rn(v, sPc[j]);
+                    if (++j < je) ld_row<W>(sPk, j, b);
+                }
+                if (++i < ie) ld_row<W>(sSk, i, a);
+            } else {
+#pragma unroll
+                for (int w = 0; w < 2 * W; ++w) ok[s][w] = b[w];
+                v = sPc[j];
                 if (++j < je) ld_row<W>(sPk, j, b);
             }
-            if (++i < ie) ld_row<W>(sSk, i, a);
-        } else {
-#pragma unroll
-            for (int w = 0; w < 2 * W; ++w) k[w] = b[w];
-            v = sPc[j];
-            if (++j < je) ld_row<W>(sPk, j, b);
-        }
-        if (v != T(0) && keep_eval<W>(keep, k, to_f64(v))) {
-            if (kStore) {
-                store_key<W>(Ok, out + count, k);
-                Oc[out + count] = v;
-                if (s_hist) {
-                    uint32_t bin;
-                    if (hist_mode == 1)
-                        bin = octave_bin<T>(v);
-                    else if (hist_mode == 2)
-                        bin = (uint32_t)(window_key(mag_key<T>(v), hist_base) >> 48);
-                    else
-                        bin = (uint32_t)(mag_key<T>(v) >> 52);
-                    atomicAdd(&s_hist[bin], 1u);
-                }
-            }
-            ++count;
+            ov[s] = v;
+            if (v != T(0) && keep_eval<W>(keep, ok[s], to_f64(v))) mask |= 1u << s;
         }
     }
-    return count;
+    return mask;
 }
 
 template <int W, typename T>
@@ -707,7 +694,7 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
                                                   uint64_t* __restrict__ Ok, T* __restrict__ Oc, uint64_t out_cap,
                                                   unsigned long long* status, Ctl* ctl,
                                                   unsigned int* __restrict__ topn_hist, int hist_mode,
-                                                  uint64_t hist_base) {
+                                                  uint64_t hist_base, unsigned int* __restrict__ slot_count) {
     using SM = MergeSmem<W, T>;
     constexpr int ITEMS = RotTile<W>::kMergeItems;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -789,12 +776,36 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
     __syncthreads();
     const uint32_t i0 = s_si[tid], j0 = s_sj[tid];
     const uint32_t ie = max(s_si[tid + 1], i0), je = max(s_sj[tid + 1], j0);
-    const uint32_t count =
-        merge_walk<W, T, false>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, A, keep, nullptr, nullptr, 0ull, nullptr, 0,
-                                0ull);
+    constexpr int STEPS = ITEMS + 1;
+    uint64_t ok[STEPS][2 * W];
+    T ov[STEPS];
+    uint32_t i = i0, j = j0;
+    const uint32_t mask = merge_walk<W, T, STEPS>(sSk, Sc_l, sPk, Pc_l, i, ie, j, je, L, A, keep, ok, ov);
+    PS_GUARD(ctl, i >= ie && j >= je, 305);
     unsigned int total;
-    unsigned int excl = block_exclusive_sum<kBlock>(count, s_warp, total);
-    if (tid < 32) {
+    const unsigned int excl = block_exclusive_sum<kBlock>(__popc(mask), s_warp, total);
+    // Every thread is past the walk, so the staged inputs are dead: stage the kept outputs over
+    // them in output order (keys from sK, coefficients from sC) while warp 0 looks back.
+    {
+        uint32_t r = excl;
+#pragma unroll
+        for (int s = 0; s < STEPS; ++s) {
+            if ((mask >> s) & 1u) {
+                store_key<W>(sK, r, ok[s]);
+                sC[r] = ov[s];
+                ++r;
+            }
+        }
+    }
+    fence_proxy_async_shared();  // the bulk store below reads the staged keys through the async proxy
+    if (slot_count) {
+        // slotted output: the tile's slot is fixed, so it waits for no predecessor
+        if (tid == 0) {
+            s_outoff = (unsigned long long)tile * (SM::TILE + 2);
+            slot_count[tile] = total;
+            atomicAdd(&ctl->count[1], (unsigned long long)total);
+        }
+    } else if (tid < 32) {
         unsigned long long p = 0;
         if (tile == 0) {
             if (tid == 0) st_release_u64(status + tile, kFlagInc | (unsigned long long)total);
@@ -811,13 +822,32 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
     __syncthreads();
     const unsigned long long off = s_outoff;
     if (!PS_GUARD(ctl, off + total <= out_cap, 304)) return;
-    merge_walk<W, T, true>(sSk, Sc_l, sPk, Pc_l, i0, ie, j0, je, L, A, keep, Ok, Oc, off + excl,
-                           topn_hist ? s_hist : nullptr, hist_mode, hist_base);
+    // keys: one bulk copy of the staged rows (16W bytes each, so both ends are 16-byte aligned)
+    if (tid == 0 && total) {
+        bulk_s2g(Ok + off * 2 * W, sK, total * 16u * W);
+        bulk_commit();
+    }
+    // coefficients: coalesced stores, with the fused first TopN digit
+    for (uint32_t q = tid; q < total; q += kBlock) {
+        const T v = sC[q];
+        Oc[off + q] = v;
+        if (topn_hist) {
+            uint32_t bin;
+            if (hist_mode == 1)
+                bin = octave_bin<T>(v);
+            else if (hist_mode == 2)
+                bin = (uint32_t)(window_key(mag_key<T>(v), hist_base) >> 48);
+            else
+                bin = (uint32_t)(mag_key<T>(v) >> 52);
+            atomicAdd(&s_hist[bin], 1u);
+        }
+    }
     if (topn_hist) {
         __syncthreads();
         for (int q = tid; q < kTopnHistBins; q += kBlock)
             if (s_hist[q]) atomicAdd(&topn_hist[q], s_hist[q]);
     }
+    if (tid == 0 && total) bulk_wait_read_all();  // shared memory stays valid until the copy has read it
 }
 
 // ---------------------------------------------------------------------------
@@ -890,7 +920,7 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
         *a.out_count = 0;
         return cudaSuccess;
     }
-    if (total_hi > a.out_cap) return cudaErrorMemoryAllocation;
+    if ((a.slot_count ? (uint64_t)mtiles_hi * (MT + 2) : total_hi) > a.out_cap) return cudaErrorMemoryAllocation;
     {
         uint32_t warps = mtiles_hi + 1;
         uint32_t blocks = (warps + 7) / 8;
@@ -900,7 +930,7 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     // 5. merge
-    cudaMemsetAsync(a.status, 0, (size_t)mtiles_hi * sizeof(unsigned long long), st);
+    if (!a.slot_count) cudaMemsetAsync(a.status, 0, (size_t)mtiles_hi * sizeof(unsigned long long), st);
     // failure injection: start the dispenser at tile 1, so tile 0 never publishes and tile 1's
     // bounded look-back gives up
     cudaMemsetAsync(&ctl->tile_counter[3], a.inject_stall ? 1 : 0, 1, st);
@@ -909,7 +939,7 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     a.prof->begin(K_MERGE, 0.0, st);
     k_merge<W, T><<<mtiles_hi, kBlock, smem, st>>>(a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc,
                                                   a.out_cap, a.status, ctl, a.topn_hist, a.topn_hist_mode,
-                                                  a.topn_hist_base);
+                                                  a.topn_hist_base, a.slot_count);
     a.prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // counts and error flags in one copy: count[0..7], tile_counter[0..7], err, err_info
@@ -919,6 +949,7 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     const uint64_t m = a.host_count[0];
     *a.partners_out = m;
     *a.out_count = a.host_count[1];
+    if (a.slot_count) *a.span_out = (a.n + m + MT - 1) / MT * (uint64_t)(MT + 2);
     const unsigned int* flags = reinterpret_cast<const unsigned int*>(
         reinterpret_cast<const unsigned char*>(a.host_count) + offsetof(Ctl, err));
     *a.err_flags = flags[0];
@@ -937,6 +968,21 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     a.prof->add_bytes(K_MERGE, (double)(a.n + m + *a.out_count) * (16 * W + sizeof(T)));
     return cudaSuccess;
 }
+
+template <int W>
+uint32_t merge_slot_rows() {
+    return (uint32_t)RotTile<W>::kMergeTile + 2;
+}
+template <int W>
+uint64_t merge_span_rows(uint64_t rows_in) {
+    return (rows_in + RotTile<W>::kMergeTile - 1) / RotTile<W>::kMergeTile * (uint64_t)merge_slot_rows<W>();
+}
+template uint32_t merge_slot_rows<1>();
+template uint32_t merge_slot_rows<2>();
+template uint32_t merge_slot_rows<4>();
+template uint64_t merge_span_rows<1>(uint64_t);
+template uint64_t merge_span_rows<2>(uint64_t);
+template uint64_t merge_span_rows<4>(uint64_t);
 
 template <int W, typename T>
 cudaError_t configure_rotation_kernels() {

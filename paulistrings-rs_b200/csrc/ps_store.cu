@@ -27,6 +27,30 @@ namespace psb {
 
 constexpr int kThreads = 256;
 
+// Liveness of the rows e0, e0 + 32, e0 + 64, ... of a possibly slotted store (slots hold more
+// than 32 rows), one division up front and a compare per step.
+struct SlotWalk {
+    uint32_t q = 0, r = 0;
+    __device__ SlotWalk(const SlotMap& s, uint64_t e0) {
+        if (s.count) {
+            q = (uint32_t)(e0 / s.rows);
+            r = (uint32_t)(e0 % s.rows);
+        }
+    }
+    // call only for a row below the store's span
+    __device__ bool live(const SlotMap& s) const { return !s.count || r < __ldg(s.count + q); }
+    __device__ void step32(const SlotMap& s) {
+        r += 32;
+        if (r >= s.rows) {
+            r -= s.rows;
+            ++q;
+        }
+    }
+};
+__device__ __forceinline__ bool slot_live(const SlotMap& s, uint64_t e) {
+    return !s.count || (uint32_t)(e % s.rows) < __ldg(s.count + e / s.rows);
+}
+
 // ---------------------------------------------------------------------------
 // pack / unpack
 // ---------------------------------------------------------------------------
@@ -307,11 +331,12 @@ __global__ void __launch_bounds__(kThreads) k_dedup(const uint64_t* __restrict__
 // count[4] candidates.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kThreads) k_topn_hist1(const double* __restrict__ c64, const float* __restrict__ c32,
-                                                         uint64_t n, unsigned int* __restrict__ hist) {
+                                                         uint64_t n, unsigned int* __restrict__ hist, SlotMap slots) {
     __shared__ unsigned int sh[kTopnBins1];
     for (int i = threadIdx.x; i < kTopnBins1; i += kThreads) sh[i] = 0;
     __syncthreads();
     for (uint64_t i = blockIdx.x * (uint64_t)kThreads + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kThreads) {
+        if (!slot_live(slots, i)) continue;
         uint64_t mk = c64 ? mag_key<double>(c64[i]) : mag_key<float>(c32[i]);
         atomicAdd(&sh[mk >> 52], 1u);
     }
@@ -405,7 +430,8 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) k_topn_cand(const T* __restrict__ coef, const uint64_t* __restrict__ sel,
                                                         int window, uint64_t base, uint64_t n, Ctl* ctl,
                                                         uint64_t* __restrict__ cand, uint64_t cand_cap,
-                                                        uint64_t seg_cap, unsigned int* __restrict__ seg_count) {
+                                                        uint64_t seg_cap, unsigned int* __restrict__ seg_count,
+                                                        SlotMap slots) {
     constexpr int ITEMS = 16;
     constexpr int CHUNK = kThreads * ITEMS;
     __shared__ unsigned int s_w[kThreads / 32];
@@ -423,21 +449,24 @@ __global__ void __launch_bounds__(kThreads) k_topn_cand(const T* __restrict__ co
         const uint64_t wbase = c0 + (uint64_t)warp * 32 * ITEMS;
         // every load of the chunk first, then the keys and ballots
         uint64_t key[ITEMS];
+        unsigned int live = 0;  // bit i: element i is a row of the store
+        SlotWalk sw(slots, wbase + lane);
 #pragma unroll
         for (int i = 0; i < ITEMS; ++i) {
             const uint64_t e = wbase + (uint64_t)i * 32 + lane;
-            key[i] = e < n ? (sel ? sel[e] : raw_bits(coef[e])) : 0ull;
+            if (e < n && sw.live(slots)) live |= 1u << i;
+            sw.step32(slots);
+            key[i] = (live >> i) & 1u ? (sel ? sel[e] : raw_bits(coef[e])) : 0ull;
         }
         unsigned int ball[ITEMS];
         unsigned int wc = 0;
 #pragma unroll
         for (int i = 0; i < ITEMS; ++i) {
-            const uint64_t e = wbase + (uint64_t)i * 32 + lane;
             if (!sel) {
                 const uint64_t mk = mag_key<T>(from_raw<T>(key[i]));
                 key[i] = window ? window_key(mk, base) : mk;
             }
-            const bool hit = e < n && (key[i] & mask) == prefix;
+            const bool hit = ((live >> i) & 1u) && (key[i] & mask) == prefix;
             ball[i] = __ballot_sync(0xffffffffu, hit);
             wc += __popc(ball[i]);
         }
@@ -491,12 +520,13 @@ __global__ void __launch_bounds__(kThreads) k_topn_hist_cand(const uint64_t* __r
 // Order-preserving compaction, warp-striped: keeps keys above the boundary and the first
 // `quota` boundary ties in key order, quota = keep_n - (count above the boundary), none when
 // the boundary is NaN (the select leaves boundary and count above in aux[0] / aux[3]).
+// key_mode 3 keeps every row.  Rows outside the slots of a slotted store are skipped.
 template <int W, typename T>
 __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __restrict__ keys, const T* __restrict__ coef,
                                                            const uint64_t* __restrict__ sel, int key_mode,
                                                            uint64_t base, uint64_t n, unsigned long long keep_n,
                                                            uint64_t* __restrict__ okeys, T* __restrict__ ocoef,
-                                                           unsigned long long* status, Ctl* ctl) {
+                                                           unsigned long long* status, Ctl* ctl, SlotMap slots) {
     const unsigned long long quota = ctl->aux[0] == 0 ? 0ull : keep_n - ctl->aux[3];
     constexpr int ITEMS = 16;
     constexpr int TILE = kThreads * ITEMS;
@@ -512,15 +542,21 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
     const uint64_t wbase = (uint64_t)tile * TILE + (uint64_t)warp * 32 * ITEMS;
     unsigned int ba[ITEMS], bt[ITEMS];
     unsigned int wa = 0, wt = 0;
+    SlotWalk sw(slots, wbase + lane);
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
         const uint64_t e = wbase + (uint64_t)i * 32 + lane;
         bool isa = false, ist = false;
-        if (e < n) {
-            const uint64_t mk = compact_key<T>(coef, sel, key_mode, e);
-            isa = mk > boundary;
-            ist = mk == boundary && boundary != 0;
+        if (e < n && sw.live(slots)) {
+            if (key_mode == 3) {  // keep every row (compacting a slotted store)
+                isa = true;
+            } else {
+                const uint64_t mk = compact_key<T>(coef, sel, key_mode, e);
+                isa = mk > boundary;
+                ist = mk == boundary && boundary != 0;
+            }
         }
+        sw.step32(slots);
         ba[i] = __ballot_sync(0xffffffffu, isa);
         bt[i] = __ballot_sync(0xffffffffu, ist);
         wa += __popc(ba[i]);
@@ -888,7 +924,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
                                  T* ocoef, unsigned int* hist, bool hist_ready, uint64_t* cand, uint64_t cand_cap,
                                  unsigned long long* status, Ctl* ctl, unsigned long long* host_count,
                                  uint64_t* out_n, int sms, cudaStream_t st, KernelProf* prof, const uint64_t* sel,
-                                 bool window, uint64_t base) {
+                                 bool window, uint64_t base, SlotMap slots) {
     // aux: prefix, mask, remaining rank, above, -, window miss; count[4]: candidates
     window = window && hist_ready && !sel;
     if (!window) base = 0;
@@ -911,7 +947,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
         prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
         k_topn_hist1<<<grid_for(n, sms), kThreads, 0, st>>>(std::is_same<T, double>::value ? (const double*)coef : nullptr,
                                                             std::is_same<T, float>::value ? (const float*)coef : nullptr,
-                                                            n, hist);
+                                                            n, hist, slots);
         prof->end(st);
     }
     // digit 1: the select key's top 12 bits (key >> 52), or in a window the bin of 2^48 units;
@@ -921,7 +957,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     prof->end(st);
     prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
     k_topn_cand<T><<<cgrid, kThreads, 0, st>>>(coef, sel, window ? 1 : 0, base, n, ctl, cand, key_cap, seg_cap,
-                                              seg_count);
+                                              seg_count, slots);
     prof->end(st);
     static const int kShifts[2][4] = {{39, 26, 13, 0}, {35, 22, 9, 0}};
     for (int d = 0; d < 4; ++d) {
@@ -939,7 +975,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
     k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, sel, sel ? 1 : 0, base, n,
-                                                     (unsigned long long)keep_n, okeys, ocoef, status, ctl);
+                                                     (unsigned long long)keep_n, okeys, ocoef, status, ctl, slots);
     prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // the one host synchronization of the pass: counts, error flags and the select's aux words
@@ -947,6 +983,34 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     if ((e = spin_sync(st)) != cudaSuccess) return e;
     *out_n = host_count[3];
     prof->add_bytes(K_TOPN_COMPACT, (double)*out_n * (2 * 16 * W + sizeof(T)));
+    return cudaSuccess;
+}
+
+template <int W, typename T>
+cudaError_t StoreOps<W, T>::densify(const uint64_t* keys, const T* coef, uint64_t n, SlotMap slots, uint64_t* okeys,
+                                    T* ocoef, unsigned long long* status, Ctl* ctl, unsigned long long* host_count,
+                                    uint64_t* out_n, cudaStream_t st, KernelProf* prof) {
+    if (n == 0) {
+        *out_n = 0;
+        return cudaSuccess;
+    }
+    unsigned long long* init = host_count + 8;
+    for (int q = 0; q < 4; ++q) init[q] = 0ull;  // no boundary, no quota
+    cudaMemcpyAsync(ctl->aux, init, 4 * sizeof(unsigned long long), cudaMemcpyHostToDevice, st);
+    const uint32_t tiles = (uint32_t)((n + kThreads * 16 - 1) / (kThreads * 16));
+    cudaMemsetAsync(status, 0, (size_t)tiles * sizeof(unsigned long long), st);
+    cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
+    prof->begin(K_TOPN_COMPACT, 0.0, st);
+    k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, nullptr, 3, 0ull, n, 0ull, okeys, ocoef, status, ctl,
+                                                     slots);
+    prof->end(st);
+    cudaError_t e;
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    cudaMemcpyAsync(host_count, &ctl->count[0], offsetof(Ctl, err_info) + sizeof(unsigned int),
+                    cudaMemcpyDeviceToHost, st);
+    if ((e = spin_sync(st)) != cudaSuccess) return e;
+    *out_n = host_count[3];
+    prof->add_bytes(K_TOPN_COMPACT, (double)*out_n * (2 * 16 * W + 2 * sizeof(T)));
     return cudaSuccess;
 }
 
@@ -993,7 +1057,7 @@ cudaError_t StoreOps<W, T>::approx_topn(const uint64_t* keys, const T* coef, uin
     cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
     k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, nullptr, 2, 0ull, n, (unsigned long long)keep_n,
-                                                     okeys, ocoef, status, ctl);
+                                                     okeys, ocoef, status, ctl, SlotMap{nullptr, 0u});
     prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     cudaMemcpyAsync(host_count, &ctl->count[0], offsetof(Ctl, err_info) + sizeof(unsigned int),

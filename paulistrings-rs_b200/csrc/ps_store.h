@@ -75,7 +75,12 @@ struct StoreOps {
                             unsigned int* hist, bool hist_ready, uint64_t* cand, uint64_t cand_cap,
                             unsigned long long* status, Ctl* ctl, unsigned long long* host_count, uint64_t* out_n,
                             int sms, cudaStream_t st, KernelProf* prof, const uint64_t* sel = nullptr,
-                            bool window = false, uint64_t base = 0);
+                            bool window = false, uint64_t base = 0, SlotMap slots = SlotMap{nullptr, 0u});
+    // Compact the live rows of a slotted store of n rows (its span) into okeys / ocoef, in order;
+    // *out_n = rows kept.  Reads the counts and error words into host_count (synchronizes).
+    static cudaError_t densify(const uint64_t* keys, const T* coef, uint64_t n, SlotMap slots, uint64_t* okeys,
+                               T* ocoef, unsigned long long* status, Ctl* ctl, unsigned long long* host_count,
+                               uint64_t* out_n, cudaStream_t st, KernelProf* prof);
     // ApproxTopN (crates/paulistrings/src/truncation/builtin.rs:240-468): every octave of |c|^2
     // above the boundary octave kept, then the first quota boundary terms in key order.
     // hist: 2048 words, zero on entry and exit, holding the octave histogram when hist_ready;
