@@ -1057,6 +1057,7 @@ struct Engine {
         s->fault_stall = false;
         uint64_t span = 0;
         a.slot_count = slotted ? (unsigned int*)s->slot_count.p : nullptr;
+        a.sms = s->sms;
         a.span_out = &span;
         e = launch_rotation_layer<W, T>(a, s->stream);
         s->prof.resolve();

@@ -219,6 +219,7 @@ struct RotationArgs {
                               // and its row count to slot_count[t], with no look-back (slotted
                               // output, compacted by the TopN pass that follows); >= merge tiles
     uint64_t* span_out;       // slotted output: rows its slots span
+    int sms;                  // multiprocessors of the device (persistent grids)
 };
 
 // Rows of one merge tile's output slot, and the rows a slotted merge of at most `rows_in`

@@ -21,6 +21,7 @@
 //
 // Key-preserving tables (depolarizing noise, quarter turns with sin = 0) run
 // k_partition + k_merge with an empty partner stream.
+#include <algorithm>
 #include <cstddef>
 
 #include "ps_device.cuh"
@@ -349,90 +350,93 @@ __global__ void __launch_bounds__(kBlock) k_fwd_levels(const uint32_t* __restric
     __shared__ int s_wagg[kBlock / 32][2 * LV];
     __shared__ int s_prefix[2 * LV];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[1], 1u);
-    __syncthreads();
-    const unsigned int tile = s_tile;
     const uint32_t m = (uint32_t)ctl->count[0];  // partners, published by k_classify
-    if ((uint64_t)tile * kScanTile >= m) return;  // the grid is sized for every row partnering
-    const uint32_t j0 = tile * (uint32_t)kScanTile + (uint32_t)tid * kScanItems;
     const int NL = lv.n;
+    // persistent: tiles from the dispenser until none is left (the grid is sized by residency)
+    for (;;) {
+        if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[1], 1u);
+        __syncthreads();
+        const unsigned int tile = s_tile;
+        if ((uint64_t)tile * kScanTile >= m) break;
+        const uint32_t j0 = tile * (uint32_t)kScanTile + (uint32_t)tid * kScanItems;
 
-    uint16_t d[kScanItems];
+        uint16_t d[kScanItems];
 #pragma unroll
-    for (int i = 0; i < kScanItems; ++i) {
-        uint32_t j = j0 + i;
-        d[i] = j < m ? D[j] : (uint16_t)0;
-        if (j < m && j > 0) fix_divergence<W>(idx, D, keys, n, j, d[i], ctl);
-    }
-    // thread aggregates: last start / last split position per level
-    int agg[2 * LV];
-#pragma unroll
-    for (int l = 0; l < LV; ++l) {
-        agg[2 * l] = -1;
-        agg[2 * l + 1] = -1;
-        if (l < NL) {
-            uint32_t L = lv.rank[l];
-#pragma unroll
-            for (int i = 0; i < kScanItems; ++i) {
-                uint32_t j = j0 + i;
-                if (j >= m) break;
-                if (j == 0 || d[i] < L) agg[2 * l] = (int)j;
-                if (j != 0 && d[i] == L) agg[2 * l + 1] = (int)j;
-            }
+        for (int i = 0; i < kScanItems; ++i) {
+            uint32_t j = j0 + i;
+            d[i] = j < m ? D[j] : (uint16_t)0;
+            if (j < m && j > 0) fix_divergence<W>(idx, D, keys, n, j, d[i], ctl);
         }
-    }
-    // block exclusive max-scan of the aggregates
-    int excl[2 * LV];
-#pragma unroll
-    for (int v = 0; v < 2 * LV; ++v) {
-        int x = agg[v];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x = max(x, y);
-        }
-        int e = __shfl_up_sync(0xffffffffu, x, 1);
-        excl[v] = lane == 0 ? -1 : e;
-        if (lane == 31) s_wagg[warp][v] = x;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int v = 0; v < 2 * LV; ++v)
-        for (int w = 0; w < warp; ++w) excl[v] = max(excl[v], s_wagg[w][v]);
-    // tile aggregate, publish, look back
-    __syncthreads();
-    if (tid < 32) {
-        int tagg[2 * LV], pre[2 * LV];
-        for (int v = 0; v < 2 * LV; ++v) {
-            int t = -1;
-            for (int w = 0; w < kBlock / 32; ++w) t = max(t, s_wagg[w][v]);
-            tagg[v] = t;
-        }
-        level_lookback<true, LV>(slots, tile, tagg, pre, -1, ctl, 202);
-        if (tid == 0)
-            for (int v = 0; v < 2 * LV; ++v) s_prefix[v] = pre[v];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int v = 0; v < 2 * LV; ++v) excl[v] = max(excl[v], s_prefix[v]);
-
-    // per item: F = sum over levels of -(split - start) for rows in an upper half
-#pragma unroll
-    for (int i = 0; i < kScanItems; ++i) {
-        uint32_t j = j0 + i;
-        if (j >= m) break;
-        int f = 0;
+        // thread aggregates: last start / last split position per level
+        int agg[2 * LV];
 #pragma unroll
         for (int l = 0; l < LV; ++l) {
+            agg[2 * l] = -1;
+            agg[2 * l + 1] = -1;
             if (l < NL) {
                 uint32_t L = lv.rank[l];
-                if (j == 0 || d[i] < L) excl[2 * l] = (int)j;
-                if (j != 0 && d[i] == L) excl[2 * l + 1] = (int)j;
-                int s = excl[2 * l], p = excl[2 * l + 1];
-                if (p > s) f -= (p - s);
+#pragma unroll
+                for (int i = 0; i < kScanItems; ++i) {
+                    uint32_t j = j0 + i;
+                    if (j >= m) break;
+                    if (j == 0 || d[i] < L) agg[2 * l] = (int)j;
+                    if (j != 0 && d[i] == L) agg[2 * l + 1] = (int)j;
+                }
             }
         }
-        F[j] = accumulate ? F[j] + f : f;
+        // block exclusive max-scan of the aggregates
+        int excl[2 * LV];
+#pragma unroll
+        for (int v = 0; v < 2 * LV; ++v) {
+            int x = agg[v];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x = max(x, y);
+            }
+            int e = __shfl_up_sync(0xffffffffu, x, 1);
+            excl[v] = lane == 0 ? -1 : e;
+            if (lane == 31) s_wagg[warp][v] = x;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int v = 0; v < 2 * LV; ++v)
+            for (int w = 0; w < warp; ++w) excl[v] = max(excl[v], s_wagg[w][v]);
+        // tile aggregate, publish, look back
+        __syncthreads();
+        if (tid < 32) {
+            int tagg[2 * LV], pre[2 * LV];
+            for (int v = 0; v < 2 * LV; ++v) {
+                int t = -1;
+                for (int w = 0; w < kBlock / 32; ++w) t = max(t, s_wagg[w][v]);
+                tagg[v] = t;
+            }
+            level_lookback<true, LV>(slots, tile, tagg, pre, -1, ctl, 202);
+            if (tid == 0)
+                for (int v = 0; v < 2 * LV; ++v) s_prefix[v] = pre[v];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int v = 0; v < 2 * LV; ++v) excl[v] = max(excl[v], s_prefix[v]);
+
+        // per item: F = sum over levels of -(split - start) for rows in an upper half
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i) {
+            uint32_t j = j0 + i;
+            if (j >= m) break;
+            int f = 0;
+#pragma unroll
+            for (int l = 0; l < LV; ++l) {
+                if (l < NL) {
+                    uint32_t L = lv.rank[l];
+                    if (j == 0 || d[i] < L) excl[2 * l] = (int)j;
+                    if (j != 0 && d[i] == L) excl[2 * l + 1] = (int)j;
+                    int s = excl[2 * l], p = excl[2 * l + 1];
+                    if (p > s) f -= (p - s);
+                }
+            }
+            F[j] = accumulate ? F[j] + f : f;
+        }
     }
 }
 
@@ -452,108 +456,111 @@ __global__ void __launch_bounds__(kBlock) k_bwd_levels(const uint32_t* __restric
     __shared__ AmpTab<T> A;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int INF = 0x7fffffff;
-    if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[2], 1u);
     stage_amps<W, T>(L, A);
-    __syncthreads();
-    const unsigned int tile = s_tile;  // tile 0 covers the last kScanTile partners
     const uint32_t m = (uint32_t)ctl->count[0];  // partners, published by k_classify
-    if ((uint64_t)tile * kScanTile >= m) return;  // the grid is sized for every row partnering
-    const long long hi = (long long)m - (long long)tile * kScanTile;
-    const long long lo = hi - kScanTile;  // may be negative for the first partners
-    const long long jbase = lo + (long long)tid * kScanItems;
     const int NL = lv.n;
+    // persistent: tiles from the dispenser until none is left (the grid is sized by residency)
+    for (;;) {
+        if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[2], 1u);
+        __syncthreads();
+        const unsigned int tile = s_tile;  // tile 0 covers the last kScanTile partners
+        if ((uint64_t)tile * kScanTile >= m) break;
+        const long long hi = (long long)m - (long long)tile * kScanTile;
+        const long long lo = hi - kScanTile;  // may be negative for the first partners
+        const long long jbase = lo + (long long)tid * kScanItems;
 
-    uint16_t d[kScanItems];
+        uint16_t d[kScanItems];
 #pragma unroll
-    for (int i = 0; i < kScanItems; ++i) {
-        long long j = jbase + i;
-        d[i] = (j >= 0 && j < hi) ? D[j] : (uint16_t)0;
-    }
-    int agg[2 * LV];
-#pragma unroll
-    for (int l = 0; l < LV; ++l) {
-        agg[2 * l] = INF;
-        agg[2 * l + 1] = INF;
-        if (l < NL) {
-            uint32_t Lr = lv.rank[l];
-#pragma unroll
-            for (int i = kScanItems - 1; i >= 0; --i) {
-                long long j = jbase + i;
-                if (j < 0 || j >= hi) continue;
-                if (j != 0 && d[i] < Lr) agg[2 * l] = (int)j;
-                if (j != 0 && d[i] == Lr) agg[2 * l + 1] = (int)j;
-            }
+        for (int i = 0; i < kScanItems; ++i) {
+            long long j = jbase + i;
+            d[i] = (j >= 0 && j < hi) ? D[j] : (uint16_t)0;
         }
-    }
-    // exclusive suffix min over threads
-    int excl[2 * LV];
-#pragma unroll
-    for (int v = 0; v < 2 * LV; ++v) {
-        int x = agg[v];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_down_sync(0xffffffffu, x, o);
-            if (lane + o < 32) x = min(x, y);
-        }
-        int e = __shfl_down_sync(0xffffffffu, x, 1);
-        excl[v] = lane == 31 ? INF : e;
-        if (lane == 0) s_wagg[warp][v] = x;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int v = 0; v < 2 * LV; ++v)
-        for (int w = warp + 1; w < kBlock / 32; ++w) excl[v] = min(excl[v], s_wagg[w][v]);
-    __syncthreads();
-    if (tid < 32) {
-        int tagg[2 * LV], suf[2 * LV];
-        for (int v = 0; v < 2 * LV; ++v) {
-            int t = INF;
-            for (int w = 0; w < kBlock / 32; ++w) t = min(t, s_wagg[w][v]);
-            tagg[v] = t;
-        }
-        level_lookback<false, LV>(slots, tile, tagg, suf, INF, ctl, 203);
-        if (tid == 0)
-            for (int v = 0; v < 2 * LV; ++v) s_suffix[v] = suf[v];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int v = 0; v < 2 * LV; ++v) excl[v] = min(excl[v], s_suffix[v]);
-
-#pragma unroll
-    for (int i = kScanItems - 1; i >= 0; --i) {
-        long long j = jbase + i;
-        if (j < 0 || j >= hi) continue;
-        int b = 0;
+        int agg[2 * LV];
 #pragma unroll
         for (int l = 0; l < LV; ++l) {
+            agg[2 * l] = INF;
+            agg[2 * l + 1] = INF;
             if (l < NL) {
-                int e = excl[2 * l] == INF ? (int)m : excl[2 * l];
-                int q = excl[2 * l + 1];
-                if (q < e) b += e - q;
                 uint32_t Lr = lv.rank[l];
-                if (j != 0 && d[i] < Lr) excl[2 * l] = (int)j;
-                if (j != 0 && d[i] == Lr) excl[2 * l + 1] = (int)j;
+#pragma unroll
+                for (int i = kScanItems - 1; i >= 0; --i) {
+                    long long j = jbase + i;
+                    if (j < 0 || j >= hi) continue;
+                    if (j != 0 && d[i] < Lr) agg[2 * l] = (int)j;
+                    if (j != 0 && d[i] == Lr) agg[2 * l + 1] = (int)j;
+                }
             }
         }
-        int f = F[j] + b;
-        if (!scatter) {
-            F[j] = f;
-            continue;
-        }
-        long long dest = j + f;
-        uint32_t row = idx[j];
-        if (!PS_GUARD(ctl, dest >= 0 && dest < (long long)m && row < n, 204)) continue;
-        uint64_t k[2 * W];
-        load_key<W>(keys, row, k);
-        T c = coef[row];
-        T pc = partner_coeff<W, T>(L, A, k, c);
+        // exclusive suffix min over threads
+        int excl[2 * LV];
 #pragma unroll
-        for (int w = 0; w < W; ++w) {
-            k[w] ^= L.gx[w];
-            k[W + w] ^= L.gz[w];
+        for (int v = 0; v < 2 * LV; ++v) {
+            int x = agg[v];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_down_sync(0xffffffffu, x, o);
+                if (lane + o < 32) x = min(x, y);
+            }
+            int e = __shfl_down_sync(0xffffffffu, x, 1);
+            excl[v] = lane == 31 ? INF : e;
+            if (lane == 0) s_wagg[warp][v] = x;
         }
-        store_key<W>(Pk, (uint64_t)dest, k);
-        Pc[dest] = pc;
+        __syncthreads();
+#pragma unroll
+        for (int v = 0; v < 2 * LV; ++v)
+            for (int w = warp + 1; w < kBlock / 32; ++w) excl[v] = min(excl[v], s_wagg[w][v]);
+        __syncthreads();
+        if (tid < 32) {
+            int tagg[2 * LV], suf[2 * LV];
+            for (int v = 0; v < 2 * LV; ++v) {
+                int t = INF;
+                for (int w = 0; w < kBlock / 32; ++w) t = min(t, s_wagg[w][v]);
+                tagg[v] = t;
+            }
+            level_lookback<false, LV>(slots, tile, tagg, suf, INF, ctl, 203);
+            if (tid == 0)
+                for (int v = 0; v < 2 * LV; ++v) s_suffix[v] = suf[v];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int v = 0; v < 2 * LV; ++v) excl[v] = min(excl[v], s_suffix[v]);
+
+#pragma unroll
+        for (int i = kScanItems - 1; i >= 0; --i) {
+            long long j = jbase + i;
+            if (j < 0 || j >= hi) continue;
+            int b = 0;
+#pragma unroll
+            for (int l = 0; l < LV; ++l) {
+                if (l < NL) {
+                    int e = excl[2 * l] == INF ? (int)m : excl[2 * l];
+                    int q = excl[2 * l + 1];
+                    if (q < e) b += e - q;
+                    uint32_t Lr = lv.rank[l];
+                    if (j != 0 && d[i] < Lr) excl[2 * l] = (int)j;
+                    if (j != 0 && d[i] == Lr) excl[2 * l + 1] = (int)j;
+                }
+            }
+            int f = F[j] + b;
+            if (!scatter) {
+                F[j] = f;
+                continue;
+            }
+            long long dest = j + f;
+            uint32_t row = idx[j];
+            if (!PS_GUARD(ctl, dest >= 0 && dest < (long long)m && row < n, 204)) continue;
+            uint64_t k[2 * W];
+            load_key<W>(keys, row, k);
+            T c = coef[row];
+            T pc = partner_coeff<W, T>(L, A, k, c);
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+                k[w] ^= L.gx[w];
+                k[W + w] ^= L.gz[w];
+            }
+            store_key<W>(Pk, (uint64_t)dest, k);
+            Pc[dest] = pc;
+        }
     }
 }
 
@@ -571,36 +578,48 @@ template <int W>
 __global__ void k_partition(const uint64_t* __restrict__ Sk, uint64_t n, const uint64_t* __restrict__ Pk,
                             uint32_t tile_items, ulonglong2* __restrict__ bounds, const Ctl* ctl) {
     const int lane = threadIdx.x & 31;
-    const uint32_t t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const uint64_t m = ctl->count[0];  // partners, published by k_classify (0 without partners)
     const uint32_t num_tiles = (uint32_t)((n + m + tile_items - 1) / tile_items);
-    if (t > num_tiles) return;
-    uint64_t dd = (uint64_t)t * tile_items;
-    if (dd > n + m) dd = n + m;
-    uint64_t lo = dd > m ? dd - m : 0, hi = dd < n ? dd : n;  // answer in [lo, hi]
-    while (hi - lo > 32) {
-        uint64_t span = hi - lo;
-        uint64_t p = lo + (span * (uint64_t)lane) / 32;  // p_0 = lo, all < hi
-        bool f = mp_pred<W>(Sk, Pk, p, dd);
-        unsigned int b = __ballot_sync(0xffffffffu, f);
-        int c = __popc(b);
-        if (c == 0) {
-            hi = lo;
-            break;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    // Each warp takes a run of consecutive boundaries (the grid is sized by residency).  The
+    // split moves by at most tile_items from one boundary to the next, so after the first of
+    // the run the search starts in a window of that width, on keys the last search touched.
+    const uint32_t per = (num_tiles + 1 + warps - 1) / warps;
+    const uint32_t t0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * per;
+    uint64_t prev_i = 0;
+    for (uint32_t t = t0; t <= num_tiles && t < t0 + per; ++t) {
+        uint64_t dd = (uint64_t)t * tile_items;
+        if (dd > n + m) dd = n + m;
+        uint64_t lo = dd > m ? dd - m : 0, hi = dd < n ? dd : n;  // answer in [lo, hi]
+        if (t > t0) {
+            lo = lo > prev_i ? lo : prev_i;
+            hi = hi < prev_i + tile_items ? hi : prev_i + tile_items;
         }
-        uint64_t pc1 = lo + (span * (uint64_t)(c - 1)) / 32;
-        uint64_t pc = c < 32 ? lo + (span * (uint64_t)c) / 32 : hi;
-        lo = pc1 + 1;
-        hi = pc;
-    }
-    uint64_t span = hi - lo;
-    bool f = (uint64_t)lane < span ? mp_pred<W>(Sk, Pk, lo + lane, dd) : false;
-    unsigned int b = __ballot_sync(0xffffffffu, f);
-    uint64_t i = lo + (uint64_t)__popc(b);
-    uint64_t j = dd - i;
-    if (lane == 0) {
-        if (i > 0 && j < m && key_eq<W>(Sk + (i - 1) * 2 * W, Pk + j * 2 * W)) ++j;
-        bounds[t] = make_ulonglong2(i, j);
+        while (hi - lo > 32) {
+            uint64_t span = hi - lo;
+            uint64_t p = lo + (span * (uint64_t)lane) / 32;  // p_0 = lo, all < hi
+            bool f = mp_pred<W>(Sk, Pk, p, dd);
+            unsigned int b = __ballot_sync(0xffffffffu, f);
+            int c = __popc(b);
+            if (c == 0) {
+                hi = lo;
+                break;
+            }
+            uint64_t pc1 = lo + (span * (uint64_t)(c - 1)) / 32;
+            uint64_t pc = c < 32 ? lo + (span * (uint64_t)c) / 32 : hi;
+            lo = pc1 + 1;
+            hi = pc;
+        }
+        uint64_t span = hi - lo;
+        bool f = (uint64_t)lane < span ? mp_pred<W>(Sk, Pk, lo + lane, dd) : false;
+        unsigned int b = __ballot_sync(0xffffffffu, f);
+        uint64_t i = lo + (uint64_t)__popc(b);
+        uint64_t j = dd - i;
+        prev_i = i;
+        if (lane == 0) {
+            if (i > 0 && j < m && key_eq<W>(Sk + (i - 1) * 2 * W, Pk + j * 2 * W)) ++j;
+            bounds[t] = make_ulonglong2(i, j);
+        }
     }
 }
 
@@ -709,137 +728,140 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
     __shared__ AmpTab<T> A;
 
     const int tid = threadIdx.x;
-    if (tid == 0) {
-        s_tile = atomicAdd(&ctl->tile_counter[3], 1u);
-        mbar_init(&bar, 1);
-    }
+    if (tid == 0) mbar_init(&bar, 1);
     if (topn_hist)
         for (int q = tid; q < kTopnHistBins; q += kBlock) s_hist[q] = 0;
     stage_amps<W, T>(L, A);
-    __syncthreads();
-    const unsigned int tile = s_tile;
     const uint64_t m = ctl->count[0];  // partners, published by k_classify (0 without partners)
     const uint32_t num_tiles = (uint32_t)((n + m + SM::TILE - 1) / SM::TILE);
-    if (tile >= num_tiles) return;  // the grid is sized for every row partnering
-    const ulonglong2 b0 = bounds[tile], b1 = bounds[tile + 1];
-    if (!PS_GUARD(ctl, b1.x >= b0.x && b1.y >= b0.y && b1.x - b0.x + b1.y - b0.y <= (uint64_t)SM::TILE + 2 &&
-                           b1.x <= n && b1.y <= m,
-                  301)) {
-        return;
-    }
-    const uint32_t cs = (uint32_t)(b1.x - b0.x), cp = (uint32_t)(b1.y - b0.y);
-    // stage the two input runs: keys packed (S then P), coefficients from 16-byte aligned windows
-    const uint64_t sa = b0.x & ~(uint64_t)(SM::PAD - 1), pa = b0.y & ~(uint64_t)(SM::PAD - 1);
-    const uint32_t s_off = (uint32_t)(b0.x - sa), p_off = (uint32_t)(b0.y - pa);
-    const uint32_t sc_slots = (s_off + cs + SM::PAD - 1) / SM::PAD * SM::PAD;
-    T* sSc = sC;             // S coefficient of local i at sSc[s_off + i]
-    T* sPc = sC + sc_slots;  // P coefficient of local j at sPc[p_off + j]
-    uint64_t* sSk = sK;
-    uint64_t* sPk = sK + (size_t)cs * 2 * W;
-    if (tid == 0) {
-        uint32_t kbS = cs * 16u * W, kbP = cp * 16u * W;
-        uint32_t cbS = cs ? round16((s_off + cs) * (uint32_t)sizeof(T)) : 0u;
-        uint32_t cbP = cp ? round16((p_off + cp) * (uint32_t)sizeof(T)) : 0u;
-        uint32_t tot = kbS + kbP + cbS + cbP;
-        if (tot) {
-            mbar_arrive_expect_tx(&bar, tot);
+    uint32_t phase = 0;  // completed phases of `bar`
+    // Persistent: each block takes tiles from the dispenser until none is left (the grid is
+    // sized by residency, not by the tile count, which only the device knows).
+    for (;;) {
+        if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[3], 1u);
+        __syncthreads();  // also: every thread is done with the previous tile's shared memory
+        const unsigned int tile = s_tile;
+        if (tile >= num_tiles) break;
+        const ulonglong2 b0 = bounds[tile], b1 = bounds[tile + 1];
+        if (!PS_GUARD(ctl, b1.x >= b0.x && b1.y >= b0.y && b1.x - b0.x + b1.y - b0.y <= (uint64_t)SM::TILE + 2 &&
+                               b1.x <= n && b1.y <= m,
+                      301))
+            break;
+        const uint32_t cs = (uint32_t)(b1.x - b0.x), cp = (uint32_t)(b1.y - b0.y);
+        // stage the two input runs: keys packed (S then P), coefficients from 16-byte aligned windows
+        const uint64_t sa = b0.x & ~(uint64_t)(SM::PAD - 1), pa = b0.y & ~(uint64_t)(SM::PAD - 1);
+        const uint32_t s_off = (uint32_t)(b0.x - sa), p_off = (uint32_t)(b0.y - pa);
+        const uint32_t sc_slots = (s_off + cs + SM::PAD - 1) / SM::PAD * SM::PAD;
+        T* sSc = sC;             // S coefficient of local i at sSc[s_off + i]
+        T* sPc = sC + sc_slots;  // P coefficient of local j at sPc[p_off + j]
+        uint64_t* sSk = sK;
+        uint64_t* sPk = sK + (size_t)cs * 2 * W;
+        if (tid == 0 && cs + cp) {
+            bulk_wait_read_all();  // the previous tile's bulk store has read the staged rows
+            uint32_t kbS = cs * 16u * W, kbP = cp * 16u * W;
+            uint32_t cbS = cs ? round16((s_off + cs) * (uint32_t)sizeof(T)) : 0u;
+            uint32_t cbP = cp ? round16((p_off + cp) * (uint32_t)sizeof(T)) : 0u;
+            mbar_arrive_expect_tx(&bar, kbS + kbP + cbS + cbP);
             if (kbS) bulk_g2s(sSk, Sk + b0.x * 2 * W, kbS, &bar);
             if (kbP) bulk_g2s(sPk, Pk + b0.y * 2 * W, kbP, &bar);
             if (cbS) bulk_g2s(sSc, Sc + sa, cbS, &bar);
             if (cbP) bulk_g2s(sPc, Pc + pa, cbP, &bar);
         }
-    }
-    if (cs + cp) mbar_wait(&bar, 0, ctl, 302);
-    const T* Sc_l = sSc + s_off;
-    const T* Pc_l = sPc + p_off;
+        if (cs + cp) {
+            mbar_wait(&bar, phase & 1u, ctl, 302);
+            ++phase;
+        }
+        const T* Sc_l = sSc + s_off;
+        const T* Pc_l = sPc + p_off;
 
-    // per-thread merge-path start, equal pairs kept together
-    {
-        uint32_t dd = min((uint32_t)tid * ITEMS, cs + cp);
-        uint32_t lo = dd > cp ? dd - cp : 0, hi = min(dd, cs);
-        while (lo < hi) {
-            uint32_t mid = (lo + hi) >> 1;
-            if (key_le<W>(sSk + (size_t)mid * 2 * W, sPk + (size_t)(dd - 1 - mid) * 2 * W))
-                lo = mid + 1;
-            else
-                hi = mid;
-        }
-        uint32_t i = lo, j = dd - lo;
-        if (i > 0 && j < cp && key_eq<W>(sSk + (size_t)(i - 1) * 2 * W, sPk + (size_t)j * 2 * W)) ++j;
-        s_si[tid] = i;
-        s_sj[tid] = j;
-        if (tid == 0) {
-            s_si[kBlock] = cs;
-            s_sj[kBlock] = cp;
-        }
-    }
-    __syncthreads();
-    const uint32_t i0 = s_si[tid], j0 = s_sj[tid];
-    const uint32_t ie = max(s_si[tid + 1], i0), je = max(s_sj[tid + 1], j0);
-    constexpr int STEPS = ITEMS + 1;
-    uint64_t ok[STEPS][2 * W];
-    T ov[STEPS];
-    uint32_t i = i0, j = j0;
-    const uint32_t mask = merge_walk<W, T, STEPS>(sSk, Sc_l, sPk, Pc_l, i, ie, j, je, L, A, keep, ok, ov);
-    PS_GUARD(ctl, i >= ie && j >= je, 305);
-    unsigned int total;
-    const unsigned int excl = block_exclusive_sum<kBlock>(__popc(mask), s_warp, total);
-    // Every thread is past the walk, so the staged inputs are dead: stage the kept outputs over
-    // them in output order (keys from sK, coefficients from sC) while warp 0 looks back.
-    {
-        uint32_t r = excl;
-#pragma unroll
-        for (int s = 0; s < STEPS; ++s) {
-            if ((mask >> s) & 1u) {
-                store_key<W>(sK, r, ok[s]);
-                sC[r] = ov[s];
-                ++r;
+        // per-thread merge-path start, equal pairs kept together
+        {
+            uint32_t dd = min((uint32_t)tid * ITEMS, cs + cp);
+            uint32_t lo = dd > cp ? dd - cp : 0, hi = min(dd, cs);
+            while (lo < hi) {
+                uint32_t mid = (lo + hi) >> 1;
+                if (key_le<W>(sSk + (size_t)mid * 2 * W, sPk + (size_t)(dd - 1 - mid) * 2 * W))
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            uint32_t i = lo, j = dd - lo;
+            if (i > 0 && j < cp && key_eq<W>(sSk + (size_t)(i - 1) * 2 * W, sPk + (size_t)j * 2 * W)) ++j;
+            s_si[tid] = i;
+            s_sj[tid] = j;
+            if (tid == 0) {
+                s_si[kBlock] = cs;
+                s_sj[kBlock] = cp;
             }
         }
-    }
-    fence_proxy_async_shared();  // the bulk store below reads the staged keys through the async proxy
-    if (slot_count) {
-        // slotted output: the tile's slot is fixed, so it waits for no predecessor
-        if (tid == 0) {
-            s_outoff = (unsigned long long)tile * (SM::TILE + 2);
-            slot_count[tile] = total;
-            atomicAdd(&ctl->count[1], (unsigned long long)total);
+        __syncthreads();
+        const uint32_t i0 = s_si[tid], j0 = s_sj[tid];
+        const uint32_t ie = max(s_si[tid + 1], i0), je = max(s_sj[tid + 1], j0);
+        constexpr int STEPS = ITEMS + 1;
+        uint64_t ok[STEPS][2 * W];
+        T ov[STEPS];
+        uint32_t i = i0, j = j0;
+        const uint32_t mask = merge_walk<W, T, STEPS>(sSk, Sc_l, sPk, Pc_l, i, ie, j, je, L, A, keep, ok, ov);
+        PS_GUARD(ctl, i >= ie && j >= je, 305);
+        unsigned int total;
+        const unsigned int excl = block_exclusive_sum<kBlock>(__popc(mask), s_warp, total);
+        // Every thread is past the walk, so the staged inputs are dead: stage the kept outputs
+        // over them in output order (keys from sK, coefficients from sC) while warp 0 looks back.
+        {
+            uint32_t r = excl;
+#pragma unroll
+            for (int s = 0; s < STEPS; ++s) {
+                if ((mask >> s) & 1u) {
+                    store_key<W>(sK, r, ok[s]);
+                    sC[r] = ov[s];
+                    ++r;
+                }
+            }
         }
-    } else if (tid < 32) {
-        unsigned long long p = 0;
-        if (tile == 0) {
-            if (tid == 0) st_release_u64(status + tile, kFlagInc | (unsigned long long)total);
-        } else {
-            if (tid == 0) st_release_u64(status + tile, kFlagAgg | (unsigned long long)total);
-            p = lookback_sum_warp(status, tile, ctl, 303);
-            if (tid == 0) st_release_u64(status + tile, kFlagInc | (p + total));
+        fence_proxy_async_shared();  // the bulk store below reads the staged keys through the async proxy
+        if (slot_count) {
+            // slotted output: the tile's slot is fixed, so it waits for no predecessor
+            if (tid == 0) {
+                s_outoff = (unsigned long long)tile * (SM::TILE + 2);
+                slot_count[tile] = total;
+                atomicAdd(&ctl->count[1], (unsigned long long)total);
+            }
+        } else if (tid < 32) {
+            unsigned long long p = 0;
+            if (tile == 0) {
+                if (tid == 0) st_release_u64(status + tile, kFlagInc | (unsigned long long)total);
+            } else {
+                if (tid == 0) st_release_u64(status + tile, kFlagAgg | (unsigned long long)total);
+                p = lookback_sum_warp(status, tile, ctl, 303);
+                if (tid == 0) st_release_u64(status + tile, kFlagInc | (p + total));
+            }
+            if (tid == 0) {
+                s_outoff = p;
+                if (tile == num_tiles - 1) ctl->count[1] = p + total;
+            }
         }
-        if (tid == 0) {
-            s_outoff = p;
-            if (tile == num_tiles - 1) ctl->count[1] = p + total;
+        __syncthreads();
+        const unsigned long long off = s_outoff;
+        if (!PS_GUARD(ctl, off + total <= out_cap, 304)) break;
+        // keys: one bulk copy of the staged rows (16W bytes each, so both ends are 16-byte aligned)
+        if (tid == 0 && total) {
+            bulk_s2g(Ok + off * 2 * W, sK, total * 16u * W);
+            bulk_commit();
         }
-    }
-    __syncthreads();
-    const unsigned long long off = s_outoff;
-    if (!PS_GUARD(ctl, off + total <= out_cap, 304)) return;
-    // keys: one bulk copy of the staged rows (16W bytes each, so both ends are 16-byte aligned)
-    if (tid == 0 && total) {
-        bulk_s2g(Ok + off * 2 * W, sK, total * 16u * W);
-        bulk_commit();
-    }
-    // coefficients: coalesced stores, with the fused first TopN digit
-    for (uint32_t q = tid; q < total; q += kBlock) {
-        const T v = sC[q];
-        Oc[off + q] = v;
-        if (topn_hist) {
-            uint32_t bin;
-            if (hist_mode == 1)
-                bin = octave_bin<T>(v);
-            else if (hist_mode == 2)
-                bin = (uint32_t)(window_key(mag_key<T>(v), hist_base) >> 48);
-            else
-                bin = (uint32_t)(mag_key<T>(v) >> 52);
-            atomicAdd(&s_hist[bin], 1u);
+        // coefficients: coalesced stores, with the fused first TopN digit
+        for (uint32_t q = tid; q < total; q += kBlock) {
+            const T v = sC[q];
+            Oc[off + q] = v;
+            if (topn_hist) {
+                uint32_t bin;
+                if (hist_mode == 1)
+                    bin = octave_bin<T>(v);
+                else if (hist_mode == 2)
+                    bin = (uint32_t)(window_key(mag_key<T>(v), hist_base) >> 48);
+                else
+                    bin = (uint32_t)(mag_key<T>(v) >> 52);
+                atomicAdd(&s_hist[bin], 1u);
+            }
         }
     }
     if (topn_hist) {
@@ -847,7 +869,7 @@ __global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ S
         for (int q = tid; q < kTopnHistBins; q += kBlock)
             if (s_hist[q]) atomicAdd(&topn_hist[q], s_hist[q]);
     }
-    if (tid == 0 && total) bulk_wait_read_all();  // shared memory stays valid until the copy has read it
+    if (tid == 0) bulk_wait_read_all();  // shared memory stays valid until the last copy has read it
 }
 
 // ---------------------------------------------------------------------------
@@ -877,7 +899,16 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         // 2-3. level scans (batches of kMaxLevels; one batch of four covers every gate on at
         // most two qubits), scatter on the last batch
-        uint32_t stiles = (uint32_t)((m_hi + kScanTile - 1) / kScanTile);
+        const uint32_t stiles = (uint32_t)((m_hi + kScanTile - 1) / kScanTile);
+        static int fwd_per_sm[2] = {0, 0}, bwd_per_sm[2] = {0, 0};  // resident blocks per SM
+        auto resident = [&](auto kernel, int& cache) {
+            if (cache == 0) {
+                int v = 0;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, kBlock, 0) != cudaSuccess || v < 1) v = 1;
+                cache = v;
+            }
+            return (uint32_t)std::min<uint64_t>(stiles, (uint64_t)cache * (a.sms > 0 ? a.sms : 1));
+        };
         const bool narrow = a.levels->n <= 4;
         const int per = narrow ? 4 : kMaxLevels;
         int nb = (a.levels->n + per - 1) / per;
@@ -889,11 +920,11 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
             cudaMemsetAsync(&ctl->tile_counter[1], 0, sizeof(unsigned int), st);
             a.prof->begin(K_FWD_LEVELS, 0.0, st);
             if (narrow)
-                k_fwd_levels<W, 4><<<stiles, kBlock, 0, st>>>(a.idx, a.D, a.F, a.Sk, a.n, lv, b > 0,
-                                                            reinterpret_cast<LevelSlot*>(a.slots), ctl);
+                k_fwd_levels<W, 4><<<resident(k_fwd_levels<W, 4>, fwd_per_sm[0]), kBlock, 0, st>>>(
+                    a.idx, a.D, a.F, a.Sk, a.n, lv, b > 0, reinterpret_cast<LevelSlot*>(a.slots), ctl);
             else
-                k_fwd_levels<W, kMaxLevels><<<stiles, kBlock, 0, st>>>(a.idx, a.D, a.F, a.Sk, a.n, lv, b > 0,
-                                                                     reinterpret_cast<LevelSlot*>(a.slots), ctl);
+                k_fwd_levels<W, kMaxLevels><<<resident(k_fwd_levels<W, kMaxLevels>, fwd_per_sm[1]), kBlock, 0, st>>>(
+                    a.idx, a.D, a.F, a.Sk, a.n, lv, b > 0, reinterpret_cast<LevelSlot*>(a.slots), ctl);
             a.prof->end(st);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
             cudaMemsetAsync(a.slots, 0, (size_t)stiles * sizeof(LevelSlot), st);
@@ -901,13 +932,13 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
             const bool last = b == nb - 1;
             a.prof->begin(K_BWD_LEVELS, 0.0, st);
             if (narrow)
-                k_bwd_levels<W, T, 4><<<stiles, kBlock, 0, st>>>(a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, last,
-                                                               a.Pk, a.Pc, reinterpret_cast<LevelSlot*>(a.slots),
-                                                               ctl);
-            else
-                k_bwd_levels<W, T, kMaxLevels><<<stiles, kBlock, 0, st>>>(
+                k_bwd_levels<W, T, 4><<<resident(k_bwd_levels<W, T, 4>, bwd_per_sm[0]), kBlock, 0, st>>>(
                     a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, last, a.Pk, a.Pc,
                     reinterpret_cast<LevelSlot*>(a.slots), ctl);
+            else
+                k_bwd_levels<W, T, kMaxLevels><<<resident(k_bwd_levels<W, T, kMaxLevels>, bwd_per_sm[1]), kBlock, 0,
+                                                 st>>>(a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, last, a.Pk, a.Pc,
+                                                       reinterpret_cast<LevelSlot*>(a.slots), ctl);
             a.prof->end(st);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
@@ -923,7 +954,7 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     if ((a.slot_count ? (uint64_t)mtiles_hi * (MT + 2) : total_hi) > a.out_cap) return cudaErrorMemoryAllocation;
     {
         uint32_t warps = mtiles_hi + 1;
-        uint32_t blocks = (warps + 7) / 8;
+        uint32_t blocks = std::min<uint32_t>((warps + 7) / 8, 8u * (uint32_t)(a.sms > 0 ? a.sms : 1));
         a.prof->begin(K_PARTITION, 0.0, st);
         k_partition<W><<<blocks, 256, 0, st>>>(a.Sk, a.n, a.Pk, (uint32_t)MT, a.bounds, ctl);
         a.prof->end(st);
@@ -936,8 +967,15 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     cudaMemsetAsync(&ctl->tile_counter[3], a.inject_stall ? 1 : 0, 1, st);
     cudaMemsetAsync(reinterpret_cast<unsigned char*>(&ctl->tile_counter[3]) + 1, 0, 3, st);
     size_t smem = MergeSmem<W, T>::bytes;
+    static int merge_per_sm = 0;  // resident merge blocks per SM (the same on every B200)
+    if (merge_per_sm == 0) {
+        int v = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_merge<W, T>, kBlock, smem) != cudaSuccess || v < 1) v = 1;
+        merge_per_sm = v;
+    }
+    const uint32_t mgrid = (uint32_t)std::min<uint64_t>(mtiles_hi, (uint64_t)merge_per_sm * (a.sms > 0 ? a.sms : 1));
     a.prof->begin(K_MERGE, 0.0, st);
-    k_merge<W, T><<<mtiles_hi, kBlock, smem, st>>>(a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc,
+    k_merge<W, T><<<mgrid, kBlock, smem, st>>>(a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc,
                                                   a.out_cap, a.status, ctl, a.topn_hist, a.topn_hist_mode,
                                                   a.topn_hist_base, a.slot_count);
     a.prof->end(st);
