@@ -1016,7 +1016,7 @@ struct Engine {
             if ((e = ensure(s, s->pk, n * kKeyBytes)) != cudaSuccess || (e = ensure(s, s->pc, n * sizeof(T))) != cudaSuccess ||
                 (e = ensure(s, s->idx, n * 4)) != cudaSuccess || (e = ensure(s, s->dv, n * 2)) != cudaSuccess ||
                 (e = ensure(s, s->fv, n * 4)) != cudaSuccess ||
-                (e = ensure(s, s->slots, (n / kScanTileRows + 4) * sizeof(LevelSlot))) != cudaSuccess)
+                (e = ensure(s, s->slots, (n / kScanTileRows + 4) * sizeof(LevelTile))) != cudaSuccess)
                 return cuda_fail(s, e, "apply: partner scratch");
         }
         a.Sk = K(s, s->cur);
@@ -1654,7 +1654,7 @@ ps_status ps_set_profiling(ps_sum* s, int32_t enabled) {
 
 ps_status ps_read_profile(ps_sum* s, ps_kernel_profile* out, int32_t cap, int32_t* count) {
     if (!s || !count || (cap > 0 && !out)) return PS_ERR_INVALID;
-    static const char* kNames[K_NUM_KERNELS] = {"k_classify",     "k_fwd_levels", "k_bwd_levels", "k_partition",
+    static const char* kNames[K_NUM_KERNELS] = {"k_classify",     "k_level_scan", "k_level_apply", "k_partition",
                                                 "k_merge",        "k_topn_hist",  "k_topn_step",  "k_topn_compact",
                                                 "k_pack",         "k_sort_hist",  "k_sort_pass",  "k_dedup",
                                                 "k_unpack",       "k_expect",     "k_gen_count",  "k_gen_branch",

@@ -97,8 +97,8 @@ struct GenLayer {
 // Kernel ids of the per-kernel profile.
 enum KernelId : int {
     K_CLASSIFY = 0,
-    K_FWD_LEVELS,
-    K_BWD_LEVELS,
+    K_LEVEL_SCAN,   // k_level_reduce + k_level_scan
+    K_LEVEL_APPLY,  // k_level_apply (places the partners)
     K_PARTITION,
     K_MERGE,
     K_TOPN_HIST,
@@ -162,6 +162,8 @@ struct KernelProf {
         }
         npend = 0;
     }
+    // launches timed together with the one begin() opened (a group of kernels under one id)
+    void more_launches(int id, unsigned k) { launches[id] += k; }
     void add_bytes(int id, double b) {
         if (events) bytes[id] += b;
     }
@@ -195,7 +197,7 @@ struct RotationArgs {
     uint32_t* idx;               // scratch, >= n
     uint16_t* D;                 // scratch, >= n
     int32_t* F;                  // scratch, >= n
-    void* slots;                 // level look-back slots, >= scan tiles
+    void* slots;                 // level-scan tile values (LevelTile), >= scan tiles
     unsigned long long* status;  // look-back words, >= classify / merge tiles
     ulonglong2* bounds;          // merge-path bounds, >= merge tiles + 1
     uint64_t* Pk;                // partner keys (sorted), capacity p_cap
@@ -247,11 +249,11 @@ struct GeneralOps {
     static size_t branch_tile();
 };
 
-// One scan tile's look-back slot: flag 1 = agg valid, 2 = inc (prefix combined with agg) valid.
-struct LevelSlot {
-    unsigned int flag;
-    int agg[2 * kMaxLevels];
-    int inc[2 * kMaxLevels];
+// One level-scan tile's values for both scans of a batch of levels: its aggregates and the
+// combined aggregates of the tiles before it (forward scan) and after it (backward scan).
+struct LevelTile {
+    int agg[4 * kMaxLevels];
+    int pre[4 * kMaxLevels];
 };
 
 // Rows of the smallest tile of any look-back kernel (bounds every tile count).

@@ -8,16 +8,20 @@
 // keys first differ on a bit of g (crates/paulistrings/src/engine/bucketed/
 // partner_order.rs:10-14).  So the layer is:
 //
-//   k_classify   stream the store keys (TMA bulk copies into shared memory),
-//                list anticommuting rows with a decoupled look-back count and
-//                record each one's divergence rank from its predecessor;
-//   k_fwd_levels forward max-scan per bit of g: the upper half of each group
-//                moves down by the lower half's size;
-//   k_bwd_levels backward min-scan per bit of g: the lower half moves up by
-//                the upper half's size; writes each partner at its sorted slot;
-//   k_partition  merge-path split points (one warp per tile, 32-way search);
-//   k_merge      merge own rows and partners, sum equal keys, drop exact zeros
-//                and keep-program rejects, compact with a look-back.
+//   k_classify   stream the store keys (warp-striped coalesced loads), list
+//                anticommuting rows with a decoupled look-back count and record
+//                each one's divergence rank from its predecessor;
+//   forward level scan (k_level_reduce, k_level_scan, k_fwd_apply): max-scan
+//                per bit of g, the upper half of each group moves down by the
+//                lower half's size;
+//   backward level scan (k_level_reduce, k_level_scan, k_bwd_apply): min-scan
+//                per bit of g, the lower half moves up by the upper half's size;
+//                writes each partner at its sorted slot;
+//   k_partition  merge-path split points (a warp per run of tiles, 32-way search);
+//   k_merge      merge own rows and partners (TMA bulk copies into shared
+//                memory), sum equal keys, drop exact zeros and keep-program
+//                rejects, and write the tile at its look-back offset or, before
+//                a TopN pass, at its fixed slot.
 //
 // Key-preserving tables (depolarizing noise, quarter turns with sin = 0) run
 // k_partition + k_merge with an empty partner stream.
@@ -41,6 +45,7 @@ struct RotTile {
     static constexpr int kMergeTile = kBlock * kMergeItems;
 };
 constexpr int kScanItems = 16;
+constexpr int kLevelInf = 0x7fffffff;  // identity of the backward level scan
 constexpr int kScanTile = kBlock * kScanItems;
 static_assert(kScanTile == (int)kScanTileRows, "scan tile");
 
@@ -157,7 +162,7 @@ __device__ __forceinline__ T partner_coeff(const RotLayer<W>& L, const AmpTab<T>
 // k_classify: warp-striped (lane l of warp w reads row base_w + 32 i + l, coalesced 16W-byte
 // loads), anticommuting rows compacted by ballot in row order; each listed row records its
 // divergence rank from the previous listed row (shuffled from the lane that holds it).  The
-// first listed row of each warp takes kDivUnknown and k_fwd_levels resolves it.
+// first listed row of each warp takes kDivUnknown and the forward k_level_reduce resolves it.
 // ---------------------------------------------------------------------------
 template <int W, typename T>
 __global__ void __launch_bounds__(kBlock) k_classify(const uint64_t* __restrict__ keys, uint64_t n,
@@ -265,67 +270,13 @@ __global__ void __launch_bounds__(kBlock) k_classify(const uint64_t* __restrict_
 // every key bit more significant than L, and its "split" is the first row whose
 // bit L is set.  Starts: j == 0 or D[j] < L.  Splits: D[j] == L.
 // ---------------------------------------------------------------------------
-// Look-back over the tiles before `tile` in scan order for the forward (max) or backward
-// (min) level scans, by one full warp: each poll reads 32 predecessors' slots, combines their
-// aggregates up to the nearest inclusive value, and moves back only when none of the 32 has
-// one.  Publishes this tile's aggregate first and its inclusive value after.
-template <bool kMax, int LV>
-__device__ __forceinline__ void level_lookback(LevelSlot* slots, unsigned int tile, const int (&tile_agg)[2 * LV],
-                                               int (&prefix)[2 * LV], int identity, Ctl* ctl, uint32_t info) {
-    const int lane = threadIdx.x & 31;
-    auto comb = [](int a, int b) { return kMax ? max(a, b) : min(a, b); };
-#pragma unroll
-    for (int v = 0; v < 2 * LV; ++v) prefix[v] = identity;
-    if (tile == 0) {
-        if (lane == 0) {
-            for (int v = 0; v < 2 * LV; ++v) slots[0].inc[v] = tile_agg[v];
-            __threadfence();
-            st_release_u32(&slots[0].flag, 2u);
-        }
-        __syncwarp();
-        return;
-    }
-    if (lane == 0) {
-        for (int v = 0; v < 2 * LV; ++v) slots[tile].agg[v] = tile_agg[v];
-        __threadfence();
-        st_release_u32(&slots[tile].flag, 1u);
-    }
-    long long base = (long long)tile - 1;
-    long long spins = 0;
-    while (base >= 0) {
-        const long long t = base - lane;
-        const unsigned int f = t >= 0 ? ld_acquire_u32(&slots[t].flag) : 2u;
-        const unsigned int empty = __ballot_sync(0xffffffffu, f == 0u);
-        const unsigned int inc = __ballot_sync(0xffffffffu, f == 2u);
-        const int first_inc = inc ? __ffs(inc) - 1 : 32;
-        const unsigned int need = first_inc >= 31 ? 0xffffffffu : ((2u << first_inc) - 1u);
-        if (empty & need) {
-            if (++spins > spin_limit(ctl)) {
-                if (lane == 0) raise_err(ctl, ERR_TIMEOUT, info);
-                break;
-            }
-            __nanosleep(20);
-            continue;
-        }
-        const bool use = lane <= first_inc && t >= 0;
-        const int* src = f == 2u ? slots[t >= 0 ? t : 0].inc : slots[t >= 0 ? t : 0].agg;
-#pragma unroll
-        for (int v = 0; v < 2 * LV; ++v) {
-            int x = use ? __ldcg(src + v) : identity;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) x = comb(x, __shfl_xor_sync(0xffffffffu, x, o));
-            prefix[v] = comb(prefix[v], x);
-        }
-        if (first_inc < 32) break;
-        base -= 32;
-    }
-    if (lane == 0) {
-        for (int v = 0; v < 2 * LV; ++v) slots[tile].inc[v] = comb(prefix[v], tile_agg[v]);
-        __threadfence();
-        st_release_u32(&slots[tile].flag, 2u);
-    }
-    __syncwarp();
-}
+// The level scans run in three phases with no look-back: k_level_reduce writes each tile's
+// aggregates for both directions, k_level_scan (one block) combines them into each tile's
+// exclusive prefix (forward, max) and suffix (backward, min), and k_level_apply finishes both
+// scans per partner and, on the last batch of levels, places it.  With every tile of a scan in
+// flight at once, a decoupled look-back would walk back hundreds of tiles.  Per-tile values
+// (LevelTile: forward values at [0, 2LV), backward at [2LV, 4LV)) live in the caller's level
+// slot buffer.
 
 template <int W>
 __device__ __forceinline__ void fix_divergence(const uint32_t* __restrict__ idx, uint16_t* __restrict__ D,
@@ -341,218 +292,248 @@ __device__ __forceinline__ void fix_divergence(const uint32_t* __restrict__ idx,
     D[j] = d;
 }
 
-template <int W, int LV>
-__global__ void __launch_bounds__(kBlock) k_fwd_levels(const uint32_t* __restrict__ idx, uint16_t* __restrict__ D,
-                                                       int32_t* __restrict__ F, const uint64_t* __restrict__ keys,
-                                                       uint64_t n, const Levels lv, int accumulate, LevelSlot* slots,
-                                                       Ctl* ctl) {
-    __shared__ unsigned int s_tile;
-    __shared__ int s_wagg[kBlock / 32][2 * LV];
-    __shared__ int s_prefix[2 * LV];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t m = (uint32_t)ctl->count[0];  // partners, published by k_classify
+// One thread's aggregates over its kScanItems partners starting at j0 (those below m).
+// Forward, agg[2l], agg[2l+1]: last start / last split of level l (identity -1, max).
+// Backward, agg[2LV+2l], agg[2LV+2l+1]: first start after a group / first split (identity
+// kLevelInf, min).
+template <int LV>
+__device__ __forceinline__ void level_thread_agg(const uint16_t (&d)[kScanItems], uint32_t j0, uint32_t m,
+                                                 const Levels& lv, int (&agg)[4 * LV]) {
     const int NL = lv.n;
-    // persistent: tiles from the dispenser until none is left (the grid is sized by residency)
-    for (;;) {
-        if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[1], 1u);
-        __syncthreads();
-        const unsigned int tile = s_tile;
-        if ((uint64_t)tile * kScanTile >= m) break;
-        const uint32_t j0 = tile * (uint32_t)kScanTile + (uint32_t)tid * kScanItems;
-
-        uint16_t d[kScanItems];
 #pragma unroll
-        for (int i = 0; i < kScanItems; ++i) {
-            uint32_t j = j0 + i;
-            d[i] = j < m ? D[j] : (uint16_t)0;
-            if (j < m && j > 0) fix_divergence<W>(idx, D, keys, n, j, d[i], ctl);
-        }
-        // thread aggregates: last start / last split position per level
-        int agg[2 * LV];
+    for (int l = 0; l < LV; ++l) {
+        agg[2 * l] = agg[2 * l + 1] = -1;
+        agg[2 * LV + 2 * l] = agg[2 * LV + 2 * l + 1] = kLevelInf;
+        if (l < NL) {
+            const uint32_t Lr = lv.rank[l];
 #pragma unroll
-        for (int l = 0; l < LV; ++l) {
-            agg[2 * l] = -1;
-            agg[2 * l + 1] = -1;
-            if (l < NL) {
-                uint32_t L = lv.rank[l];
-#pragma unroll
-                for (int i = 0; i < kScanItems; ++i) {
-                    uint32_t j = j0 + i;
-                    if (j >= m) break;
-                    if (j == 0 || d[i] < L) agg[2 * l] = (int)j;
-                    if (j != 0 && d[i] == L) agg[2 * l + 1] = (int)j;
+            for (int i = 0; i < kScanItems; ++i) {
+                const uint32_t j = j0 + i;
+                if (j < m) {
+                    if (j == 0 || d[i] < Lr) agg[2 * l] = (int)j;
+                    if (j != 0 && d[i] == Lr) agg[2 * l + 1] = (int)j;
                 }
             }
-        }
-        // block exclusive max-scan of the aggregates
-        int excl[2 * LV];
 #pragma unroll
-        for (int v = 0; v < 2 * LV; ++v) {
-            int x = agg[v];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                int y = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x = max(x, y);
-            }
-            int e = __shfl_up_sync(0xffffffffu, x, 1);
-            excl[v] = lane == 0 ? -1 : e;
-            if (lane == 31) s_wagg[warp][v] = x;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int v = 0; v < 2 * LV; ++v)
-            for (int w = 0; w < warp; ++w) excl[v] = max(excl[v], s_wagg[w][v]);
-        // tile aggregate, publish, look back
-        __syncthreads();
-        if (tid < 32) {
-            int tagg[2 * LV], pre[2 * LV];
-            for (int v = 0; v < 2 * LV; ++v) {
-                int t = -1;
-                for (int w = 0; w < kBlock / 32; ++w) t = max(t, s_wagg[w][v]);
-                tagg[v] = t;
-            }
-            level_lookback<true, LV>(slots, tile, tagg, pre, -1, ctl, 202);
-            if (tid == 0)
-                for (int v = 0; v < 2 * LV; ++v) s_prefix[v] = pre[v];
-        }
-        __syncthreads();
-#pragma unroll
-        for (int v = 0; v < 2 * LV; ++v) excl[v] = max(excl[v], s_prefix[v]);
-
-        // per item: F = sum over levels of -(split - start) for rows in an upper half
-#pragma unroll
-        for (int i = 0; i < kScanItems; ++i) {
-            uint32_t j = j0 + i;
-            if (j >= m) break;
-            int f = 0;
-#pragma unroll
-            for (int l = 0; l < LV; ++l) {
-                if (l < NL) {
-                    uint32_t L = lv.rank[l];
-                    if (j == 0 || d[i] < L) excl[2 * l] = (int)j;
-                    if (j != 0 && d[i] == L) excl[2 * l + 1] = (int)j;
-                    int s = excl[2 * l], p = excl[2 * l + 1];
-                    if (p > s) f -= (p - s);
+            for (int i = kScanItems - 1; i >= 0; --i) {
+                const uint32_t j = j0 + i;
+                if (j < m) {
+                    if (j != 0 && d[i] < Lr) agg[2 * LV + 2 * l] = (int)j;
+                    if (j != 0 && d[i] == Lr) agg[2 * LV + 2 * l + 1] = (int)j;
                 }
             }
-            F[j] = accumulate ? F[j] + f : f;
         }
     }
 }
 
-// Backward pass: B = sum over levels of (group end - split) for rows in a lower half; then
-// (last batch only) place each partner at j + F + B.
-template <int W, typename T, int LV>
-__global__ void __launch_bounds__(kBlock) k_bwd_levels(const uint32_t* __restrict__ idx,
-                                                       const uint16_t* __restrict__ D, int32_t* __restrict__ F,
-                                                       const uint64_t* __restrict__ keys,
-                                                       const T* __restrict__ coef, uint64_t n, const Levels lv,
-                                                       const RotLayer<W> L, int scatter,
-                                                       uint64_t* __restrict__ Pk, T* __restrict__ Pc,
-                                                       LevelSlot* slots, Ctl* ctl) {
-    __shared__ unsigned int s_tile;
-    __shared__ int s_wagg[kBlock / 32][2 * LV];
-    __shared__ int s_suffix[2 * LV];
-    __shared__ AmpTab<T> A;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int INF = 0x7fffffff;
-    stage_amps<W, T>(L, A);
-    const uint32_t m = (uint32_t)ctl->count[0];  // partners, published by k_classify
-    const int NL = lv.n;
-    // persistent: tiles from the dispenser until none is left (the grid is sized by residency)
-    for (;;) {
-        if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[2], 1u);
-        __syncthreads();
-        const unsigned int tile = s_tile;  // tile 0 covers the last kScanTile partners
-        if ((uint64_t)tile * kScanTile >= m) break;
-        const long long hi = (long long)m - (long long)tile * kScanTile;
-        const long long lo = hi - kScanTile;  // may be negative for the first partners
-        const long long jbase = lo + (long long)tid * kScanItems;
+// value v of a LevelTile row combines by max (forward half) or min (backward half)
+template <int LV>
+__device__ __forceinline__ int level_comb(int v, int a, int b) {
+    return v < 2 * LV ? max(a, b) : min(a, b);
+}
+template <int LV>
+__device__ __forceinline__ int level_id(int v) {
+    return v < 2 * LV ? -1 : kLevelInf;
+}
 
+// Phase 1: each tile's aggregates.  It also resolves the divergence ranks that k_classify left
+// unknown (the first listed row of each warp), so the later phases read them.
+template <int W, int LV>
+__global__ void __launch_bounds__(kBlock) k_level_reduce(const uint32_t* __restrict__ idx, uint16_t* __restrict__ D,
+                                                         const uint64_t* __restrict__ keys, uint64_t n, const Levels lv,
+                                                         LevelTile* __restrict__ tiles, Ctl* ctl) {
+    __shared__ int s_w[kBlock / 32][4 * LV];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t m = (uint32_t)ctl->count[0];  // partners, published by k_classify
+    const uint32_t ntiles = (m + kScanTile - 1) / kScanTile;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint32_t j0 = tile * (uint32_t)kScanTile + (uint32_t)tid * kScanItems;
         uint16_t d[kScanItems];
 #pragma unroll
         for (int i = 0; i < kScanItems; ++i) {
-            long long j = jbase + i;
-            d[i] = (j >= 0 && j < hi) ? D[j] : (uint16_t)0;
+            const uint32_t j = j0 + i;
+            d[i] = j < m ? D[j] : (uint16_t)0;
+            if (j < m && j > 0) fix_divergence<W>(idx, D, keys, n, j, d[i], ctl);
         }
-        int agg[2 * LV];
+        int agg[4 * LV];
+        level_thread_agg<LV>(d, j0, m, lv, agg);
 #pragma unroll
-        for (int l = 0; l < LV; ++l) {
-            agg[2 * l] = INF;
-            agg[2 * l + 1] = INF;
-            if (l < NL) {
-                uint32_t Lr = lv.rank[l];
+        for (int v = 0; v < 4 * LV; ++v) {
+            int x = agg[v];
 #pragma unroll
-                for (int i = kScanItems - 1; i >= 0; --i) {
-                    long long j = jbase + i;
-                    if (j < 0 || j >= hi) continue;
-                    if (j != 0 && d[i] < Lr) agg[2 * l] = (int)j;
-                    if (j != 0 && d[i] == Lr) agg[2 * l + 1] = (int)j;
-                }
-            }
+            for (int o = 16; o > 0; o >>= 1) x = level_comb<LV>(v, x, __shfl_xor_sync(0xffffffffu, x, o));
+            if (lane == 0) s_w[warp][v] = x;
         }
-        // exclusive suffix min over threads
-        int excl[2 * LV];
+        __syncthreads();
+        if (tid < 4 * LV) {
+            int x = level_id<LV>(tid);
+            for (int w = 0; w < kBlock / 32; ++w) x = level_comb<LV>(tid, x, s_w[w][tid]);
+            tiles[tile].agg[tid] = x;
+        }
+        __syncthreads();
+    }
+}
+
+// Phase 2, one block of kScanThreads: pre = the forward aggregates of the tiles before (max)
+// and the backward aggregates of the tiles after (min).  Thread k takes a contiguous chunk.
+constexpr int kScanThreads = 1024;
+template <int LV>
+__global__ void __launch_bounds__(kScanThreads) k_level_scan(LevelTile* __restrict__ tiles, Ctl* ctl) {
+    __shared__ int s_w[kScanThreads / 32][4 * LV];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t m = (uint32_t)ctl->count[0];
+    const uint32_t ntiles = (m + kScanTile - 1) / kScanTile;
+    const uint32_t per = (ntiles + kScanThreads - 1) / kScanThreads;
+    const uint32_t c0 = min((uint32_t)tid * per, ntiles), c1 = min(c0 + per, ntiles);
+    int chunk[4 * LV];
+#pragma unroll
+    for (int v = 0; v < 4 * LV; ++v) chunk[v] = level_id<LV>(v);
+    for (uint32_t t = c0; t < c1; ++t)
+#pragma unroll
+        for (int v = 0; v < 4 * LV; ++v) chunk[v] = level_comb<LV>(v, chunk[v], tiles[t].agg[v]);
+    int excl[4 * LV];
+#pragma unroll
+    for (int v = 0; v < 4 * LV; ++v) {
+        const bool fwd = v < 2 * LV;
+        int x = chunk[v];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = fwd ? __shfl_up_sync(0xffffffffu, x, o) : __shfl_down_sync(0xffffffffu, x, o);
+            if (fwd ? lane >= o : lane + o < 32) x = level_comb<LV>(v, x, y);
+        }
+        const int e = fwd ? __shfl_up_sync(0xffffffffu, x, 1) : __shfl_down_sync(0xffffffffu, x, 1);
+        excl[v] = (fwd ? lane == 0 : lane == 31) ? level_id<LV>(v) : e;
+        if (fwd ? lane == 31 : lane == 0) s_w[warp][v] = x;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 4 * LV; ++v) {
+        if (v < 2 * LV) {
+            for (int w = 0; w < warp; ++w) excl[v] = max(excl[v], s_w[w][v]);
+        } else {
+            for (int w = warp + 1; w < kScanThreads / 32; ++w) excl[v] = min(excl[v], s_w[w][v]);
+        }
+    }
+    // forward: ascending through the chunk
+    int run[2 * LV];
+#pragma unroll
+    for (int v = 0; v < 2 * LV; ++v) run[v] = excl[v];
+    for (uint32_t t = c0; t < c1; ++t)
 #pragma unroll
         for (int v = 0; v < 2 * LV; ++v) {
+            tiles[t].pre[v] = run[v];
+            run[v] = max(run[v], tiles[t].agg[v]);
+        }
+    // backward: descending through the chunk
+#pragma unroll
+    for (int v = 0; v < 2 * LV; ++v) run[v] = excl[2 * LV + v];
+    for (uint32_t t = c1; t > c0; --t)
+#pragma unroll
+        for (int v = 0; v < 2 * LV; ++v) {
+            tiles[t - 1].pre[2 * LV + v] = run[v];
+            run[v] = min(run[v], tiles[t - 1].agg[2 * LV + v]);
+        }
+}
+
+// Phase 3: per partner j, F = sum over levels of -(split - start) for rows in an upper half
+// (forward) plus (group end - split) for rows in a lower half (backward), added to the F of
+// earlier batches; on the last batch each partner goes to j + F.
+template <int W, typename T, int LV>
+__global__ void __launch_bounds__(kBlock) k_level_apply(const uint32_t* __restrict__ idx,
+                                                        const uint16_t* __restrict__ D, int32_t* __restrict__ F,
+                                                        const uint64_t* __restrict__ keys, const T* __restrict__ coef,
+                                                        uint64_t n, const Levels lv, const RotLayer<W> L,
+                                                        int accumulate, int scatter, uint64_t* __restrict__ Pk,
+                                                        T* __restrict__ Pc, const LevelTile* __restrict__ tiles,
+                                                        Ctl* ctl) {
+    __shared__ int s_w[kBlock / 32][4 * LV];
+    __shared__ AmpTab<T> A;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    stage_amps<W, T>(L, A);
+    __syncthreads();
+    const uint32_t m = (uint32_t)ctl->count[0];
+    const uint32_t ntiles = (m + kScanTile - 1) / kScanTile;
+    const int NL = lv.n;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint32_t j0 = tile * (uint32_t)kScanTile + (uint32_t)tid * kScanItems;
+        uint16_t d[kScanItems];
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i) {
+            const uint32_t j = j0 + i;
+            d[i] = j < m ? D[j] : (uint16_t)0;
+        }
+        int agg[4 * LV];
+        level_thread_agg<LV>(d, j0, m, lv, agg);
+        // exclusive scans over the block's threads (prefix max / suffix min), then the tile's pre
+        int excl[4 * LV];
+#pragma unroll
+        for (int v = 0; v < 4 * LV; ++v) {
+            const bool fwd = v < 2 * LV;
             int x = agg[v];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                int y = __shfl_down_sync(0xffffffffu, x, o);
-                if (lane + o < 32) x = min(x, y);
+                const int y = fwd ? __shfl_up_sync(0xffffffffu, x, o) : __shfl_down_sync(0xffffffffu, x, o);
+                if (fwd ? lane >= o : lane + o < 32) x = level_comb<LV>(v, x, y);
             }
-            int e = __shfl_down_sync(0xffffffffu, x, 1);
-            excl[v] = lane == 31 ? INF : e;
-            if (lane == 0) s_wagg[warp][v] = x;
+            const int e = fwd ? __shfl_up_sync(0xffffffffu, x, 1) : __shfl_down_sync(0xffffffffu, x, 1);
+            excl[v] = (fwd ? lane == 0 : lane == 31) ? level_id<LV>(v) : e;
+            if (fwd ? lane == 31 : lane == 0) s_w[warp][v] = x;
         }
         __syncthreads();
 #pragma unroll
-        for (int v = 0; v < 2 * LV; ++v)
-            for (int w = warp + 1; w < kBlock / 32; ++w) excl[v] = min(excl[v], s_wagg[w][v]);
-        __syncthreads();
-        if (tid < 32) {
-            int tagg[2 * LV], suf[2 * LV];
-            for (int v = 0; v < 2 * LV; ++v) {
-                int t = INF;
-                for (int w = 0; w < kBlock / 32; ++w) t = min(t, s_wagg[w][v]);
-                tagg[v] = t;
+        for (int v = 0; v < 4 * LV; ++v) {
+            if (v < 2 * LV) {
+                for (int w = 0; w < warp; ++w) excl[v] = max(excl[v], s_w[w][v]);
+            } else {
+                for (int w = warp + 1; w < kBlock / 32; ++w) excl[v] = min(excl[v], s_w[w][v]);
             }
-            level_lookback<false, LV>(slots, tile, tagg, suf, INF, ctl, 203);
-            if (tid == 0)
-                for (int v = 0; v < 2 * LV; ++v) s_suffix[v] = suf[v];
+            excl[v] = level_comb<LV>(v, excl[v], tiles[tile].pre[v]);
         }
-        __syncthreads();
+        __syncthreads();  // s_w is rewritten by the next tile
+        int f[kScanItems];
 #pragma unroll
-        for (int v = 0; v < 2 * LV; ++v) excl[v] = min(excl[v], s_suffix[v]);
-
+        for (int i = 0; i < kScanItems; ++i) {
+            const uint32_t j = j0 + i;
+            f[i] = 0;
+#pragma unroll
+            for (int l = 0; l < LV; ++l) {
+                if (l < NL && j < m) {
+                    const uint32_t Lr = lv.rank[l];
+                    if (j == 0 || d[i] < Lr) excl[2 * l] = (int)j;
+                    if (j != 0 && d[i] == Lr) excl[2 * l + 1] = (int)j;
+                    const int st = excl[2 * l], sp = excl[2 * l + 1];
+                    if (sp > st) f[i] -= (sp - st);
+                }
+            }
+        }
 #pragma unroll
         for (int i = kScanItems - 1; i >= 0; --i) {
-            long long j = jbase + i;
-            if (j < 0 || j >= hi) continue;
-            int b = 0;
+            const uint32_t j = j0 + i;
+            if (j >= m) continue;
 #pragma unroll
             for (int l = 0; l < LV; ++l) {
                 if (l < NL) {
-                    int e = excl[2 * l] == INF ? (int)m : excl[2 * l];
-                    int q = excl[2 * l + 1];
-                    if (q < e) b += e - q;
-                    uint32_t Lr = lv.rank[l];
-                    if (j != 0 && d[i] < Lr) excl[2 * l] = (int)j;
-                    if (j != 0 && d[i] == Lr) excl[2 * l + 1] = (int)j;
+                    int* ex = excl + 2 * LV;
+                    const int e = ex[2 * l] == kLevelInf ? (int)m : ex[2 * l];
+                    const int q = ex[2 * l + 1];
+                    if (q < e) f[i] += e - q;
+                    const uint32_t Lr = lv.rank[l];
+                    if (j != 0 && d[i] < Lr) ex[2 * l] = (int)j;
+                    if (j != 0 && d[i] == Lr) ex[2 * l + 1] = (int)j;
                 }
             }
-            int f = F[j] + b;
+            const int ft = accumulate ? F[j] + f[i] : f[i];
             if (!scatter) {
-                F[j] = f;
+                F[j] = ft;
                 continue;
             }
-            long long dest = j + f;
-            uint32_t row = idx[j];
+            const long long dest = (long long)j + ft;
+            const uint32_t row = idx[j];
             if (!PS_GUARD(ctl, dest >= 0 && dest < (long long)m && row < n, 204)) continue;
             uint64_t k[2 * W];
             load_key<W>(keys, row, k);
-            T c = coef[row];
-            T pc = partner_coeff<W, T>(L, A, k, c);
+            const T c = coef[row];
+            const T pc = partner_coeff<W, T>(L, A, k, c);
 #pragma unroll
             for (int w = 0; w < W; ++w) {
                 k[w] ^= L.gx[w];
@@ -900,15 +881,18 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
         // 2-3. level scans (batches of kMaxLevels; one batch of four covers every gate on at
         // most two qubits), scatter on the last batch
         const uint32_t stiles = (uint32_t)((m_hi + kScanTile - 1) / kScanTile);
-        static int fwd_per_sm[2] = {0, 0}, bwd_per_sm[2] = {0, 0};  // resident blocks per SM
-        auto resident = [&](auto kernel, int& cache) {
-            if (cache == 0) {
-                int v = 0;
-                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, kBlock, 0) != cudaSuccess || v < 1) v = 1;
-                cache = v;
-            }
-            return (uint32_t)std::min<uint64_t>(stiles, (uint64_t)cache * (a.sms > 0 ? a.sms : 1));
-        };
+        // grid-stride kernels over the scan tiles, at most the resident blocks
+        static int level_per_sm = 0;
+        if (level_per_sm == 0) {
+            int v = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_level_apply<W, T, kMaxLevels>, kBlock, 0) !=
+                    cudaSuccess ||
+                v < 1)
+                v = 1;
+            level_per_sm = v;
+        }
+        const uint32_t sgrid = std::min<uint32_t>(stiles, (uint32_t)level_per_sm * (uint32_t)(a.sms > 0 ? a.sms : 1));
+        LevelTile* lt = reinterpret_cast<LevelTile*>(a.slots);
         const bool narrow = a.levels->n <= 4;
         const int per = narrow ? 4 : kMaxLevels;
         int nb = (a.levels->n + per - 1) / per;
@@ -916,29 +900,26 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
             Levels lv{};
             lv.n = min(per, a.levels->n - b * per);
             for (int l = 0; l < lv.n; ++l) lv.rank[l] = a.levels->rank[b * per + l];
-            cudaMemsetAsync(a.slots, 0, (size_t)stiles * sizeof(LevelSlot), st);
-            cudaMemsetAsync(&ctl->tile_counter[1], 0, sizeof(unsigned int), st);
-            a.prof->begin(K_FWD_LEVELS, 0.0, st);
-            if (narrow)
-                k_fwd_levels<W, 4><<<resident(k_fwd_levels<W, 4>, fwd_per_sm[0]), kBlock, 0, st>>>(
-                    a.idx, a.D, a.F, a.Sk, a.n, lv, b > 0, reinterpret_cast<LevelSlot*>(a.slots), ctl);
-            else
-                k_fwd_levels<W, kMaxLevels><<<resident(k_fwd_levels<W, kMaxLevels>, fwd_per_sm[1]), kBlock, 0, st>>>(
-                    a.idx, a.D, a.F, a.Sk, a.n, lv, b > 0, reinterpret_cast<LevelSlot*>(a.slots), ctl);
+            const bool last = b == nb - 1;
+            // forward and backward scans of this batch of levels; the last batch places the partners
+            a.prof->begin(K_LEVEL_SCAN, 0.0, st);
+            a.prof->more_launches(K_LEVEL_SCAN, 1);  // reduce and scan
+            if (narrow) {
+                k_level_reduce<W, 4><<<sgrid, kBlock, 0, st>>>(a.idx, a.D, a.Sk, a.n, lv, lt, ctl);
+                k_level_scan<4><<<1, kScanThreads, 0, st>>>(lt, ctl);
+            } else {
+                k_level_reduce<W, kMaxLevels><<<sgrid, kBlock, 0, st>>>(a.idx, a.D, a.Sk, a.n, lv, lt, ctl);
+                k_level_scan<kMaxLevels><<<1, kScanThreads, 0, st>>>(lt, ctl);
+            }
             a.prof->end(st);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
-            cudaMemsetAsync(a.slots, 0, (size_t)stiles * sizeof(LevelSlot), st);
-            cudaMemsetAsync(&ctl->tile_counter[2], 0, sizeof(unsigned int), st);
-            const bool last = b == nb - 1;
-            a.prof->begin(K_BWD_LEVELS, 0.0, st);
+            a.prof->begin(K_LEVEL_APPLY, 0.0, st);
             if (narrow)
-                k_bwd_levels<W, T, 4><<<resident(k_bwd_levels<W, T, 4>, bwd_per_sm[0]), kBlock, 0, st>>>(
-                    a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, last, a.Pk, a.Pc,
-                    reinterpret_cast<LevelSlot*>(a.slots), ctl);
+                k_level_apply<W, T, 4><<<sgrid, kBlock, 0, st>>>(a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, b > 0, last,
+                                                               a.Pk, a.Pc, lt, ctl);
             else
-                k_bwd_levels<W, T, kMaxLevels><<<resident(k_bwd_levels<W, T, kMaxLevels>, bwd_per_sm[1]), kBlock, 0,
-                                                 st>>>(a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, last, a.Pk, a.Pc,
-                                                       reinterpret_cast<LevelSlot*>(a.slots), ctl);
+                k_level_apply<W, T, kMaxLevels><<<sgrid, kBlock, 0, st>>>(a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L,
+                                                                        b > 0, last, a.Pk, a.Pc, lt, ctl);
             a.prof->end(st);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
@@ -999,8 +980,9 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     const int nb = m ? (nlv + per - 1) / per : 0;
     for (int b = 0; b < nb; ++b) {
         const bool last = b == nb - 1;
-        a.prof->add_bytes(K_FWD_LEVELS, (double)m * (2 + 4 + (b > 0 ? 4 : 0)));
-        a.prof->add_bytes(K_BWD_LEVELS, (double)m * (2 + 4 + (last ? 4 + 2.0 * (16 * W + sizeof(T)) : 4)));
+        a.prof->add_bytes(K_LEVEL_SCAN, (double)m * 2);  // divergence reads
+        // divergence reads, earlier batches' F, then F written or (last) index, gather and place
+        a.prof->add_bytes(K_LEVEL_APPLY, (double)m * (2 + (b > 0 ? 4 : 0) + (last ? 4 + 2.0 * (16 * W + sizeof(T)) : 4)));
     }
     a.prof->add_bytes(K_PARTITION, (double)((a.n + m + MT - 1) / MT + 1) * 16);
     a.prof->add_bytes(K_MERGE, (double)(a.n + m + *a.out_count) * (16 * W + sizeof(T)));
