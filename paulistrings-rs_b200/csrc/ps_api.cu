@@ -1002,8 +1002,9 @@ struct Engine {
         const int first_pass = policy && policy->num_passes > 0 ? policy->passes[0].kind : PS_PASS_NONE;
         const bool fuse_topn = (first_pass == PS_PASS_TOPN || first_pass == PS_PASS_APPROX_TOPN) &&
                                out_rows > policy->passes[0].n;
-        const bool slotted = fuse_topn && first_pass == PS_PASS_TOPN && !s->fault_stall;
         const uint64_t span_rows = merge_span_rows<W>(out_rows);
+        // (the TopN kernels index a slotted store's rows in 32 bits)
+        const bool slotted = fuse_topn && first_pass == PS_PASS_TOPN && !s->fault_stall && span_rows < (1ull << 32);
         cudaError_t e = reserve_store(s, spare, slotted ? span_rows : out_rows);
         if (e == cudaSuccess && slotted)
             e = ensure(s, s->slot_count, (span_rows / merge_slot_rows<W>() + 1) * sizeof(unsigned int));

@@ -278,20 +278,6 @@ __global__ void __launch_bounds__(kBlock) k_classify(const uint64_t* __restrict_
 // (LevelTile: forward values at [0, 2LV), backward at [2LV, 4LV)) live in the caller's level
 // slot buffer.
 
-template <int W>
-__device__ __forceinline__ void fix_divergence(const uint32_t* __restrict__ idx, uint16_t* __restrict__ D,
-                                               const uint64_t* __restrict__ keys, uint64_t n, uint32_t j,
-                                               uint16_t& d, Ctl* ctl) {
-    if (d != kDivUnknown) return;
-    uint32_t ra = idx[j - 1], rb = idx[j];
-    if (!PS_BOUNDS(ctl, ra < n && rb < n, 201)) return;
-    uint64_t ka[2 * W], kb[2 * W];
-    load_key<W>(keys, ra, ka);
-    load_key<W>(keys, rb, kb);
-    d = (uint16_t)divergence<W>(ka, kb);
-    D[j] = d;
-}
-
 // One thread's aggregates over its kScanItems partners starting at j0 (those below m).
 // Forward, agg[2l], agg[2l+1]: last start / last split of level l (identity -1, max).
 // Backward, agg[2LV+2l], agg[2LV+2l+1]: first start after a group / first split (identity
@@ -349,11 +335,33 @@ __global__ void __launch_bounds__(kBlock) k_level_reduce(const uint32_t* __restr
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const uint32_t j0 = tile * (uint32_t)kScanTile + (uint32_t)tid * kScanItems;
         uint16_t d[kScanItems];
+        unsigned int unknown = 0;  // bit i: item i's rank is left for this kernel to resolve
 #pragma unroll
         for (int i = 0; i < kScanItems; ++i) {
             const uint32_t j = j0 + i;
             d[i] = j < m ? D[j] : (uint16_t)0;
-            if (j < m && j > 0) fix_divergence<W>(idx, D, keys, n, j, d[i], ctl);
+        }
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i)
+            if (j0 + i < m && j0 + i > 0 && d[i] == kDivUnknown) unknown |= 1u << i;
+        // one pass per unknown item of this thread (rarely more than one), its loads issued
+        // together rather than item by item
+        while (unknown) {
+            const int i = __ffs(unknown) - 1;
+            unknown &= unknown - 1;
+            const uint32_t j = j0 + i;
+            const uint32_t ra = idx[j - 1], rb = idx[j];
+            uint16_t r = kDivUnknown;
+            if (PS_BOUNDS(ctl, ra < n && rb < n, 201)) {
+                uint64_t ka[2 * W], kb[2 * W];
+                load_key<W>(keys, ra, ka);
+                load_key<W>(keys, rb, kb);
+                r = (uint16_t)divergence<W>(ka, kb);
+                D[j] = r;
+            }
+#pragma unroll
+            for (int q = 0; q < kScanItems; ++q)
+                if (q == i) d[q] = r;
         }
         int agg[4 * LV];
         level_thread_agg<LV>(d, j0, m, lv, agg);
@@ -375,64 +383,65 @@ __global__ void __launch_bounds__(kBlock) k_level_reduce(const uint32_t* __restr
 }
 
 // Phase 2, one block of kScanThreads: pre = the forward aggregates of the tiles before (max)
-// and the backward aggregates of the tiles after (min).  Thread k takes a contiguous chunk.
+// and the backward aggregates of the tiles after (min).  Rounds of kScanThreads tiles, one
+// tile per thread with a block scan and a carry: ascending for the forward values, descending
+// for the backward ones.
 constexpr int kScanThreads = 1024;
+template <bool kFwd, int LV>
+__device__ __forceinline__ void level_scan_pass(LevelTile* __restrict__ tiles, uint32_t ntiles,
+                                                int (&s_w)[kScanThreads / 32][2 * LV], int (&s_carry)[2 * LV]) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int ID = kFwd ? -1 : kLevelInf;
+    constexpr int OFF = kFwd ? 0 : 2 * LV;
+    auto comb = [](int a, int b) { return kFwd ? max(a, b) : min(a, b); };
+    if (tid < 2 * LV) s_carry[tid] = ID;
+    const uint32_t rounds = (ntiles + kScanThreads - 1) / kScanThreads;
+    for (uint32_t r = 0; r < rounds; ++r) {
+        // forward: tile r * kScanThreads + tid; backward: counted from the last tile
+        const long long pos = kFwd ? (long long)r * kScanThreads + tid
+                                   : (long long)ntiles - 1 - ((long long)r * kScanThreads + tid);
+        const bool have = kFwd ? pos < (long long)ntiles : pos >= 0;
+        int x[2 * LV];
+#pragma unroll
+        for (int v = 0; v < 2 * LV; ++v) x[v] = have ? tiles[pos].agg[OFF + v] : ID;
+        int excl[2 * LV];
+#pragma unroll
+        for (int v = 0; v < 2 * LV; ++v) {
+            int y = x[v];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int z = __shfl_up_sync(0xffffffffu, y, o);
+                if (lane >= o) y = comb(y, z);
+            }
+            const int e = __shfl_up_sync(0xffffffffu, y, 1);
+            excl[v] = lane == 0 ? ID : e;
+            if (lane == 31) s_w[warp][v] = y;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int v = 0; v < 2 * LV; ++v) {
+            int c = s_carry[v];
+            for (int w = 0; w < warp; ++w) c = comb(c, s_w[w][v]);
+            if (have) tiles[pos].pre[OFF + v] = comb(c, excl[v]);
+        }
+        __syncthreads();
+        if (tid < 2 * LV) {
+            int c = s_carry[tid];
+            for (int w = 0; w < kScanThreads / 32; ++w) c = comb(c, s_w[w][tid]);
+            s_carry[tid] = c;
+        }
+        __syncthreads();
+    }
+}
+
 template <int LV>
 __global__ void __launch_bounds__(kScanThreads) k_level_scan(LevelTile* __restrict__ tiles, Ctl* ctl) {
-    __shared__ int s_w[kScanThreads / 32][4 * LV];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    __shared__ int s_w[kScanThreads / 32][2 * LV];
+    __shared__ int s_carry[2 * LV];
     const uint32_t m = (uint32_t)ctl->count[0];
     const uint32_t ntiles = (m + kScanTile - 1) / kScanTile;
-    const uint32_t per = (ntiles + kScanThreads - 1) / kScanThreads;
-    const uint32_t c0 = min((uint32_t)tid * per, ntiles), c1 = min(c0 + per, ntiles);
-    int chunk[4 * LV];
-#pragma unroll
-    for (int v = 0; v < 4 * LV; ++v) chunk[v] = level_id<LV>(v);
-    for (uint32_t t = c0; t < c1; ++t)
-#pragma unroll
-        for (int v = 0; v < 4 * LV; ++v) chunk[v] = level_comb<LV>(v, chunk[v], tiles[t].agg[v]);
-    int excl[4 * LV];
-#pragma unroll
-    for (int v = 0; v < 4 * LV; ++v) {
-        const bool fwd = v < 2 * LV;
-        int x = chunk[v];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = fwd ? __shfl_up_sync(0xffffffffu, x, o) : __shfl_down_sync(0xffffffffu, x, o);
-            if (fwd ? lane >= o : lane + o < 32) x = level_comb<LV>(v, x, y);
-        }
-        const int e = fwd ? __shfl_up_sync(0xffffffffu, x, 1) : __shfl_down_sync(0xffffffffu, x, 1);
-        excl[v] = (fwd ? lane == 0 : lane == 31) ? level_id<LV>(v) : e;
-        if (fwd ? lane == 31 : lane == 0) s_w[warp][v] = x;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int v = 0; v < 4 * LV; ++v) {
-        if (v < 2 * LV) {
-            for (int w = 0; w < warp; ++w) excl[v] = max(excl[v], s_w[w][v]);
-        } else {
-            for (int w = warp + 1; w < kScanThreads / 32; ++w) excl[v] = min(excl[v], s_w[w][v]);
-        }
-    }
-    // forward: ascending through the chunk
-    int run[2 * LV];
-#pragma unroll
-    for (int v = 0; v < 2 * LV; ++v) run[v] = excl[v];
-    for (uint32_t t = c0; t < c1; ++t)
-#pragma unroll
-        for (int v = 0; v < 2 * LV; ++v) {
-            tiles[t].pre[v] = run[v];
-            run[v] = max(run[v], tiles[t].agg[v]);
-        }
-    // backward: descending through the chunk
-#pragma unroll
-    for (int v = 0; v < 2 * LV; ++v) run[v] = excl[2 * LV + v];
-    for (uint32_t t = c1; t > c0; --t)
-#pragma unroll
-        for (int v = 0; v < 2 * LV; ++v) {
-            tiles[t - 1].pre[2 * LV + v] = run[v];
-            run[v] = min(run[v], tiles[t - 1].agg[2 * LV + v]);
-        }
+    level_scan_pass<true, LV>(tiles, ntiles, s_w, s_carry);
+    level_scan_pass<false, LV>(tiles, ntiles, s_w, s_carry);
 }
 
 // Phase 3: per partner j, F = sum over levels of -(split - start) for rows in an upper half

@@ -32,9 +32,9 @@ constexpr int kThreads = 256;
 struct SlotWalk {
     uint32_t q = 0, r = 0;
     __device__ SlotWalk(const SlotMap& s, uint64_t e0) {
-        if (s.count) {
-            q = (uint32_t)(e0 / s.rows);
-            r = (uint32_t)(e0 % s.rows);
+        if (s.count) {  // a slotted store spans fewer than 2^32 rows
+            q = (uint32_t)e0 / s.rows;
+            r = (uint32_t)e0 - q * s.rows;
         }
     }
     // call only for a row below the store's span
@@ -48,7 +48,9 @@ struct SlotWalk {
     }
 };
 __device__ __forceinline__ bool slot_live(const SlotMap& s, uint64_t e) {
-    return !s.count || (uint32_t)(e % s.rows) < __ldg(s.count + e / s.rows);
+    if (!s.count) return true;
+    const uint32_t q = (uint32_t)e / s.rows;  // a slotted store spans fewer than 2^32 rows
+    return (uint32_t)e - q * s.rows < __ldg(s.count + q);
 }
 
 // ---------------------------------------------------------------------------
@@ -449,14 +451,10 @@ __global__ void __launch_bounds__(kThreads) k_topn_cand(const T* __restrict__ co
         const uint64_t wbase = c0 + (uint64_t)warp * 32 * ITEMS;
         // every load of the chunk first, then the keys and ballots
         uint64_t key[ITEMS];
-        unsigned int live = 0;  // bit i: element i is a row of the store
-        SlotWalk sw(slots, wbase + lane);
 #pragma unroll
         for (int i = 0; i < ITEMS; ++i) {
             const uint64_t e = wbase + (uint64_t)i * 32 + lane;
-            if (e < n && sw.live(slots)) live |= 1u << i;
-            sw.step32(slots);
-            key[i] = (live >> i) & 1u ? (sel ? sel[e] : raw_bits(coef[e])) : 0ull;
+            key[i] = e < n ? (sel ? sel[e] : raw_bits(coef[e])) : 0ull;
         }
         unsigned int ball[ITEMS];
         unsigned int wc = 0;
@@ -466,7 +464,10 @@ __global__ void __launch_bounds__(kThreads) k_topn_cand(const T* __restrict__ co
                 const uint64_t mk = mag_key<T>(from_raw<T>(key[i]));
                 key[i] = window ? window_key(mk, base) : mk;
             }
-            const bool hit = ((live >> i) & 1u) && (key[i] & mask) == prefix;
+            const uint64_t e = wbase + (uint64_t)i * 32 + lane;
+            // a row in a slot's unused tail is no row: tested only for the few hits (a slot's
+            // tail is allocated, so its value load above stays in bounds)
+            const bool hit = e < n && (key[i] & mask) == prefix && slot_live(slots, e);
             ball[i] = __ballot_sync(0xffffffffu, hit);
             wc += __popc(ball[i]);
         }
@@ -547,13 +548,12 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
     for (int i = 0; i < ITEMS; ++i) {
         const uint64_t e = wbase + (uint64_t)i * 32 + lane;
         bool isa = false, ist = false;
-        if (e < n && sw.live(slots)) {
-            if (key_mode == 3) {  // keep every row (compacting a slotted store)
-                isa = true;
-            } else {
-                const uint64_t mk = compact_key<T>(coef, sel, key_mode, e);
-                isa = mk > boundary;
-                ist = mk == boundary && boundary != 0;
+        if (e < n) {
+            // the key load does not wait for the liveness test (a slot's tail is allocated)
+            const uint64_t mk = key_mode == 3 ? 0ull : compact_key<T>(coef, sel, key_mode, e);
+            if (sw.live(slots)) {
+                isa = key_mode == 3 || mk > boundary;  // key_mode 3 keeps every row (compacting slots)
+                ist = key_mode != 3 && mk == boundary && boundary != 0;
             }
         }
         sw.step32(slots);
