@@ -696,7 +696,7 @@ __device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc
 }
 
 template <int W, typename T>
-__global__ void __launch_bounds__(kBlock) k_merge(const uint64_t* __restrict__ Sk, const T* __restrict__ Sc,
+__global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t* __restrict__ Sk, const T* __restrict__ Sc,
                                                   uint64_t n, const uint64_t* __restrict__ Pk,
                                                   const T* __restrict__ Pc, const ulonglong2* __restrict__ bounds,
                                                   const RotLayer<W> L, const KeepProg keep,
@@ -890,17 +890,20 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
         // 2-3. level scans (batches of kMaxLevels; one batch of four covers every gate on at
         // most two qubits), scatter on the last batch
         const uint32_t stiles = (uint32_t)((m_hi + kScanTile - 1) / kScanTile);
-        // grid-stride kernels over the scan tiles, at most the resident blocks
-        static int level_per_sm = 0;
-        if (level_per_sm == 0) {
+        // grid-stride kernels over the scan tiles, at most the resident blocks of the apply
+        // variant that runs
+        const bool narrow_lv = a.levels->n <= 4;
+        static int level_per_sm[2] = {0, 0};
+        int& per_sm = level_per_sm[narrow_lv ? 0 : 1];
+        if (per_sm == 0) {
             int v = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_level_apply<W, T, kMaxLevels>, kBlock, 0) !=
-                    cudaSuccess ||
-                v < 1)
-                v = 1;
-            level_per_sm = v;
+            cudaError_t oe = narrow_lv
+                                 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_level_apply<W, T, 4>, kBlock, 0)
+                                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_level_apply<W, T, kMaxLevels>,
+                                                                                 kBlock, 0);
+            per_sm = (oe != cudaSuccess || v < 1) ? 1 : v;
         }
-        const uint32_t sgrid = std::min<uint32_t>(stiles, (uint32_t)level_per_sm * (uint32_t)(a.sms > 0 ? a.sms : 1));
+        const uint32_t sgrid = std::min<uint32_t>(stiles, (uint32_t)per_sm * (uint32_t)(a.sms > 0 ? a.sms : 1));
         LevelTile* lt = reinterpret_cast<LevelTile*>(a.slots);
         const bool narrow = a.levels->n <= 4;
         const int per = narrow ? 4 : kMaxLevels;
@@ -1015,8 +1018,13 @@ template uint64_t merge_span_rows<4>(uint64_t);
 
 template <int W, typename T>
 cudaError_t configure_rotation_kernels() {
-    return cudaFuncSetAttribute(k_merge<W, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)MergeSmem<W, T>::bytes);
+    cudaError_t e = cudaFuncSetAttribute(k_merge<W, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)MergeSmem<W, T>::bytes);
+    // all of the unified L1 as shared memory, so residency is set by registers, not the carveout
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_merge<W, T>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+    return e;
 }
 
 #define PS_INSTANTIATE_ROT(W, T)                                                                 \
