@@ -47,6 +47,7 @@ struct RotTile {
 constexpr int kScanItems = 16;
 constexpr int kLevelInf = 0x7fffffff;  // identity of the backward level scan
 constexpr int kScanTile = kBlock * kScanItems;
+constexpr int kApplyThreads = 512;  // k_level_apply block: 8 partners per thread
 static_assert(kScanTile == (int)kScanTileRows, "scan tile");
 
 // word `wi` of a key held in registers, by an unrolled select (a runtime index into a
@@ -282,8 +283,8 @@ __global__ void __launch_bounds__(kBlock) k_classify(const uint64_t* __restrict_
 // Forward, agg[2l], agg[2l+1]: last start / last split of level l (identity -1, max).
 // Backward, agg[2LV+2l], agg[2LV+2l+1]: first start after a group / first split (identity
 // kLevelInf, min).
-template <int LV>
-__device__ __forceinline__ void level_thread_agg(const uint16_t (&d)[kScanItems], uint32_t j0, uint32_t m,
+template <int LV, int IT = kScanItems>
+__device__ __forceinline__ void level_thread_agg(const uint16_t (&d)[IT], uint32_t j0, uint32_t m,
                                                  const Levels& lv, int (&agg)[4 * LV]) {
     const int NL = lv.n;
 #pragma unroll
@@ -293,7 +294,7 @@ __device__ __forceinline__ void level_thread_agg(const uint16_t (&d)[kScanItems]
         if (l < NL) {
             const uint32_t Lr = lv.rank[l];
 #pragma unroll
-            for (int i = 0; i < kScanItems; ++i) {
+            for (int i = 0; i < IT; ++i) {
                 const uint32_t j = j0 + i;
                 if (j < m) {
                     if (j == 0 || d[i] < Lr) agg[2 * l] = (int)j;
@@ -301,7 +302,7 @@ __device__ __forceinline__ void level_thread_agg(const uint16_t (&d)[kScanItems]
                 }
             }
 #pragma unroll
-            for (int i = kScanItems - 1; i >= 0; --i) {
+            for (int i = IT - 1; i >= 0; --i) {
                 const uint32_t j = j0 + i;
                 if (j < m) {
                     if (j != 0 && d[i] < Lr) agg[2 * LV + 2 * l] = (int)j;
@@ -444,18 +445,20 @@ __global__ void __launch_bounds__(kScanThreads) k_level_scan(LevelTile* __restri
     level_scan_pass<false, LV>(tiles, ntiles, s_w, s_carry);
 }
 
-// Phase 3: per partner j, F = sum over levels of -(split - start) for rows in an upper half
+// Phase 3 (blocks of NT threads over the same 4096-partner tiles: at 8 partners per thread the
+// apply's registers allow more resident warps to cover its gather latency): per partner j, F = sum over levels of -(split - start) for rows in an upper half
 // (forward) plus (group end - split) for rows in a lower half (backward), added to the F of
 // earlier batches; on the last batch each partner goes to j + F.
-template <int W, typename T, int LV>
-__global__ void __launch_bounds__(kBlock) k_level_apply(const uint32_t* __restrict__ idx,
+template <int W, typename T, int LV, int NT>
+__global__ void __launch_bounds__(NT) k_level_apply(const uint32_t* __restrict__ idx,
                                                         const uint16_t* __restrict__ D, int32_t* __restrict__ F,
                                                         const uint64_t* __restrict__ keys, const T* __restrict__ coef,
                                                         uint64_t n, const Levels lv, const RotLayer<W> L,
                                                         int accumulate, int scatter, uint64_t* __restrict__ Pk,
                                                         T* __restrict__ Pc, const LevelTile* __restrict__ tiles,
                                                         Ctl* ctl) {
-    __shared__ int s_w[kBlock / 32][4 * LV];
+    constexpr int IT = kScanTile / NT;  // partners per thread
+    __shared__ int s_w[NT / 32][4 * LV];
     __shared__ AmpTab<T> A;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     stage_amps<W, T>(L, A);
@@ -464,15 +467,15 @@ __global__ void __launch_bounds__(kBlock) k_level_apply(const uint32_t* __restri
     const uint32_t ntiles = (m + kScanTile - 1) / kScanTile;
     const int NL = lv.n;
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const uint32_t j0 = tile * (uint32_t)kScanTile + (uint32_t)tid * kScanItems;
-        uint16_t d[kScanItems];
+        const uint32_t j0 = tile * (uint32_t)kScanTile + (uint32_t)tid * IT;
+        uint16_t d[IT];
 #pragma unroll
-        for (int i = 0; i < kScanItems; ++i) {
+        for (int i = 0; i < IT; ++i) {
             const uint32_t j = j0 + i;
             d[i] = j < m ? D[j] : (uint16_t)0;
         }
         int agg[4 * LV];
-        level_thread_agg<LV>(d, j0, m, lv, agg);
+        level_thread_agg<LV, IT>(d, j0, m, lv, agg);
         // exclusive scans over the block's threads (prefix max / suffix min), then the tile's pre
         int excl[4 * LV];
 #pragma unroll
@@ -494,14 +497,14 @@ __global__ void __launch_bounds__(kBlock) k_level_apply(const uint32_t* __restri
             if (v < 2 * LV) {
                 for (int w = 0; w < warp; ++w) excl[v] = max(excl[v], s_w[w][v]);
             } else {
-                for (int w = warp + 1; w < kBlock / 32; ++w) excl[v] = min(excl[v], s_w[w][v]);
+                for (int w = warp + 1; w < NT / 32; ++w) excl[v] = min(excl[v], s_w[w][v]);
             }
             excl[v] = level_comb<LV>(v, excl[v], tiles[tile].pre[v]);
         }
         __syncthreads();  // s_w is rewritten by the next tile
-        int f[kScanItems];
+        int f[IT];
 #pragma unroll
-        for (int i = 0; i < kScanItems; ++i) {
+        for (int i = 0; i < IT; ++i) {
             const uint32_t j = j0 + i;
             f[i] = 0;
 #pragma unroll
@@ -516,7 +519,7 @@ __global__ void __launch_bounds__(kBlock) k_level_apply(const uint32_t* __restri
             }
         }
 #pragma unroll
-        for (int i = kScanItems - 1; i >= 0; --i) {
+        for (int i = IT - 1; i >= 0; --i) {
             const uint32_t j = j0 + i;
             if (j >= m) continue;
 #pragma unroll
@@ -897,10 +900,11 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
         int& per_sm = level_per_sm[narrow_lv ? 0 : 1];
         if (per_sm == 0) {
             int v = 0;
-            cudaError_t oe = narrow_lv
-                                 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_level_apply<W, T, 4>, kBlock, 0)
-                                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_level_apply<W, T, kMaxLevels>,
-                                                                                 kBlock, 0);
+            cudaError_t oe =
+                narrow_lv ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_level_apply<W, T, 4, kApplyThreads>,
+                                                                          kApplyThreads, 0)
+                          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                &v, k_level_apply<W, T, kMaxLevels, kApplyThreads>, kApplyThreads, 0);
             per_sm = (oe != cudaSuccess || v < 1) ? 1 : v;
         }
         const uint32_t sgrid = std::min<uint32_t>(stiles, (uint32_t)per_sm * (uint32_t)(a.sms > 0 ? a.sms : 1));
@@ -927,11 +931,11 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
             a.prof->begin(K_LEVEL_APPLY, 0.0, st);
             if (narrow)
-                k_level_apply<W, T, 4><<<sgrid, kBlock, 0, st>>>(a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, b > 0, last,
-                                                               a.Pk, a.Pc, lt, ctl);
+                k_level_apply<W, T, 4, kApplyThreads><<<sgrid, kApplyThreads, 0, st>>>(
+                    a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, b > 0, last, a.Pk, a.Pc, lt, ctl);
             else
-                k_level_apply<W, T, kMaxLevels><<<sgrid, kBlock, 0, st>>>(a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L,
-                                                                        b > 0, last, a.Pk, a.Pc, lt, ctl);
+                k_level_apply<W, T, kMaxLevels, kApplyThreads><<<sgrid, kApplyThreads, 0, st>>>(
+                    a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, b > 0, last, a.Pk, a.Pc, lt, ctl);
             a.prof->end(st);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
