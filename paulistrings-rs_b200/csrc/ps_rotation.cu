@@ -26,6 +26,7 @@
 // Key-preserving tables (depolarizing noise, quarter turns with sin = 0) run
 // k_partition + k_merge with an empty partner stream.
 #include <algorithm>
+#include <atomic>
 #include <cstddef>
 
 #include "ps_device.cuh"
@@ -868,6 +869,18 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
+// Resident blocks per SM of a kernel, looked up on first use and kept for the process (every
+// device this library runs on is a B200, so one value serves all).
+template <typename K>
+int resident_blocks(K kernel, int threads, size_t smem, std::atomic<int>& cache) {
+    int v = cache.load(std::memory_order_relaxed);
+    if (v == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, threads, smem) != cudaSuccess || v < 1) v = 1;
+        cache.store(v, std::memory_order_relaxed);
+    }
+    return v;
+}
+
 template <int W, typename T>
 cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) {
     // One host synchronization per layer: k_classify publishes the partner count m on the
@@ -895,18 +908,12 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
         const uint32_t stiles = (uint32_t)((m_hi + kScanTile - 1) / kScanTile);
         // grid-stride kernels over the scan tiles, at most the resident blocks of the apply
         // variant that runs
-        const bool narrow_lv = a.levels->n <= 4;
-        static int level_per_sm[2] = {0, 0};
-        int& per_sm = level_per_sm[narrow_lv ? 0 : 1];
-        if (per_sm == 0) {
-            int v = 0;
-            cudaError_t oe =
-                narrow_lv ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_level_apply<W, T, 4, kApplyThreads>,
-                                                                          kApplyThreads, 0)
-                          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                                &v, k_level_apply<W, T, kMaxLevels, kApplyThreads>, kApplyThreads, 0);
-            per_sm = (oe != cudaSuccess || v < 1) ? 1 : v;
-        }
+        static std::atomic<int> level_per_sm[2];
+        const int per_sm = a.levels->n <= 4
+                               ? resident_blocks(k_level_apply<W, T, 4, kApplyThreads>, kApplyThreads, 0,
+                                                 level_per_sm[0])
+                               : resident_blocks(k_level_apply<W, T, kMaxLevels, kApplyThreads>, kApplyThreads, 0,
+                                                 level_per_sm[1]);
         const uint32_t sgrid = std::min<uint32_t>(stiles, (uint32_t)per_sm * (uint32_t)(a.sms > 0 ? a.sms : 1));
         LevelTile* lt = reinterpret_cast<LevelTile*>(a.slots);
         const bool narrow = a.levels->n <= 4;
@@ -964,13 +971,9 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     cudaMemsetAsync(&ctl->tile_counter[3], a.inject_stall ? 1 : 0, 1, st);
     cudaMemsetAsync(reinterpret_cast<unsigned char*>(&ctl->tile_counter[3]) + 1, 0, 3, st);
     size_t smem = MergeSmem<W, T>::bytes;
-    static int merge_per_sm = 0;  // resident merge blocks per SM (the same on every B200)
-    if (merge_per_sm == 0) {
-        int v = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_merge<W, T>, kBlock, smem) != cudaSuccess || v < 1) v = 1;
-        merge_per_sm = v;
-    }
-    const uint32_t mgrid = (uint32_t)std::min<uint64_t>(mtiles_hi, (uint64_t)merge_per_sm * (a.sms > 0 ? a.sms : 1));
+    static std::atomic<int> merge_per_sm;
+    const int mper = resident_blocks(k_merge<W, T>, kBlock, smem, merge_per_sm);
+    const uint32_t mgrid = (uint32_t)std::min<uint64_t>(mtiles_hi, (uint64_t)mper * (a.sms > 0 ? a.sms : 1));
     a.prof->begin(K_MERGE, 0.0, st);
     k_merge<W, T><<<mgrid, kBlock, smem, st>>>(a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc,
                                                   a.out_cap, a.status, ctl, a.topn_hist, a.topn_hist_mode,
