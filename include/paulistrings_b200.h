@@ -274,10 +274,13 @@ ps_status ps_read_profile(ps_sum* sum, ps_kernel_profile* out, int32_t cap, int3
  * held by every GPU that loads it until the process exits.  keys: n rows of 2*width u64 (x words
  * then z words) in device memory; coeffs: n float64 or float32 (dtype) in device memory; the
  * axis/sign masks are host arrays of width words; out: one float64 in device memory, written on
- * `stream` (a cudaStream_t, NULL for the default stream).  n above PS_NOALLOC_MAX_TERMS is
- * rejected with PS_ERR_INVALID.  The first call on each device looks up the scratch address
- * (make it before any stream capture); calls on one device share the scratch, so calls that
- * overlap on the GPU race.  It has no counterpart in the reference. */
+ * `stream` (a cudaStream_t, NULL for the default stream).  keys must be 16-byte aligned, coeffs
+ * aligned to its element size and out to 8 bytes; a pointer off those boundaries, or n above
+ * PS_NOALLOC_MAX_TERMS, is rejected with PS_ERR_INVALID before anything is launched.  The first
+ * call on each device looks up the scratch address, which (with the CUDA runtime's lazy module
+ * loading) is also when the library's module is loaded on that device and the array reserved:
+ * make that first call at start-up, before any stream capture.  Calls on one device share the
+ * scratch, so calls that overlap on the GPU race.  It has no counterpart in the reference. */
 ps_status ps_expectation_device_noalloc(const uint64_t* keys, const void* coeffs, int32_t dtype, int32_t width,
                                         uint64_t n, const uint64_t* axis_x, const uint64_t* axis_z,
                                         const uint64_t* negative, double* out, void* stream);
@@ -287,8 +290,9 @@ ps_status ps_expectation_device_noalloc(const uint64_t* keys, const void* coeffs
  * every further one fails as if the device were out of memory, until PS_FAULT_NONE.  PS_FAULT_STALL: the next layer's
  * merge skips its first tile, so the following tile's output-offset wait sees a flag nothing
  * sets and gives up after `arg` polls (0: the default limit), reporting PS_ERR_TIMEOUT; the
- * limit stays in force for the handle.  PS_FAULT_NONE disarms.  Either way the layer fails and
- * the store keeps the last completed layer. */
+ * shortened limit applies to that merge's output-offset waits only, and every other bounded
+ * wait keeps the default.  PS_FAULT_NONE disarms both.  Either way the layer fails and the
+ * store keeps the last completed layer. */
 typedef enum ps_fault_kind { PS_FAULT_NONE = 0, PS_FAULT_OOM = 1, PS_FAULT_STALL = 2 } ps_fault_kind;
 ps_status ps_inject_fault(ps_sum* sum, int32_t kind, uint64_t arg);
 

@@ -87,6 +87,7 @@ struct ps_sum {
     KernelProf prof;
     long long fault_oom_after = -1;   // failure injection: allocations left before all fail
     bool fault_stall = false;         // failure injection: next merge skips its first tile
+    unsigned long long stall_limit = 0;  // ... and its output-offset waits give up after this many polls
     // Slotted store: the last merge left each tile's rows at the start of a fixed slot of
     // slot_rows rows (n = the slots' span, live_n = rows in them) for the TopN pass that follows
     // to compact; every other reader compacts it first (Engine::densify).
@@ -1055,6 +1056,7 @@ struct Engine {
         }
         a.topn_hist = fuse_topn ? (unsigned int*)s->hist.p : nullptr;
         a.inject_stall = s->fault_stall ? 1 : 0;
+        a.stall_limit = s->fault_stall ? s->stall_limit : 0;
         s->fault_stall = false;
         uint64_t span = 0;
         a.slot_count = slotted ? (unsigned int*)s->slot_count.p : nullptr;
@@ -1676,22 +1678,21 @@ ps_status ps_read_profile(ps_sum* s, ps_kernel_profile* out, int32_t cap, int32_
 
 ps_status ps_inject_fault(ps_sum* s, int32_t kind, uint64_t arg) {
     if (!s) return PS_ERR_INVALID;
-    DeviceGuard g(s->device);
     switch (kind) {
     case PS_FAULT_NONE:
         s->fault_oom_after = -1;
         s->fault_stall = false;
+        s->stall_limit = 0;
         break;
     case PS_FAULT_OOM:
         s->fault_oom_after = (long long)arg;
         break;
-    case PS_FAULT_STALL: {
+    case PS_FAULT_STALL:
+        // the shortened limit reaches only the stalled merge's output-offset waits; every other
+        // bounded wait of the handle keeps kSpinLimit
         s->fault_stall = true;
-        unsigned long long limit = arg ? arg : (unsigned long long)kSpinLimit;
-        cudaError_t e = cudaMemcpy(&s->ctl->spin_limit, &limit, sizeof(limit), cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) return cuda_fail(s, e, "inject_fault");
+        s->stall_limit = arg ? arg : (unsigned long long)kSpinLimit;
         break;
-    }
     default: return PS_ERR_INVALID;
     }
     return PS_OK;

@@ -132,6 +132,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, Ctl* c
     return true;
 }
 
+// After a bounded wait gave up: wait (with a fixed limit of its own, not the handle's, which a
+// test may have shortened) for the phase `parity` of `bar`, so the bulk copies in flight into
+// this block's shared memory have landed before the block reuses or releases it.
+constexpr long long kDrainLimit = 1LL << 24;
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t parity) {
+    for (long long spins = 0; spins < kDrainLimit && !mbar_try_wait(bar, parity); ++spins) __nanosleep(64);
+}
+
 // Issue a bulk copy of `bytes` (rounded up to 16) from global `src` (16-B aligned) into shared `dst`.
 // The caller sized the source allocation with >= 16 bytes of tail padding.
 __device__ __forceinline__ uint32_t round16(uint32_t b) { return (b + 15u) & ~15u; }
@@ -342,8 +350,9 @@ constexpr unsigned long long kValMask = (1ull << 62) - 1;
 // aggregate: each poll reads 32 predecessors at once, sums the aggregates up to the nearest
 // inclusive prefix, and moves the window back only when none of the 32 holds one.
 // Returns the same value in every lane.
+// `limit` > 0 replaces the handle's spin limit for this wait (failure injection).
 __device__ __forceinline__ unsigned long long lookback_sum_warp(const unsigned long long* status, unsigned int tile,
-                                                               Ctl* ctl, uint32_t info) {
+                                                               Ctl* ctl, uint32_t info, long long limit = 0) {
     const int lane = threadIdx.x & 31;
     unsigned long long acc = 0;
     long long base = (long long)tile - 1;
@@ -357,7 +366,7 @@ __device__ __forceinline__ unsigned long long lookback_sum_warp(const unsigned l
         const int first_inc = inc ? __ffs(inc) - 1 : 32;
         const unsigned int need = first_inc >= 31 ? 0xffffffffu : ((2u << first_inc) - 1u);
         if (empty & need) {
-            if (++spins > spin_limit(ctl)) {
+            if (++spins > (limit > 0 ? limit : spin_limit(ctl))) {
                 if (lane == 0) raise_err(ctl, ERR_TIMEOUT, info);
                 return acc;
             }

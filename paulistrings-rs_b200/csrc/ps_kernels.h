@@ -217,6 +217,7 @@ struct RotationArgs {
     int topn_hist_mode;       // 0 select key >> 52, 1 octave of |c|^2 (ApproxTopN),
     uint64_t topn_hist_base;  // 2 window_key(select key, topn_hist_base) >> 48
     int inject_stall;         // failure injection: the merge skips its first tile
+    unsigned long long stall_limit;  // ... and its look-back waits give up after this many polls
     unsigned int* slot_count; // when set, the merge writes tile t at rows t * merge_slot_rows<W>()
                               // and its row count to slot_count[t], with no look-back (slotted
                               // output, compacted by the TopN pass that follows); >= merge tiles

@@ -12,8 +12,10 @@
 // The scratch is a file-scope device array of kNoAllocPartials float64 partial sums (512 KiB).
 // Every GPU that loads this library holds one copy of it until the process exits.  Host code
 // cannot use the array's name as a device address, so the first call on each device looks
-// the address up with cudaGetSymbolAddress while that device is current; make that first
-// call on a device before any stream capture.  All calls on a device share the array, so calls
+// the address up with cudaGetSymbolAddress while that device is current; with the CUDA
+// runtime's lazy module loading that lookup is also what loads this file's module on the
+// device and reserves the array, so the first call belongs at start-up, before any stream
+// capture.  All calls on a device share the array, so calls
 // whose kernels overlap on the GPU race; serialize them (one stream, or events).  Nothing in
 // the array needs clearing between calls: each call writes every partial it then reads.
 #include <cstdint>
@@ -109,6 +111,9 @@ ps_status partials_for(int device, double** out) {
     return PS_OK;
 }
 
+// Both launches go through cudaLaunchKernel, whose return value is that launch's own status: an
+// error some earlier call of the caller's left pending is neither reported as this call's
+// failure nor cleared from the caller's view.
 template <int W, typename T>
 ps_status launch(const uint64_t* keys, const void* coeffs, uint64_t n, const uint64_t* ax, const uint64_t* az,
                  const uint64_t* neg, double* out, cudaStream_t st, double* partials) {
@@ -118,12 +123,19 @@ ps_status launch(const uint64_t* keys, const void* coeffs, uint64_t n, const uin
         B.az[w] = az[w];
         B.neg[w] = neg[w];
     }
-    const uint32_t blocks = (uint32_t)((n + kNoAllocTermsPerBlock - 1) / kNoAllocTermsPerBlock);
-    if (blocks)
-        k_expect_noalloc_blocks<W, T><<<blocks, kNoAllocThreads, 0, st>>>(keys, static_cast<const T*>(coeffs), n, B,
-                                                                          partials);
-    k_expect_noalloc_final<<<1, kNoAllocThreads, 0, st>>>(partials, blocks, out);
-    return cudaGetLastError() == cudaSuccess ? PS_OK : PS_ERR_DEVICE;
+    uint32_t blocks = (uint32_t)((n + kNoAllocTermsPerBlock - 1) / kNoAllocTermsPerBlock);
+    const T* coef = static_cast<const T*>(coeffs);
+    if (blocks) {
+        void* args[] = {(void*)&keys, (void*)&coef, (void*)&n, (void*)&B, (void*)&partials};
+        if (cudaLaunchKernel((const void*)k_expect_noalloc_blocks<W, T>, dim3(blocks), dim3(kNoAllocThreads), args, 0,
+                             st) != cudaSuccess)
+            return PS_ERR_DEVICE;
+    }
+    void* fargs[] = {(void*)&partials, (void*)&blocks, (void*)&out};
+    if (cudaLaunchKernel((const void*)k_expect_noalloc_final, dim3(1), dim3(kNoAllocThreads), fargs, 0, st) !=
+        cudaSuccess)
+        return PS_ERR_DEVICE;
+    return PS_OK;
 }
 
 }  // namespace
@@ -138,6 +150,12 @@ ps_status ps_expectation_device_noalloc(const uint64_t* keys, const void* coeffs
     if (dtype != PS_F64 && dtype != PS_F32) return PS_ERR_INVALID;
     if (width != 1 && width != 2 && width != 4) return PS_ERR_UNSUPPORTED;
     if (n > PS_NOALLOC_MAX_TERMS) return PS_ERR_INVALID;  // the scratch holds one partial per 16,384 terms
+    // The kernel reads a key as 16-byte vectors and a coefficient as one T, and writes one
+    // double: a pointer off those boundaries would fault the device instead of failing here.
+    const uintptr_t csize = dtype == PS_F64 ? sizeof(double) : sizeof(float);
+    if ((reinterpret_cast<uintptr_t>(keys) & 15u) != 0 || (reinterpret_cast<uintptr_t>(coeffs) & (csize - 1)) != 0 ||
+        (reinterpret_cast<uintptr_t>(out) & 7u) != 0)
+        return PS_ERR_INVALID;
     int device = -1;
     if (cudaGetDevice(&device) != cudaSuccess) {
         cudaGetLastError();

@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(kBlock) k_level_reduce(const uint32_t* __restr
             const uint32_t j = j0 + i;
             const uint32_t ra = idx[j - 1], rb = idx[j];
             uint16_t r = kDivUnknown;
-            if (PS_BOUNDS(ctl, ra < n && rb < n, 201)) {
+            if (PS_GUARD(ctl, ra < n && rb < n, 201)) {
                 uint64_t ka[2 * W], kb[2 * W];
                 load_key<W>(keys, ra, ka);
                 load_key<W>(keys, rb, kb);
@@ -707,7 +707,8 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
                                                   uint64_t* __restrict__ Ok, T* __restrict__ Oc, uint64_t out_cap,
                                                   unsigned long long* status, Ctl* ctl,
                                                   unsigned int* __restrict__ topn_hist, int hist_mode,
-                                                  uint64_t hist_base, unsigned int* __restrict__ slot_count) {
+                                                  uint64_t hist_base, unsigned int* __restrict__ slot_count,
+                                                  long long stall_limit) {
     using SM = MergeSmem<W, T>;
     constexpr int ITEMS = RotTile<W>::kMergeItems;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -761,8 +762,14 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
             if (cbS) bulk_g2s(sSc, Sc + sa, cbS, &bar);
             if (cbP) bulk_g2s(sPc, Pc + pa, cbP, &bar);
         }
-        if (cs + cp) {
-            mbar_wait(&bar, phase & 1u, ctl, 302);
+        if (cs + cp) {  // block-uniform
+            const bool ok = mbar_wait(&bar, phase & 1u, ctl, 302);
+            // a wait that gave up (ERR_TIMEOUT is flagged) ends the block: its copies land first,
+            // and nothing reads the unfilled tile or issues another copy into it
+            if (__syncthreads_or(ok ? 0 : 1)) {
+                if (tid == 0) mbar_drain(&bar, phase & 1u);
+                break;
+            }
             ++phase;
         }
         const T* Sc_l = sSc + s_off;
@@ -826,7 +833,7 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
                 if (tid == 0) st_release_u64(status + tile, kFlagInc | (unsigned long long)total);
             } else {
                 if (tid == 0) st_release_u64(status + tile, kFlagAgg | (unsigned long long)total);
-                p = lookback_sum_warp(status, tile, ctl, 303);
+                p = lookback_sum_warp(status, tile, ctl, 303, stall_limit);
                 if (tid == 0) st_release_u64(status + tile, kFlagInc | (p + total));
             }
             if (tid == 0) {
@@ -977,7 +984,8 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     a.prof->begin(K_MERGE, 0.0, st);
     k_merge<W, T><<<mgrid, kBlock, smem, st>>>(a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc,
                                                   a.out_cap, a.status, ctl, a.topn_hist, a.topn_hist_mode,
-                                                  a.topn_hist_base, a.slot_count);
+                                                  a.topn_hist_base, a.slot_count,
+                                                  a.inject_stall ? (long long)a.stall_limit : 0ll);
     a.prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // counts and error flags in one copy: count[0..7], tile_counter[0..7], err, err_info

@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(kScoreThreads) k_score(const ScorerArgs A, con
         const bool ok = __syncthreads_and(mbar_wait(&s_bar, phase, ctl, 901) ? 1 : 0) != 0;
         phase ^= 1u;
         if (!ok) {
-            mbar_wait(&s_bar, phase ^ 1u, ctl, 903);  // let the issued MMAs drain before TMEM is freed
+            mbar_drain(&s_bar, phase ^ 1u);  // let the issued MMAs drain before TMEM is freed
             break;
         }
         tc_fence_after();
@@ -458,7 +458,7 @@ __global__ void __launch_bounds__(kScoreThreads) k_train_bwd(const ScorerArgs A,
         ok = __syncthreads_and(mbar_wait(&s_bar, phase, ctl, 902) ? 1 : 0) != 0;
         phase ^= 1u;
         if (!ok) {
-            mbar_wait(&s_bar, phase ^ 1u, ctl, 904);  // let the issued MMAs drain before TMEM is freed
+            mbar_drain(&s_bar, phase ^ 1u);  // let the issued MMAs drain before TMEM is freed
             break;
         }
         ++done;

@@ -1,8 +1,9 @@
 """Regenerate the golden fixtures in this directory from the reference repository.
 
-Run in a container where the reference is mounted (it is never read at test time):
+Run where a checkout of the reference is available (it is never read at test time), giving
+the path of that checkout:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path to the reference checkout>
 
 What it writes, and where each number comes from (paths inside the reference):
 
@@ -142,4 +143,6 @@ def main(reference: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path to the reference checkout>")
+    main(Path(sys.argv[1]))

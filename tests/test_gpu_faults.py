@@ -50,6 +50,7 @@ def test_injected_stall_times_out_boundedly_and_keeps_the_store():
         g.propagate(circ, truncation.coeff(1e-12))
     assert info.value.status == _lib.PS_ERR_TIMEOUT
     assert_same_terms(g.download(), before, what="after-stall")
+    _lib.check(_lib.lib().ps_inject_fault(g._h, _lib.PS_FAULT_NONE, 0), g._h, "disarm")
     g.propagate(circ, truncation.coeff(1e-12))
     o = oracle_sum(32, *before)
     o.propagate(oracle_channels(circ), {"keep": [("coeff", 1e-12)]})
@@ -63,3 +64,24 @@ def test_injection_can_be_disarmed():
     circ = workloads.random_pair_layers(32, 1, seed=2)
     g.propagate(circ, truncation.coeff(1e-12))
     assert len(g) > 2000
+
+
+def test_disarming_a_stall_restores_the_full_wait_limit():
+    """A stall injected with a limit of 64 polls fails its layer; after PS_FAULT_NONE a layer
+    over a few million terms (thousands of look-back tiles in flight, whose waits routinely
+    take more than 64 polls) runs with the default limit and matches the oracle."""
+    g, _ = _sum(num_qubits=48, count=200000, seed=11)
+    circ = ps.Circuit(48)
+    circ.pauli_rotation("XY", [0, 1], 0.4)
+    _lib.check(_lib.lib().ps_inject_fault(g._h, _lib.PS_FAULT_STALL, 64), g._h, "inject")
+    with pytest.raises(_lib.PauliStringsError) as info:
+        g.propagate(circ, truncation.coeff(1e-12))
+    assert info.value.status == _lib.PS_ERR_TIMEOUT
+    _lib.check(_lib.lib().ps_inject_fault(g._h, _lib.PS_FAULT_NONE, 0), g._h, "disarm")
+    before = g.download()
+    big = workloads.random_pair_layers(48, 1, seed=5)
+    g.propagate(big, truncation.coeff(1e-12))
+    assert len(g) > 1_000_000
+    o = oracle_sum(48, *before)
+    o.propagate(oracle_channels(big), {"keep": [("coeff", 1e-12)]})
+    assert_same_terms(g.download(), oracle_arrays(o), what="after-disarm")

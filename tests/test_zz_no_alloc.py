@@ -45,7 +45,7 @@ def _noalloc(tkeys, tcoef, dtype, width, state, num_qubits, out):
     return float(out.item())
 
 
-@pytest.mark.parametrize("num_qubits,dtype", [(64, "f64"), (64, "f32"), (100, "f64")])
+@pytest.mark.parametrize("num_qubits,dtype", [(64, "f64"), (64, "f32"), (100, "f64"), (256, "f64"), (200, "f32")])
 def test_noalloc_expectation_matches_the_handle_entry_point_twice(num_qubits, dtype):
     import torch
 
@@ -71,3 +71,30 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
         out.data_ptr(), out.data_ptr(), _lib.PS_F64, 1, _lib.NOALLOC_MAX_TERMS + 1,
         one.ctypes.data, one.ctypes.data, one.ctypes.data, out.data_ptr(), None)
     assert status == _lib.PS_ERR_INVALID
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_noalloc_rejects_misaligned_pointers_without_launching(dtype):
+    """keys must be 16-byte aligned, coefficients aligned to their element size and the output to
+    8 bytes: an offset view of a caller's buffer is refused with PS_ERR_INVALID before anything
+    reaches the device, and a correct call right after still matches the handle's readout."""
+    import torch
+
+    g, tkeys, tcoef = _device_store(64, dtype, seed=5)
+    out = torch.zeros(2, dtype=torch.float64, device="cuda")
+    ax, az, neg = ps.product_basis("z+", 64, 1)
+    fn = _lib.lib().ps_expectation_device_noalloc
+    code = _lib.PS_F64 if dtype == "f64" else _lib.PS_F32
+    n = tkeys.shape[0] - 1
+    esize = tcoef.element_size()
+    bad = [
+        (tkeys.data_ptr() + 8, tcoef.data_ptr(), out.data_ptr()),          # keys off 16 bytes
+        (tkeys.data_ptr(), tcoef.data_ptr() + esize // 2, out.data_ptr()),  # coefficients off their size
+        (tkeys.data_ptr(), tcoef.data_ptr(), out.data_ptr() + 4),           # output off 8 bytes
+    ]
+    for keys, coef, o in bad:
+        assert fn(keys, coef, code, 1, n, ax.ctypes.data, az.ctypes.data, neg.ctypes.data, o, None) == \
+            _lib.PS_ERR_INVALID
+    torch.cuda.synchronize()
+    assert _noalloc(tkeys, tcoef, dtype, 1, "z+", 64, out[:1]) == pytest.approx(g.expectation("z+"), rel=1e-12,
+                                                                                abs=1e-15)
