@@ -189,6 +189,10 @@ typedef struct ps_run_stats {
     uint64_t kernel_launches; /* kernels this call launched */
     double device_ms;         /* CUDA-event time of the whole run */
     uint64_t collapses;       /* CollapseSample collapses performed */
+    uint64_t layers_skipped;  /* layers that changed nothing and launched nothing: the table acts
+                                 on qubits no term touches, maps the identity there to itself,
+                                 and every term already passed the same keep program */
+    uint64_t skipped_terms_in;/* sum of terms_in over those layers */
 } ps_run_stats;
 
 /* Per-kernel profile (the phase-timing counters, crates/paulistrings/src/engine/stats.rs:12 and
@@ -341,6 +345,14 @@ ps_status ps_scorer_gradients(ps_scorer* scorer, const uint64_t* keys, const flo
 ps_status ps_scorer_train(ps_scorer* scorer, const uint64_t* keys, const float* log_abs_c, const float* remaining,
                           const float* target, uint64_t n, int32_t epochs, int32_t batch, float learning_rate,
                           float* epoch_loss);
+/* Score sums of num_sites qubits (<= 256) with this scorer's embedding rows: site q of a term
+ * adds embedding row row_of_site[q] (-1: the site is not an input), so one scorer trained on a
+ * small register serves a larger one (e.g. a window of rows around the observable's site, the
+ * sites beyond it clamped to the window's edge rows).  The weight, log|c| and remaining-depth
+ * features are unchanged (the weight counts every site).  num_sites 0 or a NULL map restores
+ * the identity (site q uses row q).  Training refuses a mapped scorer: its rows are the
+ * embedding rows' own qubits.  No counterpart in the reference, which has no learned policy. */
+ps_status ps_scorer_set_site_map(ps_scorer* scorer, int32_t num_sites, const int32_t* row_of_site);
 /* Attach a scorer for PS_PASS_SCORED_TOPN passes; remaining_layers = layers still to apply.
  * Each ps_finalize_layer (and each layer of ps_propagate) first counts one layer down, then
  * scores with the remaining depth that is left.  NULL detaches. */

@@ -75,8 +75,8 @@ def support(keys, nq, W):
     return p  # [n, nq], 0 = identity
 
 
-def features(keys, logc, rem, nq, W, fscale):
-    p = support(keys, nq, W)
+def features(keys, logc, rem, nq, W, fscale, num_sites=None):
+    p = support(keys, nq if num_sites is None else num_sites, W)
     weight = (p != 0).sum(axis=1).astype(np.float32)
     logc = np.maximum(np.asarray(logc, np.float32), np.float32(-200.0))
     f = np.stack([weight * np.float32(fscale[0]), logc * np.float32(fscale[1]),
@@ -84,14 +84,20 @@ def features(keys, logc, rem, nq, W, fscale):
     return p, f
 
 
-def forward(params, keys, logc, rem, nq, W, fscale):
+def forward(params, keys, logc, rem, nq, W, fscale, site_row=None):
+    """``site_row``: embedding row of each qubit of the scored keys (-1: ignored), the inference
+    site map; the keys then have len(site_row) qubits and W words per half."""
     embed, u, b1, w2, b2, w3, b3 = unpack(params, nq)
-    p, f = features(keys, logc, rem, nq, W, fscale)
+    sites = nq if site_row is None else len(site_row)
+    p, f = features(keys, logc, rem, nq, W, fscale, num_sites=sites)
     z1 = b1[None, :] + f[:, 0:1] * u[0][None, :] + f[:, 1:2] * u[1][None, :] + f[:, 2:3] * u[2][None, :]
-    for q in range(nq):
+    for q in range(sites):
+        r = q if site_row is None else int(site_row[q])
+        if r < 0:
+            continue
         m = p[:, q] != 0
         if m.any():
-            z1[m] += embed[q, p[m, q] - 1]
+            z1[m] += embed[r, p[m, q] - 1]
     h1 = bf16(gelu(z1))
     z2 = f32(h1.astype(np.float64) @ w2.astype(np.float64)) + b2[None, :]
     h2 = gelu(z2)

@@ -35,6 +35,10 @@ struct ps_scorer {
     int device = 0;
     int nq = 0;
     int W = 1;
+    int num_sites = 0;     // qubits of the sums it scores (nq unless a site map is set)
+    int key_W = 1;         // their width
+    Buf site_map;          // int16 embedding row per site (set by ps_scorer_set_site_map)
+    bool mapped = false;
     int sms = 148;
     ps_scorer_config cfg{};
     ScorerLayout L{};
@@ -85,6 +89,16 @@ struct ps_sum {
     Buf up_x, up_z, up_c, up_k, up_v0, up_v1, up_c0, up_st;  // ingest / readout staging, grow-only
     LevelList* levels = nullptr;  // host scratch
     KernelProf prof;
+    // Light-cone skip: `support` holds a superset of the qubits any term touches (exact after an
+    // upload, widened by each layer's support), and keep_clean says every term already passed
+    // the keep program clean_keep.  A layer whose support misses `support` and which maps the
+    // identity pattern to itself with amplitude 1 leaves every term as it is; with the same keep
+    // program it changes nothing and is skipped.
+    uint64_t support[4] = {0, 0, 0, 0};
+    bool support_known = false;
+    bool keep_clean = false;
+    uint64_t layers_skipped = 0;
+    KeepProg clean_keep{};
     long long fault_oom_after = -1;   // failure injection: allocations left before all fail
     bool fault_stall = false;         // failure injection: next merge skips its first tile
     unsigned long long stall_limit = 0;  // ... and its output-offset waits give up after this many polls
@@ -834,6 +848,18 @@ void to_gen_layer(const ps_table& t, GenLayer<W, T>& G) {
     }
 }
 
+// The qubits a table acts on, as W words (its generator for a wide rotation).
+template <int W>
+void table_support(const ps_table& t, uint64_t (&out)[W]) {
+    for (int w = 0; w < W; ++w) out[w] = 0;
+    if (t.mode == PS_TABLE_ROTATION) {
+        for (int w = 0; w < W; ++w) out[w] = t.gen_x[w] | t.gen_z[w];
+        return;
+    }
+    for (int j = 0; j < t.k && j < 2; ++j)
+        if (t.qubits[j] < 64u * W) out[t.qubits[j] / 64] |= 1ull << (t.qubits[j] % 64);
+}
+
 // ---------------------------------------------------------------------------
 // per-width / per-dtype operations
 // ---------------------------------------------------------------------------
@@ -868,6 +894,38 @@ struct Engine {
     }
 
     static uint64_t* K(ps_sum* s, int w) { return static_cast<uint64_t*>(s->keys[w].p); }
+
+    // Can this layer be skipped (see ps_sum::support)?  identity0: the table maps the identity
+    // pattern to itself alone with amplitude 1.
+    static bool skippable(const ps_sum* s, const uint64_t (&lsup)[W], const KeepProg& keep, bool identity0) {
+        if (!identity0 || !s->support_known || !s->keep_clean || s->slotted) return false;
+        if (std::memcmp(&keep, &s->clean_keep, sizeof keep) != 0) return false;
+        for (int w = 0; w < W; ++w)
+            if (lsup[w] & s->support[w]) return false;
+        return true;
+    }
+    // A layer ran with keep program `keep`: every term passed it; the support grows by the
+    // layer's own (partner rows live on it).
+    static void layer_done(ps_sum* s, const uint64_t (&lsup)[W], const KeepProg& keep, bool widens) {
+        s->keep_clean = true;
+        s->clean_keep = keep;
+        if (widens)
+            for (int w = 0; w < W; ++w) s->support[w] |= lsup[w];
+    }
+    static void skipped(ps_sum* s, ps_layer_stats* stats, int path) {
+        if (s->hist_ready) {
+            cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+            s->hist_ready = false;
+        }
+        if (stats) {
+            stats->terms_in = s->n;
+            stats->partners = 0;
+            stats->terms_out = s->n;
+            stats->terms_after_passes = s->n;
+            stats->path = path;
+        }
+        ++s->layers_skipped;
+    }
     static T* C(ps_sum* s, int w) { return static_cast<T*>(s->coef[w].p); }
 
     static ps_status upload(ps_sum* s, const uint64_t* x, const uint64_t* z, const double* c, uint64_t n) {
@@ -876,6 +934,9 @@ struct Engine {
         if (n == 0) {
             s->n = 0;
             s->slotted = false;
+            for (int w = 0; w < W; ++w) s->support[w] = 0;
+            s->support_known = true;
+            s->keep_clean = false;
             return PS_OK;
         }
         cudaError_t e = cudaSuccess;
@@ -891,8 +952,15 @@ struct Engine {
         e = StoreOps<W, T>::pack((uint64_t*)s->up_x.p, (uint64_t*)s->up_z.p, (double*)s->up_c.p, n, (uint32_t)s->nq,
                                  K(s, spare), C(s, spare), (uint32_t*)s->up_v0.p, s->ctl, s->sms, s->stream, &s->prof);
         if (e != cudaSuccess) return cuda_fail(s, e, "upload: pack");
-        ps_status fs = check_device_flags(s, "upload");
+        s->support_known = false;
+        s->keep_clean = false;
+        e = cudaMemcpyAsync(s->hcount + 48, &s->ctl->support[0], sizeof(s->ctl->support), cudaMemcpyDeviceToHost,
+                            s->stream);
+        if (e != cudaSuccess) return cuda_fail(s, e, "upload: support");
+        ps_status fs = check_device_flags(s, "upload");  // synchronizes: the support words have landed
         if (fs != PS_OK) return fs;
+        for (int w = 0; w < W; ++w) s->support[w] = s->hcount[48 + w];
+        s->support_known = true;
         bool sorted = false;
         e = StoreOps<W, T>::check_sorted(K(s, spare), C(s, spare), n, s->ctl, s->hcount, &sorted, s->sms, s->stream,
                                          &s->prof);
@@ -993,7 +1061,18 @@ struct Engine {
         bool general = false;
         ps = to_rot_layer<W, T>(t, a.L, *s->levels, why, &general);
         if (ps != PS_OK) return set_err(s, ps, why);
-        if (general) return apply_general(s, t, keep, policy, stats);
+        uint64_t lsup[W];
+        table_support<W>(t, lsup);
+        if (general) return apply_general(s, t, keep, policy, stats, lsup);
+        {
+            // a commuting term keeps c exactly on the wide path; a local table must leave the
+            // identity pattern alone
+            const bool identity0 = a.L.wide || ((T)a.L.a1[0] == T(0) && (T)a.L.a0[0] == T(1));
+            if (skippable(s, lsup, keep, identity0)) {
+                skipped(s, stats, a.L.partners ? PS_PATH_ROTATION : PS_PATH_RESCALE);
+                return PS_OK;
+            }
+        }
         const uint64_t n = s->n;
         if (n >= (1ull << 31) - 1) return set_err(s, PS_ERR_UNSUPPORTED, "apply: at most 2^31 - 2 terms");
         const int spare = 1 - s->cur;
@@ -1086,16 +1165,26 @@ struct Engine {
         s->slotted = slotted;
         s->live_n = out_n;
         s->slot_rows = slotted ? merge_slot_rows<W>() : 0u;
+        layer_done(s, lsup, keep, a.L.partners != 0);
         return PS_OK;
     }
 
     // The sort path: branch records, LSD radix sort of (key, record index), run-summing dedup
     // with the keep program (apply_layer_body's general tables, engine/gpu/layer.rs:614-763).
     static ps_status apply_general(ps_sum* s, const ps_table& t, const KeepProg& keep, const ps_policy* policy,
-                                   ps_layer_stats* stats) {
+                                   ps_layer_stats* stats, const uint64_t (&lsup)[W]) {
         (void)policy;
         GenLayer<W, T> G;
         to_gen_layer<W, T>(t, G);
+        {
+            bool identity0 = G.cnt[0] == 1 && G.amp[0][0] == T(1);
+            for (int w = 0; identity0 && w < W; ++w)
+                identity0 = G.mx[G.ent[0][0]][w] == 0 && G.mz[G.ent[0][0]][w] == 0;
+            if (skippable(s, lsup, keep, identity0)) {
+                skipped(s, stats, PS_PATH_SORT);
+                return PS_OK;
+            }
+        }
         const uint64_t n = s->n;
         if (s->hist_ready) {
             cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
@@ -1150,6 +1239,7 @@ struct Engine {
         }
         s->cur = spare;
         s->n = out_n;
+        layer_done(s, lsup, keep, true);
         return PS_OK;
     }
 
@@ -1287,6 +1377,7 @@ struct Engine {
         s->cur = spare;
         s->n = out_n;
         ++s->collapses;
+        s->keep_clean = false;  // the drawn terms carry new coefficients
         return PS_OK;
     }
 
@@ -1349,6 +1440,7 @@ struct Engine {
         A.nq = sc->nq;
         for (int f = 0; f < 3; ++f) A.fscale[f] = sc->cfg.feature_scale[f];
         A.residual = sc->cfg.residual ? 1 : 0;
+        A.site_row = sc->mapped ? static_cast<const int16_t*>(sc->site_map.p) : nullptr;
         ScoreInput in{};
         in.keys = K(s, s->cur);
         in.coef64 = std::is_same<T, double>::value ? (const double*)C(s, s->cur) : nullptr;
@@ -1612,7 +1704,12 @@ ps_status ps_propagate(ps_sum* s, const ps_channel* channels, uint64_t num_chann
     for (uint64_t li = 0; li < num_channels; ++li) {
         ps_layer_stats ls;
         rs.total_terms_in += s->n;
+        const uint64_t skipped0 = s->layers_skipped, n_in = s->n;
         ps = ps_apply_layer(s, &tables[li], policy, &ls);
+        if (s->layers_skipped != skipped0) {
+            ++rs.layers_skipped;
+            rs.skipped_terms_in += n_in;
+        }
         s->pass_call = li;  // CollapseSample's pass index of this layer
         if (ps == PS_OK) ps = ps_finalize_layer(s, policy);
         s->pass_call = 0;
@@ -1725,6 +1822,8 @@ ps_status ps_scorer_create(int32_t device, const ps_scorer_config* cfg, ps_score
     sc->device = device;
     sc->nq = cfg->num_qubits;
     sc->W = width_for(cfg->num_qubits);
+    sc->num_sites = sc->nq;
+    sc->key_W = sc->W;
     sc->cfg = *cfg;
     sc->L = scorer_layout(sc->nq);
     cudaDeviceGetAttribute(&sc->sms, cudaDevAttrMultiProcessorCount, device);
@@ -1787,7 +1886,7 @@ ps_status ps_scorer_destroy(ps_scorer* sc) {
     DeviceGuard g(sc->device);
     if (sc->stream) cudaStreamSynchronize(sc->stream);
     for (Buf* b : {&sc->master, &sc->bf, &sc->grads, &sc->m, &sc->v, &sc->keys, &sc->logc, &sc->rem, &sc->target,
-                   &sc->h1, &sc->gz1, &sc->dz2, &sc->scores, &sc->loss})
+                   &sc->h1, &sc->gz1, &sc->dz2, &sc->scores, &sc->loss, &sc->site_map})
         release(*b);
     if (sc->ctl) cudaFree(sc->ctl);
     sc->prof.destroy();
@@ -1827,20 +1926,22 @@ ps_status scorer_flags(ps_scorer* sc, const char* where) {
     return scorer_fail(sc, (flags[0] & ERR_TIMEOUT) ? PS_ERR_TIMEOUT : PS_ERR_DEVICE, msg);
 }
 
-ScorerArgs scorer_args(const ps_scorer* sc) {
+// inference: the site map applies; training (inference = false): always the identity
+ScorerArgs scorer_args(const ps_scorer* sc, bool inference) {
     ScorerArgs A;
     A.p = static_cast<const uint16_t*>(sc->bf.p);
     A.L = sc->L;
     A.nq = sc->nq;
     for (int f = 0; f < 3; ++f) A.fscale[f] = sc->cfg.feature_scale[f];
     A.residual = sc->cfg.residual ? 1 : 0;
+    A.site_row = inference && sc->mapped ? static_cast<const int16_t*>(sc->site_map.p) : nullptr;
     return A;
 }
 
 // Host feature arrays of n terms into the scorer's staging buffers.
 cudaError_t scorer_stage(ps_scorer* sc, const uint64_t* keys, const float* logc, const float* rem, const float* target,
-                         uint64_t n) {
-    const size_t kb = (size_t)n * 16 * sc->W;
+                         uint64_t n, int key_W = 0) {
+    const size_t kb = (size_t)n * 16 * (key_W ? key_W : sc->W);
     cudaError_t e = ensure(sc->keys, kb ? kb : 16);
     if (e == cudaSuccess) e = ensure(sc->logc, n * 4 + 16);
     if (e == cudaSuccess) e = ensure(sc->rem, n * 4 + 16);
@@ -1864,7 +1965,7 @@ cudaError_t scorer_batch(ps_scorer* sc, uint64_t offset, uint64_t nb) {
     TrainScratch S{static_cast<uint16_t*>(sc->h1.p), static_cast<uint16_t*>(sc->gz1.p),
                    static_cast<uint16_t*>(sc->dz2.p)};
     const float* tgt = static_cast<const float*>(sc->target.p) + offset;
-    const ScorerArgs A = scorer_args(sc);
+    const ScorerArgs A = scorer_args(sc, false);
     float* grads = static_cast<float*>(sc->grads.p);
     float* loss = static_cast<float*>(sc->loss.p);
     switch (sc->W) {
@@ -1906,7 +2007,7 @@ ps_status ps_scorer_score(ps_scorer* sc, const uint64_t* keys, const float* logc
                           float* out) {
     if (!sc || (n && (!keys || !logc || !rem || !out))) return PS_ERR_INVALID;
     DeviceGuard g(sc->device);
-    cudaError_t e = scorer_stage(sc, keys, logc, rem, nullptr, n);
+    cudaError_t e = scorer_stage(sc, keys, logc, rem, nullptr, n, sc->key_W);
     if (e == cudaSuccess) e = ensure(sc->scores, n * 4 + 16);
     if (e != cudaSuccess) return scorer_cuda(sc, e, "score: staging");
     if (!n) return PS_OK;
@@ -1915,9 +2016,9 @@ ps_status ps_scorer_score(ps_scorer* sc, const uint64_t* keys, const float* logc
     in.logc = static_cast<const float*>(sc->logc.p);
     in.rem = static_cast<const float*>(sc->rem.p);
     in.n = n;
-    const ScorerArgs A = scorer_args(sc);
+    const ScorerArgs A = scorer_args(sc, true);
     float* sco = static_cast<float*>(sc->scores.p);
-    switch (sc->W) {
+    switch (sc->key_W) {
     case 1: e = launch_score<1>(A, in, sco, nullptr, nullptr, sc->ctl, sc->sms, sc->stream, &sc->prof); break;
     case 2: e = launch_score<2>(A, in, sco, nullptr, nullptr, sc->ctl, sc->sms, sc->stream, &sc->prof); break;
     default: e = launch_score<4>(A, in, sco, nullptr, nullptr, sc->ctl, sc->sms, sc->stream, &sc->prof); break;
@@ -1933,6 +2034,7 @@ ps_status ps_scorer_score(ps_scorer* sc, const uint64_t* keys, const float* logc
 ps_status ps_scorer_gradients(ps_scorer* sc, const uint64_t* keys, const float* logc, const float* rem,
                               const float* target, uint64_t n, float* grads_out, float* loss) {
     if (!sc || !n || n > 65536 || !keys || !logc || !rem || !target || !grads_out) return PS_ERR_INVALID;
+    if (sc->mapped) return scorer_fail(sc, PS_ERR_INVALID, "gradients: clear the site map first (training rows use the embedding rows' own qubits)");
     DeviceGuard g(sc->device);
     cudaError_t e = scorer_stage(sc, keys, logc, rem, target, n);
     if (e == cudaSuccess) e = scorer_train_scratch(sc, n);
@@ -1957,6 +2059,7 @@ ps_status ps_scorer_train(ps_scorer* sc, const uint64_t* keys, const float* logc
                           uint64_t n, int32_t epochs, int32_t batch, float lr, float* epoch_loss) {
     if (!sc || !n || !keys || !logc || !rem || !target || epochs < 1 || batch < 1 || batch > 65536 || !(lr > 0.f))
         return PS_ERR_INVALID;
+    if (sc->mapped) return scorer_fail(sc, PS_ERR_INVALID, "train: clear the site map first (training rows use the embedding rows' own qubits)");
     DeviceGuard g(sc->device);
     const int K = 2 * sc->W;
     std::vector<uint64_t> pk((size_t)n * K);
@@ -2004,10 +2107,46 @@ ps_status ps_scorer_train(ps_scorer* sc, const uint64_t* keys, const float* logc
     return PS_OK;
 }
 
+ps_status ps_scorer_set_site_map(ps_scorer* sc, int32_t num_sites, const int32_t* row_of_site) {
+    if (!sc) return PS_ERR_INVALID;
+    DeviceGuard g(sc->device);
+    if (num_sites == 0 || !row_of_site) {
+        sc->mapped = false;
+        sc->num_sites = sc->nq;
+        sc->key_W = sc->W;
+        return PS_OK;
+    }
+    if (num_sites < 1 || num_sites > 256) return scorer_fail(sc, PS_ERR_INVALID, "set_site_map: 1 to 256 sites");
+    std::vector<int16_t> rows(num_sites);
+    for (int q = 0; q < num_sites; ++q) {
+        if (row_of_site[q] < -1 || row_of_site[q] >= sc->nq)
+            return scorer_fail(sc, PS_ERR_INVALID, "set_site_map: site " + std::to_string(q) + " maps outside the embedding rows");
+        rows[q] = (int16_t)row_of_site[q];
+    }
+    const int kw = width_for(num_sites);
+    cudaError_t e = ensure(sc->site_map, (size_t)num_sites * sizeof(int16_t) + 16);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(sc->site_map.p, rows.data(), (size_t)num_sites * sizeof(int16_t), cudaMemcpyHostToDevice,
+                            sc->stream);
+    if (e == cudaSuccess) {
+        switch (kw) {
+        case 1: e = configure_scorer_kernels<1>(); break;
+        case 2: e = configure_scorer_kernels<2>(); break;
+        default: e = configure_scorer_kernels<4>(); break;
+        }
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sc->stream);
+    if (e != cudaSuccess) return scorer_cuda(sc, e, "set_site_map");
+    sc->mapped = true;
+    sc->num_sites = num_sites;
+    sc->key_W = kw;
+    return PS_OK;
+}
+
 ps_status ps_set_scorer(ps_sum* s, ps_scorer* sc, double remaining_layers) {
     if (!s) return PS_ERR_INVALID;
-    if (sc && (sc->device != s->device || sc->nq != s->nq))
-        return set_err(s, PS_ERR_INVALID, "set_scorer: the scorer was built for another device or qubit count");
+    if (sc && (sc->device != s->device || sc->num_sites != s->nq))
+        return set_err(s, PS_ERR_INVALID, "set_scorer: the scorer was built (or site-mapped) for another device or qubit count");
     s->scorer = sc;
     s->scorer_remaining = remaining_layers;
     return PS_OK;

@@ -34,6 +34,7 @@ struct Ctl {
     unsigned int err_info;         // id of the first check that failed
     unsigned long long aux[8];     // small per-pass values (TopN boundary, quota, ...)
     unsigned long long spin_limit; // polls before a bounded device wait gives up
+    unsigned long long support[4]; // ingest: OR of every key's x | z words (the qubits any term touches)
 };
 
 // Lowered keep program (postfix), KeepProgram in the reference's device path.

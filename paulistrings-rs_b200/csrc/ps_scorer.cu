@@ -16,6 +16,7 @@
 //
 // Every mbarrier wait is bounded; a block whose wait gives up records ERR_TIMEOUT, stops
 // issuing, frees its TMEM and returns.
+#include <algorithm>
 #include <cuda_bf16.h>
 
 #include "ps_device.cuh"
@@ -45,10 +46,10 @@ __device__ __forceinline__ uint32_t kmaj_off(int row, int k) {
     return (uint32_t)((row >> 3) * 2048 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
 }
 
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t sbo = 2048u) {
     uint64_t d = (uint64_t)((saddr & 0x3FFFFu) >> 4);  // start address, bits 0-13
     d |= (uint64_t)(128u >> 4) << 16;                   // leading byte offset, bits 16-29
-    d |= (uint64_t)(2048u >> 4) << 32;                  // stride byte offset, bits 32-45
+    d |= (uint64_t)(sbo >> 4) << 32;                    // stride byte offset, bits 32-45
     d |= (uint64_t)1 << 46;                             // descriptor version 1 (sm_100)
     return d;                                           // base offset 0, no swizzle
 }
@@ -101,16 +102,24 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// GELU, tanh form, and its derivative.
+// GELU, tanh form (Hendrycks & Gimpel 2016), and its derivative.  tanh is the hardware's
+// single-instruction approximation (PTX tanh.approx.f32, maximum relative error about 2^-11):
+// one SFU operation per hidden unit instead of a libm evaluation, which was the scorer's
+// bottleneck; the network's inputs and weights are bf16, so 2^-11 is below their rounding.
 constexpr float kGeluS = 0.7978845608028654f;  // sqrt(2 / pi)
 constexpr float kGeluA = 0.044715f;
+__device__ __forceinline__ float tanh_hw(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
 __device__ __forceinline__ float gelu(float x) {
-    const float t = tanhf(kGeluS * (x + kGeluA * x * x * x));
+    const float t = tanh_hw(kGeluS * (x + kGeluA * x * x * x));
     return 0.5f * x * (1.0f + t);
 }
 __device__ __forceinline__ float gelu_grad(float x) {
     const float x2 = x * x;
-    const float t = tanhf(kGeluS * (x + kGeluA * x2 * x));
+    const float t = tanh_hw(kGeluS * (x + kGeluA * x2 * x));
     return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * kGeluS * (1.0f + 3.0f * kGeluA * x2);
 }
 
@@ -189,7 +198,8 @@ __device__ __forceinline__ void z1_chunk(const ScorerArgs& A, const uint64_t (&k
         while (live) {
             const int bit = __ffsll((long long)live) - 1;
             live &= live - 1;
-            const int q = 64 * w + bit;
+            const int q = A.site_row ? (int)A.site_row[64 * w + bit] : 64 * w + bit;
+            if (q < 0) continue;
             const int p = (int)((k[w] >> bit) & 1u) | ((int)((k[W + w] >> bit) & 1u) << 1);
             float e[32];
             load_bf16x32(A.p + A.L.embed + ((size_t)q * 3 + (size_t)(p - 1)) * kHid + 32 * c, e);
@@ -535,6 +545,225 @@ __global__ void __launch_bounds__(kScoreThreads) k_train_bwd(const ScorerArgs A,
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// inference on the tensor cores (scorers of at most kTcRows embedding rows)
+//
+// Both layers are GEMMs per tile of 128 terms.  Layer 1: the tile's one-hot operand A1
+// (128 terms x K1, K1 = 3 kTcRows + 16: the count of each (row, X/Z/Y) among the term's
+// non-identity qubits, then the three scalar features each split into a bf16 high and low part,
+// then a 1 for the bias) times B1 (128 hidden x K1: the embedding rows, the feature columns u
+// twice, b1) gives z1 = b1 + f.u + the embedding bag, accumulated in f32 in TMEM.  The counts are
+// small integers and the split features carry 16 significant bits, so the product equals the
+// CUDA-core embedding bag up to the order of f32 additions.  Layer 2 is the 128 x 128 GEMM of the
+// other kernel.  A CTA holds two warpgroups, each owning one tile at a time (its own operand,
+// mbarrier and 128 TMEM columns, shared by the two accumulators in turn) and synchronising on its
+// own named barrier, so one warpgroup's GELUs overlap the other's MMAs.
+// ---------------------------------------------------------------------------
+constexpr int kK1 = 3 * kTcRows + 16;
+constexpr uint32_t kK1Sbo = (uint32_t)(kK1 / 8) * 128u;     // bytes between 8-row groups (K1 wide)
+constexpr uint32_t kOpA1Bytes = (uint32_t)kScoreTile * kK1 * 2u;
+constexpr uint32_t kOpB1Bytes = (uint32_t)kHid * kK1 * 2u;
+constexpr int kTcThreads = 256;
+constexpr size_t kTcSmem = kOpB1Bytes + kTileBytes + 2 * (size_t)kOpA1Bytes + 2 * kHid * sizeof(float) +
+                           kTopnBins1 * sizeof(unsigned int);
+
+// Byte offset of element (row, k) of a K1-wide K-major operand (core matrix (row / 8, k / 8)).
+__device__ __forceinline__ uint32_t kmaj1_off(int row, int k) {
+    return (uint32_t)((row >> 3) * kK1Sbo + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+// Named barrier over one warpgroup (ids 1 and 2; 0 is __syncthreads).
+__device__ __forceinline__ void wg_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+__device__ __forceinline__ bool wg_and(int id, bool v) {
+    uint32_t out;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(out)
+        : "r"(v ? 1u : 0u), "r"(id)
+        : "memory");
+    return out != 0;
+}
+
+// D (TMEM) = A (128 x K1) * B1^T: K1 / 16 MMAs, each 2 core matrices (256 bytes) further along K.
+__device__ __forceinline__ void umma_tile_k1(uint32_t d_tmem, uint32_t a_saddr, uint32_t b_saddr) {
+    const uint64_t ad = umma_desc(a_saddr, kK1Sbo), bd = umma_desc(b_saddr, kK1Sbo);
+#pragma unroll
+    for (int j = 0; j < kK1 / 16; ++j) {
+        const uint32_t acc = j > 0 ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(d_tmem), "l"(ad + 16ull * j), "l"(bd + 16ull * j), "r"(kIdesc), "r"(acc));
+    }
+}
+
+__device__ __forceinline__ void split_bf16(float v, uint16_t& hi, uint16_t& lo) {
+    hi = f2bf(v);
+    lo = f2bf(v - bf2f(hi));
+}
+
+template <int W>
+__global__ void __launch_bounds__(kTcThreads, 1) k_score_tc(const ScorerArgs A, const ScoreInput in,
+                                                            float* __restrict__ scores, uint64_t* __restrict__ sel,
+                                                            unsigned int* __restrict__ hist, Ctl* ctl) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint8_t* sB1 = smem;
+    uint8_t* sB2 = smem + kOpB1Bytes;
+    float* s_b2 = reinterpret_cast<float*>(smem + kOpB1Bytes + kTileBytes + 2 * (size_t)kOpA1Bytes);
+    float* s_w3 = s_b2 + kHid;
+    unsigned int* s_hist = reinterpret_cast<unsigned int*>(s_w3 + kHid);
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ uint32_t s_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int g = tid >> 7, t = tid & 127;  // warpgroup, row of its tile
+    uint8_t* sA = smem + kOpB1Bytes + kTileBytes + (size_t)g * kOpA1Bytes;
+
+    // B1 (hidden n, input column k): embedding rows, u (twice: high and low feature parts), b1
+    for (int i = tid; i < kHid * kK1; i += kTcThreads) {
+        const int k = i / kHid, n = i % kHid;  // n fastest: the global reads are contiguous
+        uint16_t v = 0;
+        if (k < 3 * kTcRows) {
+            if (k / 3 < A.nq) v = A.p[A.L.embed + (size_t)k * kHid + n];  // embed[q][p][n], k = 3 q + p
+        } else if (k < 3 * kTcRows + 6) {
+            v = A.p[A.L.u + (size_t)((k - 3 * kTcRows) >> 1) * kHid + n];
+        } else if (k == 3 * kTcRows + 6) {
+            v = A.p[A.L.b1 + n];
+        }
+        *reinterpret_cast<uint16_t*>(sB1 + kmaj1_off(n, k)) = v;
+    }
+    stage_w2(A, sB2, true);
+    for (int i = tid; i < kHid; i += kTcThreads) {
+        s_b2[i] = bf2f(A.p[A.L.b2 + i]);
+        s_w3[i] = bf2f(A.p[A.L.w3 + i]);
+    }
+    if (hist)
+        for (int i = tid; i < kTopnBins1; i += kTcThreads) s_hist[i] = 0;
+    const float b3 = bf2f(A.p[A.L.b3]);
+    if (tid == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+    }
+    if (warp == 0) tmem_alloc(&s_tmem, 2 * kHid);
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem + (uint32_t)(g * kHid);           // this warpgroup's columns
+    const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;  // its warp's TMEM lanes
+    const int bar_id = 1 + g;
+
+    const uint64_t ntiles = (in.n + kScoreTile - 1) / kScoreTile;
+    uint32_t phase = 0;
+    for (uint64_t tile = 2 * (uint64_t)blockIdx.x + g; tile < ntiles; tile += 2 * (uint64_t)gridDim.x) {
+        const uint64_t row = tile * kScoreTile + t;
+        const bool valid = row < in.n;
+        uint64_t k[2 * W];
+        float f[3];
+        const float logc = term_features<W>(A, in, row, valid, k, f);
+        // A1 row t: zeros, the split scalar features and the bias column, then the counts
+        {
+            const uint4 zero = make_uint4(0, 0, 0, 0);
+#pragma unroll
+            for (int c = 0; c < 3 * kTcRows / 8; ++c) *reinterpret_cast<uint4*>(sA + kmaj1_off(t, 8 * c)) = zero;
+            uint16_t h0, l0, h1, l1, h2, l2;
+            split_bf16(f[0], h0, l0);
+            split_bf16(f[1], h1, l1);
+            split_bf16(f[2], h2, l2);
+            const uint16_t one = valid ? f2bf(1.0f) : 0;
+            *reinterpret_cast<uint4*>(sA + kmaj1_off(t, 3 * kTcRows)) =
+                make_uint4((uint32_t)h0 | (uint32_t)l0 << 16, (uint32_t)h1 | (uint32_t)l1 << 16,
+                           (uint32_t)h2 | (uint32_t)l2 << 16, (uint32_t)one);
+            *reinterpret_cast<uint4*>(sA + kmaj1_off(t, 3 * kTcRows + 8)) = zero;
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+                uint64_t live = k[w] | k[W + w];
+                while (live) {
+                    const int bit = __ffsll((long long)live) - 1;
+                    live &= live - 1;
+                    const int r = A.site_row ? (int)A.site_row[64 * w + bit] : 64 * w + bit;
+                    if (r < 0 || r >= kTcRows) continue;
+                    const int p = (int)((k[w] >> bit) & 1u) | ((int)((k[W + w] >> bit) & 1u) << 1);
+                    uint16_t* e = reinterpret_cast<uint16_t*>(sA + kmaj1_off(t, 3 * r + p - 1));
+                    *e = f2bf(bf2f(*e) + 1.0f);
+                }
+            }
+        }
+        fence_async_smem();
+        tc_fence_before();
+        wg_sync(bar_id);
+        if (t == 0) {
+            tc_fence_after();
+            umma_tile_k1(tmem, smem_u32(sA), smem_u32(sB1));
+            umma_commit(&s_bar[g]);
+        }
+        bool ok = wg_and(bar_id, mbar_wait(&s_bar[g], phase, ctl, 905));
+        phase ^= 1u;
+        if (!ok) {
+            mbar_drain(&s_bar[g], phase ^ 1u);
+            break;
+        }
+        tc_fence_after();
+        // GELU(z1) as the layer-2 operand, over the dead A1 (128-wide K-major layout)
+#pragma unroll 1
+        for (int c = 0; c < kHid / 32; ++c) {
+            float z[32];
+            tmem_ld32(tmem + lane_base + 32u * c, z);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) z[j] = gelu(z[j]);
+            store_row_chunk(sA, t, c, z);
+        }
+        fence_async_smem();
+        tc_fence_before();
+        wg_sync(bar_id);
+        if (t == 0) {
+            tc_fence_after();
+            umma_tile(tmem, smem_u32(sA), smem_u32(sB2), false);
+            umma_commit(&s_bar[g]);
+        }
+        ok = wg_and(bar_id, mbar_wait(&s_bar[g], phase, ctl, 906));
+        phase ^= 1u;
+        if (!ok) {
+            mbar_drain(&s_bar[g], phase ^ 1u);
+            break;
+        }
+        tc_fence_after();
+        float y = b3;
+#pragma unroll 1
+        for (int c = 0; c < kHid / 32; ++c) {
+            float z2[32];
+            tmem_ld32(tmem + lane_base + 32u * c, z2);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) y += gelu(z2[j] + s_b2[32 * c + j]) * s_w3[32 * c + j];
+        }
+        if (A.residual) y += logc;
+        if (valid) {
+            if (scores) scores[row] = y;
+            if (sel) {
+                const uint64_t sk = score_select_key(y);
+                sel[row] = sk;
+                if (hist) atomicAdd(&s_hist[sk >> 52], 1u);
+            }
+        }
+        tc_fence_before();
+        wg_sync(bar_id);  // every lane has read the accumulator and left A before the next tile
+    }
+    __syncthreads();
+    if (hist)
+        for (int i = tid; i < kTopnBins1; i += kTcThreads)
+            if (s_hist[i]) atomicAdd(&hist[i], s_hist[i]);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(s_tmem, 2 * kHid);
+    }
+}
+
 __global__ void k_adam(float* __restrict__ master, uint16_t* __restrict__ bf, float* __restrict__ g,
                        float* __restrict__ m, float* __restrict__ v, size_t count, float lr, float b1, float b2,
                        float eps, float c1, float c2) {
@@ -571,6 +800,8 @@ template <int W>
 cudaError_t configure_scorer_kernels() {
     cudaError_t e = cudaFuncSetAttribute(k_score<W, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScoreSmem);
     if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_score_tc<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+    if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_score<W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScoreSmem);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_train_bwd<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdSmem);
@@ -584,10 +815,17 @@ cudaError_t launch_score(const ScorerArgs& A, const ScoreInput& in, float* score
     // 2 x (128 x 128) bf16 GEMM flops per term plus the output dot; bytes: key + coefficient
     prof->begin(K_SCORE, (double)in.n * (16 * W + 8 + (sel_keys ? 8 : 4)), st);
     TrainScratch none{nullptr, nullptr, nullptr};
-    // three blocks per SM: 3 x 128 TMEM columns and 3 x ~75 KB of shared memory fit one SM
-    k_score<W, false><<<score_grid(in.n, sms, 3), kScoreThreads, kScoreSmem, st>>>(A, in, scores, sel_keys, hist,
-                                                                                  nullptr, 0.0f, none, nullptr,
-                                                                                  nullptr, ctl);
+    if (A.nq <= kTcRows) {
+        // one CTA per SM (~200 KB of shared memory, 256 TMEM columns), two tiles in flight per CTA
+        const uint64_t tiles = (in.n + kScoreTile - 1) / kScoreTile;
+        const unsigned int grid = (unsigned int)std::min<uint64_t>((tiles + 1) / 2, (uint64_t)(sms > 0 ? sms : 1));
+        k_score_tc<W><<<grid, kTcThreads, kTcSmem, st>>>(A, in, scores, sel_keys, hist, ctl);
+    } else {
+        // three blocks per SM: 3 x 128 TMEM columns and 3 x ~75 KB of shared memory fit one SM
+        k_score<W, false><<<score_grid(in.n, sms, 3), kScoreThreads, kScoreSmem, st>>>(A, in, scores, sel_keys, hist,
+                                                                                      nullptr, 0.0f, none, nullptr,
+                                                                                      nullptr, ctl);
+    }
     prof->end(st);
     return cudaGetLastError();
 }

@@ -42,10 +42,16 @@ inline ScorerLayout scorer_layout(int nq) {
 struct ScorerArgs {
     const uint16_t* p;        // bf16 parameters (device)
     ScorerLayout L;
-    int nq;
+    int nq;                   // embedding rows
     float fscale[3];          // feature scales: weight, log|c|, remaining depth
     int residual;             // scores = log|c| + output
+    const int16_t* site_row;  // inference: embedding row of each qubit of the scored sums (-1: none);
+                              // nullptr: qubit q uses row q
 };
+
+// Embedding rows the tensor-core inference kernel holds in its one-hot operand: scorers with at
+// most this many rows (after a site map, any number of qubits) score on the tensor cores.
+constexpr int kTcRows = 64;
 
 // Per-term features: the key, and log|c| from a coefficient column (coef64 / coef32) or an
 // array (logc); the remaining depth uniform (rem_uniform) or from an array (rem).

@@ -60,6 +60,9 @@ template <int W, typename T>
 __global__ void k_pack(const uint64_t* __restrict__ x, const uint64_t* __restrict__ z, const double* __restrict__ c,
                        uint64_t n, uint32_t num_qubits, uint64_t* __restrict__ keys, T* __restrict__ coef,
                        uint32_t* __restrict__ vals, Ctl* ctl) {
+    uint64_t sup[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) sup[w] = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t k[2 * W];
         uint64_t leak = 0;
@@ -67,6 +70,7 @@ __global__ void k_pack(const uint64_t* __restrict__ x, const uint64_t* __restric
         for (int w = 0; w < W; ++w) {
             k[w] = x[i * W + w];
             k[W + w] = z[i * W + w];
+            sup[w] |= k[w] | k[W + w];
             uint32_t first = 64u * w;
             uint64_t live = num_qubits >= first + 64 ? ~0ull : (num_qubits <= first ? 0ull : ((1ull << (num_qubits - first)) - 1));
             leak |= (k[w] | k[W + w]) & ~live;
@@ -75,6 +79,14 @@ __global__ void k_pack(const uint64_t* __restrict__ x, const uint64_t* __restric
         store_key<W>(keys, i, k);
         coef[i] = (T)c[i];
         vals[i] = (uint32_t)i;
+    }
+    // the union of the supports (ctl->support, cleared by the launcher), one atomic per warp and word
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+        const uint32_t lo = __reduce_or_sync(0xffffffffu, (uint32_t)sup[w]);
+        const uint32_t hi = __reduce_or_sync(0xffffffffu, (uint32_t)(sup[w] >> 32));
+        const uint64_t v = (uint64_t)hi << 32 | lo;
+        if ((threadIdx.x & 31) == 0 && v) atomicOr(&ctl->support[w], (unsigned long long)v);
     }
 }
 
@@ -814,6 +826,7 @@ template <int W, typename T>
 cudaError_t StoreOps<W, T>::pack(const uint64_t* x, const uint64_t* z, const double* c, uint64_t n, uint32_t nq,
                                  uint64_t* keys, T* coef, uint32_t* vals, Ctl* ctl, int sms, cudaStream_t st,
                                  KernelProf* prof) {
+    cudaMemsetAsync(&ctl->support[0], 0, sizeof(ctl->support), st);
     if (!n) return cudaSuccess;
     prof->begin(K_PACK, (double)n * (16 * W + 8 + 16 * W + sizeof(T) + 4), st);
     k_pack<W, T><<<grid_for(n, sms), kThreads, 0, st>>>(x, z, c, n, nq, keys, coef, vals, ctl);

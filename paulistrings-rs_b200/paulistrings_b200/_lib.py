@@ -63,6 +63,7 @@ EXPORTED = (
     "ps_scorer_score",
     "ps_scorer_gradients",
     "ps_scorer_train",
+    "ps_scorer_set_site_map",
     "ps_set_scorer",
 )
 
@@ -159,6 +160,8 @@ class RunStats(ctypes.Structure):
         ("kernel_launches", ctypes.c_uint64),
         ("device_ms", ctypes.c_double),
         ("collapses", ctypes.c_uint64),
+        ("layers_skipped", ctypes.c_uint64),
+        ("skipped_terms_in", ctypes.c_uint64),
     ]
 
 
@@ -238,6 +241,7 @@ def lib():
     L.ps_scorer_gradients.argtypes = [vp, vp, vp, vp, vp, u64, vp, vp]
     L.ps_scorer_train.argtypes = [vp, vp, vp, vp, vp, u64, i32, i32, ctypes.c_float, vp]
     L.ps_set_scorer.argtypes = [vp, vp, ctypes.c_double]
+    L.ps_scorer_set_site_map.argtypes = [vp, i32, vp]
     for name in EXPORTED:
         fn = getattr(L, name)
         if name not in ("ps_abi_version", "ps_device_count", "ps_last_error", "ps_width", "ps_num_qubits",

@@ -74,6 +74,7 @@ class Scorer:
         self.feature_scale = tuple(float(v) for v in feature_scale)
         self.layout = layout(self.num_qubits)
         self.residual = bool(residual)
+        self.num_sites, self.key_W = self.num_qubits, self.W
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -106,8 +107,8 @@ class Scorer:
             raise ValueError(f"expected {self.num_params} parameters")
         self._check(_lib.lib().ps_scorer_set_params(self._h, p.ctypes.data), "set_params")
 
-    def _arrays(self, keys, logc, rem, target=None):
-        keys = np.ascontiguousarray(keys, np.uint64).reshape(-1, 2 * self.W)
+    def _arrays(self, keys, logc, rem, target=None, key_W=None):
+        keys = np.ascontiguousarray(keys, np.uint64).reshape(-1, 2 * (key_W or self.W))
         n = keys.shape[0]
         logc = np.ascontiguousarray(np.broadcast_to(np.asarray(logc, np.float32), (n,)))
         rem = np.ascontiguousarray(np.broadcast_to(np.asarray(rem, np.float32), (n,)))
@@ -115,11 +116,23 @@ class Scorer:
         return keys, logc, rem, t, n
 
     def score(self, keys, logc, rem) -> np.ndarray:
-        keys, logc, rem, _, n = self._arrays(keys, logc, rem)
+        """Scores of terms of ``self.num_sites`` qubits (the site map's, if one is set)."""
+        keys, logc, rem, _, n = self._arrays(keys, logc, rem, key_W=self.key_W)
         out = np.zeros(n, np.float32)
         self._check(_lib.lib().ps_scorer_score(self._h, keys.ctypes.data, logc.ctypes.data, rem.ctypes.data, n,
                                                out.ctypes.data), "score")
         return out
+
+    def set_site_map(self, row_of_site=None) -> None:
+        """Score sums of ``len(row_of_site)`` qubits: site q adds embedding row ``row_of_site[q]``
+        (-1: not an input).  ``None`` restores the identity.  Train before mapping."""
+        if row_of_site is None:
+            self._check(_lib.lib().ps_scorer_set_site_map(self._h, 0, None), "set_site_map")
+            self.num_sites, self.key_W = self.num_qubits, self.W
+            return
+        rows = np.ascontiguousarray(row_of_site, np.int32)
+        self._check(_lib.lib().ps_scorer_set_site_map(self._h, len(rows), rows.ctypes.data), "set_site_map")
+        self.num_sites, self.key_W = len(rows), width_for(len(rows))
 
     def gradients(self, keys, logc, rem, target):
         """Gradients of mean((y - target)^2) over one batch (no update), and that loss."""
@@ -245,6 +258,69 @@ def attribution_data(observable: PauliSum, step: Circuit, steps: int, state: str
     finally:
         g.close()
     return tuple(np.concatenate(r) for r in rows)
+
+
+# ---------------------------------------------------------------------------
+# Trotter series with a readout after every step, and a scorer trained for a circuit family
+# ---------------------------------------------------------------------------
+
+def trotter_series(observable: dict, num_qubits: int, step: Circuit, steps: int, policy, dtype: str, state: str,
+                   device: int = 0) -> dict:
+    """Heisenberg propagation of ``steps`` repetitions of ``step`` from ``observable``
+    ({label: coefficient}), reading <state| O(t) |state> after every step (the reference's quench
+    protocol, docs/figures/ising-quench-convergence/quench_convergence.py:85-94).  Returns the
+    readouts (t = 0 .. steps), the wall time of the loop (propagation and readouts, the device
+    synchronised at both ends), the device time of the propagations, and term counts."""
+    import time
+
+    g = PauliSum.from_strings(observable, num_qubits=num_qubits, dtype=dtype).to_device(device)
+    layers = len(step)
+    values = [g.expectation(state)]
+    dev_ms = 0.0
+    terms_in = skipped = launches = 0
+    peak = len(g)
+    _lib.check(_lib.lib().ps_synchronize(g._h), g._h, "synchronize")
+    t0 = time.perf_counter()
+    for k in range(steps):
+        st = g.propagate(step, policy, "heisenberg", with_stats=True, remaining_layers=layers * (steps - k))
+        dev_ms += st.device_ms
+        terms_in += st.total_terms_in - st.skipped_terms_in
+        skipped += st.layers_skipped
+        launches += st.kernel_launches
+        peak = max(peak, st.peak_terms)
+        values.append(g.expectation(state))
+    wall = time.perf_counter() - t0
+    final = len(g)
+    g.close()
+    return {"values": values, "wall_s": wall, "device_ms": dev_ms, "terms_in": terms_in, "layers": layers * steps,
+            "layers_skipped": skipped, "peak_terms": peak, "final_terms": final, "gpu_launches": launches}
+
+
+def train_scorer(observable: dict, num_qubits: int, steps_for, h_values, steps: int, state: str, threshold: float,
+                 samples_per_step: int = 1024, every: int = 4, chunk: int = 256, epochs: int = 40,
+                 batch: int = 1024, lr: float = 1e-3, seed: int = 5, device: int = 0) -> tuple:
+    """A residual scorer trained on attribution rows from tight-threshold runs of the circuit
+    family ``steps_for(h)`` (one Trotter step) at each training field in ``h_values``.  Returns
+    (scorer, per-epoch losses, rows used, seconds spent on data and on training)."""
+    import time
+
+    t0 = time.perf_counter()
+    obs = PauliSum.from_strings(observable, num_qubits=num_qubits)
+    rows = [[], [], [], []]
+    for h in h_values:
+        data = attribution_data(obs, steps_for(h), steps, state, threshold, samples_per_step=samples_per_step,
+                                seed=int(round(h * 1000)), chunk=chunk, floor=1e-10, every=every,
+                                top_fraction=0.75, top_pool=1 << 16, device=device)
+        for r, a in zip(rows, data):
+            r.append(a)
+    keys, logc, rem, target = (np.concatenate(r) for r in rows)
+    t_data = time.perf_counter() - t0
+    sc = Scorer(num_qubits, layers_per_unit=len(steps_for(h_values[0])), feature_scale=(0.1, 0.1, 0.1), seed=seed,
+                residual=True, device=device)
+    t1 = time.perf_counter()
+    losses = sc.train(keys, logc, rem, target - logc, epochs=epochs, batch=batch, lr=lr)
+    t_train = time.perf_counter() - t1
+    return sc, losses, len(target), t_data, t_train
 
 
 def _score_benchmark(log2_terms: int = 22, num_qubits: int = 64) -> None:

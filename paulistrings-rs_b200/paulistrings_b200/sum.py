@@ -124,6 +124,8 @@ class PropagationStats:
     total_terms_in: int = 0
     kernel_launches: int = 0
     collapses: int = 0
+    layers_skipped: int = 0     # layers that acted only on qubits no term touched (nothing ran)
+    skipped_terms_in: int = 0   # terms entering those layers
 
 
 class GpuPauliSum:
@@ -247,6 +249,8 @@ class GpuPauliSum:
                 total_terms_in=int(rs.total_terms_in),
                 kernel_launches=int(rs.kernel_launches),
                 collapses=int(rs.collapses),
+                layers_skipped=int(rs.layers_skipped),
+                skipped_terms_in=int(rs.skipped_terms_in),
             )
         return None
 

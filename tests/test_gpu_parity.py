@@ -341,3 +341,71 @@ def test_upload_fast_path_and_fallback_agree():
     o = oracle_sum(64, dx, dz, dc)
     assert_same_terms(g2.download(), oracle_arrays(o), what="fallback")
     assert len(g2) == 9
+
+
+# --- light-cone skip: layers that act only where no term lives ---------------------------------
+
+
+def test_light_cone_layers_are_skipped_and_stay_bit_exact():
+    """The XXZ chain from Z on the middle site: most bond gates of the first steps act outside
+    the operator's support, change nothing and launch nothing; the result is the oracle's."""
+    n = 40
+    circ = workloads.xxz_chain(n, 3, Jz=0.5, dt=0.1)
+    x, z, c = labels_to_arrays({"I" * 20 + "Z" + "I" * 19: 1.0}, n)
+    g = ps.GpuPauliSum(n, "f64")
+    g.upload(x, z, c)
+    st = g.propagate(circ, truncation.coeff(1e-8), "heisenberg", with_stats=True)
+    got = g.download()
+    o = oracle_sum(n, x, z, c)
+    after = o.propagate(oracle_channels(circ), {"keep": [("coeff", 1e-8)]}, "heisenberg")
+    assert st.terms_after == [int(v) for v in after]
+    assert_same_terms(got, oracle_arrays(o), what="light-cone")
+    assert st.layers_skipped > len(circ) // 2, st.layers_skipped
+    assert g.expectation(workloads.neel_state(n)) == pytest.approx(o.expectation(workloads.neel_state(n)),
+                                                                   rel=1e-12, abs=1e-15)
+
+
+def test_first_layer_after_an_upload_is_never_skipped():
+    """Uploaded terms have not met the keep program: the first layer drops the one below the
+    threshold even though the gate acts elsewhere; the next layer, also elsewhere, is skipped."""
+    n = 16
+    labels = {"Z" + "I" * 15: 1.0, "IX" + "I" * 14: 1e-9}
+    x, z, c = labels_to_arrays(labels, n)
+    circ = ps.Circuit(n)
+    circ.pauli_rotation("XX", [10, 11], 0.3)
+    circ.pauli_rotation("YY", [12, 13], 0.3)
+    g = ps.GpuPauliSum(n, "f64")
+    g.upload(x, z, c)
+    st = g.propagate(circ, truncation.coeff(1e-8), "forward", with_stats=True)
+    assert st.terms_after == [1, 1]
+    assert st.layers_skipped == 1
+    got = g.download()
+    o = oracle_sum(n, x, z, c)
+    o.propagate(oracle_channels(circ), {"keep": [("coeff", 1e-8)]}, "forward")
+    assert_same_terms(got, oracle_arrays(o), what="first-layer")
+
+
+def test_skip_covers_noise_and_general_tables_outside_the_support():
+    """Depolarizing noise and a CNOT on qubits no term touches are skipped too; a CNOT whose
+    control is in the support is not, and the support grows by its target."""
+    n = 12
+    x, z, c = labels_to_arrays({"XZ" + "I" * 10: 0.6, "ZY" + "I" * 10: 0.8}, n)
+    circ = ps.Circuit(n)
+    circ.depolarize(1e-3, [5])
+    circ.cnot(6, 7)
+    circ.cnot(1, 8)
+    circ.pauli_rotation("XX", [8, 9], 0.4)
+    circ.depolarize(1e-3, [10])
+    g = ps.GpuPauliSum(n, "f64")
+    g.upload(x, z, c)
+    g.propagate(ps.Circuit(n), truncation.coeff(1e-12))  # nothing: the store has not met the program
+    first = ps.Circuit(n)
+    first.pauli_rotation("ZZ", [0, 1], 0.2)  # acts on the support: runs and cleans the store
+    g.propagate(first, truncation.coeff(1e-12))
+    st = g.propagate(circ, truncation.coeff(1e-12), "forward", with_stats=True)
+    assert st.layers_skipped == 3, st.layers_skipped  # depolarize(5), cnot(6, 7), depolarize(10)
+    got = g.download()
+    o = oracle_sum(n, x, z, c)
+    o.propagate(oracle_channels(first), {"keep": [("coeff", 1e-12)]}, "forward")
+    o.propagate(oracle_channels(circ), {"keep": [("coeff", 1e-12)]}, "forward")
+    assert_same_terms(got, oracle_arrays(o), what="skip-noise-general")

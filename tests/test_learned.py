@@ -104,7 +104,7 @@ def test_scored_topn_lowering():
 # ---------------------------------------------------------------------------
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("nq", [16, 64, 100])
+@pytest.mark.parametrize("nq", [16, 64, 100, 200, 256])
 def test_device_scores_match_the_reference(nq):
     W = ps.width_for(nq)
     sc = learned.Scorer(nq, layers_per_unit=10.0, feature_scale=FSCALE, seed=2)
@@ -117,6 +117,63 @@ def test_device_scores_match_the_reference(nq):
     want, _ = scorer_ref.forward(p, keys, logc, rem, nq, W, FSCALE)
     assert np.all(np.isfinite(got))
     np.testing.assert_allclose(got, want, rtol=2e-3, atol=2e-3)
+
+
+def dense_rows(nq, n, seed):
+    """Keys with every qubit drawn uniformly from I/X/Y/Z (weight ~ 3/4 of the register)."""
+    rng = np.random.default_rng(seed)
+    W = ps.width_for(nq)
+    x = rng.integers(0, 1 << 63, size=(n, W), dtype=np.int64).astype(np.uint64) << np.uint64(1)
+    z = rng.integers(0, 1 << 63, size=(n, W), dtype=np.int64).astype(np.uint64) << np.uint64(1)
+    x |= rng.integers(0, 2, size=(n, W)).astype(np.uint64)
+    z |= rng.integers(0, 2, size=(n, W)).astype(np.uint64)
+    if nq % 64:
+        mask = np.uint64((1 << (nq % 64)) - 1)
+        x[:, -1] &= mask
+        z[:, -1] &= mask
+    keys = learned.pack_keys(x, z)
+    logc = rng.normal(-8.0, 3.0, size=n).astype(np.float32)
+    rem = rng.integers(0, 50, size=n).astype(np.float32)
+    return keys, logc, rem
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nq", [64, 200])
+def test_device_scores_of_dense_strings_match_the_reference(nq):
+    """Strings with about 3/4 of the qubits non-identity: the one-hot operand's sums (the tensor-core
+    path at 64 rows, the embedding bag at 200) add dozens of rows per term."""
+    W = ps.width_for(nq)
+    sc = learned.Scorer(nq, layers_per_unit=10.0, feature_scale=FSCALE, seed=2)
+    p = random_params(nq, 19, scale=0.05)
+    sc.set_params(p)
+    keys, logc, rem = dense_rows(nq, 2000, seed=31)
+    got = sc.score(keys, logc, rem)
+    want, _ = scorer_ref.forward(p, keys, logc, rem, nq, W, FSCALE)
+    np.testing.assert_allclose(got, want, rtol=2e-3, atol=2e-3)
+
+
+@pytest.mark.gpu
+def test_site_mapped_scorer_scores_a_wider_register_like_the_reference():
+    """A 64-row scorer on 256-qubit strings through a window map (sites 96..159 onto rows 0..63,
+    the sites beyond clamped to the edge rows, every seventh site ignored): the tensor-core
+    one-hot operand carries counts up to dozens per row, and the scores must match the
+    restatement with the same map.  Training refuses a mapped scorer."""
+    rows, sites = 64, 256
+    sc = learned.Scorer(rows, layers_per_unit=10.0, feature_scale=FSCALE, seed=2)
+    p = random_params(rows, 23, scale=0.05)
+    sc.set_params(p)
+    site_row = np.clip(np.arange(sites) - 128 + 32, 0, rows - 1).astype(np.int32)
+    site_row[::7] = -1
+    sc.set_site_map(site_row)
+    for keys, logc, rem in (random_rows(sites, 1000, seed=29)[:3], dense_rows(sites, 1000, seed=37)):
+        got = sc.score(keys, logc, rem)
+        want, _ = scorer_ref.forward(p, keys, logc, rem, rows, 4, FSCALE, site_row=site_row)
+        np.testing.assert_allclose(got, want, rtol=2e-3, atol=2e-3)
+    k64, l64, r64, t64 = random_rows(rows, 256, seed=41)
+    with pytest.raises(Exception):
+        sc.train(k64, l64, r64, t64, epochs=1, batch=128)
+    sc.set_site_map(None)
+    sc.train(k64, l64, r64, t64, epochs=1, batch=128)
 
 
 @pytest.mark.gpu
