@@ -306,6 +306,7 @@ def run_ours(args, world, rank, local):
         g.propagate(layers[li], policy, "heisenberg")
     barrier(world)
     terms = 0
+    terms_out = 0
     dev_ms = 0.0
     launches = 0
     torch.cuda.synchronize()
@@ -315,6 +316,7 @@ def run_ours(args, world, rank, local):
         for li in range(args.warmup, args.warmup + args.steps):
             st = g.propagate(layers[li], policy, "heisenberg", with_stats=True)
             terms += st.total_terms_in
+            terms_out += sum(st.terms_after)
             dev_ms += st.device_ms
             launches += st.kernel_launches
     torch.cuda.cudart().cudaProfilerStop()
@@ -338,7 +340,7 @@ def run_ours(args, world, rank, local):
     if args.no_e2e:
         e2e_value, h2d, d2h = None, 0, 0
         return finish(args, world, rank, value, max_ms, launches, prof, dev_ms, clocks, state_after, cap,
-                      e2e_value, h2d, d2h)
+                      e2e_value, h2d, d2h, terms, terms_out)
     rows = cap + 1024
     pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True).numpy()
     hx = pin((rows, 1), torch.int64).view(np.uint64)
@@ -376,10 +378,11 @@ def run_ours(args, world, rank, local):
     e2e_value = dist_sum(e2e_terms, world) / e2e_s
     g.close()
     return finish(args, world, rank, value, max_ms, launches, prof, dev_ms, clocks, state_after, cap, e2e_value,
-                  h2d, d2h)
+                  h2d, d2h, terms, terms_out)
 
 
-def finish(args, world, rank, value, max_ms, launches, prof, dev_ms, clocks, state_after, cap, e2e_value, h2d, d2h):
+def finish(args, world, rank, value, max_ms, launches, prof, dev_ms, clocks, state_after, cap, e2e_value, h2d, d2h,
+           terms_in, terms_out):
     if rank != 0:
         return
     peak, peak_kind = measured_peaks()
@@ -410,6 +413,8 @@ def finish(args, world, rank, value, max_ms, launches, prof, dev_ms, clocks, sta
     # the layer's algorithmic bytes over the timed channels' device time, and over the kernels' own time
     layer_frac = bytes_per_channel / (timed_ms_per_channel * 1e-3) / 1e9 / peak
     kernel_layer_frac = all_bytes / (all_ms * 1e-3) / 1e9 / peak
+    # the least a channel can move: read every input row once and write every output row once
+    min_frac = (terms_in + terms_out) * (16 + 8) / (dev_ms * 1e-3) / 1e9 / peak
     cb = cpu_baseline(args.cpu_seconds) if world == 1 and args.cpu_seconds > 0 else None
     line = {
         "metric": METRIC,
@@ -431,6 +436,7 @@ def finish(args, world, rank, value, max_ms, launches, prof, dev_ms, clocks, sta
         "gpu_launches": launches,
         "roofline": roofline,
         "layer_roofline_frac": round(layer_frac, 4),
+        "min_traffic_frac": round(min_frac, 4),
         "kernel_profile": {k: {"launches": v["timed_launches"], "ms": round(v["total_ms"], 3),
                                "GB": round(v["algorithmic_bytes"] / 1e9, 3)} for k, v in prof.items() if v["launches"]},
         "ms_per_channel": {"timed": round(timed_ms_per_channel, 4),
@@ -440,6 +446,8 @@ def finish(args, world, rank, value, max_ms, launches, prof, dev_ms, clocks, sta
         "clocks": clocks.summary(),
         "cpu_baseline": cb,
     }
+    # the other configurations run on one GPU (rank 0 of an N = 1 run); replicas add nothing
+    line["configs"] = run_configs(args) if world == 1 else "measured by the N=1 run"
     print(json.dumps(line))
 
 
@@ -583,62 +591,156 @@ def config_noisy_tfim6(args):
     }
 
 
-def precision_report(args):
-    """The precision form of the workload (random layers + depolarizing noise p = 1e-3 on every
-    qubit after each layer), run in float64 and in float32 with compensated sums: one JSON line
-    with the <O> error on |0...0> and the largest coefficient error over the strings both runs
-    kept.  Not the headline metric; a report for the f32 form."""
+def _max_error(values, ref):
+    return float(max(abs(a - b) for a, b in zip(values[1:], ref[1:])))
+
+
+def _time_to_error(plain, learned):
+    """For each plain f64 budget, the error it reached and the cheapest learned run (by wall time)
+    whose error is at most that: the learned form's time to the same <O> error and the ratio."""
+    out = []
+    for b, p in sorted(plain.items()):
+        hits = [(r["wall_s"], lb) for lb, r in learned.items() if r["max_error"] <= p["max_error"]]
+        row = {"plain_budget_log2": b, "error": p["max_error"], "plain_wall_s": round(p["wall_s"], 4)}
+        if hits:
+            t, lb = min(hits)
+            row.update({"learned_budget_log2": lb, "learned_wall_s": round(t, 4), "ratio": round(p["wall_s"] / t, 3)})
+        else:
+            row.update({"learned_budget_log2": None, "learned_wall_s": None, "ratio": None})
+        out.append(row)
+    return out
+
+
+def config_learned_tfim8(args):
+    """Learned truncation against plain TopN on the 8 x 8 periodic TFIM quench (64 qubits):
+    observable (1/64) sum X_i, per Trotter step RZZ(-2 J dt) on the 128 bonds (horizontal then
+    vertical, row-major) and RX(2 h dt) on every qubit, J = 1, dt = 0.05, 20 steps, <X>(t) read in
+    |+...+> after every step (the reference's quench protocol).  Reference: f64 with
+    coeff(LEARN_REF_EPS) & TopN(2^LEARN_REF_CAP).  Plain: f64 TopN at 2^20 / 2^22 / 2^24.
+    Learned: f32 scored TopN with a scorer trained (on this GPU, by this library's kernels) on
+    attribution rows from coeff(LEARN_TRAIN_EPS) runs at h in {0.75, 1.5, 2.5}, at budgets down to
+    2^16.  Error: max over t of |<X>(t) - <X>_ref(t)|.  Time to error: for each plain budget, the
+    cheapest learned run reaching its error."""
     import numpy as np
-    import torch
 
-    import paulistrings_b200 as ps
-    from paulistrings_b200 import _lib, truncation, workloads
+    from paulistrings_b200 import learned, truncation, workloads
 
-    seed = SEED
-    policy = truncation.topn(args.term_cap) & truncation.coeff(EPS)
-    layers = layer_circuits(seed)[: args.precision_layers]
-    for c in layers:
-        c.depolarize(1e-3, range(NUM_QUBITS))
-    x0, z0, c0 = workloads.random_observable(NUM_QUBITS, 65536, seed + 1)
-    out = {}
-    for dtype in ("f64", "f32"):
-        g = ps.GpuPauliSum(NUM_QUBITS, dtype)
-        if dtype == "f32":
-            _lib.check(_lib.lib().ps_set_compensated_sums(g._h, 1), g._h, "compensated")
-        g.upload(x0, z0, c0)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for c in layers:
-            g.propagate(c, policy, "heisenberg")
-        torch.cuda.synchronize()
-        secs = time.perf_counter() - t0
-        out[dtype] = (g.expectation("z+"), g.download(), secs)
-        g.close()
-    e64, (x64, z64, c64), s64 = out["f64"]
-    e32, (x32, z32, c32), s32 = out["f32"]
-    k64 = torch.from_numpy(np.concatenate([x64, z64], axis=1).view(np.int64)).cuda()
-    k32 = torch.from_numpy(np.concatenate([x32, z32], axis=1).view(np.int64)).cuda()
-    _, inv = torch.unique(torch.cat([k64, k32]), dim=0, return_inverse=True)
-    m = int(inv.max().item()) + 1
-    a = torch.full((m,), float("nan"), dtype=torch.float64, device="cuda")
-    b = torch.full((m,), float("nan"), dtype=torch.float64, device="cuda")
-    a[inv[: len(c64)]] = torch.from_numpy(c64).cuda()
-    b[inv[len(c64):]] = torch.from_numpy(c32.astype(np.float64)).cuda()
-    both = ~torch.isnan(a) & ~torch.isnan(b)
-    diff = (a - b)[both].abs()
-    line = {
-        "report": "precision (f32 with compensated sums vs f64)",
-        "config": {"workload": "random two-qubit rotation layers + depolarizing p=1e-3 on every qubit after each "
-                               "layer, 64 qubits, 65,536-term random observable, Heisenberg, "
-                               f"TopN({args.term_cap}) & coeff(1e-10)", "layers": len(layers)},
-        "expectation_f64": e64, "expectation_f32": e32,
-        "abs_error": abs(e32 - e64), "rel_error": abs(e32 - e64) / abs(e64) if e64 else None,
-        "terms_f64": int(len(c64)), "terms_f32": int(len(c32)), "common_terms": int(both.sum().item()),
-        "max_coeff_abs_error_common": float(diff.max().item()) if diff.numel() else 0.0,
-        "max_abs_coeff_f64": float(np.max(np.abs(c64))) if len(c64) else 0.0,
-        "seconds": {"f64": round(s64, 3), "f32": round(s32, 3)},
+    L, steps, dt = 8, 20, 0.05
+    nq = L * L
+    obs = workloads.tfim_magnetization(L, "X")
+
+    def step(h):
+        return workloads.tfim_2d(L, 1, J=1.0, h=h, dt=dt)
+
+    sc, losses, rows, t_data, t_train = learned.train_scorer(
+        obs, nq, step, (0.75, 1.5, 2.5), steps, "x+", args.learn_train_eps, samples_per_step=args.learn_samples,
+        every=4, chunk=256, epochs=40, batch=1024, lr=1e-3)
+    result = {
+        "workload": "config 3: 8x8 TFIM quench, J=1, dt=0.05, 20 steps (3,840 channels), <X>(t) in |+...+>; plain "
+        "f64 TopN vs f32 + learned (scored) TopN",
+        "reference": f"f64 coeff({args.learn_ref_eps:g}) & TopN(2^{args.learn_ref_cap})",
+        "scorer": {"train_fields": [0.75, 1.5, 2.5], "attribution_threshold": args.learn_train_eps, "rows": rows,
+                   "data_s": round(t_data, 2), "train_s": round(t_train, 2),
+                   "loss_first_last": [float(losses[0]), float(losses[-1])]},
+        "fields": {},
     }
-    print(json.dumps(line))
+    ref_pol = truncation.coeff(args.learn_ref_eps) & truncation.topn(1 << args.learn_ref_cap)
+    for h in args.learn_fields:
+        ref = learned.trotter_series(obs, nq, step(h), steps, ref_pol, "f64", "x+")
+        plain, scored = {}, {}
+        for b in args.learn_plain_budgets:
+            r = learned.trotter_series(obs, nq, step(h), steps, truncation.topn(1 << b), "f64", "x+")
+            r["max_error"] = _max_error(r["values"], ref["values"])
+            plain[b] = r
+        for b in args.learn_budgets:
+            r = learned.trotter_series(obs, nq, step(h), steps, truncation.scored_topn(1 << b, sc), "f32", "x+")
+            r["max_error"] = _max_error(r["values"], ref["values"])
+            scored[b] = r
+        slim = lambda d: {str(k): {"max_error": v["max_error"], "wall_s": round(v["wall_s"], 4),
+                                   "device_ms": round(v["device_ms"], 2), "peak_terms": v["peak_terms"],
+                                   "terms_per_s_per_layer": v["terms_in"] / max(1e-9, v["device_ms"] * 1e-3)}
+                          for k, v in d.items()}
+        result["fields"][str(h)] = {
+            "reference": {"wall_s": round(ref["wall_s"], 3), "peak_terms": ref["peak_terms"],
+                          "X_final": ref["values"][-1]},
+            "plain_f64": slim(plain), "learned_f32": slim(scored),
+            "time_to_error": _time_to_error(plain, scored),
+        }
+    sc.close()
+    ratios = [r["ratio"] for f in result["fields"].values() for r in f["time_to_error"] if r["ratio"]]
+    result["ratio_median"] = float(np.median(ratios)) if ratios else None
+    return result
+
+
+def config_learned_xxz256(args):
+    """Learned truncation on the open XXZ chain, L = 256 (W = 4): observable Z_128, per Trotter
+    step RXX(2 dt), RYY(2 dt), RZZ(2 Jz dt) on every bond, even bonds then odd (the reference's
+    examples/common/circuits.py:326-338), Jz = 0.5, dt = 0.1, read out in the Neel state
+    |0101...> after every step.  Plain: f64 TopN at 2^XXZ_BUDGET.  Learned: f32 scored TopN with
+    the config-3 architecture retrained on attribution rows of the L = 64 chain (observable Z_32)
+    and applied to L = 256 through a site map (a 64-site window centred on the observable's site,
+    the sites beyond it clamped to the window's edge rows).  Error: against a plain f64 run at
+    4x the budget (the tightest this measurement affords)."""
+    import numpy as np
+
+    from paulistrings_b200 import learned, truncation, workloads
+
+    L, steps, dt, jz = 256, args.xxz_steps, 0.1, 0.5
+    obs = {"I" * 128 + "Z" + "I" * 127: 1.0}
+    state = workloads.neel_state(L)
+    step = workloads.xxz_chain(L, 1, Jz=jz, dt=dt)
+    # scorer: attribution rows of the 64-site chain
+    obs64 = {"I" * 32 + "Z" + "I" * 31: 1.0}
+    sc, losses, rows, t_data, t_train = learned.train_scorer(
+        obs64, 64, lambda _h: workloads.xxz_chain(64, 1, Jz=jz, dt=dt), (jz,), steps, workloads.neel_state(64),
+        args.learn_train_eps, samples_per_step=args.learn_samples, every=5, chunk=256, epochs=40, batch=1024,
+        lr=1e-3)
+    sc.set_site_map(np.clip(np.arange(L) - 128 + 32, 0, 63))
+    b = args.xxz_budget
+    ref = learned.trotter_series(obs, L, step, steps, truncation.topn(1 << (b + 2)), "f64", state)
+    plain = learned.trotter_series(obs, L, step, steps, truncation.topn(1 << b), "f64", state)
+    runs = {"plain_f64": {b: plain}, "learned_f32": {}}
+    for lb in (b - 2, b):
+        runs["learned_f32"][lb] = learned.trotter_series(obs, L, step, steps, truncation.scored_topn(1 << lb, sc),
+                                                         "f32", state)
+    sc.close()
+    out = {
+        "workload": f"config 4: open XXZ chain L=256, Jz=0.5, dt=0.1, {steps} steps ({765 * steps} channels), Z_128 "
+        "in the Neel state; plain f64 TopN vs f32 + learned (scored) TopN",
+        "reference": f"f64 TopN(2^{b + 2})",
+        "scorer": {"trained_on": "XXZ L=64, Z_32", "attribution_threshold": args.learn_train_eps, "rows": rows,
+                   "data_s": round(t_data, 2), "train_s": round(t_train, 2),
+                   "site_map": "sites 96..159 -> rows 0..63, beyond clamped to the edge rows",
+                   "loss_first_last": [float(losses[0]), float(losses[-1])]},
+        "reference_run": {"wall_s": round(ref["wall_s"], 3), "peak_terms": ref["peak_terms"],
+                          "Z_final": ref["values"][-1], "layers_skipped": ref["layers_skipped"]},
+    }
+    for form, d in runs.items():
+        out[form] = {}
+        for k, r in d.items():
+            r["max_error"] = _max_error(r["values"], ref["values"])
+            out[form][str(k)] = {"max_error": r["max_error"], "wall_s": round(r["wall_s"], 3),
+                                 "device_ms": round(r["device_ms"], 1), "peak_terms": r["peak_terms"],
+                                 "layers_skipped": r["layers_skipped"],
+                                 "terms_per_s_per_layer": r["terms_in"] / max(1e-9, r["device_ms"] * 1e-3)}
+    out["time_to_error"] = _time_to_error(runs["plain_f64"], runs["learned_f32"])
+    return out
+
+
+CONFIGS = {"tfim6": config_tfim6, "noisy": config_noisy_tfim6, "learned": config_learned_tfim8,
+           "xxz": config_learned_xxz256}
+
+
+def run_configs(args):
+    out = {}
+    for name in [c for c in args.configs.split(",") if c and c != "none"]:
+        t0 = time.perf_counter()
+        try:
+            out[name] = CONFIGS[name](args)
+        except Exception as exc:  # one failed configuration must not hide the others' numbers
+            out[name] = {"error": f"{type(exc).__name__}: {exc}"}
+        out[name]["bench_s"] = round(time.perf_counter() - t0, 1)
+    return out
 
 
 def main():
@@ -651,14 +753,25 @@ def main():
     ap.add_argument("--term-cap", type=int, default=TERM_CAP,
                     help="TopN cap; smaller values give the small cases profiled under ncu")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
-    ap.add_argument("--precision-report", action="store_true",
-                    help="print the f32-vs-f64 precision report of the noisy workload instead of the bench line")
-    ap.add_argument("--precision-layers", type=int, default=LAYERS)
+    ap.add_argument("--configs", default="tfim6,noisy,learned,xxz",
+                    help="the other configurations measured after the headline (comma list of "
+                         f"{','.join(CONFIGS)}; 'none' for the headline alone)")
+    ap.add_argument("--configs-only", action="store_true", help="print only the configurations' object")
+    ap.add_argument("--learn-fields", type=float, nargs="+", default=[0.5, 1.0, 2.0, 3.0])
+    ap.add_argument("--learn-plain-budgets", type=int, nargs="+", default=[20, 22, 24], help="log2 TopN budgets")
+    ap.add_argument("--learn-budgets", type=int, nargs="+", default=[16, 18, 20, 22, 24],
+                    help="log2 budgets of the learned form")
+    ap.add_argument("--learn-ref-eps", type=float, default=1e-7)
+    ap.add_argument("--learn-ref-cap", type=int, default=29, help="log2 TopN cap of the reference run")
+    ap.add_argument("--learn-train-eps", type=float, default=1e-5, help="threshold of the attribution runs")
+    ap.add_argument("--learn-samples", type=int, default=1024, help="attribution samples per step boundary")
+    ap.add_argument("--xxz-budget", type=int, default=24, help="log2 TopN budget of the L=256 XXZ comparison")
+    ap.add_argument("--xxz-steps", type=int, default=50)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
-    if args.precision_report:
-        precision_report(args)
+    if args.configs_only:
+        print(json.dumps({"configs": run_configs(args)}))
         return
     world, rank, local = dist_setup(args.gpus)
     try:

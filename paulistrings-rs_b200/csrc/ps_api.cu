@@ -98,6 +98,8 @@ struct ps_sum {
     bool support_known = false;
     bool keep_clean = false;
     uint64_t layers_skipped = 0;
+    Buf noise_drops;                      // folded noise: own rows first dropped after channel j
+    unsigned long long* hnoise = nullptr; // pinned, kMaxNoise + 1 words
     KeepProg clean_keep{};
     long long fault_oom_after = -1;   // failure injection: allocations left before all fail
     bool fault_stall = false;         // failure injection: next merge skips its first tile
@@ -1050,7 +1052,21 @@ struct Engine {
         return PS_OK;
     }
 
-    static ps_status apply(ps_sum* s, const ps_table& t, const ps_policy* policy, ps_layer_stats* stats) {
+    // Does table t run on the partner path with a partner stream (where noise can be folded)?
+    static bool folds_noise(const ps_table& t) {
+        RotLayer<W> L;
+        LevelList* lv = new LevelList();
+        std::string why;
+        bool general = false;
+        const bool ok = to_rot_layer<W, T>(t, L, *lv, why, &general) == PS_OK && !general && L.partners;
+        delete lv;
+        return ok;
+    }
+
+    // noise (optional): single-qubit key-preserving channels to fold in before the table, in
+    // order; noise_after[j] receives the terms left after channel j.
+    static ps_status apply(ps_sum* s, const ps_table& t, const ps_policy* policy, ps_layer_stats* stats,
+                           const NoiseList* noise = nullptr, uint64_t* noise_after = nullptr) {
         KeepProg keep;
         std::string why;
         ps_status ps = lower_keep(policy, keep, why);
@@ -1068,7 +1084,7 @@ struct Engine {
             // a commuting term keeps c exactly on the wide path; a local table must leave the
             // identity pattern alone
             const bool identity0 = a.L.wide || ((T)a.L.a1[0] == T(0) && (T)a.L.a0[0] == T(1));
-            if (skippable(s, lsup, keep, identity0)) {
+            if (!noise && skippable(s, lsup, keep, identity0)) {
                 skipped(s, stats, a.L.partners ? PS_PATH_ROTATION : PS_PATH_RESCALE);
                 return PS_OK;
             }
@@ -1141,6 +1157,18 @@ struct Engine {
         a.slot_count = slotted ? (unsigned int*)s->slot_count.p : nullptr;
         a.sms = s->sms;
         a.span_out = &span;
+        if (noise && noise->n > 0) {
+            if (!a.L.partners) return set_err(s, PS_ERR_INVALID, "apply: noise folded into a layer without partners");
+            if ((e = ensure(s, s->noise_drops, (kMaxNoise + 1) * sizeof(unsigned long long))) != cudaSuccess)
+                return cuda_fail(s, e, "apply: noise scratch");
+            if (!s->hnoise && (e = cudaMallocHost(&s->hnoise, (kMaxNoise + 1) * sizeof(unsigned long long))) != cudaSuccess) {
+                s->hnoise = nullptr;
+                return cuda_fail(s, e, "apply: noise scratch");
+            }
+            a.noise = noise;
+            a.noise_drops = static_cast<unsigned long long*>(s->noise_drops.p);
+            a.host_noise_drops = s->hnoise;
+        }
         e = launch_rotation_layer<W, T>(a, s->stream);
         s->prof.resolve();
         if (e != cudaSuccess) return cuda_fail(s, e, "apply: rotation layer");
@@ -1153,8 +1181,15 @@ struct Engine {
         s->hist_kind = first_pass;
         s->hist_window = fuse_topn && window;
         s->hist_base = a.topn_hist_base;
+        uint64_t n_rot = n;  // terms entering the rotation, after the folded noise
+        if (a.noise) {
+            for (int j = 0; j < noise->n; ++j) {
+                n_rot -= s->hnoise[j];
+                if (noise_after) noise_after[j] = n_rot;
+            }
+        }
         if (stats) {
-            stats->terms_in = n;
+            stats->terms_in = n_rot;
             stats->partners = partners;
             stats->terms_out = out_n;
             stats->terms_after_passes = out_n;
@@ -1352,6 +1387,7 @@ struct Engine {
         }
         if (e == cudaSuccess && s->hfirst_cap < nb + 1) {
             if (s->hfirst) cudaFreeHost(s->hfirst);
+    if (s->hnoise) cudaFreeHost(s->hnoise);
             s->hfirst = nullptr;
             s->hfirst_cap = 0;
             e = cudaMallocHost(&s->hfirst, (nb + 1) * sizeof(uint64_t));
@@ -1519,6 +1555,26 @@ ps_status dispatch(ps_sum* s, F&& f) {
     return set_err(s, PS_ERR_UNSUPPORTED, "widths above 4 words (256 qubits) are not built");
 }
 
+// A single-qubit key-preserving channel whose factors can be folded into the next layer: it
+// leaves the identity alone and shrinks no coefficient's magnitude by less than nothing
+// (|factor| <= 1), so the keep program passes after it only if it passed before it.
+bool foldable_noise(const ps_table& t, int nq) {
+    if (t.mode != PS_TABLE_LOCAL || t.k != 1 || t.num_entries != 1 || t.entries[0].local_delta != 0) return false;
+    if (t.qubits[0] >= (uint32_t)nq || t.entries[0].amplitude[0] != 1.0) return false;
+    for (int s = 1; s < 4; ++s)
+        if (!(std::fabs(t.entries[0].amplitude[s]) <= 1.0)) return false;
+    return true;
+}
+
+// Would every layer pass of the policy leave a sum of the handle's current size (or smaller)
+// unchanged?  Then folding noise layers skips only passes that would have done nothing.
+bool passes_idle(const ps_policy* p, const ps_sum* s) {
+    const uint64_t n = s->slotted ? s->live_n : s->n;
+    for (int i = 0; p && i < p->num_passes; ++i)
+        if (p->passes[i].kind != PS_PASS_NONE && n > p->passes[i].n) return false;
+    return true;
+}
+
 struct DeviceGuard {
     int prev = -1;
     explicit DeviceGuard(int dev) {
@@ -1605,7 +1661,7 @@ ps_status ps_destroy(ps_sum* s) {
     for (Buf* b : {&s->keys[0], &s->keys[1], &s->coef[0], &s->coef[1], &s->pk, &s->pc, &s->idx, &s->dv, &s->fv,
                    &s->slots, &s->status, &s->bounds, &s->hist, &s->cand, &s->partial, &s->dout, &s->sort_status,
                    &s->up_x, &s->up_z, &s->up_c, &s->up_k, &s->up_v0, &s->up_v1, &s->up_c0, &s->up_st, &s->sel,
-                   &s->cnorms, &s->cfirst, &s->slot_count})
+                   &s->cnorms, &s->cfirst, &s->slot_count, &s->noise_drops})
         release(*b);
     if (s->ctl) cudaFree(s->ctl);
     if (s->sort.hist) cudaFree(s->sort.hist);
@@ -1703,6 +1759,49 @@ ps_status ps_propagate(ps_sum* s, const ps_channel* channels, uint64_t num_chann
     const uint64_t collapses0 = s->collapses;
     for (uint64_t li = 0; li < num_channels; ++li) {
         ps_layer_stats ls;
+        // A run of single-qubit noise channels folds into the rotation layer that follows it:
+        // their factors are applied, in order and with the keep program after each, to every term
+        // as the rotation reads it, so the run costs no pass of its own.
+        uint64_t fj = li;
+        while (fj < num_channels && fj - li < (uint64_t)kMaxNoise && foldable_noise(tables[fj], s->nq)) ++fj;
+        if (fj > li && fj < num_channels && passes_idle(policy, s) &&
+            dispatch<Engine>(s, [&](auto op) { return decltype(op)::folds_noise(tables[fj]) ? PS_OK : PS_ERR_UNSUPPORTED; }) ==
+                PS_OK) {
+            NoiseList N;
+            std::memset(&N, 0, sizeof N);
+            N.n = (int32_t)(fj - li);
+            for (uint64_t q = li; q < fj; ++q) {
+                const ps_table& t = tables[q];
+                N.q[q - li] = (uint16_t)t.qubits[0];
+                for (int p = 0; p < 4; ++p) {
+                    N.f[q - li][p] = t.entries[0].amplitude[p];
+                    N.ff[q - li][p] = (float)t.entries[0].amplitude[p];
+                }
+            }
+            uint64_t after[kMaxNoise];
+            const uint64_t n0 = s->n;
+            ps = dispatch<Engine>(s, [&](auto op) { return decltype(op)::apply(s, tables[fj], policy, &ls, &N, after); });
+            if (ps == PS_OK && s->scorer) s->scorer_remaining -= (double)(fj - li);  // the folded layers' count-downs
+            s->pass_call = fj;
+            if (ps == PS_OK) ps = ps_finalize_layer(s, policy);
+            s->pass_call = 0;
+            if (ps != PS_OK) {
+                s->err = "layer " + std::to_string(fj) + " (with the noise of layers " + std::to_string(li) + "-" +
+                         std::to_string(fj - 1) + " folded in): " + s->err;
+                break;
+            }
+            for (uint64_t q = li; q < fj; ++q) {
+                rs.total_terms_in += q == li ? n0 : after[q - li - 1];
+                if (terms_after) terms_after[q] = after[q - li];
+                ++rs.layers;
+            }
+            rs.total_terms_in += after[fj - li - 1];
+            if (ls.terms_out > rs.peak_terms) rs.peak_terms = ls.terms_out;
+            if (terms_after) terms_after[fj] = s->n;
+            ++rs.layers;
+            li = fj;
+            continue;
+        }
         rs.total_terms_in += s->n;
         const uint64_t skipped0 = s->layers_skipped, n_in = s->n;
         ps = ps_apply_layer(s, &tables[li], policy, &ls);

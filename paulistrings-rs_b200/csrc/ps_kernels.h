@@ -80,6 +80,18 @@ struct RotLayer {
     float cos32, sin32;
 };
 
+// Single-qubit key-preserving channels (depolarizing, dephasing, Pauli channels) that precede a
+// rotation layer, folded into it: per channel its qubit and the factor of each pattern of that
+// qubit (x | z << 1).  Applied in order to a term's coefficient, the keep program checked after
+// each as the separate layers would, before the rotation's branches.
+constexpr int kMaxNoise = 64;
+struct NoiseList {
+    int32_t n;
+    uint16_t q[kMaxNoise];
+    double f[kMaxNoise][4];
+    float ff[kMaxNoise][4];
+};
+
 // Device form of a general local table (LocalPtm with any entries), per input support
 // pattern s: the records it emits, in ascending entry order (DeltaEntry::emit,
 // crates/paulistrings/src/channel/prepared.rs:50-68).
@@ -224,6 +236,9 @@ struct RotationArgs {
                               // output, compacted by the TopN pass that follows); >= merge tiles
     uint64_t* span_out;       // slotted output: rows its slots span
     int sms;                  // multiprocessors of the device (persistent grids)
+    const NoiseList* noise;   // host copy of the folded noise channels (nullptr: none)
+    unsigned long long* noise_drops;       // device, kMaxNoise + 1: own rows first dropped after channel j
+    unsigned long long* host_noise_drops;  // pinned, kMaxNoise + 1: the same, after the layer's sync
 };
 
 // Rows of one merge tile's output slot, and the rows a slotted merge of at most `rows_in`

@@ -27,6 +27,7 @@
 // k_partition + k_merge with an empty partner stream.
 #include <algorithm>
 #include <atomic>
+#include <type_traits>
 #include <cstddef>
 
 #include "ps_device.cuh"
@@ -158,6 +159,65 @@ __device__ __forceinline__ T partner_coeff(const RotLayer<W>& L, const AmpTab<T>
         return mul_rn(m, Amp<T>::sn(L));
     }
     return mul_rn(c, A.a1[pattern_of<W>(L, k)]);
+}
+
+// The folded noise channels, staged in shared memory (their factors are indexed by each lane's
+// pattern).
+template <typename T>
+struct NoiseSmem {
+    T f[kMaxNoise][4];
+    uint16_t q[kMaxNoise];
+    int n;
+};
+
+// The kernels that fold no noise take an empty argument in its place.
+struct NoNoise {};
+template <bool NOISE>
+using NoiseArg = typename std::conditional<NOISE, NoiseList, NoNoise>::type;
+
+// Shared storage for the staged channels only in the kernels that fold noise.
+template <typename T, bool ON>
+struct NoiseShared {
+    NoiseSmem<T> s;
+    unsigned int drop[kMaxNoise + 1];
+    __device__ NoiseSmem<T>* tab() { return &s; }
+    __device__ unsigned int* drops() { return drop; }
+};
+template <typename T>
+struct NoiseShared<T, false> {
+    __device__ NoiseSmem<T>* tab() { return nullptr; }
+    __device__ unsigned int* drops() { return nullptr; }
+};
+
+template <typename T>
+__device__ __forceinline__ void stage_noise(const NoiseList& N, NoiseSmem<T>& S) {
+    for (int i = threadIdx.x; i < N.n * 4; i += blockDim.x) {
+        if constexpr (std::is_same<T, double>::value)
+            S.f[i >> 2][i & 3] = N.f[i >> 2][i & 3];
+        else
+            S.f[i >> 2][i & 3] = N.ff[i >> 2][i & 3];
+    }
+    for (int i = threadIdx.x; i < N.n; i += blockDim.x) S.q[i] = N.q[i];
+    if (threadIdx.x == 0) S.n = N.n;
+}
+
+// The folded channels applied to coefficient v of key k in order, as the separate layers would:
+// a channel multiplies by its factor for k's pattern on its qubit (the identity's factor is 1,
+// skipped), then the term must stay nonzero and pass the keep program.  Returns the index of the
+// channel after which the term is dropped, or S.n when it survives all of them.
+template <int W, typename T>
+__device__ __forceinline__ int noise_apply(const NoiseSmem<T>& S, const KeepProg& keep, const uint64_t* k, T& v) {
+    if (!(v != T(0) && keep_eval<W>(keep, k, to_f64(v)))) return 0;
+    for (int j = 0; j < S.n; ++j) {
+        const int q = S.q[j];
+        const uint32_t s = (uint32_t)((pick<W>(k, q >> 6) >> (q & 63)) & 1u) |
+                           (uint32_t)((pick<W>(k, W + (q >> 6)) >> (q & 63)) & 1u) << 1;
+        if (s) {
+            v = mul_rn(v, S.f[j][s]);
+            if (!(v != T(0) && keep_eval<W>(keep, k, to_f64(v)))) return j;
+        }
+    }
+    return S.n;
 }
 
 // ---------------------------------------------------------------------------
@@ -450,19 +510,21 @@ __global__ void __launch_bounds__(kScanThreads) k_level_scan(LevelTile* __restri
 // apply's registers allow more resident warps to cover its gather latency): per partner j, F = sum over levels of -(split - start) for rows in an upper half
 // (forward) plus (group end - split) for rows in a lower half (backward), added to the F of
 // earlier batches; on the last batch each partner goes to j + F.
-template <int W, typename T, int LV, int NT>
+template <int W, typename T, int LV, int NT, bool NOISE>
 __global__ void __launch_bounds__(NT) k_level_apply(const uint32_t* __restrict__ idx,
                                                         const uint16_t* __restrict__ D, int32_t* __restrict__ F,
                                                         const uint64_t* __restrict__ keys, const T* __restrict__ coef,
                                                         uint64_t n, const Levels lv, const RotLayer<W> L,
                                                         int accumulate, int scatter, uint64_t* __restrict__ Pk,
                                                         T* __restrict__ Pc, const LevelTile* __restrict__ tiles,
-                                                        Ctl* ctl) {
+                                                        Ctl* ctl, const KeepProg keep, const NoiseArg<NOISE> N) {
     constexpr int IT = kScanTile / NT;  // partners per thread
     __shared__ int s_w[NT / 32][4 * LV];
     __shared__ AmpTab<T> A;
+    __shared__ NoiseShared<T, NOISE> NSH;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     stage_amps<W, T>(L, A);
+    if constexpr (NOISE) stage_noise<T>(N, *NSH.tab());
     __syncthreads();
     const uint32_t m = (uint32_t)ctl->count[0];
     const uint32_t ntiles = (m + kScanTile - 1) / kScanTile;
@@ -545,8 +607,15 @@ __global__ void __launch_bounds__(NT) k_level_apply(const uint32_t* __restrict__
             if (!PS_GUARD(ctl, dest >= 0 && dest < (long long)m && row < n, 204)) continue;
             uint64_t k[2 * W];
             load_key<W>(keys, row, k);
-            const T c = coef[row];
-            const T pc = partner_coeff<W, T>(L, A, k, c);
+            T c = coef[row];
+            T pc;
+            if constexpr (NOISE) {
+                // a parent the folded noise drops has no partner: a zero partner adds nothing to
+                // an equal own row and is dropped as an exact zero otherwise
+                pc = noise_apply<W, T>(*NSH.tab(), keep, k, c) < NSH.tab()->n ? T(0) : partner_coeff<W, T>(L, A, k, c);
+            } else {
+                pc = partner_coeff<W, T>(L, A, k, c);
+            }
 #pragma unroll
             for (int w = 0; w < W; ++w) {
                 k[w] ^= L.gx[w];
@@ -663,11 +732,12 @@ __device__ __forceinline__ bool eq_regs(const uint64_t (&a)[2 * W], const uint64
 // pair is consumed in one step, so STEPS = ITEMS + 1 unrolled steps cover it (the caller checks
 // that nothing is left).  Step s leaves its output in ok[s] / ov[s] and sets bit s of the
 // returned mask when the output is kept (nonzero and passing the keep program).
-template <int W, typename T, int STEPS>
+template <int W, typename T, int STEPS, bool NOISE>
 __device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc, const uint64_t* sPk, const T* sPc,
                                                uint32_t& i, uint32_t ie, uint32_t& j, uint32_t je,
                                                const RotLayer<W>& L, const AmpTab<T>& A, const KeepProg& keep,
-                                               uint64_t (&ok)[STEPS][2 * W], T (&ov)[STEPS]) {
+                                               uint64_t (&ok)[STEPS][2 * W], T (&ov)[STEPS],
+                                               const NoiseSmem<T>* NS, unsigned int* s_drop) {
     uint32_t mask = 0;
     uint64_t a[2 * W], b[2 * W];
     if (i < ie) ld_row<W>(sSk, i, a);
@@ -680,7 +750,18 @@ __device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc
             if (takeS) {
 #pragma unroll
                 for (int w = 0; w < 2 * W; ++w) ok[s][w] = a[w];
-                v = own_coeff<W, T>(L, A, a, sSc[i]);
+                if constexpr (NOISE) {
+                    T c = sSc[i];
+                    const int d = noise_apply<W, T>(*NS, keep, a, c);
+                    if (d < NS->n) {
+                        atomicAdd(&s_drop[d], 1u);
+                        v = T(0);
+                    } else {
+                        v = own_coeff<W, T>(L, A, a, c);
+                    }
+                } else {
+                    v = own_coeff<W, T>(L, A, a, sSc[i]);
+                }
                 if (j < je && eq_regs<W>(a, b)) {
                     v = add_rn(v, sPc[j]);
                     if (++j < je) ld_row<W>(sPk, j, b);
@@ -699,7 +780,7 @@ __device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc
     return mask;
 }
 
-template <int W, typename T>
+template <int W, typename T, bool NOISE>
 __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t* __restrict__ Sk, const T* __restrict__ Sc,
                                                   uint64_t n, const uint64_t* __restrict__ Pk,
                                                   const T* __restrict__ Pc, const ulonglong2* __restrict__ bounds,
@@ -708,7 +789,8 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
                                                   unsigned long long* status, Ctl* ctl,
                                                   unsigned int* __restrict__ topn_hist, int hist_mode,
                                                   uint64_t hist_base, unsigned int* __restrict__ slot_count,
-                                                  long long stall_limit) {
+                                                  long long stall_limit, const NoiseArg<NOISE> N,
+                                                  unsigned long long* __restrict__ noise_drops) {
     using SM = MergeSmem<W, T>;
     constexpr int ITEMS = RotTile<W>::kMergeItems;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -721,12 +803,19 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
     __shared__ unsigned long long s_outoff;
     __shared__ unsigned int s_hist[kTopnHistBins];
     __shared__ AmpTab<T> A;
+    __shared__ NoiseShared<T, NOISE> NSH;
+    NoiseSmem<T>* NS = NSH.tab();
+    unsigned int* s_drop = NSH.drops();
 
     const int tid = threadIdx.x;
     if (tid == 0) mbar_init(&bar, 1);
     if (topn_hist)
         for (int q = tid; q < kTopnHistBins; q += kBlock) s_hist[q] = 0;
     stage_amps<W, T>(L, A);
+    if constexpr (NOISE) {
+        stage_noise<T>(N, *NS);
+        for (int q = tid; q <= kMaxNoise; q += kBlock) s_drop[q] = 0;
+    }
     const uint64_t m = ctl->count[0];  // partners, published by k_classify (0 without partners)
     const uint32_t num_tiles = (uint32_t)((n + m + SM::TILE - 1) / SM::TILE);
     uint32_t phase = 0;  // completed phases of `bar`
@@ -802,7 +891,8 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
         uint64_t ok[STEPS][2 * W];
         T ov[STEPS];
         uint32_t i = i0, j = j0;
-        const uint32_t mask = merge_walk<W, T, STEPS>(sSk, Sc_l, sPk, Pc_l, i, ie, j, je, L, A, keep, ok, ov);
+        const uint32_t mask =
+            merge_walk<W, T, STEPS, NOISE>(sSk, Sc_l, sPk, Pc_l, i, ie, j, je, L, A, keep, ok, ov, NS, s_drop);
         PS_GUARD(ctl, i >= ie && j >= je, 305);
         unsigned int total;
         const unsigned int excl = block_exclusive_sum<kBlock>(__popc(mask), s_warp, total);
@@ -870,6 +960,11 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
         for (int q = tid; q < kTopnHistBins; q += kBlock)
             if (s_hist[q]) atomicAdd(&topn_hist[q], s_hist[q]);
     }
+    if constexpr (NOISE) {
+        __syncthreads();
+        for (int q = tid; q <= kMaxNoise; q += kBlock)
+            if (s_drop[q]) atomicAdd(&noise_drops[q], (unsigned long long)s_drop[q]);
+    }
     if (tid == 0) bulk_wait_read_all();  // shared memory stays valid until the last copy has read it
 }
 
@@ -917,10 +1012,10 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
         // variant that runs
         static std::atomic<int> level_per_sm[2];
         const int per_sm = a.levels->n <= 4
-                               ? resident_blocks(k_level_apply<W, T, 4, kApplyThreads>, kApplyThreads, 0,
+                               ? resident_blocks(k_level_apply<W, T, 4, kApplyThreads, false>, kApplyThreads, 0,
                                                  level_per_sm[0])
-                               : resident_blocks(k_level_apply<W, T, kMaxLevels, kApplyThreads>, kApplyThreads, 0,
-                                                 level_per_sm[1]);
+                               : resident_blocks(k_level_apply<W, T, kMaxLevels, kApplyThreads, false>, kApplyThreads,
+                                                 0, level_per_sm[1]);
         const uint32_t sgrid = std::min<uint32_t>(stiles, (uint32_t)per_sm * (uint32_t)(a.sms > 0 ? a.sms : 1));
         LevelTile* lt = reinterpret_cast<LevelTile*>(a.slots);
         const bool narrow = a.levels->n <= 4;
@@ -944,12 +1039,24 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
             a.prof->end(st);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
             a.prof->begin(K_LEVEL_APPLY, 0.0, st);
-            if (narrow)
-                k_level_apply<W, T, 4, kApplyThreads><<<sgrid, kApplyThreads, 0, st>>>(
-                    a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, b > 0, last, a.Pk, a.Pc, lt, ctl);
-            else
-                k_level_apply<W, T, kMaxLevels, kApplyThreads><<<sgrid, kApplyThreads, 0, st>>>(
-                    a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, b > 0, last, a.Pk, a.Pc, lt, ctl);
+            // the folded noise matters only where the partners are placed (the last batch)
+            if (a.noise && last) {
+                if (narrow)
+                    k_level_apply<W, T, 4, kApplyThreads, true><<<sgrid, kApplyThreads, 0, st>>>(
+                        a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, b > 0, last, a.Pk, a.Pc, lt, ctl, a.keep, *a.noise);
+                else
+                    k_level_apply<W, T, kMaxLevels, kApplyThreads, true><<<sgrid, kApplyThreads, 0, st>>>(
+                        a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, b > 0, last, a.Pk, a.Pc, lt, ctl, a.keep, *a.noise);
+            } else {
+                if (narrow)
+                    k_level_apply<W, T, 4, kApplyThreads, false><<<sgrid, kApplyThreads, 0, st>>>(
+                        a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, b > 0, last, a.Pk, a.Pc, lt, ctl, a.keep,
+                        NoNoise{});
+                else
+                    k_level_apply<W, T, kMaxLevels, kApplyThreads, false><<<sgrid, kApplyThreads, 0, st>>>(
+                        a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, b > 0, last, a.Pk, a.Pc, lt, ctl, a.keep,
+                        NoNoise{});
+            }
             a.prof->end(st);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
@@ -978,19 +1085,33 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     cudaMemsetAsync(&ctl->tile_counter[3], a.inject_stall ? 1 : 0, 1, st);
     cudaMemsetAsync(reinterpret_cast<unsigned char*>(&ctl->tile_counter[3]) + 1, 0, 3, st);
     size_t smem = MergeSmem<W, T>::bytes;
-    static std::atomic<int> merge_per_sm;
-    const int mper = resident_blocks(k_merge<W, T>, kBlock, smem, merge_per_sm);
-    const uint32_t mgrid = (uint32_t)std::min<uint64_t>(mtiles_hi, (uint64_t)mper * (a.sms > 0 ? a.sms : 1));
+    static std::atomic<int> merge_per_sm[2];
+    const long long stall = a.inject_stall ? (long long)a.stall_limit : 0ll;
     a.prof->begin(K_MERGE, 0.0, st);
-    k_merge<W, T><<<mgrid, kBlock, smem, st>>>(a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc,
-                                                  a.out_cap, a.status, ctl, a.topn_hist, a.topn_hist_mode,
-                                                  a.topn_hist_base, a.slot_count,
-                                                  a.inject_stall ? (long long)a.stall_limit : 0ll);
+    if (a.noise) {
+        cudaMemsetAsync(a.noise_drops, 0, (kMaxNoise + 1) * sizeof(unsigned long long), st);
+        const int mper = resident_blocks(k_merge<W, T, true>, kBlock, smem, merge_per_sm[1]);
+        const uint32_t mgrid = (uint32_t)std::min<uint64_t>(mtiles_hi, (uint64_t)mper * (a.sms > 0 ? a.sms : 1));
+        k_merge<W, T, true><<<mgrid, kBlock, smem, st>>>(a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok,
+                                                           a.Oc, a.out_cap, a.status, ctl, a.topn_hist,
+                                                           a.topn_hist_mode, a.topn_hist_base, a.slot_count, stall,
+                                                           *a.noise, a.noise_drops);
+    } else {
+        const int mper = resident_blocks(k_merge<W, T, false>, kBlock, smem, merge_per_sm[0]);
+        const uint32_t mgrid = (uint32_t)std::min<uint64_t>(mtiles_hi, (uint64_t)mper * (a.sms > 0 ? a.sms : 1));
+        k_merge<W, T, false><<<mgrid, kBlock, smem, st>>>(a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok,
+                                                            a.Oc, a.out_cap, a.status, ctl, a.topn_hist,
+                                                            a.topn_hist_mode, a.topn_hist_base, a.slot_count, stall,
+                                                            NoNoise{}, nullptr);
+    }
     a.prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // counts and error flags in one copy: count[0..7], tile_counter[0..7], err, err_info
     cudaMemcpyAsync(a.host_count, &ctl->count[0], offsetof(Ctl, err_info) + sizeof(unsigned int),
                     cudaMemcpyDeviceToHost, st);
+    if (a.noise)
+        cudaMemcpyAsync(a.host_noise_drops, a.noise_drops, (kMaxNoise + 1) * sizeof(unsigned long long),
+                        cudaMemcpyDeviceToHost, st);
     if ((e = spin_sync(st)) != cudaSuccess) return e;
     const uint64_t m = a.host_count[0];
     *a.partners_out = m;
@@ -1033,12 +1154,16 @@ template uint64_t merge_span_rows<4>(uint64_t);
 
 template <int W, typename T>
 cudaError_t configure_rotation_kernels() {
-    cudaError_t e = cudaFuncSetAttribute(k_merge<W, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)MergeSmem<W, T>::bytes);
-    // all of the unified L1 as shared memory, so residency is set by registers, not the carveout
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_merge<W, T>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 (int)cudaSharedmemCarveoutMaxShared);
+    cudaError_t e = cudaSuccess;
+    const void* kernels[2] = {(const void*)k_merge<W, T, false>, (const void*)k_merge<W, T, true>};
+    for (const void* k : kernels) {
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MergeSmem<W, T>::bytes);
+        // all of the unified L1 as shared memory, so residency is set by registers, not the carveout
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared);
+    }
     return e;
 }
 
