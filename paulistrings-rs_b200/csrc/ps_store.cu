@@ -20,6 +20,8 @@
 #include "ps_device.cuh"
 #include "ps_store.h"
 
+#include <algorithm>
+#include <atomic>
 #include <cstddef>
 #include <type_traits>
 
@@ -405,6 +407,192 @@ __global__ void __launch_bounds__(1024) k_topn_select(unsigned int* __restrict__
         ctl->aux[1] |= ((1ull << bits) - 1ull) << shift;
         ctl->aux[2] = r - above;
         ctl->aux[3] += above;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The whole select in one cooperative launch (every block resident): block 0 picks the digit-1
+// bin from the histogram the merge built, every block gathers the boundary bin's keys into its
+// own candidate segment, then four 13-bit digits each histogram the candidates grid-wide and
+// block 0 picks the bin.  Phases are separated by bounded grid barriers; a barrier that gives
+// up flags ERR_TIMEOUT and every block returns.  Replaces ten launches per pass.
+// ---------------------------------------------------------------------------
+constexpr int kSelThreads = 256;
+
+// Grid barrier on two words (arrivals, generation), zero at launch.  Bounded by the handle's
+// spin limit.  Values other blocks wrote before the barrier are read after it with L1-bypassing
+// loads (__ldcg): a line this SM cached before the barrier may be stale.
+__device__ __forceinline__ bool grid_barrier(unsigned int* bar, Ctl* ctl, uint32_t info) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_ok = 1;
+        const unsigned int gen = ld_acquire_u32(&bar[1]);  // before arriving: the release cannot come earlier
+        __threadfence();
+        if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
+            bar[0] = 0;  // every other block waits on the generation word
+            __threadfence();
+            st_release_u32(&bar[1], gen + 1);
+        } else {
+            long long spins = 0;
+            while (ld_acquire_u32(&bar[1]) == gen) {
+                if (++spins > spin_limit(ctl)) {
+                    raise_err(ctl, ERR_TIMEOUT, info);
+                    s_ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// One block of kSelThreads: pick the bin of hist (BINS bins, counted from the top) holding the
+// remaining rank aux[2]; update prefix, mask, rank and count above; clear hist.
+template <int BINS>
+__device__ __forceinline__ void block_select(unsigned int* __restrict__ hist, int shift, int bits, Ctl* ctl,
+                                             unsigned long long* s_part) {
+    constexpr int PER = BINS / kSelThreads;
+    __shared__ int s_choice;
+    __shared__ unsigned long long s_above;
+    const int t = threadIdx.x;
+    if (t == 0) {
+        s_choice = 0;
+        s_above = 0;
+    }
+    unsigned long long mine = 0;
+    for (int q = 0; q < PER; ++q) mine += __ldcg(&hist[BINS - 1 - (t * PER + q)]);
+    s_part[t] = mine;
+    __syncthreads();
+    for (int o = 1; o < kSelThreads; o <<= 1) {
+        unsigned long long v = t >= o ? s_part[t - o] : 0ull;
+        __syncthreads();
+        s_part[t] += v;
+        __syncthreads();
+    }
+    const unsigned long long r = __ldcg(&ctl->aux[2]);
+    const unsigned long long before = t ? s_part[t - 1] : 0ull;
+    if (before < r && s_part[t] >= r) {
+        unsigned long long acc = before;
+        for (int q = 0; q < PER; ++q) {
+            const int bin = BINS - 1 - (t * PER + q);
+            const unsigned long long c = __ldcg(&hist[bin]);
+            if (acc + c >= r) {
+                s_choice = bin;
+                s_above = acc;
+                break;
+            }
+            acc += c;
+        }
+    }
+    __syncthreads();
+    for (int q = 0; q < PER; ++q) hist[t * PER + q] = 0;
+    if (t == 0) {
+        const unsigned long long above = s_above;
+        ctl->aux[0] |= (unsigned long long)s_choice << shift;
+        ctl->aux[1] |= ((1ull << bits) - 1ull) << shift;
+        ctl->aux[2] = r - above;
+        ctl->aux[3] += above;
+    }
+    __syncthreads();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSelThreads) k_topn_select_all(const T* __restrict__ coef,
+                                                                 const uint64_t* __restrict__ sel, int window,
+                                                                 uint64_t base, uint64_t n, Ctl* ctl,
+                                                                 unsigned int* __restrict__ hist,
+                                                                 uint64_t* __restrict__ cand, uint64_t cand_cap,
+                                                                 uint64_t seg_cap, unsigned int* __restrict__ seg_count,
+                                                                 SlotMap slots, unsigned int* bar) {
+    constexpr int ITEMS = 16;
+    constexpr int CHUNK = kSelThreads * ITEMS;
+    __shared__ unsigned int sh[kTopnBinsN];
+    __shared__ unsigned long long s_part[kSelThreads];
+    __shared__ unsigned int s_w[kSelThreads / 32];
+    __shared__ unsigned long long s_base;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned int lt = (1u << lane) - 1u;
+    // digit 1
+    if (blockIdx.x == 0) block_select<kTopnBins1>(hist, window ? 48 : 52, window ? 11 : 12, ctl, s_part);
+    if (!grid_barrier(bar, ctl, 720)) return;
+    // the boundary bin's keys into this block's segment
+    {
+        const uint64_t prefix = __ldcg(&ctl->aux[0]), mask = __ldcg(&ctl->aux[1]);
+        if (window && blockIdx.x == 0 && tid == 0) {
+            const uint64_t bin = prefix >> 48;
+            if (bin == 0 || bin == 2047) ctl->aux[5] = 1;  // the boundary left the window: retry in full range
+        }
+        if (tid == 0) s_base = 0;
+        __syncthreads();
+        for (uint64_t c0 = (uint64_t)blockIdx.x * CHUNK; c0 < n; c0 += (uint64_t)gridDim.x * CHUNK) {
+            const uint64_t wbase = c0 + (uint64_t)warp * 32 * ITEMS;
+            uint64_t key[ITEMS];
+#pragma unroll
+            for (int i = 0; i < ITEMS; ++i) {
+                const uint64_t e = wbase + (uint64_t)i * 32 + lane;
+                key[i] = e < n ? (sel ? sel[e] : raw_bits(coef[e])) : 0ull;
+            }
+            unsigned int ball[ITEMS];
+            unsigned int wc = 0;
+#pragma unroll
+            for (int i = 0; i < ITEMS; ++i) {
+                if (!sel) {
+                    const uint64_t mk = mag_key<T>(from_raw<T>(key[i]));
+                    key[i] = window ? window_key(mk, base) : mk;
+                }
+                const uint64_t e = wbase + (uint64_t)i * 32 + lane;
+                const bool hit = e < n && (key[i] & mask) == prefix && slot_live(slots, e);
+                ball[i] = __ballot_sync(0xffffffffu, hit);
+                wc += __popc(ball[i]);
+            }
+            if (lane == 0) s_w[warp] = wc;
+            __syncthreads();
+            unsigned int wx = 0, tot = 0;
+#pragma unroll
+            for (int w = 0; w < kSelThreads / 32; ++w) {
+                wx += w < warp ? s_w[w] : 0u;
+                tot += s_w[w];
+            }
+            const unsigned long long seg_used = s_base;
+            __syncthreads();
+            if (tid == 0) s_base = seg_used + tot;
+            unsigned long long slot = (uint64_t)blockIdx.x * seg_cap + seg_used + wx;
+#pragma unroll
+            for (int i = 0; i < ITEMS; ++i) {
+                if ((ball[i] >> lane) & 1u) {
+                    const unsigned long long q = slot + __popc(ball[i] & lt);
+                    if (PS_GUARD(ctl, q < cand_cap, 721)) cand[q] = key[i];
+                }
+                slot += __popc(ball[i]);
+            }
+            __syncthreads();
+        }
+        if (tid == 0) seg_count[blockIdx.x] = (unsigned int)s_base;
+    }
+    if (!grid_barrier(bar, ctl, 722)) return;
+    // four 13-bit digits over this block's own candidates (it reads what it wrote)
+    const unsigned int len = seg_count[blockIdx.x];
+    const uint64_t* seg = cand + (uint64_t)blockIdx.x * seg_cap;
+    const int shifts[2][4] = {{39, 26, 13, 0}, {35, 22, 9, 0}};
+    for (int d = 0; d < 4; ++d) {
+        const int shift = shifts[window ? 1 : 0][d];
+        for (int i = tid; i < kTopnBinsN; i += kSelThreads) sh[i] = 0;
+        __syncthreads();
+        const uint64_t prefix = __ldcg(&ctl->aux[0]), mask = __ldcg(&ctl->aux[1]);
+        for (unsigned int i = tid; i < len; i += kSelThreads) {
+            const uint64_t mk = seg[i];
+            if ((mk & mask) == prefix) atomicAdd(&sh[(mk >> shift) & (kTopnBinsN - 1)], 1u);
+        }
+        __syncthreads();
+        for (int i = tid; i < kTopnBinsN; i += kSelThreads)
+            if (sh[i]) atomicAdd(&hist[i], sh[i]);
+        if (!grid_barrier(bar, ctl, 723)) return;
+        if (blockIdx.x == 0) block_select<kTopnBinsN>(hist, shift, 13, ctl, s_part);
+        if (!grid_barrier(bar, ctl, 724)) return;
     }
 }
 
@@ -817,9 +1005,12 @@ static inline uint64_t topn_seg_cap(uint64_t n, int sms) {
     return (nchunks + g - 1) / g * (kThreads * 16);
 }
 
+// Words of the TopN candidate buffer: block segments holding every element of their chunks and
+// the segment lengths, for any grid of at most 8 blocks per multiprocessor (the multi-launch
+// select's grid_for and the cooperative select's resident grid).
 uint64_t topn_cand_words(uint64_t n, int sms) {
-    const uint64_t g = grid_for(n, sms);
-    return topn_seg_cap(n, sms) * g + (g + 1) / 2;
+    const uint64_t gmax = (uint64_t)(sms > 0 ? sms : 1) * 8, nchunks = (n + kThreads * 16 - 1) / (kThreads * 16);
+    return (nchunks + gmax) * (kThreads * 16) + (gmax + 1) / 2;
 }
 
 template <int W, typename T>
@@ -963,24 +1154,64 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
                                                             n, hist, slots);
         prof->end(st);
     }
-    // digit 1: the select key's top 12 bits (key >> 52), or in a window the bin of 2^48 units;
-    // then 13-bit digits down to bit 0 (a window's last digit overlaps bits already fixed)
-    prof->begin(K_TOPN_STEP, kTopnBins1 * 8.0, st);
-    k_topn_select<kTopnBins1><<<1, 1024, 0, st>>>(hist, window ? 48 : 52, window ? 11 : 12, ctl);
-    prof->end(st);
-    prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
-    k_topn_cand<T><<<cgrid, kThreads, 0, st>>>(coef, sel, window ? 1 : 0, base, n, ctl, cand, key_cap, seg_cap,
-                                              seg_count, slots);
-    prof->end(st);
-    static const int kShifts[2][4] = {{39, 26, 13, 0}, {35, 22, 9, 0}};
-    for (int d = 0; d < 4; ++d) {
-        const int shift = kShifts[window ? 1 : 0][d];
-        prof->begin(K_TOPN_HIST, 0.0, st);
-        k_topn_hist_cand<<<2 * sms, kThreads, 0, st>>>(cand, ctl, shift, hist, seg_cap, seg_count, cgrid);
+    // the whole select in one cooperative launch when the device runs it (the multi-launch path
+    // below otherwise)
+    bool selected = false;
+    {
+        static std::atomic<int> per_sm{0};
+        int per = per_sm.load(std::memory_order_relaxed);
+        if (per == 0) {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_topn_select_all<T>, kSelThreads, 0) !=
+                    cudaSuccess ||
+                per < 1)
+                per = -1;
+            cudaGetLastError();
+            per_sm.store(per, std::memory_order_relaxed);
+        }
+        if (per > 0) {
+            const uint64_t nchunks = (n + kSelThreads * 16 - 1) / (kSelThreads * 16);
+            const unsigned int G =
+                (unsigned int)std::max<uint64_t>(1, std::min<uint64_t>(std::min<uint64_t>(grid_for(n, sms), nchunks),
+                                                                       (uint64_t)per * (sms > 0 ? sms : 1)));
+            const uint64_t gseg = (nchunks + G - 1) / G * (kSelThreads * 16);
+            const uint64_t gkey = gseg * G;
+            if (gkey + (G + 1) / 2 <= cand_cap) {
+                unsigned int* gcount = reinterpret_cast<unsigned int*>(cand + gkey);
+                unsigned int* bar = &ctl->tile_counter[4];
+                cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned int), st);
+                const int win = window ? 1 : 0;
+                void* args[] = {(void*)&coef, (void*)&sel,  (void*)&win,   (void*)&base, (void*)&n,
+                                (void*)&ctl,  (void*)&hist, (void*)&cand,  (void*)&gkey, (void*)&gseg,
+                                (void*)&gcount, (void*)&slots, (void*)&bar};
+                prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
+                e = cudaLaunchCooperativeKernel((const void*)k_topn_select_all<T>, dim3(G), dim3(kSelThreads), args,
+                                                0, st);
+                prof->end(st);
+                selected = e == cudaSuccess;
+                if (!selected) cudaGetLastError();  // not launched: the multi-launch path selects instead
+            }
+        }
+    }
+    if (!selected) {
+        // digit 1: the select key's top 12 bits (key >> 52), or in a window the bin of 2^48 units;
+        // then 13-bit digits down to bit 0 (a window's last digit overlaps bits already fixed)
+        prof->begin(K_TOPN_STEP, kTopnBins1 * 8.0, st);
+        k_topn_select<kTopnBins1><<<1, 1024, 0, st>>>(hist, window ? 48 : 52, window ? 11 : 12, ctl);
         prof->end(st);
-        prof->begin(K_TOPN_STEP, kTopnBinsN * 8.0, st);
-        k_topn_select<kTopnBinsN><<<1, 1024, 0, st>>>(hist, shift, 13, ctl);
+        prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
+        k_topn_cand<T><<<cgrid, kThreads, 0, st>>>(coef, sel, window ? 1 : 0, base, n, ctl, cand, key_cap, seg_cap,
+                                                  seg_count, slots);
         prof->end(st);
+        static const int kShifts[2][4] = {{39, 26, 13, 0}, {35, 22, 9, 0}};
+        for (int d = 0; d < 4; ++d) {
+            const int shift = kShifts[window ? 1 : 0][d];
+            prof->begin(K_TOPN_HIST, 0.0, st);
+            k_topn_hist_cand<<<2 * sms, kThreads, 0, st>>>(cand, ctl, shift, hist, seg_cap, seg_count, cgrid);
+            prof->end(st);
+            prof->begin(K_TOPN_STEP, kTopnBinsN * 8.0, st);
+            k_topn_select<kTopnBinsN><<<1, 1024, 0, st>>>(hist, shift, 13, ctl);
+            prof->end(st);
+        }
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const uint32_t tiles = (uint32_t)((n + kThreads * 16 - 1) / (kThreads * 16));
