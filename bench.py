@@ -653,7 +653,9 @@ def config_learned_tfim8(args):
             r["max_error"] = _max_error(r["values"], ref["values"])
             plain[b] = r
         for b in args.learn_budgets:
-            r = learned.trotter_series(obs, nq, step(h), steps, truncation.scored_topn(1 << b, sc), "f32", "x+")
+            r = learned.trotter_series(obs, nq, step(h), steps,
+                                       truncation.scored_topn(1 << b, sc, rescore_every=args.learn_rescore or len(step(h))),
+                                       "f32", "x+")
             r["max_error"] = _max_error(r["values"], ref["values"])
             scored[b] = r
         slim = lambda d: {str(k): {"max_error": v["max_error"], "wall_s": round(v["wall_s"], 4),
@@ -701,8 +703,9 @@ def config_learned_xxz256(args):
     plain = learned.trotter_series(obs, L, step, steps, truncation.topn(1 << b), "f64", state)
     runs = {"plain_f64": {b: plain}, "learned_f32": {}}
     for lb in (b - 2, b):
-        runs["learned_f32"][lb] = learned.trotter_series(obs, L, step, steps, truncation.scored_topn(1 << lb, sc),
-                                                         "f32", state)
+        runs["learned_f32"][lb] = learned.trotter_series(
+            obs, L, step, steps, truncation.scored_topn(1 << lb, sc, rescore_every=args.learn_rescore or len(step)), "f32",
+            state)
     sc.close()
     out = {
         "workload": f"config 4: open XXZ chain L=256, Jz=0.5, dt=0.1, {steps} steps ({765 * steps} channels), Z_128 "
@@ -765,6 +768,8 @@ def main():
     ap.add_argument("--learn-ref-cap", type=int, default=29, help="log2 TopN cap of the reference run")
     ap.add_argument("--learn-train-eps", type=float, default=1e-5, help="threshold of the attribution runs")
     ap.add_argument("--learn-samples", type=int, default=1024, help="attribution samples per step boundary")
+    ap.add_argument("--learn-rescore", type=int, default=0,
+                    help="layers between the learned pass's fresh predictions (0: one Trotter step)")
     ap.add_argument("--xxz-budget", type=int, default=24, help="log2 TopN budget of the L=256 XXZ comparison")
     ap.add_argument("--xxz-steps", type=int, default=50)
     args = ap.parse_args()

@@ -67,7 +67,11 @@ typedef enum ps_pass_kind {
     PS_PASS_NONE = 0,
     PS_PASS_TOPN = 1,    /* keep the n largest |c|^2; ties first in key order (builtin.rs:73-129) */
     PS_PASS_SCORED_TOPN = 2, /* keep the n terms the handle's scorer ranks highest (ps_set_scorer);
-                               ties first in key order, a NaN score never kept */
+                               ties first in key order, a NaN score never kept.  samples > 1 (a
+                               residual scorer, the only pass of the policy): the scorer predicts
+                               for every term only every `samples` layers; in between, each term
+                               carries its prediction f (a partner its parent's) and ranks by
+                               log|c| + f inside the layer's merge and select */
     PS_PASS_APPROX_TOPN = 3, /* ApproxTopN (builtin.rs:240-468): every octave of |c|^2 above the
                                boundary octave kept whole, then the first of the boundary octave
                                in key order up to n in all; a NaN never kept */

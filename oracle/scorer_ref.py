@@ -84,9 +84,20 @@ def features(keys, logc, rem, nq, W, fscale, num_sites=None):
     return p, f
 
 
-def forward(params, keys, logc, rem, nq, W, fscale, site_row=None):
+def f16(a):
+    """Round float32 values to IEEE half (nearest even), returned as float32."""
+    if EXACT:
+        return np.asarray(a, np.float64)
+    return np.asarray(a, np.float32).astype(np.float16).astype(np.float32)
+
+
+def forward(params, keys, logc, rem, nq, W, fscale, site_row=None, tc=None):
     """``site_row``: embedding row of each qubit of the scored keys (-1: ignored), the inference
-    site map; the keys then have len(site_row) qubits and W words per half."""
+    site map; the keys then have len(site_row) qubits and W words per half.  ``tc``: the device's
+    tensor-core inference path (scorers of at most 64 rows; the default decides by nq), whose
+    first hidden activation is an f16 operand instead of bf16."""
+    if tc is None:
+        tc = nq <= 64 and not EXACT
     embed, u, b1, w2, b2, w3, b3 = unpack(params, nq)
     sites = nq if site_row is None else len(site_row)
     p, f = features(keys, logc, rem, nq, W, fscale, num_sites=sites)
@@ -98,7 +109,7 @@ def forward(params, keys, logc, rem, nq, W, fscale, site_row=None):
         m = p[:, q] != 0
         if m.any():
             z1[m] += embed[r, p[m, q] - 1]
-    h1 = bf16(gelu(z1))
+    h1 = f16(gelu(z1)) if tc else bf16(gelu(z1))
     z2 = f32(h1.astype(np.float64) @ w2.astype(np.float64)) + b2[None, :]
     h2 = gelu(z2)
     y = b3 + (h2 * w3[None, :]).sum(axis=1)
@@ -107,7 +118,7 @@ def forward(params, keys, logc, rem, nq, W, fscale, site_row=None):
 
 def gradients(params, keys, logc, rem, target, nq, W, fscale):
     embed, u, b1, w2, b2, w3, b3 = unpack(params, nq)
-    y, c = forward(params, keys, logc, rem, nq, W, fscale)
+    y, c = forward(params, keys, logc, rem, nq, W, fscale, tc=False)  # training runs the bf16 kernels
     n = len(y)
     err = y - np.asarray(target, np.float32)
     dy = (2.0 / n) * err if EXACT else np.float32(2.0 / n) * err

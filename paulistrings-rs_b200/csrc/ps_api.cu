@@ -84,6 +84,14 @@ struct ps_sum {
     ps_scorer* scorer = nullptr;   // PS_PASS_SCORED_TOPN
     double scorer_remaining = 0;   // layers still to apply
     Buf sel;                       // scored TopN select keys
+    // Inherited scoring (a scored pass with a rescore interval above 1): each row carries the
+    // scorer's prediction f (its score is log|c| + f) in fcol[buffer]; partners inherit their
+    // parent's; every `interval` layers the scorer predicts afresh for every row.
+    Buf fcol[2], pf;
+    bool f_valid = false;          // fcol[cur] holds the current rows' predictions
+    uint64_t f_age = 0;            // layers since the predictions were made
+    bool score_window = false;     // the next score select may bin in the window at score_base
+    uint64_t score_base = 0;
     SortScratch sort{};
     Buf sort_status;
     Buf up_x, up_z, up_c, up_k, up_v0, up_v1, up_c0, up_st;  // ingest / readout staging, grow-only
@@ -862,6 +870,14 @@ void table_support(const ps_table& t, uint64_t (&out)[W]) {
         if (t.qubits[j] < 64u * W) out[t.qubits[j] / 64] |= 1ull << (t.qubits[j] % 64);
 }
 
+// The rescore interval of an inherited scored pass (the policy's first and only pass is a
+// scored TopN whose `samples` field is above 1, with a residual scorer attached), else 0.
+uint64_t inherit_interval(const ps_policy* p, const ps_sum* s) {
+    if (!p || p->num_passes != 1 || p->passes[0].kind != PS_PASS_SCORED_TOPN || p->passes[0].samples <= 1) return 0;
+    if (!s->scorer || !s->scorer->cfg.residual) return 0;
+    return p->passes[0].samples;
+}
+
 // ---------------------------------------------------------------------------
 // per-width / per-dtype operations
 // ---------------------------------------------------------------------------
@@ -896,6 +912,9 @@ struct Engine {
     }
 
     static uint64_t* K(ps_sum* s, int w) { return static_cast<uint64_t*>(s->keys[w].p); }
+    static float* F(ps_sum* s, int w) { return static_cast<float*>(s->fcol[w].p); }
+    // a prediction column as long as store buffer w
+    static cudaError_t reserve_f(ps_sum* s, int w) { return ensure(s, s->fcol[w], s->cap[w] * sizeof(float)); }
 
     // Can this layer be skipped (see ps_sum::support)?  identity0: the table maps the identity
     // pattern to itself alone with amplitude 1.
@@ -939,6 +958,7 @@ struct Engine {
             for (int w = 0; w < W; ++w) s->support[w] = 0;
             s->support_known = true;
             s->keep_clean = false;
+            s->f_valid = false;
             return PS_OK;
         }
         cudaError_t e = cudaSuccess;
@@ -956,6 +976,7 @@ struct Engine {
         if (e != cudaSuccess) return cuda_fail(s, e, "upload: pack");
         s->support_known = false;
         s->keep_clean = false;
+        s->f_valid = false;
         e = cudaMemcpyAsync(s->hcount + 48, &s->ctl->support[0], sizeof(s->ctl->support), cudaMemcpyDeviceToHost,
                             s->stream);
         if (e != cudaSuccess) return cuda_fail(s, e, "upload: support");
@@ -1010,9 +1031,12 @@ struct Engine {
         cudaError_t e = reserve_store(s, spare, s->live_n);
         if (e == cudaSuccess) e = ensure(s, s->status, (s->n / 4096 + 4) * sizeof(unsigned long long));
         if (e != cudaSuccess) return cuda_fail(s, e, what);
+        if (e == cudaSuccess && s->f_valid) e = reserve_f(s, spare);
+        if (e != cudaSuccess) return cuda_fail(s, e, what);
         uint64_t out_n = 0;
         e = StoreOps<W, T>::densify(K(s, s->cur), C(s, s->cur), s->n, slot_map(s), K(s, spare), C(s, spare),
-                                    (unsigned long long*)s->status.p, s->ctl, s->hcount, &out_n, s->stream, &s->prof);
+                                    (unsigned long long*)s->status.p, s->ctl, s->hcount, &out_n, s->stream, &s->prof,
+                                    s->f_valid ? F(s, s->cur) : nullptr, s->f_valid ? F(s, spare) : nullptr);
         s->prof.resolve();
         if (e != cudaSuccess) return cuda_fail(s, e, what);
         unsigned int fl = 0, fi = 0;
@@ -1096,12 +1120,19 @@ struct Engine {
         // the first layer pass is TopN (or ApproxTopN) and could trigger: the merge builds its
         // first select digit (the octave histogram); before plain TopN the merge writes slots
         const int first_pass = policy && policy->num_passes > 0 ? policy->passes[0].kind : PS_PASS_NONE;
-        const bool fuse_topn = (first_pass == PS_PASS_TOPN || first_pass == PS_PASS_APPROX_TOPN) &&
+        // an inherited scored pass: the predictions ride along with the rows (folded noise cannot)
+        const bool carry_f = inherit_interval(policy, s) > 1 && s->f_valid && !noise;
+        if (!carry_f) s->f_valid = false;
+        const bool scored_fuse = carry_f && first_pass == PS_PASS_SCORED_TOPN;
+        const bool fuse_topn = (first_pass == PS_PASS_TOPN || first_pass == PS_PASS_APPROX_TOPN || scored_fuse) &&
                                out_rows > policy->passes[0].n;
         const uint64_t span_rows = merge_span_rows<W>(out_rows);
         // (the TopN kernels index a slotted store's rows in 32 bits)
-        const bool slotted = fuse_topn && first_pass == PS_PASS_TOPN && !s->fault_stall && span_rows < (1ull << 32);
+        const bool slotted = fuse_topn && (first_pass == PS_PASS_TOPN || scored_fuse) && !s->fault_stall &&
+                             span_rows < (1ull << 32);
         cudaError_t e = reserve_store(s, spare, slotted ? span_rows : out_rows);
+        if (e == cudaSuccess && carry_f) e = reserve_f(s, spare);
+        if (e == cudaSuccess && carry_f && a.L.partners) e = ensure(s, s->pf, n * sizeof(float));
         if (e == cudaSuccess && slotted)
             e = ensure(s, s->slot_count, (span_rows / merge_slot_rows<W>() + 1) * sizeof(unsigned int));
         if (e != cudaSuccess) return cuda_fail(s, e, "apply: output store");
@@ -1142,9 +1173,14 @@ struct Engine {
         a.err_flags = &err_flags;
         a.err_info = &err_info;
         a.prof = &s->prof;
-        const bool window = first_pass == PS_PASS_TOPN && s->topn_window;
-        a.topn_hist_mode = first_pass == PS_PASS_APPROX_TOPN ? 1 : (window ? 2 : 0);
-        a.topn_hist_base = window ? s->topn_base : 0;
+        const bool window = (first_pass == PS_PASS_TOPN && s->topn_window) || (scored_fuse && s->score_window);
+        a.topn_hist_mode = first_pass == PS_PASS_APPROX_TOPN ? 1 : (scored_fuse ? (window ? 4 : 3) : (window ? 2 : 0));
+        a.topn_hist_base = window ? (scored_fuse ? s->score_base : s->topn_base) : 0;
+        if (carry_f) {
+            a.Sf = F(s, s->cur);
+            a.Pf = a.L.partners ? static_cast<float*>(s->pf.p) : nullptr;
+            a.Of = F(s, spare);
+        }
         if (s->hist_ready) {
             cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
             s->hist_ready = false;
@@ -1211,6 +1247,7 @@ struct Engine {
         (void)policy;
         GenLayer<W, T> G;
         to_gen_layer<W, T>(t, G);
+        s->f_valid = false;  // the sort path carries no predictions
         {
             bool identity0 = G.cnt[0] == 1 && G.amp[0][0] == T(1);
             for (int w = 0; identity0 && w < W; ++w)
@@ -1279,7 +1316,8 @@ struct Engine {
     }
 
     static ps_status finalize(ps_sum* s, const ps_policy* policy) {
-        if (!(policy && policy->num_passes > 0 && policy->passes[0].kind == PS_PASS_TOPN)) {
+        const uint64_t interval = inherit_interval(policy, s);
+        if (!(policy && policy->num_passes > 0 && (policy->passes[0].kind == PS_PASS_TOPN || interval > 1))) {
             ps_status ps = densify(s, "finalize");
             if (ps != PS_OK) return ps;
         }
@@ -1290,6 +1328,12 @@ struct Engine {
         for (int i = 0; policy && i < policy->num_passes; ++i) {
             const ps_pass& p = policy->passes[i];
             if (p.kind == PS_PASS_SCORED_TOPN) {
+                if (interval > 1) {
+                    ps_status ps = scored_inherited(s, p.n, interval,
+                                                    ready && i == 0 && s->hist_kind == PS_PASS_SCORED_TOPN);
+                    if (ps != PS_OK) return ps;
+                    continue;
+                }
                 if (ready && i == 0) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
                 ps_status ps = scored_topn(s, p.n);
                 if (ps != PS_OK) return ps;
@@ -1414,6 +1458,7 @@ struct Engine {
         s->n = out_n;
         ++s->collapses;
         s->keep_clean = false;  // the drawn terms carry new coefficients
+        s->f_valid = false;
         return PS_OK;
     }
 
@@ -1450,6 +1495,101 @@ struct Engine {
         if (ps != PS_OK) return ps;
         s->cur = spare;
         s->n = out_n;
+        return PS_OK;
+    }
+
+    // The inherited learned pass.  Every `interval` layers (and whenever the rows carry no valid
+    // predictions) the scorer predicts afresh for every row, writing the predictions, the select
+    // keys and their first-digit histogram in one pass, and the select runs on those keys; in
+    // the layers between, the merge carried each row's prediction (partners their parent's) and
+    // histogrammed log|c| + f, and the select computes the same score from the coefficient and
+    // the prediction.  Either way the compaction carries the predictions with the kept rows.
+    // hist_ok: the layer's merge left a histogram of the scores in s->hist.
+    static ps_status scored_inherited(ps_sum* s, uint64_t keep_n, uint64_t interval, bool hist_ok) {
+        ps_scorer* sc = s->scorer;
+        const bool rescore = !s->f_valid || s->f_age + 1 >= interval;
+        const uint64_t live = s->slotted ? s->live_n : s->n;
+        auto drop_hist = [&]() {
+            if (hist_ok) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+            hist_ok = false;
+        };
+        cudaError_t e;
+        if (rescore) {
+            drop_hist();
+            if ((e = ensure(s, s->fcol[s->cur], s->cap[s->cur] * sizeof(float))) != cudaSuccess ||
+                (e = ensure(s, s->sel, std::max<uint64_t>(s->n, 1) * sizeof(uint64_t))) != cudaSuccess)
+                return cuda_fail(s, e, "scored TopN: scratch");
+            if (s->n) {
+                ScorerArgs A;
+                A.p = static_cast<const uint16_t*>(sc->bf.p);
+                A.L = sc->L;
+                A.nq = sc->nq;
+                for (int f = 0; f < 3; ++f) A.fscale[f] = sc->cfg.feature_scale[f];
+                A.residual = 1;
+                A.site_row = sc->mapped ? static_cast<const int16_t*>(sc->site_map.p) : nullptr;
+                ScoreInput in{};
+                in.keys = K(s, s->cur);
+                in.coef64 = std::is_same<T, double>::value ? (const double*)C(s, s->cur) : nullptr;
+                in.coef32 = std::is_same<T, float>::value ? (const float*)C(s, s->cur) : nullptr;
+                in.rem_uniform = (float)(s->scorer_remaining / sc->cfg.layers_per_unit);
+                in.n = s->n;  // a slotted store's gaps are scored too and never read
+                e = launch_score<W>(A, in, nullptr, (uint64_t*)s->sel.p, (unsigned int*)s->hist.p, s->ctl, s->sms,
+                                    s->stream, &s->prof, F(s, s->cur));
+                if (e != cudaSuccess) return cuda_fail(s, e, "scored TopN: score");
+                hist_ok = true;
+            }
+            s->f_valid = true;
+            s->f_age = 0;
+        } else {
+            ++s->f_age;
+        }
+        if (live <= keep_n || keep_n == 0) {
+            drop_hist();
+            if (keep_n == 0 && live > 0) {
+                s->n = 0;
+                s->slotted = false;
+                return PS_OK;
+            }
+            return densify(s, "scored TopN");
+        }
+        const int spare = 1 - s->cur;
+        e = reserve_store(s, spare, keep_n);
+        if (e == cudaSuccess) e = reserve_f(s, spare);
+        if (e == cudaSuccess) e = ensure(s, s->cand, topn_cand_words(s->n, s->sms) * sizeof(uint64_t));
+        if (e == cudaSuccess) e = ensure(s, s->status, (s->n / 4096 + 4) * sizeof(unsigned long long));
+        if (e != cudaSuccess) {
+            drop_hist();
+            return cuda_fail(s, e, "scored TopN: scratch");
+        }
+        uint64_t out_n = 0;
+        const bool window = !rescore && hist_ok && s->score_window;
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            const bool win = window && attempt == 0;
+            e = StoreOps<W, T>::topn(K(s, s->cur), C(s, s->cur), s->n, keep_n, K(s, spare), C(s, spare),
+                                     (unsigned int*)s->hist.p, hist_ok && attempt == 0, (uint64_t*)s->cand.p,
+                                     topn_cand_words(s->n, s->sms), (unsigned long long*)s->status.p, s->ctl, s->hcount,
+                                     &out_n, s->sms, s->stream, &s->prof, rescore ? (const uint64_t*)s->sel.p : nullptr,
+                                     win, win ? s->score_base : 0, slot_map(s), F(s, s->cur), F(s, spare));
+            s->prof.resolve();
+            if (e != cudaSuccess) return cuda_fail(s, e, "scored TopN");
+            unsigned int fl = 0, fi = 0;
+            topn_flags(s->hcount, &fl, &fi);
+            ps_status ps = flags_status(s, fl, fi, "scored TopN");
+            if (ps != PS_OK) {
+                cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
+                return ps;
+            }
+            if (!(win && topn_window_missed(s->hcount))) {
+                const uint64_t boundary = topn_boundary(s->hcount, win ? s->score_base : 0);
+                const uint64_t half = 1024ull << 48;
+                s->score_window = boundary != 0;
+                s->score_base = boundary > half ? boundary - half : 0;
+                break;
+            }
+        }
+        s->cur = spare;
+        s->n = out_n;
+        s->slotted = false;
         return PS_OK;
     }
 
@@ -1658,6 +1798,8 @@ ps_status ps_destroy(ps_sum* s) {
     if (!s) return PS_OK;
     DeviceGuard g(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
+    for (Buf* b : {&s->fcol[0], &s->fcol[1], &s->pf})
+        release(*b);
     for (Buf* b : {&s->keys[0], &s->keys[1], &s->coef[0], &s->coef[1], &s->pk, &s->pc, &s->idx, &s->dv, &s->fv,
                    &s->slots, &s->status, &s->bounds, &s->hist, &s->cand, &s->partial, &s->dout, &s->sort_status,
                    &s->up_x, &s->up_z, &s->up_c, &s->up_k, &s->up_v0, &s->up_v1, &s->up_c0, &s->up_st, &s->sel,
@@ -1764,7 +1906,7 @@ ps_status ps_propagate(ps_sum* s, const ps_channel* channels, uint64_t num_chann
         // as the rotation reads it, so the run costs no pass of its own.
         uint64_t fj = li;
         while (fj < num_channels && fj - li < (uint64_t)kMaxNoise && foldable_noise(tables[fj], s->nq)) ++fj;
-        if (fj > li && fj < num_channels && passes_idle(policy, s) &&
+        if (fj > li && fj < num_channels && passes_idle(policy, s) && inherit_interval(policy, s) <= 1 &&
             dispatch<Engine>(s, [&](auto op) { return decltype(op)::folds_noise(tables[fj]) ? PS_OK : PS_ERR_UNSUPPORTED; }) ==
                 PS_OK) {
             NoiseList N;
@@ -2246,6 +2388,7 @@ ps_status ps_set_scorer(ps_sum* s, ps_scorer* sc, double remaining_layers) {
     if (!s) return PS_ERR_INVALID;
     if (sc && (sc->device != s->device || sc->num_sites != s->nq))
         return set_err(s, PS_ERR_INVALID, "set_scorer: the scorer was built (or site-mapped) for another device or qubit count");
+    if (sc != s->scorer) s->f_valid = false;  // predictions of another scorer
     s->scorer = sc;
     s->scorer_remaining = remaining_layers;
     return PS_OK;

@@ -278,6 +278,30 @@ __device__ __forceinline__ uint64_t octave_key(T c) {
     return ((uint64_t)__double_as_longlong(m) >> 52) + 1ull;
 }
 
+// The learned pass's ranking: score = log|c| (floored at -200, so a zero coefficient stays
+// finite) + the scorer's prediction f, as a select key: the score's order-preserving f32
+// pattern shifted up (0 for a NaN score, never kept), larger kept first.
+template <typename T>
+__device__ __forceinline__ float log_abs_coeff(T c);
+template <>
+__device__ __forceinline__ float log_abs_coeff<double>(double c) {
+    return fmaxf((float)log(fabs(c)), -200.0f);
+}
+template <>
+__device__ __forceinline__ float log_abs_coeff<float>(float c) {
+    return fmaxf(logf(fabsf(c)), -200.0f);
+}
+__device__ __forceinline__ uint64_t score_select_key(float y) {
+    const uint32_t u = __float_as_uint(y);
+    if (y != y) return 0;  // NaN: never kept
+    const uint32_t order = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    return (uint64_t)order << 31;
+}
+template <typename T>
+__device__ __forceinline__ uint64_t score_key(T c, float f) {
+    return score_select_key(__fadd_rn(log_abs_coeff<T>(c), f));
+}
+
 // A coefficient's bit pattern in a 64-bit word and back, so a loop can issue all of its loads
 // before it uses any of them.
 __device__ __forceinline__ uint64_t raw_bits(double v) { return (uint64_t)__double_as_longlong(v); }

@@ -237,6 +237,9 @@ struct RotationArgs {
     uint64_t* span_out;       // slotted output: rows its slots span
     int sms;                  // multiprocessors of the device (persistent grids)
     const NoiseList* noise;   // host copy of the folded noise channels (nullptr: none)
+    const float* Sf;          // the learned pass's predictions: of the store rows (nullptr: none),
+    float* Pf;                // of the partners (inherited from their parents),
+    float* Of;                // and of the output rows
     unsigned long long* noise_drops;       // device, kMaxNoise + 1: own rows first dropped after channel j
     unsigned long long* host_noise_drops;  // pinned, kMaxNoise + 1: the same, after the layer's sync
 };

@@ -517,7 +517,8 @@ __global__ void __launch_bounds__(NT) k_level_apply(const uint32_t* __restrict__
                                                         uint64_t n, const Levels lv, const RotLayer<W> L,
                                                         int accumulate, int scatter, uint64_t* __restrict__ Pk,
                                                         T* __restrict__ Pc, const LevelTile* __restrict__ tiles,
-                                                        Ctl* ctl, const KeepProg keep, const NoiseArg<NOISE> N) {
+                                                        Ctl* ctl, const KeepProg keep, const NoiseArg<NOISE> N,
+                                                        const float* __restrict__ Sf, float* __restrict__ Pf) {
     constexpr int IT = kScanTile / NT;  // partners per thread
     __shared__ int s_w[NT / 32][4 * LV];
     __shared__ AmpTab<T> A;
@@ -623,6 +624,7 @@ __global__ void __launch_bounds__(NT) k_level_apply(const uint32_t* __restrict__
             }
             store_key<W>(Pk, (uint64_t)dest, k);
             Pc[dest] = pc;
+            if (Pf) Pf[dest] = Sf[row];  // a partner inherits its parent's prediction
         }
     }
 }
@@ -698,6 +700,9 @@ struct MergeSmem {
     static constexpr size_t key_bytes = (size_t)KEY_ROWS * 16 * W;
     static constexpr size_t coef_bytes = ((size_t)COEF_SLOTS * sizeof(T) + 15) / 16 * 16;
     static constexpr size_t bytes = key_bytes + coef_bytes;
+    // the learned pass's prediction column (floats, 16-byte windows of 4), after the coefficients
+    static constexpr int F_SLOTS = TILE + 4 + 16;
+    static constexpr size_t f_bytes = ((size_t)F_SLOTS * sizeof(float) + 15) / 16 * 16;
 };
 
 template <int W>
@@ -732,12 +737,13 @@ __device__ __forceinline__ bool eq_regs(const uint64_t (&a)[2 * W], const uint64
 // pair is consumed in one step, so STEPS = ITEMS + 1 unrolled steps cover it (the caller checks
 // that nothing is left).  Step s leaves its output in ok[s] / ov[s] and sets bit s of the
 // returned mask when the output is kept (nonzero and passing the keep program).
-template <int W, typename T, int STEPS, bool NOISE>
+template <int W, typename T, int STEPS, bool NOISE, bool HASF>
 __device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc, const uint64_t* sPk, const T* sPc,
                                                uint32_t& i, uint32_t ie, uint32_t& j, uint32_t je,
                                                const RotLayer<W>& L, const AmpTab<T>& A, const KeepProg& keep,
                                                uint64_t (&ok)[STEPS][2 * W], T (&ov)[STEPS],
-                                               const NoiseSmem<T>* NS, unsigned int* s_drop) {
+                                               const NoiseSmem<T>* NS, unsigned int* s_drop, const float* sSf,
+                                               const float* sPf, float (&of)[STEPS]) {
     uint32_t mask = 0;
     uint64_t a[2 * W], b[2 * W];
     if (i < ie) ld_row<W>(sSk, i, a);
@@ -750,6 +756,7 @@ __device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc
             if (takeS) {
 #pragma unroll
                 for (int w = 0; w < 2 * W; ++w) ok[s][w] = a[w];
+                if constexpr (HASF) of[s] = sSf[i];  // the string's own prediction
                 if constexpr (NOISE) {
                     T c = sSc[i];
                     const int d = noise_apply<W, T>(*NS, keep, a, c);
@@ -770,6 +777,7 @@ __device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc
             } else {
 #pragma unroll
                 for (int w = 0; w < 2 * W; ++w) ok[s][w] = b[w];
+                if constexpr (HASF) of[s] = sPf[j];  // a new string: its parent's prediction
                 v = sPc[j];
                 if (++j < je) ld_row<W>(sPk, j, b);
             }
@@ -780,7 +788,7 @@ __device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc
     return mask;
 }
 
-template <int W, typename T, bool NOISE>
+template <int W, typename T, bool NOISE, bool HASF>
 __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t* __restrict__ Sk, const T* __restrict__ Sc,
                                                   uint64_t n, const uint64_t* __restrict__ Pk,
                                                   const T* __restrict__ Pc, const ulonglong2* __restrict__ bounds,
@@ -790,12 +798,15 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
                                                   unsigned int* __restrict__ topn_hist, int hist_mode,
                                                   uint64_t hist_base, unsigned int* __restrict__ slot_count,
                                                   long long stall_limit, const NoiseArg<NOISE> N,
-                                                  unsigned long long* __restrict__ noise_drops) {
+                                                  unsigned long long* __restrict__ noise_drops,
+                                                  const float* __restrict__ Sf, const float* __restrict__ Pf,
+                                                  float* __restrict__ Of) {
     using SM = MergeSmem<W, T>;
     constexpr int ITEMS = RotTile<W>::kMergeItems;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     uint64_t* sK = reinterpret_cast<uint64_t*>(smem_raw);
     T* sC = reinterpret_cast<T*>(smem_raw + SM::key_bytes);
+    float* sF = reinterpret_cast<float*>(smem_raw + SM::bytes);  // HASF only
     __shared__ uint64_t bar;
     __shared__ unsigned int s_tile;
     __shared__ unsigned int s_warp[kBlock / 32];
@@ -840,16 +851,31 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
         T* sPc = sC + sc_slots;  // P coefficient of local j at sPc[p_off + j]
         uint64_t* sSk = sK;
         uint64_t* sPk = sK + (size_t)cs * 2 * W;
+        // the prediction column, in windows of 4 floats (16 bytes)
+        const uint64_t fsa = b0.x & ~(uint64_t)3, fpa = b0.y & ~(uint64_t)3;
+        const uint32_t fs_off = (uint32_t)(b0.x - fsa), fp_off = (uint32_t)(b0.y - fpa);
+        const uint32_t sf_slots = (fs_off + cs + 3) / 4 * 4;
+        float* sSf = sF;
+        float* sPf = sF + sf_slots;
         if (tid == 0 && cs + cp) {
             bulk_wait_read_all();  // the previous tile's bulk store has read the staged rows
             uint32_t kbS = cs * 16u * W, kbP = cp * 16u * W;
             uint32_t cbS = cs ? round16((s_off + cs) * (uint32_t)sizeof(T)) : 0u;
             uint32_t cbP = cp ? round16((p_off + cp) * (uint32_t)sizeof(T)) : 0u;
-            mbar_arrive_expect_tx(&bar, kbS + kbP + cbS + cbP);
+            uint32_t fbS = 0, fbP = 0;
+            if constexpr (HASF) {
+                fbS = cs ? round16((fs_off + cs) * 4u) : 0u;
+                fbP = cp ? round16((fp_off + cp) * 4u) : 0u;
+            }
+            mbar_arrive_expect_tx(&bar, kbS + kbP + cbS + cbP + fbS + fbP);
             if (kbS) bulk_g2s(sSk, Sk + b0.x * 2 * W, kbS, &bar);
             if (kbP) bulk_g2s(sPk, Pk + b0.y * 2 * W, kbP, &bar);
             if (cbS) bulk_g2s(sSc, Sc + sa, cbS, &bar);
             if (cbP) bulk_g2s(sPc, Pc + pa, cbP, &bar);
+            if constexpr (HASF) {
+                if (fbS) bulk_g2s(sSf, Sf + fsa, fbS, &bar);
+                if (fbP) bulk_g2s(sPf, Pf + fpa, fbP, &bar);
+            }
         }
         if (cs + cp) {  // block-uniform
             const bool ok = mbar_wait(&bar, phase & 1u, ctl, 302);
@@ -890,9 +916,10 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
         constexpr int STEPS = ITEMS + 1;
         uint64_t ok[STEPS][2 * W];
         T ov[STEPS];
+        float of[STEPS];
         uint32_t i = i0, j = j0;
-        const uint32_t mask =
-            merge_walk<W, T, STEPS, NOISE>(sSk, Sc_l, sPk, Pc_l, i, ie, j, je, L, A, keep, ok, ov, NS, s_drop);
+        const uint32_t mask = merge_walk<W, T, STEPS, NOISE, HASF>(sSk, Sc_l, sPk, Pc_l, i, ie, j, je, L, A, keep, ok,
+                                                                  ov, NS, s_drop, sSf + fs_off, sPf + fp_off, of);
         PS_GUARD(ctl, i >= ie && j >= je, 305);
         unsigned int total;
         const unsigned int excl = block_exclusive_sum<kBlock>(__popc(mask), s_warp, total);
@@ -905,6 +932,7 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
                 if ((mask >> s) & 1u) {
                     store_key<W>(sK, r, ok[s]);
                     sC[r] = ov[s];
+                    if constexpr (HASF) sF[r] = of[s];
                     ++r;
                 }
             }
@@ -939,16 +967,25 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
             bulk_s2g(Ok + off * 2 * W, sK, total * 16u * W);
             bulk_commit();
         }
-        // coefficients: coalesced stores, with the fused first TopN digit
+        // coefficients (and predictions): coalesced stores, with the fused first TopN digit
         for (uint32_t q = tid; q < total; q += kBlock) {
             const T v = sC[q];
             Oc[off + q] = v;
+            float fv = 0.0f;
+            if constexpr (HASF) {
+                fv = sF[q];
+                Of[off + q] = fv;
+            }
             if (topn_hist) {
                 uint32_t bin;
                 if (hist_mode == 1)
                     bin = octave_bin<T>(v);
                 else if (hist_mode == 2)
                     bin = (uint32_t)(window_key(mag_key<T>(v), hist_base) >> 48);
+                else if (hist_mode == 3)
+                    bin = (uint32_t)(score_key<T>(v, fv) >> 52);
+                else if (hist_mode == 4)
+                    bin = (uint32_t)(window_key(score_key<T>(v, fv), hist_base) >> 48);
                 else
                     bin = (uint32_t)(mag_key<T>(v) >> 52);
                 atomicAdd(&s_hist[bin], 1u);
@@ -1043,19 +1080,21 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
             if (a.noise && last) {
                 if (narrow)
                     k_level_apply<W, T, 4, kApplyThreads, true><<<sgrid, kApplyThreads, 0, st>>>(
-                        a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, b > 0, last, a.Pk, a.Pc, lt, ctl, a.keep, *a.noise);
+                        a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, b > 0, last, a.Pk, a.Pc, lt, ctl, a.keep, *a.noise,
+                        a.Sf, a.Pf);
                 else
                     k_level_apply<W, T, kMaxLevels, kApplyThreads, true><<<sgrid, kApplyThreads, 0, st>>>(
-                        a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, b > 0, last, a.Pk, a.Pc, lt, ctl, a.keep, *a.noise);
+                        a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, b > 0, last, a.Pk, a.Pc, lt, ctl, a.keep, *a.noise,
+                        a.Sf, a.Pf);
             } else {
                 if (narrow)
                     k_level_apply<W, T, 4, kApplyThreads, false><<<sgrid, kApplyThreads, 0, st>>>(
                         a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, b > 0, last, a.Pk, a.Pc, lt, ctl, a.keep,
-                        NoNoise{});
+                        NoNoise{}, a.Sf, a.Pf);
                 else
                     k_level_apply<W, T, kMaxLevels, kApplyThreads, false><<<sgrid, kApplyThreads, 0, st>>>(
                         a.idx, a.D, a.F, a.Sk, a.Sc, a.n, lv, a.L, b > 0, last, a.Pk, a.Pc, lt, ctl, a.keep,
-                        NoNoise{});
+                        NoNoise{}, a.Sf, a.Pf);
             }
             a.prof->end(st);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1084,25 +1123,30 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     // bounded look-back gives up
     cudaMemsetAsync(&ctl->tile_counter[3], a.inject_stall ? 1 : 0, 1, st);
     cudaMemsetAsync(reinterpret_cast<unsigned char*>(&ctl->tile_counter[3]) + 1, 0, 3, st);
-    size_t smem = MergeSmem<W, T>::bytes;
-    static std::atomic<int> merge_per_sm[2];
+    const size_t smem = MergeSmem<W, T>::bytes;
+    static std::atomic<int> merge_per_sm[3];
     const long long stall = a.inject_stall ? (long long)a.stall_limit : 0ll;
     a.prof->begin(K_MERGE, 0.0, st);
     if (a.noise) {
         cudaMemsetAsync(a.noise_drops, 0, (kMaxNoise + 1) * sizeof(unsigned long long), st);
-        const int mper = resident_blocks(k_merge<W, T, true>, kBlock, smem, merge_per_sm[1]);
+        const int mper = resident_blocks(k_merge<W, T, true, false>, kBlock, smem, merge_per_sm[1]);
         const uint32_t mgrid = (uint32_t)std::min<uint64_t>(mtiles_hi, (uint64_t)mper * (a.sms > 0 ? a.sms : 1));
-        k_merge<W, T, true><<<mgrid, kBlock, smem, st>>>(a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok,
-                                                           a.Oc, a.out_cap, a.status, ctl, a.topn_hist,
-                                                           a.topn_hist_mode, a.topn_hist_base, a.slot_count, stall,
-                                                           *a.noise, a.noise_drops);
+        k_merge<W, T, true, false><<<mgrid, kBlock, smem, st>>>(
+            a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc, a.out_cap, a.status, ctl, a.topn_hist,
+            a.topn_hist_mode, a.topn_hist_base, a.slot_count, stall, *a.noise, a.noise_drops, nullptr, nullptr, nullptr);
+    } else if (a.Sf) {
+        const size_t fsmem = smem + MergeSmem<W, T>::f_bytes;
+        const int mper = resident_blocks(k_merge<W, T, false, true>, kBlock, fsmem, merge_per_sm[2]);
+        const uint32_t mgrid = (uint32_t)std::min<uint64_t>(mtiles_hi, (uint64_t)mper * (a.sms > 0 ? a.sms : 1));
+        k_merge<W, T, false, true><<<mgrid, kBlock, fsmem, st>>>(
+            a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc, a.out_cap, a.status, ctl, a.topn_hist,
+            a.topn_hist_mode, a.topn_hist_base, a.slot_count, stall, NoNoise{}, nullptr, a.Sf, a.Pf, a.Of);
     } else {
-        const int mper = resident_blocks(k_merge<W, T, false>, kBlock, smem, merge_per_sm[0]);
+        const int mper = resident_blocks(k_merge<W, T, false, false>, kBlock, smem, merge_per_sm[0]);
         const uint32_t mgrid = (uint32_t)std::min<uint64_t>(mtiles_hi, (uint64_t)mper * (a.sms > 0 ? a.sms : 1));
-        k_merge<W, T, false><<<mgrid, kBlock, smem, st>>>(a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok,
-                                                            a.Oc, a.out_cap, a.status, ctl, a.topn_hist,
-                                                            a.topn_hist_mode, a.topn_hist_base, a.slot_count, stall,
-                                                            NoNoise{}, nullptr);
+        k_merge<W, T, false, false><<<mgrid, kBlock, smem, st>>>(
+            a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc, a.out_cap, a.status, ctl, a.topn_hist,
+            a.topn_hist_mode, a.topn_hist_base, a.slot_count, stall, NoNoise{}, nullptr, nullptr, nullptr, nullptr);
     }
     a.prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1155,10 +1199,12 @@ template uint64_t merge_span_rows<4>(uint64_t);
 template <int W, typename T>
 cudaError_t configure_rotation_kernels() {
     cudaError_t e = cudaSuccess;
-    const void* kernels[2] = {(const void*)k_merge<W, T, false>, (const void*)k_merge<W, T, true>};
+    const void* kernels[3] = {(const void*)k_merge<W, T, false, false>, (const void*)k_merge<W, T, true, false>,
+                              (const void*)k_merge<W, T, false, true>};
     for (const void* k : kernels) {
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MergeSmem<W, T>::bytes);
+            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(MergeSmem<W, T>::bytes + MergeSmem<W, T>::f_bytes));
         // all of the unified L1 as shared memory, so residency is set by registers, not the carveout
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,

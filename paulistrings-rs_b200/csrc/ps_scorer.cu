@@ -18,6 +18,7 @@
 // issuing, frees its TMEM and returns.
 #include <algorithm>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "ps_device.cuh"
 #include "ps_scorer.h"
@@ -54,9 +55,13 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t sbo = 204
     return d;                                           // base offset 0, no swizzle
 }
 
+// kind::f16 with A and B both f16 (bits 7-12 zero): the inference kernel's second layer
+constexpr uint32_t kIdescF16 = (1u << 4) | ((uint32_t)(kHid >> 3) << 17) | ((uint32_t)(kScoreTile >> 4) << 24);
+
 // D (TMEM, 128 lanes x 128 f32 columns) (+)= A (128 x 128) * B^T, A and B K-major in shared
 // memory.  K-step j starts 2 core matrices (256 bytes) further along K.
-__device__ __forceinline__ void umma_tile(uint32_t d_tmem, uint32_t a_saddr, uint32_t b_saddr, bool accumulate) {
+__device__ __forceinline__ void umma_tile(uint32_t d_tmem, uint32_t a_saddr, uint32_t b_saddr, bool accumulate,
+                                          uint32_t idesc = kIdesc) {
     const uint64_t ad = umma_desc(a_saddr), bd = umma_desc(b_saddr);
 #pragma unroll
     for (int j = 0; j < kHid / 16; ++j) {
@@ -65,7 +70,7 @@ __device__ __forceinline__ void umma_tile(uint32_t d_tmem, uint32_t a_saddr, uin
             "{\n\t.reg .pred p;\n\t"
             "setp.ne.b32 p, %4, 0;\n\t"
             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-            ::"r"(d_tmem), "l"(ad + 16ull * j), "l"(bd + 16ull * j), "r"(kIdesc), "r"(acc));
+            ::"r"(d_tmem), "l"(ad + 16ull * j), "l"(bd + 16ull * j), "r"(idesc), "r"(acc));
     }
 }
 
@@ -122,6 +127,24 @@ __device__ __forceinline__ float gelu_grad(float x) {
     const float t = tanh_hw(kGeluS * (x + kGeluA * x2 * x));
     return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * kGeluS * (1.0f + 3.0f * kGeluA * x2);
 }
+
+// The inference kernel's GELU on two f16 lanes at once: tanh.approx.f16x2 and packed f16
+// arithmetic (6 instructions per pair).  Its results feed an f16 operand (11 significant
+// bits, finer than the bf16 operand of the other paths).  Beyond |x| ~ 40 the cube overflows
+// to +-inf, where tanh gives +-1 and the GELU its exact limits x and 0.
+__device__ __forceinline__ __half2 tanh_h2(__half2 x) {
+    uint32_t in = *reinterpret_cast<uint32_t*>(&x), out;
+    asm("tanh.approx.f16x2 %0, %1;" : "=r"(out) : "r"(in));
+    return *reinterpret_cast<__half2*>(&out);
+}
+__device__ __forceinline__ __half2 gelu_h2(__half2 x) {
+    const __half2 s = __float2half2_rn(kGeluS), sa = __float2half2_rn(kGeluS * kGeluA), h = __float2half2_rn(0.5f);
+    const __half2 x2 = __hmul2(x, x);
+    const __half2 u = __hmul2(x, __hfma2(x2, sa, s));
+    const __half2 hx = __hmul2(x, h);
+    return __hfma2(hx, tanh_h2(u), hx);
+}
+__device__ __forceinline__ uint32_t h2_bits(__half2 v) { return *reinterpret_cast<uint32_t*>(&v); }
 
 // Column sums of a warp's 32 x 32 block: lane l holds row l's 32 values on entry and the sum
 // of column l on exit (v[0]); 31 shuffles.
@@ -222,12 +245,6 @@ __device__ __forceinline__ void store_row_chunk(uint8_t* op, int row, int c, con
     }
 }
 
-__device__ __forceinline__ uint64_t score_select_key(float y) {
-    const uint32_t u = __float_as_uint(y);
-    if (y != y) return 0;  // NaN: never kept
-    const uint32_t order = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-    return (uint64_t)order << 31;
-}
 
 // Shared prologue: B operand from w2 (transposed for the forward GEMM: element (out, in) = w2[in][out];
 // as stored for dh1 = dz2 W2^T: element (in, out) = w2[in][out]).
@@ -247,7 +264,7 @@ __global__ void __launch_bounds__(kScoreThreads) k_score(const ScorerArgs A, con
                                                          float* __restrict__ scores, uint64_t* __restrict__ sel,
                                                          unsigned int* __restrict__ hist, const float* __restrict__ target,
                                                          float inv_batch, TrainScratch S, float* __restrict__ grads,
-                                                         float* __restrict__ loss, Ctl* ctl) {
+                                                         float* __restrict__ loss, Ctl* ctl, float* __restrict__ fout) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* sA = smem;
     uint8_t* sB = smem + kTileBytes;
@@ -331,6 +348,7 @@ __global__ void __launch_bounds__(kScoreThreads) k_score(const ScorerArgs A, con
             for (int j = 0; j < 32; ++j) y += gelu(z2[j] + s_b2[32 * c + j]) * s_w3[32 * c + j];
         }
         if (!TRAIN) {
+            if (fout && valid) fout[row] = y;
             if (A.residual) y += logc;
             if (valid) {
                 if (scores) scores[row] = y;
@@ -546,6 +564,16 @@ __global__ void __launch_bounds__(kScoreThreads) k_train_bwd(const ScorerArgs A,
 }
 
 
+// B operand of the inference kernel's layer 2 in f16: element (out, in) = w2[in][out] (every
+// bf16 weight in f16's normal range converts exactly).
+__device__ __forceinline__ void stage_w2_f16(const ScorerArgs& A, uint8_t* sB) {
+    const uint16_t* w2 = A.p + A.L.w2;
+    for (int i = threadIdx.x; i < kHid * kHid; i += blockDim.x) {
+        const int r = i / kHid, c = i % kHid;  // w2[r][c], r = in, c = out
+        *reinterpret_cast<__half*>(sB + kmaj_off(c, r)) = __float2half_rn(bf2f(w2[i]));
+    }
+}
+
 // ---------------------------------------------------------------------------
 // inference on the tensor cores (scorers of at most kTcRows embedding rows)
 //
@@ -556,7 +584,8 @@ __global__ void __launch_bounds__(kScoreThreads) k_train_bwd(const ScorerArgs A,
 // twice, b1) gives z1 = b1 + f.u + the embedding bag, accumulated in f32 in TMEM.  The counts are
 // small integers and the split features carry 16 significant bits, so the product equals the
 // CUDA-core embedding bag up to the order of f32 additions.  Layer 2 is the 128 x 128 GEMM of the
-// other kernel.  A CTA holds two warpgroups, each owning one tile at a time (its own operand,
+// other kernel, in f16 here: both GELUs run on packed f16 pairs (gelu_h2), the first feeding the
+// f16 operand directly, the second's outputs weighted and summed in f32.  A CTA holds two warpgroups, each owning one tile at a time (its own operand,
 // mbarrier and 128 TMEM columns, shared by the two accumulators in turn) and synchronising on its
 // own named barrier, so one warpgroup's GELUs overlap the other's MMAs.
 // ---------------------------------------------------------------------------
@@ -610,7 +639,8 @@ __device__ __forceinline__ void split_bf16(float v, uint16_t& hi, uint16_t& lo) 
 template <int W>
 __global__ void __launch_bounds__(kTcThreads, 1) k_score_tc(const ScorerArgs A, const ScoreInput in,
                                                             float* __restrict__ scores, uint64_t* __restrict__ sel,
-                                                            unsigned int* __restrict__ hist, Ctl* ctl) {
+                                                            unsigned int* __restrict__ hist, Ctl* ctl,
+                                                            float* __restrict__ fout) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* sB1 = smem;
     uint8_t* sB2 = smem + kOpB1Bytes;
@@ -636,7 +666,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_score_tc(const ScorerArgs A, 
         }
         *reinterpret_cast<uint16_t*>(sB1 + kmaj1_off(n, k)) = v;
     }
-    stage_w2(A, sB2, true);
+    stage_w2_f16(A, sB2);
     for (int i = tid; i < kHid; i += kTcThreads) {
         s_b2[i] = bf2f(A.p[A.L.b2 + i]);
         s_w3[i] = bf2f(A.p[A.L.w3 + i]);
@@ -708,21 +738,27 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_score_tc(const ScorerArgs A, 
             break;
         }
         tc_fence_after();
-        // GELU(z1) as the layer-2 operand, over the dead A1 (128-wide K-major layout)
+        // GELU(z1) as the f16 layer-2 operand, over the dead A1 (128-wide K-major layout)
 #pragma unroll 1
         for (int c = 0; c < kHid / 32; ++c) {
             float z[32];
             tmem_ld32(tmem + lane_base + 32u * c, z);
 #pragma unroll
-            for (int j = 0; j < 32; ++j) z[j] = gelu(z[j]);
-            store_row_chunk(sA, t, c, z);
+            for (int q = 0; q < 4; ++q) {
+                uint4 u;
+                u.x = h2_bits(gelu_h2(__floats2half2_rn(z[8 * q + 0], z[8 * q + 1])));
+                u.y = h2_bits(gelu_h2(__floats2half2_rn(z[8 * q + 2], z[8 * q + 3])));
+                u.z = h2_bits(gelu_h2(__floats2half2_rn(z[8 * q + 4], z[8 * q + 5])));
+                u.w = h2_bits(gelu_h2(__floats2half2_rn(z[8 * q + 6], z[8 * q + 7])));
+                *reinterpret_cast<uint4*>(sA + kmaj_off(t, 32 * c + 8 * q)) = u;
+            }
         }
         fence_async_smem();
         tc_fence_before();
         wg_sync(bar_id);
         if (t == 0) {
             tc_fence_after();
-            umma_tile(tmem, smem_u32(sA), smem_u32(sB2), false);
+            umma_tile(tmem, smem_u32(sA), smem_u32(sB2), false, kIdescF16);
             umma_commit(&s_bar[g]);
         }
         ok = wg_and(bar_id, mbar_wait(&s_bar[g], phase, ctl, 906));
@@ -738,8 +774,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_score_tc(const ScorerArgs A, 
             float z2[32];
             tmem_ld32(tmem + lane_base + 32u * c, z2);
 #pragma unroll
-            for (int j = 0; j < 32; ++j) y += gelu(z2[j] + s_b2[32 * c + j]) * s_w3[32 * c + j];
+            for (int j = 0; j < 32; j += 2) {
+                const float2 g = __half22float2(
+                    gelu_h2(__floats2half2_rn(z2[j] + s_b2[32 * c + j], z2[j + 1] + s_b2[32 * c + j + 1])));
+                y = __fmaf_rn(g.x, s_w3[32 * c + j], y);
+                y = __fmaf_rn(g.y, s_w3[32 * c + j + 1], y);
+            }
         }
+        if (fout && valid) fout[row] = y;  // the network's own output (the prediction a row carries)
         if (A.residual) y += logc;
         if (valid) {
             if (scores) scores[row] = y;
@@ -810,7 +852,7 @@ cudaError_t configure_scorer_kernels() {
 
 template <int W>
 cudaError_t launch_score(const ScorerArgs& A, const ScoreInput& in, float* scores, uint64_t* sel_keys,
-                         unsigned int* hist, Ctl* ctl, int sms, cudaStream_t st, KernelProf* prof) {
+                         unsigned int* hist, Ctl* ctl, int sms, cudaStream_t st, KernelProf* prof, float* fout) {
     if (!in.n) return cudaSuccess;
     // 2 x (128 x 128) bf16 GEMM flops per term plus the output dot; bytes: key + coefficient
     prof->begin(K_SCORE, (double)in.n * (16 * W + 8 + (sel_keys ? 8 : 4)), st);
@@ -819,12 +861,12 @@ cudaError_t launch_score(const ScorerArgs& A, const ScoreInput& in, float* score
         // one CTA per SM (~200 KB of shared memory, 256 TMEM columns), two tiles in flight per CTA
         const uint64_t tiles = (in.n + kScoreTile - 1) / kScoreTile;
         const unsigned int grid = (unsigned int)std::min<uint64_t>((tiles + 1) / 2, (uint64_t)(sms > 0 ? sms : 1));
-        k_score_tc<W><<<grid, kTcThreads, kTcSmem, st>>>(A, in, scores, sel_keys, hist, ctl);
+        k_score_tc<W><<<grid, kTcThreads, kTcSmem, st>>>(A, in, scores, sel_keys, hist, ctl, fout);
     } else {
         // three blocks per SM: 3 x 128 TMEM columns and 3 x ~75 KB of shared memory fit one SM
         k_score<W, false><<<score_grid(in.n, sms, 3), kScoreThreads, kScoreSmem, st>>>(A, in, scores, sel_keys, hist,
                                                                                       nullptr, 0.0f, none, nullptr,
-                                                                                      nullptr, ctl);
+                                                                                      nullptr, ctl, fout);
     }
     prof->end(st);
     return cudaGetLastError();
@@ -838,7 +880,7 @@ cudaError_t launch_train_batch(const ScorerArgs& A, const ScoreInput& in, const 
     prof->begin(K_SCORE_TRAIN, (double)in.n * (16 * W + 12 + 6 * kHid), st);
     k_score<W, true><<<score_grid(in.n, sms, 3), kScoreThreads, kScoreSmem, st>>>(A, in, nullptr, nullptr, nullptr,
                                                                                  target, inv_batch, S, grads, loss,
-                                                                                 ctl);
+                                                                                 ctl, nullptr);
     // one block per SM: 256 TMEM columns and 130 KB of shared memory
     k_train_bwd<W><<<score_grid(in.n, sms, 1), kScoreThreads, kBwdSmem, st>>>(A, in, S, grads, ctl);
     prof->end(st);
@@ -861,11 +903,11 @@ template cudaError_t configure_scorer_kernels<1>();
 template cudaError_t configure_scorer_kernels<2>();
 template cudaError_t configure_scorer_kernels<4>();
 template cudaError_t launch_score<1>(const ScorerArgs&, const ScoreInput&, float*, uint64_t*, unsigned int*, Ctl*,
-                                     int, cudaStream_t, KernelProf*);
+                                     int, cudaStream_t, KernelProf*, float*);
 template cudaError_t launch_score<2>(const ScorerArgs&, const ScoreInput&, float*, uint64_t*, unsigned int*, Ctl*,
-                                     int, cudaStream_t, KernelProf*);
+                                     int, cudaStream_t, KernelProf*, float*);
 template cudaError_t launch_score<4>(const ScorerArgs&, const ScoreInput&, float*, uint64_t*, unsigned int*, Ctl*,
-                                     int, cudaStream_t, KernelProf*);
+                                     int, cudaStream_t, KernelProf*, float*);
 template cudaError_t launch_train_batch<1>(const ScorerArgs&, const ScoreInput&, const float*, float,
                                            const TrainScratch&, float*, float*, Ctl*, int, cudaStream_t, KernelProf*);
 template cudaError_t launch_train_batch<2>(const ScorerArgs&, const ScoreInput&, const float*, float,

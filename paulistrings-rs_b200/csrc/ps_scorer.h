@@ -67,9 +67,12 @@ struct ScoreInput {
 
 // Select keys for the TopN machinery: (order-preserving bits of the score) << 31, 0 for NaN;
 // also histograms their top 11 bits into hist (kTopnBins1 words, zero on entry) when non-null.
+// fout (optional): the network's output per term, before the residual log|c| (the prediction a
+// row carries through the layers of an inherited scored pass).
 template <int W>
 cudaError_t launch_score(const ScorerArgs& A, const ScoreInput& in, float* scores, uint64_t* sel_keys,
-                         unsigned int* hist, Ctl* ctl, int sms, cudaStream_t st, KernelProf* prof);
+                         unsigned int* hist, Ctl* ctl, int sms, cudaStream_t st, KernelProf* prof,
+                         float* fout = nullptr);
 
 // Training: one minibatch.  Forward stores h1, gelu'(z1) and dz2 (bf16) per term and adds
 // dw3, db2, db3 and the summed squared error; backward adds dW2 (tensor cores), db1, du and

@@ -347,13 +347,18 @@ __global__ void __launch_bounds__(kThreads) k_dedup(const uint64_t* __restrict__
 // count[4] candidates.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kThreads) k_topn_hist1(const double* __restrict__ c64, const float* __restrict__ c32,
-                                                         uint64_t n, unsigned int* __restrict__ hist, SlotMap slots) {
+                                                         uint64_t n, unsigned int* __restrict__ hist, SlotMap slots,
+                                                         const float* __restrict__ fpred) {
     __shared__ unsigned int sh[kTopnBins1];
     for (int i = threadIdx.x; i < kTopnBins1; i += kThreads) sh[i] = 0;
     __syncthreads();
     for (uint64_t i = blockIdx.x * (uint64_t)kThreads + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kThreads) {
         if (!slot_live(slots, i)) continue;
-        uint64_t mk = c64 ? mag_key<double>(c64[i]) : mag_key<float>(c32[i]);
+        uint64_t mk;
+        if (fpred)
+            mk = c64 ? score_key<double>(c64[i], fpred[i]) : score_key<float>(c32[i], fpred[i]);
+        else
+            mk = c64 ? mag_key<double>(c64[i]) : mag_key<float>(c32[i]);
         atomicAdd(&sh[mk >> 52], 1u);
     }
     __syncthreads();
@@ -507,7 +512,8 @@ __global__ void __launch_bounds__(kSelThreads) k_topn_select_all(const T* __rest
                                                                  unsigned int* __restrict__ hist,
                                                                  uint64_t* __restrict__ cand, uint64_t cand_cap,
                                                                  uint64_t seg_cap, unsigned int* __restrict__ seg_count,
-                                                                 SlotMap slots, unsigned int* bar) {
+                                                                 SlotMap slots, unsigned int* bar,
+                                                                 const float* __restrict__ fpred) {
     constexpr int ITEMS = 16;
     constexpr int CHUNK = kSelThreads * ITEMS;
     __shared__ unsigned int sh[kTopnBinsN];
@@ -531,17 +537,19 @@ __global__ void __launch_bounds__(kSelThreads) k_topn_select_all(const T* __rest
         for (uint64_t c0 = (uint64_t)blockIdx.x * CHUNK; c0 < n; c0 += (uint64_t)gridDim.x * CHUNK) {
             const uint64_t wbase = c0 + (uint64_t)warp * 32 * ITEMS;
             uint64_t key[ITEMS];
+            float fp[ITEMS];
 #pragma unroll
             for (int i = 0; i < ITEMS; ++i) {
                 const uint64_t e = wbase + (uint64_t)i * 32 + lane;
                 key[i] = e < n ? (sel ? sel[e] : raw_bits(coef[e])) : 0ull;
+                fp[i] = fpred && e < n ? fpred[e] : 0.0f;
             }
             unsigned int ball[ITEMS];
             unsigned int wc = 0;
 #pragma unroll
             for (int i = 0; i < ITEMS; ++i) {
                 if (!sel) {
-                    const uint64_t mk = mag_key<T>(from_raw<T>(key[i]));
+                    const uint64_t mk = fpred ? score_key<T>(from_raw<T>(key[i]), fp[i]) : mag_key<T>(from_raw<T>(key[i]));
                     key[i] = window ? window_key(mk, base) : mk;
                 }
                 const uint64_t e = wbase + (uint64_t)i * 32 + lane;
@@ -603,10 +611,12 @@ __device__ __forceinline__ uint64_t select_key(const T* __restrict__ coef, const
     return sel ? sel[e] : mag_key<T>(coef[e]);
 }
 
-// The compaction's key: 0 mag_key, 1 precomputed, 2 ApproxTopN's octave key.
+// The compaction's key: 0 mag_key, 1 precomputed, 2 ApproxTopN's octave key, 4 the learned
+// score from the coefficient and the row's prediction.
 template <typename T>
 __device__ __forceinline__ uint64_t compact_key(const T* __restrict__ coef, const uint64_t* __restrict__ sel, int mode,
-                                                uint64_t e) {
+                                                uint64_t e, const float* __restrict__ fpred) {
+    if (mode == 4) return score_key<T>(coef[e], fpred[e]);
     return mode == 2 ? octave_key<T>(coef[e]) : select_key<T>(coef, sel, e);
 }
 
@@ -633,7 +643,7 @@ __global__ void __launch_bounds__(kThreads) k_topn_cand(const T* __restrict__ co
                                                         int window, uint64_t base, uint64_t n, Ctl* ctl,
                                                         uint64_t* __restrict__ cand, uint64_t cand_cap,
                                                         uint64_t seg_cap, unsigned int* __restrict__ seg_count,
-                                                        SlotMap slots) {
+                                                        SlotMap slots, const float* __restrict__ fpred) {
     constexpr int ITEMS = 16;
     constexpr int CHUNK = kThreads * ITEMS;
     __shared__ unsigned int s_w[kThreads / 32];
@@ -651,17 +661,19 @@ __global__ void __launch_bounds__(kThreads) k_topn_cand(const T* __restrict__ co
         const uint64_t wbase = c0 + (uint64_t)warp * 32 * ITEMS;
         // every load of the chunk first, then the keys and ballots
         uint64_t key[ITEMS];
+        float fp[ITEMS];
 #pragma unroll
         for (int i = 0; i < ITEMS; ++i) {
             const uint64_t e = wbase + (uint64_t)i * 32 + lane;
             key[i] = e < n ? (sel ? sel[e] : raw_bits(coef[e])) : 0ull;
+            fp[i] = fpred && e < n ? fpred[e] : 0.0f;
         }
         unsigned int ball[ITEMS];
         unsigned int wc = 0;
 #pragma unroll
         for (int i = 0; i < ITEMS; ++i) {
             if (!sel) {
-                const uint64_t mk = mag_key<T>(from_raw<T>(key[i]));
+                const uint64_t mk = fpred ? score_key<T>(from_raw<T>(key[i]), fp[i]) : mag_key<T>(from_raw<T>(key[i]));
                 key[i] = window ? window_key(mk, base) : mk;
             }
             const uint64_t e = wbase + (uint64_t)i * 32 + lane;
@@ -727,7 +739,8 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
                                                            const uint64_t* __restrict__ sel, int key_mode,
                                                            uint64_t base, uint64_t n, unsigned long long keep_n,
                                                            uint64_t* __restrict__ okeys, T* __restrict__ ocoef,
-                                                           unsigned long long* status, Ctl* ctl, SlotMap slots) {
+                                                           unsigned long long* status, Ctl* ctl, SlotMap slots,
+                                                           const float* __restrict__ fin, float* __restrict__ fout) {
     const unsigned long long quota = ctl->aux[0] == 0 ? 0ull : keep_n - ctl->aux[3];
     constexpr int ITEMS = 16;
     constexpr int TILE = kThreads * ITEMS;
@@ -750,7 +763,7 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
         bool isa = false, ist = false;
         if (e < n) {
             // the key load does not wait for the liveness test (a slot's tail is allocated)
-            const uint64_t mk = key_mode == 3 ? 0ull : compact_key<T>(coef, sel, key_mode, e);
+            const uint64_t mk = key_mode == 3 ? 0ull : compact_key<T>(coef, sel, key_mode, e, fin);
             if (sw.live(slots)) {
                 isa = key_mode == 3 || mk > boundary;  // key_mode 3 keeps every row (compacting slots)
                 ist = key_mode != 3 && mk == boundary && boundary != 0;
@@ -808,6 +821,7 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
             if (PS_GUARD(ctl, pos < n, 702)) {
                 store_key<W>(okeys, pos, k);
                 ocoef[pos] = coef[e];
+                if (fout) fout[pos] = fin[e];  // the learned pass's prediction travels with its row
             }
         }
         arank += __popc(ba[i]);
@@ -1128,7 +1142,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
                                  T* ocoef, unsigned int* hist, bool hist_ready, uint64_t* cand, uint64_t cand_cap,
                                  unsigned long long* status, Ctl* ctl, unsigned long long* host_count,
                                  uint64_t* out_n, int sms, cudaStream_t st, KernelProf* prof, const uint64_t* sel,
-                                 bool window, uint64_t base, SlotMap slots) {
+                                 bool window, uint64_t base, SlotMap slots, const float* fpred, float* fout) {
     // aux: prefix, mask, remaining rank, above, -, window miss; count[4]: candidates
     window = window && hist_ready && !sel;
     if (!window) base = 0;
@@ -1151,7 +1165,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
         prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
         k_topn_hist1<<<grid_for(n, sms), kThreads, 0, st>>>(std::is_same<T, double>::value ? (const double*)coef : nullptr,
                                                             std::is_same<T, float>::value ? (const float*)coef : nullptr,
-                                                            n, hist, slots);
+                                                            n, hist, slots, sel ? nullptr : fpred);
         prof->end(st);
     }
     // the whole select in one cooperative launch when the device runs it (the multi-launch path
@@ -1180,9 +1194,10 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
                 unsigned int* bar = &ctl->tile_counter[4];
                 cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned int), st);
                 const int win = window ? 1 : 0;
+                const float* fp = sel ? nullptr : fpred;
                 void* args[] = {(void*)&coef, (void*)&sel,  (void*)&win,   (void*)&base, (void*)&n,
                                 (void*)&ctl,  (void*)&hist, (void*)&cand,  (void*)&gkey, (void*)&gseg,
-                                (void*)&gcount, (void*)&slots, (void*)&bar};
+                                (void*)&gcount, (void*)&slots, (void*)&bar, (void*)&fp};
                 prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
                 e = cudaLaunchCooperativeKernel((const void*)k_topn_select_all<T>, dim3(G), dim3(kSelThreads), args,
                                                 0, st);
@@ -1200,7 +1215,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
         prof->end(st);
         prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
         k_topn_cand<T><<<cgrid, kThreads, 0, st>>>(coef, sel, window ? 1 : 0, base, n, ctl, cand, key_cap, seg_cap,
-                                                  seg_count, slots);
+                                                  seg_count, slots, sel ? nullptr : fpred);
         prof->end(st);
         static const int kShifts[2][4] = {{39, 26, 13, 0}, {35, 22, 9, 0}};
         for (int d = 0; d < 4; ++d) {
@@ -1218,8 +1233,9 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     cudaMemsetAsync(status, 0, (size_t)tiles * sizeof(unsigned long long), st);
     cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
-    k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, sel, sel ? 1 : 0, base, n,
-                                                     (unsigned long long)keep_n, okeys, ocoef, status, ctl, slots);
+    k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, sel, sel ? 1 : (fpred ? 4 : 0), base, n,
+                                                     (unsigned long long)keep_n, okeys, ocoef, status, ctl, slots, fpred,
+                                                     fout);
     prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // the one host synchronization of the pass: counts, error flags and the select's aux words
@@ -1233,7 +1249,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
 template <int W, typename T>
 cudaError_t StoreOps<W, T>::densify(const uint64_t* keys, const T* coef, uint64_t n, SlotMap slots, uint64_t* okeys,
                                     T* ocoef, unsigned long long* status, Ctl* ctl, unsigned long long* host_count,
-                                    uint64_t* out_n, cudaStream_t st, KernelProf* prof) {
+                                    uint64_t* out_n, cudaStream_t st, KernelProf* prof, const float* fin, float* fout) {
     if (n == 0) {
         *out_n = 0;
         return cudaSuccess;
@@ -1246,7 +1262,7 @@ cudaError_t StoreOps<W, T>::densify(const uint64_t* keys, const T* coef, uint64_
     cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     prof->begin(K_TOPN_COMPACT, 0.0, st);
     k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, nullptr, 3, 0ull, n, 0ull, okeys, ocoef, status, ctl,
-                                                     slots);
+                                                     slots, fin, fout);
     prof->end(st);
     cudaError_t e;
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1301,7 +1317,7 @@ cudaError_t StoreOps<W, T>::approx_topn(const uint64_t* keys, const T* coef, uin
     cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
     k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, nullptr, 2, 0ull, n, (unsigned long long)keep_n,
-                                                     okeys, ocoef, status, ctl, SlotMap{nullptr, 0u});
+                                                     okeys, ocoef, status, ctl, SlotMap{nullptr, 0u}, nullptr, nullptr);
     prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     cudaMemcpyAsync(host_count, &ctl->count[0], offsetof(Ctl, err_info) + sizeof(unsigned int),

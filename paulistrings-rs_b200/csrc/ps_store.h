@@ -70,17 +70,21 @@ struct StoreOps {
     // host_count: pinned scratch of at least 20 words; on return it holds the control block's
     // counts, tile counters and error words (read the flags with topn_flags).
     // sel: when non-null, precomputed select keys (larger kept first, 0 never) replace mag_key(c);
-    // hist_ready must then hold their digit-1 histogram.
+    // hist_ready must then hold their digit-1 histogram.  fpred: the learned pass's predictions;
+    // the select key is then score_key(c, f) (windowed like mag_key when window), and the kept
+    // rows' predictions are written to fout.
     static cudaError_t topn(const uint64_t* keys, const T* coef, uint64_t n, uint64_t keep_n, uint64_t* okeys, T* ocoef,
                             unsigned int* hist, bool hist_ready, uint64_t* cand, uint64_t cand_cap,
                             unsigned long long* status, Ctl* ctl, unsigned long long* host_count, uint64_t* out_n,
                             int sms, cudaStream_t st, KernelProf* prof, const uint64_t* sel = nullptr,
-                            bool window = false, uint64_t base = 0, SlotMap slots = SlotMap{nullptr, 0u});
+                            bool window = false, uint64_t base = 0, SlotMap slots = SlotMap{nullptr, 0u},
+                            const float* fpred = nullptr, float* fout = nullptr);
     // Compact the live rows of a slotted store of n rows (its span) into okeys / ocoef, in order;
     // *out_n = rows kept.  Reads the counts and error words into host_count (synchronizes).
     static cudaError_t densify(const uint64_t* keys, const T* coef, uint64_t n, SlotMap slots, uint64_t* okeys,
                                T* ocoef, unsigned long long* status, Ctl* ctl, unsigned long long* host_count,
-                               uint64_t* out_n, cudaStream_t st, KernelProf* prof);
+                               uint64_t* out_n, cudaStream_t st, KernelProf* prof, const float* fin = nullptr,
+                               float* fout = nullptr);
     // ApproxTopN (crates/paulistrings/src/truncation/builtin.rs:240-468): every octave of |c|^2
     // above the boundary octave kept, then the first quota boundary terms in key order.
     // hist: 2048 words, zero on entry and exit, holding the octave histogram when hist_ready;

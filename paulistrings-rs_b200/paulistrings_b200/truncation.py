@@ -49,7 +49,7 @@ class Truncation:
             op = " & " if self.kind == "and" else " | "
             return f"({self.args[0]!r}{op}{self.args[1]!r})"
         if self.kind == "scored_topn":
-            return f"truncation.scored_topn({self.args[0]!r}, <scorer>)"
+            return f"truncation.scored_topn({self.args[0]!r}, <scorer>, rescore_every={self.args[2]!r})"
         if self.kind == "collapse_sample":
             return f"truncation.collapse_sample({self.args[0]!r}, {self.args[1]!r}, {self.args[2]!r})"
         return f"truncation.{self.kind}({', '.join(repr(a) for a in self.args)})"
@@ -65,7 +65,7 @@ class Truncation:
             passes.append((_lib.PS_PASS_TOPN, int(self.args[0])))
         elif self.kind == "scored_topn":
             nodes.append((_lib.PS_KEEP_TRUE, 0, 0.0))
-            passes.append((_lib.PS_PASS_SCORED_TOPN, int(self.args[0])))
+            passes.append((_lib.PS_PASS_SCORED_TOPN, int(self.args[0]), int(self.args[2]), 0, 0))
         elif self.kind == "approx_topn":
             nodes.append((_lib.PS_KEEP_TRUE, 0, 0.0))
             passes.append((_lib.PS_PASS_APPROX_TOPN, int(self.args[0])))
@@ -199,12 +199,19 @@ def collapse_sample(cache: int, samples: int, seed: int) -> CollapseSample:
     return CollapseSample(cache, samples, seed)
 
 
-def scored_topn(n: int, scorer) -> Truncation:
+def scored_topn(n: int, scorer, rescore_every: int = 1) -> Truncation:
     """Keep the ``n`` terms ``scorer`` (a ``paulistrings_b200.learned.Scorer``) ranks highest
-    after every layer; ties first in key order, NaN scores never kept."""
+    after every layer; ties first in key order, NaN scores never kept.
+
+    ``rescore_every`` > 1 (a residual scorer, the policy's only pass): the network predicts for
+    every term only every ``rescore_every`` layers; in the layers between, each term carries its
+    prediction (a partner its parent's) and ranks by log|c| + that prediction, so a layer costs
+    about what a plain TopN layer costs."""
     if n < 0:
         raise ValueError("scored_topn needs n >= 0")
-    return Truncation("scored_topn", int(n), scorer)
+    if rescore_every < 1:
+        raise ValueError("scored_topn needs rescore_every >= 1")
+    return Truncation("scored_topn", int(n), scorer, int(rescore_every))
 
 
 def policy_to_c(policy):

@@ -16,6 +16,7 @@ import paulistrings_b200 as ps
 from oracle import scorer_ref
 from paulistrings_b200 import _lib, learned, truncation, workloads
 from paulistrings_b200.circuit import Circuit
+from tests._util import oracle_sum
 
 
 def random_params(nq, seed, scale=0.3):
@@ -90,7 +91,10 @@ def test_scored_topn_lowering():
     sc = object()
     pol = truncation.coeff(1e-8) & truncation.scored_topn(1000, sc)
     nodes, passes = pol.lowered()
-    assert passes == [(_lib.PS_PASS_SCORED_TOPN, 1000)]
+    assert passes == [(_lib.PS_PASS_SCORED_TOPN, 1000, 1, 0, 0)]  # samples = the rescore interval
+    assert truncation.scored_topn(64, sc, rescore_every=192).lowered()[1] == [(_lib.PS_PASS_SCORED_TOPN, 64, 192, 0, 0)]
+    with pytest.raises(ValueError):
+        truncation.scored_topn(64, sc, rescore_every=0)
     assert pol.scorer() is sc
     assert truncation.topn(5).scorer() is None
     with pytest.raises(ValueError):
@@ -236,3 +240,100 @@ def test_scored_pass_keeps_the_highest_scored_terms(dtype):
     # boundary disagreement from that
     assert len(kept ^ want) <= 4
     assert np.array_equal(kc, fc[np.isin(np.arange(len(fc)), chosen)]) or len(kept ^ want) > 0
+
+
+# ---------------------------------------------------------------------------
+# inherited scores (scored_topn with rescore_every > 1)
+# ---------------------------------------------------------------------------
+
+def _rotation_circuit(nq, gates, seed):
+    rng = np.random.default_rng(seed)
+    circ = Circuit(nq)
+    for _ in range(gates):
+        a, b = (int(q) for q in rng.choice(nq, size=2, replace=False))
+        circ.pauli_rotation("".join(rng.choice(list("XYZ"), size=2)), [a, b], float(rng.uniform(0.3, 1.2)))
+    return circ
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_inherited_scores_of_a_constant_network_rank_by_magnitude(dtype):
+    """A network whose output is a constant makes log|c| + f a monotone function of |c|: the
+    inherited pass (predictions carried by the merge, partners inheriting, the select on
+    log|c| + f) must keep what plain TopN keeps, up to |c| values that tie in f32's log."""
+    nq, keep = 64, 6000
+    sc = learned.Scorer(nq, layers_per_unit=4.0, feature_scale=FSCALE, seed=6, residual=True)
+    p = np.zeros(learned.layout(nq)["total"], np.float32)
+    p[learned.layout(nq)["b3"]] = 0.5
+    sc.set_params(p)
+    x, z, c = workloads.random_observable(nq, 4000, seed=8)
+    circ = _rotation_circuit(nq, 6, seed=3)
+    a = ps.GpuPauliSum(nq, dtype)
+    a.upload(x, z, c)
+    sa = a.propagate(circ, truncation.scored_topn(keep, sc, rescore_every=4), "forward", with_stats=True)
+    b = ps.GpuPauliSum(nq, dtype)
+    b.upload(x, z, c)
+    sb = b.propagate(circ, truncation.topn(keep), "forward", with_stats=True)
+    assert sa.terms_after == sb.terms_after
+    ka, kb = a.download(), b.download()
+    got = {(u.tobytes(), v.tobytes()) for u, v in zip(ka[0], ka[1])}
+    want = {(u.tobytes(), v.tobytes()) for u, v in zip(kb[0], kb[1])}
+    assert len(got ^ want) <= 8, len(got ^ want)
+
+
+def _host_layer(nq, dtype, keys, coefs, channel):
+    """One layer through the oracle, no truncation: (keys, coefficients)."""
+    W = ps.width_for(nq)
+    o = oracle_sum(nq, keys[:, :W], keys[:, W:], coefs, dtype)
+    o.apply(("rotation", channel.paulis, list(channel.qubits), channel.theta), adjoint=False, policy=None)
+    return o.get()
+
+
+@pytest.mark.gpu
+def test_inherited_scores_follow_their_rows():
+    """Three layers, rescored every third: layer 1 scores every row afresh, layers 2 and 3 rank by
+    log|c| + the carried prediction (an own row keeps its string's, a new partner takes its
+    parent's).  A host restatement (oracle layers, the device scorer's predictions at the
+    rescoring, the inheritance rule) must keep nearly the same rows (predictions recovered from
+    the device's scores can differ from the carried ones in the last bit)."""
+    nq, keep = 40, 1500
+    W = ps.width_for(nq)
+    sc = learned.Scorer(nq, layers_per_unit=3.0, feature_scale=FSCALE, seed=6, residual=True)
+    sc.set_params(random_params(nq, 29, scale=0.3))
+    x, z, c = workloads.random_observable(nq, 1200, seed=12)
+    circ = _rotation_circuit(nq, 3, seed=5)
+    chans = list(circ)
+    g = ps.GpuPauliSum(nq, "f64")
+    g.upload(x, z, c)
+    g.propagate(circ, truncation.scored_topn(keep, sc, rescore_every=3), "forward", remaining_layers=3)
+    gx, gz, gc = g.download()
+
+    keys = np.concatenate([x, z], axis=1).astype(np.uint64)
+    coefs = c.astype(np.float64)
+    order = np.lexsort(keys.T[::-1])
+    keys, coefs = keys[order], coefs[order]
+    f = None
+    for li, ch in enumerate(chans):
+        out_k, out_c = _host_layer(nq, "f64", keys, coefs, ch)
+        logc = np.maximum(np.log(np.abs(out_c)).astype(np.float32), np.float32(-200.0))
+        rem = np.float32((3 - (li + 1)) / 3.0)
+        if li == 0:
+            y = sc.score(out_k, logc, rem)
+            new_f = (y - logc).astype(np.float32)
+        else:
+            gx_, gz_ = (np.zeros(W, np.uint64) for _ in range(2))
+            for q, pch in zip(ch.qubits, ch.paulis):
+                if pch in "XY":
+                    gx_[q // 64] |= np.uint64(1 << (q % 64))
+                if pch in "ZY":
+                    gz_[q // 64] |= np.uint64(1 << (q % 64))
+            prev = {kk.tobytes(): ff for kk, ff in zip(keys, f)}
+            gen = np.concatenate([gx_, gz_])
+            new_f = np.array([prev.get(kk.tobytes(), prev.get((kk ^ gen).tobytes())) for kk in out_k], np.float32)
+            y = (logc + new_f).astype(np.float32)
+        top = np.sort(np.argsort(-y, kind="stable")[:keep])
+        keys, coefs, f = out_k[top], out_c[top], new_f[top]
+    got = {(u.tobytes(), v.tobytes()) for u, v in zip(gx, gz)}
+    want = {(kk[:W].tobytes(), kk[W:].tobytes()) for kk in keys}
+    assert len(got) == keep
+    assert len(got ^ want) <= 0.01 * keep, len(got ^ want)
