@@ -1005,6 +1005,19 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
     if (tid == 0) bulk_wait_read_all();  // shared memory stays valid until the last copy has read it
 }
 
+// One launch resets what a rotation layer's kernels count on: the partner and output counts,
+// the tile dispensers (the merge's starts at `merge_start`, 1 under failure injection), the
+// look-back words of the classify and the merge (disjoint ranges of `status`) and the folded
+// noise's drop counters.
+__global__ void k_layer_prep(Ctl* ctl, unsigned long long* __restrict__ status, uint32_t nstatus,
+                             unsigned int merge_start, unsigned long long* __restrict__ noise_drops) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < 2) ctl->count[t] = 0;
+    if (t < 4) ctl->tile_counter[t] = t == 3 ? merge_start : 0u;
+    if (noise_drops && t <= (uint32_t)kMaxNoise) noise_drops[t] = 0;
+    for (uint32_t i = t; i < nstatus; i += gridDim.x * blockDim.x) status[i] = 0;
+}
+
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
@@ -1032,12 +1045,20 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     cudaError_t e;
     const uint64_t m_hi = a.L.partners ? a.n : 0;  // partners cannot outnumber the terms
     if (m_hi > a.p_cap) return cudaErrorMemoryAllocation;  // caller sized the partner buffers by n
-    cudaMemsetAsync(&ctl->count[0], 0, 2 * sizeof(unsigned long long), st);
+    // look-back words: the classify's tiles first, then the merge's (when it is not slotted)
+    const uint32_t ctiles = m_hi > 0 ? (uint32_t)((a.n + CT - 1) / CT) : 0u;
+    const uint32_t mtiles_max = (uint32_t)((a.n + m_hi + MT - 1) / MT);
+    unsigned long long* merge_status = a.status + ctiles;
+    {
+        const uint32_t nstatus = ctiles + (a.slot_count ? 0u : mtiles_max);
+        const uint32_t blocks = std::max<uint32_t>(1u, std::min<uint32_t>((nstatus + 255) / 256, 4u * (uint32_t)a.sms));
+        k_layer_prep<<<blocks, 256, 0, st>>>(ctl, a.status, nstatus, a.inject_stall ? 1u : 0u,
+                                             a.noise ? a.noise_drops : nullptr);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     if (m_hi > 0) {
         // 1. classify
-        uint32_t tiles = (uint32_t)((a.n + CT - 1) / CT);
-        cudaMemsetAsync(a.status, 0, (size_t)tiles * sizeof(unsigned long long), st);
-        cudaMemsetAsync(&ctl->tile_counter[0], 0, 4 * sizeof(unsigned int), st);
+        const uint32_t tiles = ctiles;
         a.prof->begin(K_CLASSIFY, (double)a.n * 16 * W, st);
         k_classify<W, T><<<tiles, kBlock, 0, st>>>(a.Sk, a.n, a.L, a.idx, a.D, a.status, ctl);
         a.prof->end(st);
@@ -1117,35 +1138,31 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
         a.prof->end(st);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
-    // 5. merge
-    if (!a.slot_count) cudaMemsetAsync(a.status, 0, (size_t)mtiles_hi * sizeof(unsigned long long), st);
-    // failure injection: start the dispenser at tile 1, so tile 0 never publishes and tile 1's
-    // bounded look-back gives up
-    cudaMemsetAsync(&ctl->tile_counter[3], a.inject_stall ? 1 : 0, 1, st);
-    cudaMemsetAsync(reinterpret_cast<unsigned char*>(&ctl->tile_counter[3]) + 1, 0, 3, st);
+    // 5. merge (its look-back words and dispenser were reset by k_layer_prep; under failure
+    // injection the dispenser starts at tile 1, so tile 0 never publishes and tile 1's bounded
+    // look-back gives up)
     const size_t smem = MergeSmem<W, T>::bytes;
     static std::atomic<int> merge_per_sm[3];
     const long long stall = a.inject_stall ? (long long)a.stall_limit : 0ll;
     a.prof->begin(K_MERGE, 0.0, st);
     if (a.noise) {
-        cudaMemsetAsync(a.noise_drops, 0, (kMaxNoise + 1) * sizeof(unsigned long long), st);
         const int mper = resident_blocks(k_merge<W, T, true, false>, kBlock, smem, merge_per_sm[1]);
         const uint32_t mgrid = (uint32_t)std::min<uint64_t>(mtiles_hi, (uint64_t)mper * (a.sms > 0 ? a.sms : 1));
         k_merge<W, T, true, false><<<mgrid, kBlock, smem, st>>>(
-            a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc, a.out_cap, a.status, ctl, a.topn_hist,
+            a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc, a.out_cap, merge_status, ctl, a.topn_hist,
             a.topn_hist_mode, a.topn_hist_base, a.slot_count, stall, *a.noise, a.noise_drops, nullptr, nullptr, nullptr);
     } else if (a.Sf) {
         const size_t fsmem = smem + MergeSmem<W, T>::f_bytes;
         const int mper = resident_blocks(k_merge<W, T, false, true>, kBlock, fsmem, merge_per_sm[2]);
         const uint32_t mgrid = (uint32_t)std::min<uint64_t>(mtiles_hi, (uint64_t)mper * (a.sms > 0 ? a.sms : 1));
         k_merge<W, T, false, true><<<mgrid, kBlock, fsmem, st>>>(
-            a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc, a.out_cap, a.status, ctl, a.topn_hist,
+            a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc, a.out_cap, merge_status, ctl, a.topn_hist,
             a.topn_hist_mode, a.topn_hist_base, a.slot_count, stall, NoNoise{}, nullptr, a.Sf, a.Pf, a.Of);
     } else {
         const int mper = resident_blocks(k_merge<W, T, false, false>, kBlock, smem, merge_per_sm[0]);
         const uint32_t mgrid = (uint32_t)std::min<uint64_t>(mtiles_hi, (uint64_t)mper * (a.sms > 0 ? a.sms : 1));
         k_merge<W, T, false, false><<<mgrid, kBlock, smem, st>>>(
-            a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc, a.out_cap, a.status, ctl, a.topn_hist,
+            a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc, a.out_cap, merge_status, ctl, a.topn_hist,
             a.topn_hist_mode, a.topn_hist_base, a.slot_count, stall, NoNoise{}, nullptr, nullptr, nullptr, nullptr);
     }
     a.prof->end(st);

@@ -513,7 +513,10 @@ __global__ void __launch_bounds__(kSelThreads) k_topn_select_all(const T* __rest
                                                                  uint64_t* __restrict__ cand, uint64_t cand_cap,
                                                                  uint64_t seg_cap, unsigned int* __restrict__ seg_count,
                                                                  SlotMap slots, unsigned int* bar,
-                                                                 const float* __restrict__ fpred) {
+                                                                 const float* __restrict__ fpred,
+                                                                 unsigned long long keep_n,
+                                                                 unsigned long long* __restrict__ cstatus,
+                                                                 uint32_t ncstatus) {
     constexpr int ITEMS = 16;
     constexpr int CHUNK = kSelThreads * ITEMS;
     __shared__ unsigned int sh[kTopnBinsN];
@@ -522,8 +525,15 @@ __global__ void __launch_bounds__(kSelThreads) k_topn_select_all(const T* __rest
     __shared__ unsigned long long s_base;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned int lt = (1u << lane) - 1u;
-    // digit 1
-    if (blockIdx.x == 0) block_select<kTopnBins1>(hist, window ? 48 : 52, window ? 11 : 12, ctl, s_part);
+    // the compaction's look-back words and dispenser, reset here for the launch that follows
+    for (uint32_t i = blockIdx.x * kSelThreads + tid; i < ncstatus; i += gridDim.x * kSelThreads) cstatus[i] = 0;
+    // digit 1 (block 0 first sets the select's state: no prefix, rank keep_n from the top)
+    if (blockIdx.x == 0) {
+        if (tid < 6) ctl->aux[tid] = tid == 2 ? keep_n : 0ull;
+        if (tid == 0) ctl->tile_counter[6] = 0;
+        __syncthreads();
+        block_select<kTopnBins1>(hist, window ? 48 : 52, window ? 11 : 12, ctl, s_part);
+    }
     if (!grid_barrier(bar, ctl, 720)) return;
     // the boundary bin's keys into this block's segment
     {
@@ -582,6 +592,90 @@ __global__ void __launch_bounds__(kSelThreads) k_topn_select_all(const T* __rest
         if (tid == 0) seg_count[blockIdx.x] = (unsigned int)s_base;
     }
     if (!grid_barrier(bar, ctl, 722)) return;
+    // Few candidates (the usual case at small sums): block 0 sorts them all in shared memory and
+    // reads the boundary off the sorted order; no further grid barrier.  Every block sums the
+    // segment lengths, so all take the same branch.
+    {
+        constexpr int kSortCap = kTopnBinsN / 2;  // 64-bit keys in the 8192-word histogram's space
+        constexpr int SEGS_PER = 8;               // segments a thread of block 0 gathers (G <= 2048)
+        unsigned long long mine = 0;
+        for (unsigned int g = tid; g < gridDim.x; g += kSelThreads) mine += __ldcg(&seg_count[g]);
+        s_part[tid] = mine;
+        __syncthreads();
+        for (int o = kSelThreads / 2; o > 0; o >>= 1) {
+            if (tid < o) s_part[tid] += s_part[tid + o];
+            __syncthreads();
+        }
+        const unsigned long long total = s_part[0];
+        __syncthreads();
+        const unsigned long long r = __ldcg(&ctl->aux[2]);
+        if (total <= (unsigned long long)kSortCap && gridDim.x <= (unsigned int)(SEGS_PER * kSelThreads) && r >= 1 &&
+            r <= total) {
+            if (blockIdx.x != 0) return;
+            uint64_t* sk = reinterpret_cast<uint64_t*>(sh);
+            // gather: thread t takes segments [SEGS_PER t, SEGS_PER (t + 1)) at the exclusive sum of
+            // the lengths before them
+            unsigned int lens[SEGS_PER];
+            unsigned long long own = 0;
+#pragma unroll
+            for (int q = 0; q < SEGS_PER; ++q) {
+                const unsigned int g = (unsigned int)(SEGS_PER * tid + q);
+                lens[q] = g < gridDim.x ? __ldcg(&seg_count[g]) : 0u;
+                own += lens[q];
+            }
+            s_part[tid] = own;
+            __syncthreads();
+            for (int o = 1; o < kSelThreads; o <<= 1) {  // inclusive scan
+                const unsigned long long v = tid >= o ? s_part[tid - o] : 0ull;
+                __syncthreads();
+                s_part[tid] += v;
+                __syncthreads();
+            }
+            // each warp copies its 32 threads' segments in turn, its lanes side by side
+            const unsigned long long first = s_part[tid] - own;
+            for (int l = 0; l < 32; ++l) {
+                unsigned long long at = __shfl_sync(0xffffffffu, first, l);
+#pragma unroll
+                for (int q = 0; q < SEGS_PER; ++q) {
+                    const unsigned int len = __shfl_sync(0xffffffffu, lens[q], l);
+                    const uint64_t* sg = cand + (uint64_t)(SEGS_PER * (warp * 32 + l) + q) * seg_cap;
+                    for (unsigned int i = lane; i < len; i += 32) sk[at + i] = __ldcg(&sg[i]);
+                    at += len;
+                }
+            }
+            // pad to a power of two with zeros (the lowest key), then a descending bitonic sort
+            unsigned int np = 1;
+            while (np < total) np <<= 1;
+            for (unsigned int i = (unsigned int)total + tid; i < np; i += kSelThreads) sk[i] = 0ull;
+            __syncthreads();
+            for (unsigned int k = 2; k <= np; k <<= 1) {
+                for (unsigned int j = k >> 1; j > 0; j >>= 1) {
+                    for (unsigned int i = tid; i < np; i += kSelThreads) {
+                        const unsigned int l = i ^ j;
+                        if (l > i) {
+                            const uint64_t a = sk[i], b = sk[l];
+                            const bool desc = (i & k) == 0;
+                            if (desc ? a < b : a > b) {
+                                sk[i] = b;
+                                sk[l] = a;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+            // the boundary is the r-th largest; "above" counts the candidates strictly larger
+            const uint64_t B = sk[r - 1];
+            for (unsigned int i = tid; i < (unsigned int)total; i += kSelThreads)
+                if (sk[i] == B && (i == 0 || sk[i - 1] != B)) {
+                    ctl->aux[0] = B;
+                    ctl->aux[1] = ~0ull;
+                    ctl->aux[2] = r - i;
+                    ctl->aux[3] += i;
+                }
+            return;
+        }
+    }
     // four 13-bit digits over this block's own candidates (it reads what it wrote)
     const unsigned int len = seg_count[blockIdx.x];
     const uint64_t* seg = cand + (uint64_t)blockIdx.x * seg_cap;
@@ -1146,14 +1240,6 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     // aux: prefix, mask, remaining rank, above, -, window miss; count[4]: candidates
     window = window && hist_ready && !sel;
     if (!window) base = 0;
-    unsigned long long* init = host_count + 8;
-    init[0] = 0ull;
-    init[1] = 0ull;
-    init[2] = (unsigned long long)keep_n;
-    init[3] = 0ull;
-    init[4] = 0ull;
-    init[5] = 0ull;
-    cudaMemcpyAsync(ctl->aux, init, 6 * sizeof(unsigned long long), cudaMemcpyHostToDevice, st);
     const unsigned int cgrid = grid_for(n, sms);
     const uint64_t seg_cap = topn_seg_cap(n, sms);
     const uint64_t key_cap = seg_cap * cgrid;  // segments, then the segment lengths
@@ -1195,9 +1281,12 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
                 cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned int), st);
                 const int win = window ? 1 : 0;
                 const float* fp = sel ? nullptr : fpred;
+                unsigned long long kn = keep_n;
+                const uint32_t ctiles = (uint32_t)((n + kThreads * 16 - 1) / (kThreads * 16));
                 void* args[] = {(void*)&coef, (void*)&sel,  (void*)&win,   (void*)&base, (void*)&n,
                                 (void*)&ctl,  (void*)&hist, (void*)&cand,  (void*)&gkey, (void*)&gseg,
-                                (void*)&gcount, (void*)&slots, (void*)&bar, (void*)&fp};
+                                (void*)&gcount, (void*)&slots, (void*)&bar, (void*)&fp, (void*)&kn,
+                                (void*)&status, (void*)&ctiles};
                 prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
                 e = cudaLaunchCooperativeKernel((const void*)k_topn_select_all<T>, dim3(G), dim3(kSelThreads), args,
                                                 0, st);
@@ -1208,6 +1297,14 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
         }
     }
     if (!selected) {
+        unsigned long long* init = host_count + 8;
+        init[0] = 0ull;
+        init[1] = 0ull;
+        init[2] = (unsigned long long)keep_n;
+        init[3] = 0ull;
+        init[4] = 0ull;
+        init[5] = 0ull;
+        cudaMemcpyAsync(ctl->aux, init, 6 * sizeof(unsigned long long), cudaMemcpyHostToDevice, st);
         // digit 1: the select key's top 12 bits (key >> 52), or in a window the bin of 2^48 units;
         // then 13-bit digits down to bit 0 (a window's last digit overlaps bits already fixed)
         prof->begin(K_TOPN_STEP, kTopnBins1 * 8.0, st);
@@ -1230,8 +1327,10 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const uint32_t tiles = (uint32_t)((n + kThreads * 16 - 1) / (kThreads * 16));
-    cudaMemsetAsync(status, 0, (size_t)tiles * sizeof(unsigned long long), st);
-    cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
+    if (!selected) {  // the cooperative select reset these itself
+        cudaMemsetAsync(status, 0, (size_t)tiles * sizeof(unsigned long long), st);
+        cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
+    }
     prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
     k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, sel, sel ? 1 : (fpred ? 4 : 0), base, n,
                                                      (unsigned long long)keep_n, okeys, ocoef, status, ctl, slots, fpred,
