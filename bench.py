@@ -84,44 +84,90 @@ def layer_circuits(seed):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle-reason samples during the timed region."""
+    """SM clock and throttle-reason samples during the timed region.
+
+    Sampled in-process through NVML on a background thread (the device found by its UUID, so
+    CUDA_VISIBLE_DEVICES cannot point it at another GPU), every `period` seconds: an
+    `nvidia-smi -lms` process polling beside the timed steps measurably delays the host's
+    stream synchronizations, which this path does twice per channel.  Falls back to
+    `nvidia-smi` when NVML is not importable.
+    """
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
-    def __init__(self, device):
+    def __init__(self, device, period=0.25):
         self.device = device
+        self.period = period
         self.proc = None
+        self.thread = None
+        self.stop = threading.Event()
         self.lines = []
+        self.samples = []  # (sm MHz, max sm MHz, reason bits)
 
     def __enter__(self):
         try:
+            import pynvml
+            import torch
+
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+            h = pynvml.nvmlDeviceGetHandleByUUID(uuid)
+            mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            self.thread = threading.Thread(target=self._poll_nvml, args=(pynvml, h, mx), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
+        try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", str(int(self.period * 1000))], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
             self.proc = None
         return self
 
+    def _poll_nvml(self, pynvml, h, mx):
+        while True:
+            try:
+                sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                bits = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), float(mx), int(bits)))
+            except Exception:
+                pass
+            if self.stop.wait(self.period):
+                return
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        if self.thread:
             self.thread.join(timeout=5)
 
     def summary(self):
         sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s, m, bits in self.samples:
+            sm.append(s)
+            mx = max(mx, m)
+            for nm, bit in self.REASONS:
+                if bits & bit:
+                    reasons.add(nm)
+        names = [nm for nm, _ in self.REASONS]
         for line in self.lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
@@ -134,10 +180,12 @@ class ClockSampler:
             for nm, v in zip(names, parts[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
+        src = "nvml" if self.samples else ("nvidia-smi" if self.lines else None)
         if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "source": src}
         sm.sort()
-        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm),
+                "source": src, "period_s": self.period}
 
 
 def measured_peaks():

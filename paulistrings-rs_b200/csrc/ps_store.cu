@@ -456,17 +456,19 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* bar, Ctl* ctl, uint32
 }
 
 // One block of kSelThreads: pick the bin of hist (BINS bins, counted from the top) holding the
-// remaining rank aux[2]; update prefix, mask, rank and count above; clear hist.
+// remaining rank aux[2]; update prefix, mask, rank and count above, record the bin's count in
+// aux[4]; clear hist.
 template <int BINS>
 __device__ __forceinline__ void block_select(unsigned int* __restrict__ hist, int shift, int bits, Ctl* ctl,
                                              unsigned long long* s_part) {
     constexpr int PER = BINS / kSelThreads;
     __shared__ int s_choice;
-    __shared__ unsigned long long s_above;
+    __shared__ unsigned long long s_above, s_count;
     const int t = threadIdx.x;
     if (t == 0) {
         s_choice = 0;
         s_above = 0;
+        s_count = 0;
     }
     unsigned long long mine = 0;
     for (int q = 0; q < PER; ++q) mine += __ldcg(&hist[BINS - 1 - (t * PER + q)]);
@@ -488,6 +490,7 @@ __device__ __forceinline__ void block_select(unsigned int* __restrict__ hist, in
             if (acc + c >= r) {
                 s_choice = bin;
                 s_above = acc;
+                s_count = c;
                 break;
             }
             acc += c;
@@ -501,12 +504,52 @@ __device__ __forceinline__ void block_select(unsigned int* __restrict__ hist, in
         ctl->aux[1] |= ((1ull << bits) - 1ull) << shift;
         ctl->aux[2] = r - above;
         ctl->aux[3] += above;
+        ctl->aux[4] = s_count;  // keys in the chosen bin
     }
     __syncthreads();
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kSelThreads) k_topn_select_all(const T* __restrict__ coef,
+// Block-wide: the boundary of `total` candidate keys in sk (shared memory, room for the next
+// power of two) at rank r from the top (1 <= r <= total): pads with zeros (the lowest key),
+// sorts descending (bitonic), and sets the select's final prefix (the boundary key itself, full
+// mask), remaining rank and count above ("above" counts the candidates strictly larger).
+__device__ __forceinline__ void block_sort_boundary(uint64_t* sk, unsigned int total, unsigned long long r,
+                                                    Ctl* ctl) {
+    const int tid = threadIdx.x;
+    unsigned int np = 1;
+    while (np < total) np <<= 1;
+    for (unsigned int i = total + tid; i < np; i += kSelThreads) sk[i] = 0ull;
+    __syncthreads();
+    for (unsigned int k = 2; k <= np; k <<= 1) {
+        for (unsigned int j = k >> 1; j > 0; j >>= 1) {
+            for (unsigned int i = tid; i < np; i += kSelThreads) {
+                const unsigned int l = i ^ j;
+                if (l > i) {
+                    const uint64_t a = sk[i], b = sk[l];
+                    const bool desc = (i & k) == 0;
+                    if (desc ? a < b : a > b) {
+                        sk[i] = b;
+                        sk[l] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    const uint64_t B = sk[r - 1];
+    for (unsigned int i = tid; i < total; i += kSelThreads)
+        if (sk[i] == B && (i == 0 || sk[i - 1] != B)) {
+            ctl->aux[0] = B;
+            ctl->aux[1] = ~0ull;
+            ctl->aux[2] = r - i;
+            ctl->aux[3] += i;
+        }
+}
+
+// SCORE: the learned pass's variant (select keys from score_key of the coefficient and the
+// prediction); the plain variant stays within four resident blocks per SM, the scored one three.
+template <typename T, bool SCORE>
+__global__ void __launch_bounds__(kSelThreads, SCORE ? 3 : 4) k_topn_select_all(const T* __restrict__ coef,
                                                                  const uint64_t* __restrict__ sel, int window,
                                                                  uint64_t base, uint64_t n, Ctl* ctl,
                                                                  unsigned int* __restrict__ hist,
@@ -521,7 +564,6 @@ __global__ void __launch_bounds__(kSelThreads) k_topn_select_all(const T* __rest
     constexpr int CHUNK = kSelThreads * ITEMS;
     __shared__ unsigned int sh[kTopnBinsN];
     __shared__ unsigned long long s_part[kSelThreads];
-    __shared__ unsigned int s_w[kSelThreads / 32];
     __shared__ unsigned long long s_base;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned int lt = (1u << lane) - 1u;
@@ -529,7 +571,7 @@ __global__ void __launch_bounds__(kSelThreads) k_topn_select_all(const T* __rest
     for (uint32_t i = blockIdx.x * kSelThreads + tid; i < ncstatus; i += gridDim.x * kSelThreads) cstatus[i] = 0;
     // digit 1 (block 0 first sets the select's state: no prefix, rank keep_n from the top)
     if (blockIdx.x == 0) {
-        if (tid < 6) ctl->aux[tid] = tid == 2 ? keep_n : 0ull;
+        if (tid < 7) ctl->aux[tid] = tid == 2 ? keep_n : 0ull;
         if (tid == 0) ctl->tile_counter[6] = 0;
         __syncthreads();
         block_select<kTopnBins1>(hist, window ? 48 : 52, window ? 11 : 12, ctl, s_part);
@@ -547,19 +589,23 @@ __global__ void __launch_bounds__(kSelThreads) k_topn_select_all(const T* __rest
         for (uint64_t c0 = (uint64_t)blockIdx.x * CHUNK; c0 < n; c0 += (uint64_t)gridDim.x * CHUNK) {
             const uint64_t wbase = c0 + (uint64_t)warp * 32 * ITEMS;
             uint64_t key[ITEMS];
-            float fp[ITEMS];
+            float fp[SCORE ? ITEMS : 1];
 #pragma unroll
             for (int i = 0; i < ITEMS; ++i) {
                 const uint64_t e = wbase + (uint64_t)i * 32 + lane;
                 key[i] = e < n ? (sel ? sel[e] : raw_bits(coef[e])) : 0ull;
-                fp[i] = fpred && e < n ? fpred[e] : 0.0f;
+                if constexpr (SCORE) fp[i] = e < n ? fpred[e] : 0.0f;
             }
             unsigned int ball[ITEMS];
             unsigned int wc = 0;
 #pragma unroll
             for (int i = 0; i < ITEMS; ++i) {
                 if (!sel) {
-                    const uint64_t mk = fpred ? score_key<T>(from_raw<T>(key[i]), fp[i]) : mag_key<T>(from_raw<T>(key[i]));
+                    uint64_t mk;
+                    if constexpr (SCORE)
+                        mk = score_key<T>(from_raw<T>(key[i]), fp[i]);
+                    else
+                        mk = mag_key<T>(from_raw<T>(key[i]));
                     key[i] = window ? window_key(mk, base) : mk;
                 }
                 const uint64_t e = wbase + (uint64_t)i * 32 + lane;
@@ -567,28 +613,23 @@ __global__ void __launch_bounds__(kSelThreads) k_topn_select_all(const T* __rest
                 ball[i] = __ballot_sync(0xffffffffu, hit);
                 wc += __popc(ball[i]);
             }
-            if (lane == 0) s_w[warp] = wc;
-            __syncthreads();
-            unsigned int wx = 0, tot = 0;
+            // the warp's place in the block's segment: the order of the candidates does not
+            // matter, so one shared atomic per warp replaces a block-wide scan (and its barriers)
+            if (wc) {
+                unsigned long long slot = 0;
+                if (lane == 0) slot = atomicAdd(&s_base, (unsigned long long)wc);
+                slot = __shfl_sync(0xffffffffu, slot, 0) + (uint64_t)blockIdx.x * seg_cap;
 #pragma unroll
-            for (int w = 0; w < kSelThreads / 32; ++w) {
-                wx += w < warp ? s_w[w] : 0u;
-                tot += s_w[w];
-            }
-            const unsigned long long seg_used = s_base;
-            __syncthreads();
-            if (tid == 0) s_base = seg_used + tot;
-            unsigned long long slot = (uint64_t)blockIdx.x * seg_cap + seg_used + wx;
-#pragma unroll
-            for (int i = 0; i < ITEMS; ++i) {
-                if ((ball[i] >> lane) & 1u) {
-                    const unsigned long long q = slot + __popc(ball[i] & lt);
-                    if (PS_GUARD(ctl, q < cand_cap, 721)) cand[q] = key[i];
+                for (int i = 0; i < ITEMS; ++i) {
+                    if ((ball[i] >> lane) & 1u) {
+                        const unsigned long long q = slot + __popc(ball[i] & lt);
+                        if (PS_GUARD(ctl, q < cand_cap, 721)) cand[q] = key[i];
+                    }
+                    slot += __popc(ball[i]);
                 }
-                slot += __popc(ball[i]);
             }
-            __syncthreads();
         }
+        __syncthreads();
         if (tid == 0) seg_count[blockIdx.x] = (unsigned int)s_base;
     }
     if (!grid_barrier(bar, ctl, 722)) return;
@@ -643,36 +684,8 @@ __global__ void __launch_bounds__(kSelThreads) k_topn_select_all(const T* __rest
                     at += len;
                 }
             }
-            // pad to a power of two with zeros (the lowest key), then a descending bitonic sort
-            unsigned int np = 1;
-            while (np < total) np <<= 1;
-            for (unsigned int i = (unsigned int)total + tid; i < np; i += kSelThreads) sk[i] = 0ull;
             __syncthreads();
-            for (unsigned int k = 2; k <= np; k <<= 1) {
-                for (unsigned int j = k >> 1; j > 0; j >>= 1) {
-                    for (unsigned int i = tid; i < np; i += kSelThreads) {
-                        const unsigned int l = i ^ j;
-                        if (l > i) {
-                            const uint64_t a = sk[i], b = sk[l];
-                            const bool desc = (i & k) == 0;
-                            if (desc ? a < b : a > b) {
-                                sk[i] = b;
-                                sk[l] = a;
-                            }
-                        }
-                    }
-                    __syncthreads();
-                }
-            }
-            // the boundary is the r-th largest; "above" counts the candidates strictly larger
-            const uint64_t B = sk[r - 1];
-            for (unsigned int i = tid; i < (unsigned int)total; i += kSelThreads)
-                if (sk[i] == B && (i == 0 || sk[i - 1] != B)) {
-                    ctl->aux[0] = B;
-                    ctl->aux[1] = ~0ull;
-                    ctl->aux[2] = r - i;
-                    ctl->aux[3] += i;
-                }
+            block_sort_boundary(sk, (unsigned int)total, r, ctl);
             return;
         }
     }
@@ -695,24 +708,47 @@ __global__ void __launch_bounds__(kSelThreads) k_topn_select_all(const T* __rest
         if (!grid_barrier(bar, ctl, 723)) return;
         if (blockIdx.x == 0) block_select<kTopnBinsN>(hist, shift, 13, ctl, s_part);
         if (!grid_barrier(bar, ctl, 724)) return;
+        // Once the chosen bin holds at most kSortCap keys, the remaining digits give way to one
+        // block's sort: every block appends its keys of the bin to a list in the (now zero)
+        // histogram's space, and block 0 sorts them, then zeroes the words it used.
+        constexpr unsigned int kSortCap = kTopnBinsN / 2;
+        const unsigned long long cnt = __ldcg(&ctl->aux[4]), r = __ldcg(&ctl->aux[2]);
+        if (d < 3 && cnt <= kSortCap && r >= 1 && r <= cnt) {
+            const uint64_t pfx = __ldcg(&ctl->aux[0]), msk = __ldcg(&ctl->aux[1]);
+            uint64_t* list = reinterpret_cast<uint64_t*>(hist);
+            unsigned long long* fill = &ctl->aux[6];
+            for (unsigned int i0 = 0; i0 < len; i0 += kSelThreads) {
+                const unsigned int i = i0 + tid;
+                const uint64_t mk = i < len ? seg[i] : 0ull;
+                const bool hit = i < len && (mk & msk) == pfx;
+                const unsigned int b = __ballot_sync(0xffffffffu, hit);
+                if (b) {
+                    unsigned long long at = 0;
+                    if (lane == 0) at = atomicAdd(fill, (unsigned long long)__popc(b));
+                    at = __shfl_sync(0xffffffffu, at, 0) + __popc(b & lt);
+                    if (hit && PS_GUARD(ctl, at < kSortCap, 725)) list[at] = mk;
+                }
+            }
+            if (!grid_barrier(bar, ctl, 726)) return;
+            if (blockIdx.x != 0) return;
+            uint64_t* sk = reinterpret_cast<uint64_t*>(sh);
+            const unsigned long long filled = __ldcg(fill);
+            if (tid == 0) PS_GUARD(ctl, filled == cnt, 727);
+            const unsigned int total = (unsigned int)min(cnt, (unsigned long long)kSortCap);
+            const unsigned int used = (unsigned int)min(filled, (unsigned long long)kSortCap);
+            for (unsigned int i = tid; i < total; i += kSelThreads) sk[i] = __ldcg(&list[i]);
+            for (unsigned int i = tid; i < used; i += kSelThreads) list[i] = 0ull;
+            __syncthreads();
+            block_sort_boundary(sk, total, r, ctl);
+            return;
+        }
     }
 }
 
-// The select key of element e: mag_key of its coefficient, or a precomputed key (the scored
-// TopN's score keys, same conventions: 0 never kept, larger kept first).
-template <typename T>
-__device__ __forceinline__ uint64_t select_key(const T* __restrict__ coef, const uint64_t* __restrict__ sel, uint64_t e) {
-    return sel ? sel[e] : mag_key<T>(coef[e]);
-}
-
-// The compaction's key: 0 mag_key, 1 precomputed, 2 ApproxTopN's octave key, 4 the learned
-// score from the coefficient and the row's prediction.
-template <typename T>
-__device__ __forceinline__ uint64_t compact_key(const T* __restrict__ coef, const uint64_t* __restrict__ sel, int mode,
-                                                uint64_t e, const float* __restrict__ fpred) {
-    if (mode == 4) return score_key<T>(coef[e], fpred[e]);
-    return mode == 2 ? octave_key<T>(coef[e]) : select_key<T>(coef, sel, e);
-}
+// The compaction's key (key_mode): 0 mag_key of the coefficient, 1 a precomputed key (the
+// scored TopN's score keys, same conventions: 0 never kept, larger kept first), 2 ApproxTopN's
+// octave key, 3 none (every live row kept), 4 the learned score from the coefficient and the
+// row's prediction.
 
 // ApproxTopN's octave histogram of |c|^2 (2048 bins, NaN in the top one).
 template <typename T>
@@ -732,7 +768,7 @@ __global__ void __launch_bounds__(kThreads) k_octave_hist(const T* __restrict__ 
 // takes chunks of kThreads * 16 elements and appends their candidates to its own segment of
 // the candidate buffer (seg_cap keys, room for every element of the block's chunks), so no
 // counter is shared between blocks; seg_count[block] receives the segment's length.
-template <typename T>
+template <typename T, bool SCORE>
 __global__ void __launch_bounds__(kThreads) k_topn_cand(const T* __restrict__ coef, const uint64_t* __restrict__ sel,
                                                         int window, uint64_t base, uint64_t n, Ctl* ctl,
                                                         uint64_t* __restrict__ cand, uint64_t cand_cap,
@@ -755,19 +791,23 @@ __global__ void __launch_bounds__(kThreads) k_topn_cand(const T* __restrict__ co
         const uint64_t wbase = c0 + (uint64_t)warp * 32 * ITEMS;
         // every load of the chunk first, then the keys and ballots
         uint64_t key[ITEMS];
-        float fp[ITEMS];
+        float fp[SCORE ? ITEMS : 1];
 #pragma unroll
         for (int i = 0; i < ITEMS; ++i) {
             const uint64_t e = wbase + (uint64_t)i * 32 + lane;
             key[i] = e < n ? (sel ? sel[e] : raw_bits(coef[e])) : 0ull;
-            fp[i] = fpred && e < n ? fpred[e] : 0.0f;
+            if constexpr (SCORE) fp[i] = e < n ? fpred[e] : 0.0f;
         }
         unsigned int ball[ITEMS];
         unsigned int wc = 0;
 #pragma unroll
         for (int i = 0; i < ITEMS; ++i) {
             if (!sel) {
-                const uint64_t mk = fpred ? score_key<T>(from_raw<T>(key[i]), fp[i]) : mag_key<T>(from_raw<T>(key[i]));
+                uint64_t mk;
+                if constexpr (SCORE)
+                    mk = score_key<T>(from_raw<T>(key[i]), fp[i]);
+                else
+                    mk = mag_key<T>(from_raw<T>(key[i]));
                 key[i] = window ? window_key(mk, base) : mk;
             }
             const uint64_t e = wbase + (uint64_t)i * 32 + lane;
@@ -828,13 +868,18 @@ __global__ void __launch_bounds__(kThreads) k_topn_hist_cand(const uint64_t* __r
 // `quota` boundary ties in key order, quota = keep_n - (count above the boundary), none when
 // the boundary is NaN (the select leaves boundary and count above in aux[0] / aux[3]).
 // key_mode 3 keeps every row.  Rows outside the slots of a slotted store are skipped.
-template <int W, typename T>
+// SCORE: the learned pass's variant (score keys from the prediction column, which the kept rows
+// carry); the plain variant keeps its registers, and with them its residency, free of the log.
+template <int W, typename T, bool SCORE>
 __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __restrict__ keys, const T* __restrict__ coef,
                                                            const uint64_t* __restrict__ sel, int key_mode,
                                                            uint64_t base, uint64_t n, unsigned long long keep_n,
                                                            uint64_t* __restrict__ okeys, T* __restrict__ ocoef,
                                                            unsigned long long* status, Ctl* ctl, SlotMap slots,
                                                            const float* __restrict__ fin, float* __restrict__ fout) {
+    // A select whose windowed boundary left the window writes nothing: the pass reruns in full
+    // range and rewrites the output.
+    if (key_mode != 2 && key_mode != 3 && ctl->aux[5]) return;
     const unsigned long long quota = ctl->aux[0] == 0 ? 0ull : keep_n - ctl->aux[3];
     constexpr int ITEMS = 16;
     constexpr int TILE = kThreads * ITEMS;
@@ -857,7 +902,16 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
         bool isa = false, ist = false;
         if (e < n) {
             // the key load does not wait for the liveness test (a slot's tail is allocated)
-            const uint64_t mk = key_mode == 3 ? 0ull : compact_key<T>(coef, sel, key_mode, e, fin);
+            uint64_t mk = 0ull;
+            if (key_mode == 1)
+                mk = sel[e];
+            else if (key_mode == 2)
+                mk = octave_key<T>(coef[e]);
+            else if (key_mode == 0)
+                mk = mag_key<T>(coef[e]);
+            if constexpr (SCORE) {
+                if (key_mode == 4) mk = score_key<T>(coef[e], fin[e]);
+            }
             if (sw.live(slots)) {
                 isa = key_mode == 3 || mk > boundary;  // key_mode 3 keeps every row (compacting slots)
                 ist = key_mode != 3 && mk == boundary && boundary != 0;
@@ -915,7 +969,7 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
             if (PS_GUARD(ctl, pos < n, 702)) {
                 store_key<W>(okeys, pos, k);
                 ocoef[pos] = coef[e];
-                if (fout) fout[pos] = fin[e];  // the learned pass's prediction travels with its row
+                if constexpr (SCORE) fout[pos] = fin[e];  // the learned pass's prediction travels with its row
             }
         }
         arank += __popc(ba[i]);
@@ -1237,7 +1291,8 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
                                  unsigned long long* status, Ctl* ctl, unsigned long long* host_count,
                                  uint64_t* out_n, int sms, cudaStream_t st, KernelProf* prof, const uint64_t* sel,
                                  bool window, uint64_t base, SlotMap slots, const float* fpred, float* fout) {
-    // aux: prefix, mask, remaining rank, above, -, window miss; count[4]: candidates
+    // aux: prefix, mask, remaining rank, above, keys in the last chosen bin, window miss, keys
+    // gathered for the in-block sort (cooperative select); count[4]: candidates
     window = window && hist_ready && !sel;
     if (!window) base = 0;
     const unsigned int cgrid = grid_for(n, sms);
@@ -1258,15 +1313,16 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     // below otherwise)
     bool selected = false;
     {
-        static std::atomic<int> per_sm{0};
-        int per = per_sm.load(std::memory_order_relaxed);
+        const float* fp = sel ? nullptr : fpred;
+        const void* kern = fp ? (const void*)k_topn_select_all<T, true> : (const void*)k_topn_select_all<T, false>;
+        static std::atomic<int> per_sm[2] = {{0}, {0}};
+        std::atomic<int>& per_v = per_sm[fp ? 1 : 0];
+        int per = per_v.load(std::memory_order_relaxed);
         if (per == 0) {
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_topn_select_all<T>, kSelThreads, 0) !=
-                    cudaSuccess ||
-                per < 1)
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kSelThreads, 0) != cudaSuccess || per < 1)
                 per = -1;
             cudaGetLastError();
-            per_sm.store(per, std::memory_order_relaxed);
+            per_v.store(per, std::memory_order_relaxed);
         }
         if (per > 0) {
             const uint64_t nchunks = (n + kSelThreads * 16 - 1) / (kSelThreads * 16);
@@ -1280,7 +1336,6 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
                 unsigned int* bar = &ctl->tile_counter[4];
                 cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned int), st);
                 const int win = window ? 1 : 0;
-                const float* fp = sel ? nullptr : fpred;
                 unsigned long long kn = keep_n;
                 const uint32_t ctiles = (uint32_t)((n + kThreads * 16 - 1) / (kThreads * 16));
                 void* args[] = {(void*)&coef, (void*)&sel,  (void*)&win,   (void*)&base, (void*)&n,
@@ -1288,8 +1343,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
                                 (void*)&gcount, (void*)&slots, (void*)&bar, (void*)&fp, (void*)&kn,
                                 (void*)&status, (void*)&ctiles};
                 prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
-                e = cudaLaunchCooperativeKernel((const void*)k_topn_select_all<T>, dim3(G), dim3(kSelThreads), args,
-                                                0, st);
+                e = cudaLaunchCooperativeKernel(kern, dim3(G), dim3(kSelThreads), args, 0, st);
                 prof->end(st);
                 selected = e == cudaSuccess;
                 if (!selected) cudaGetLastError();  // not launched: the multi-launch path selects instead
@@ -1311,8 +1365,12 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
         k_topn_select<kTopnBins1><<<1, 1024, 0, st>>>(hist, window ? 48 : 52, window ? 11 : 12, ctl);
         prof->end(st);
         prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
-        k_topn_cand<T><<<cgrid, kThreads, 0, st>>>(coef, sel, window ? 1 : 0, base, n, ctl, cand, key_cap, seg_cap,
-                                                  seg_count, slots, sel ? nullptr : fpred);
+        if (!sel && fpred)
+            k_topn_cand<T, true><<<cgrid, kThreads, 0, st>>>(coef, sel, window ? 1 : 0, base, n, ctl, cand, key_cap,
+                                                             seg_cap, seg_count, slots, fpred);
+        else
+            k_topn_cand<T, false><<<cgrid, kThreads, 0, st>>>(coef, sel, window ? 1 : 0, base, n, ctl, cand, key_cap,
+                                                              seg_cap, seg_count, slots, nullptr);
         prof->end(st);
         static const int kShifts[2][4] = {{39, 26, 13, 0}, {35, 22, 9, 0}};
         for (int d = 0; d < 4; ++d) {
@@ -1332,9 +1390,14 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
         cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     }
     prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
-    k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, sel, sel ? 1 : (fpred ? 4 : 0), base, n,
-                                                     (unsigned long long)keep_n, okeys, ocoef, status, ctl, slots, fpred,
-                                                     fout);
+    if (fout)
+        k_topn_compact<W, T, true><<<tiles, kThreads, 0, st>>>(keys, coef, sel, sel ? 1 : (fpred ? 4 : 0), base, n,
+                                                               (unsigned long long)keep_n, okeys, ocoef, status, ctl,
+                                                               slots, fpred, fout);
+    else
+        k_topn_compact<W, T, false><<<tiles, kThreads, 0, st>>>(keys, coef, sel, sel ? 1 : 0, base, n,
+                                                                (unsigned long long)keep_n, okeys, ocoef, status, ctl,
+                                                                slots, nullptr, nullptr);
     prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // the one host synchronization of the pass: counts, error flags and the select's aux words
@@ -1360,8 +1423,12 @@ cudaError_t StoreOps<W, T>::densify(const uint64_t* keys, const T* coef, uint64_
     cudaMemsetAsync(status, 0, (size_t)tiles * sizeof(unsigned long long), st);
     cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     prof->begin(K_TOPN_COMPACT, 0.0, st);
-    k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, nullptr, 3, 0ull, n, 0ull, okeys, ocoef, status, ctl,
-                                                     slots, fin, fout);
+    if (fout)
+        k_topn_compact<W, T, true><<<tiles, kThreads, 0, st>>>(keys, coef, nullptr, 3, 0ull, n, 0ull, okeys, ocoef,
+                                                               status, ctl, slots, fin, fout);
+    else
+        k_topn_compact<W, T, false><<<tiles, kThreads, 0, st>>>(keys, coef, nullptr, 3, 0ull, n, 0ull, okeys, ocoef,
+                                                                status, ctl, slots, nullptr, nullptr);
     prof->end(st);
     cudaError_t e;
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1415,7 +1482,7 @@ cudaError_t StoreOps<W, T>::approx_topn(const uint64_t* keys, const T* coef, uin
     cudaMemsetAsync(status, 0, (size_t)tiles * sizeof(unsigned long long), st);
     cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
-    k_topn_compact<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, nullptr, 2, 0ull, n, (unsigned long long)keep_n,
+    k_topn_compact<W, T, false><<<tiles, kThreads, 0, st>>>(keys, coef, nullptr, 2, 0ull, n, (unsigned long long)keep_n,
                                                      okeys, ocoef, status, ctl, SlotMap{nullptr, 0u}, nullptr, nullptr);
     prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
