@@ -106,6 +106,13 @@ struct ps_sum {
     bool support_known = false;
     bool keep_clean = false;
     uint64_t layers_skipped = 0;
+    // The TopN compaction classifies its kept rows for the next rotation layer (ps_propagate
+    // names that layer's table in next_table while it finalizes a layer); pre_valid: the store
+    // of pre_n terms has its partner list for the table pre_table in idx / dv and count[0].
+    const ps_table* next_table = nullptr;
+    bool pre_valid = false;
+    const ps_table* pre_table = nullptr;
+    uint64_t pre_n = 0;
     Buf noise_drops;                      // folded noise: own rows first dropped after channel j
     unsigned long long* hnoise = nullptr; // pinned, kMaxNoise + 1 words
     KeepProg clean_keep{};
@@ -1093,6 +1100,9 @@ struct Engine {
                            const NoiseList* noise = nullptr, uint64_t* noise_after = nullptr) {
         KeepProg keep;
         std::string why;
+        // the last TopN pass wrote this layer's partner list (the store is as it left it)
+        const bool preclassified = s->pre_valid && s->pre_table == &t && !s->slotted && s->n == s->pre_n;
+        s->pre_valid = false;
         ps_status ps = lower_keep(policy, keep, why);
         if (ps != PS_OK) return set_err(s, ps, why);
         if ((ps = densify(s, "apply")) != PS_OK) return ps;
@@ -1150,6 +1160,7 @@ struct Engine {
         a.Sk = K(s, s->cur);
         a.Sc = C(s, s->cur);
         a.n = n;
+        a.preclassified = preclassified && a.L.partners && !noise ? 1 : 0;
         a.levels = s->levels;
         a.keep = keep;
         a.idx = (uint32_t*)s->idx.p;
@@ -1373,6 +1384,18 @@ struct Engine {
             cudaError_t e = reserve_store(s, spare, p.n);
             if (e == cudaSuccess) e = ensure(s, s->cand, topn_cand_words(s->n, s->sms) * sizeof(uint64_t));
             if (e == cudaSuccess) e = ensure(s, s->status, (s->n / 4096 + 4) * sizeof(unsigned long long));
+            // the layer's last pass, with a rotation layer (with partners) next: the compaction also
+            // writes that layer's partner list, so it skips its own classify pass
+            RotLayer<W> next_L;
+            bool classify = false;
+            if (e == cudaSuccess && s->next_table && i == policy->num_passes - 1 && p.n < (1ull << 31) - 1) {
+                std::string why_next;
+                bool general = false;
+                classify = to_rot_layer<W, T>(*s->next_table, next_L, *s->levels, why_next, &general) == PS_OK &&
+                           !general && next_L.partners;
+                if (classify) e = ensure(s, s->idx, p.n * 4);
+                if (classify && e == cudaSuccess) e = ensure(s, s->dv, p.n * 2);
+            }
             if (e != cudaSuccess) {
                 if (use_hist) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
                 return cuda_fail(s, e, "topn: scratch");
@@ -1387,7 +1410,10 @@ struct Engine {
                                          (unsigned int*)s->hist.p, use_hist && attempt == 0, (uint64_t*)s->cand.p,
                                          topn_cand_words(s->n, s->sms), (unsigned long long*)s->status.p, s->ctl,
                                          s->hcount, &out_n, s->sms,
-                                         s->stream, &s->prof, nullptr, win, win ? s->hist_base : 0, slot_map(s));
+                                         s->stream, &s->prof, nullptr, win, win ? s->hist_base : 0, slot_map(s),
+                                         nullptr, nullptr, classify ? &next_L : nullptr,
+                                         classify ? (uint32_t*)s->idx.p : nullptr,
+                                         classify ? (uint16_t*)s->dv.p : nullptr);
                 s->prof.resolve();
                 if (e != cudaSuccess) return cuda_fail(s, e, "topn");
                 unsigned int fl = 0, fi = 0;
@@ -1408,6 +1434,11 @@ struct Engine {
             s->cur = spare;
             s->n = out_n;
             s->slotted = false;
+            if (classify && !topn_unclassified(s->hcount)) {
+                s->pre_valid = true;
+                s->pre_table = s->next_table;
+                s->pre_n = out_n;
+            }
         }
         return result;
     }
@@ -1893,6 +1924,7 @@ ps_status ps_propagate(ps_sum* s, const ps_channel* channels, uint64_t num_chann
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, s->stream);
+    s->pre_valid = false;  // a partner list names a table of this call only
     ps_run_stats rs;
     std::memset(&rs, 0, sizeof rs);
     rs.peak_terms = s->n;
@@ -1925,7 +1957,9 @@ ps_status ps_propagate(ps_sum* s, const ps_channel* channels, uint64_t num_chann
             ps = dispatch<Engine>(s, [&](auto op) { return decltype(op)::apply(s, tables[fj], policy, &ls, &N, after); });
             if (ps == PS_OK && s->scorer) s->scorer_remaining -= (double)(fj - li);  // the folded layers' count-downs
             s->pass_call = fj;
+            s->next_table = fj + 1 < num_channels ? &tables[fj + 1] : nullptr;
             if (ps == PS_OK) ps = ps_finalize_layer(s, policy);
+            s->next_table = nullptr;
             s->pass_call = 0;
             if (ps != PS_OK) {
                 s->err = "layer " + std::to_string(fj) + " (with the noise of layers " + std::to_string(li) + "-" +
@@ -1952,7 +1986,9 @@ ps_status ps_propagate(ps_sum* s, const ps_channel* channels, uint64_t num_chann
             rs.skipped_terms_in += n_in;
         }
         s->pass_call = li;  // CollapseSample's pass index of this layer
+        s->next_table = li + 1 < num_channels ? &tables[li + 1] : nullptr;
         if (ps == PS_OK) ps = ps_finalize_layer(s, policy);
+        s->next_table = nullptr;
         s->pass_call = 0;
         if (ps != PS_OK) {
             s->err = "layer " + std::to_string(li) + ": " + s->err;
@@ -1962,6 +1998,7 @@ ps_status ps_propagate(ps_sum* s, const ps_channel* channels, uint64_t num_chann
         if (terms_after) terms_after[li] = s->n;
         ++rs.layers;
     }
+    s->pre_valid = false;
     cudaEventRecord(e1, s->stream);
     cudaEventSynchronize(e1);
     float ms = 0.f;

@@ -230,6 +230,8 @@ struct RotationArgs {
     int topn_hist_mode;       // 0 select key >> 52, 1 octave of |c|^2 (ApproxTopN),
     uint64_t topn_hist_base;  // 2 window_key(select key, topn_hist_base) >> 48
     int inject_stall;         // failure injection: the merge skips its first tile
+    int preclassified;        // idx, D and count[0] already hold this layer's partner list (written
+                              // by the TopN compaction before it): no classify pass
     unsigned long long stall_limit;  // ... and its look-back waits give up after this many polls
     unsigned int* slot_count; // when set, the merge writes tile t at rows t * merge_slot_rows<W>()
                               // and its row count to slot_count[t], with no look-back (slotted

@@ -32,6 +32,7 @@
 
 #include "ps_device.cuh"
 #include "ps_kernels.h"
+#include "ps_rotlayer.cuh"
 
 namespace psb {
 
@@ -52,95 +53,11 @@ constexpr int kScanTile = kBlock * kScanItems;
 constexpr int kApplyThreads = 512;  // k_level_apply block: 8 partners per thread
 static_assert(kScanTile == (int)kScanTileRows, "scan tile");
 
-// word `wi` of a key held in registers, by an unrolled select (a runtime index into a
-// register array would move the array to local memory)
-template <int W>
-__device__ __forceinline__ uint64_t pick(const uint64_t* k, int wi) {
-    uint64_t v = k[0];
-#pragma unroll
-    for (int w = 1; w < 2 * W; ++w) v = (w == wi) ? k[w] : v;
-    return v;
-}
-
-// support pattern of key k (LocalPtm::support_bits, channel/prepared.rs:141-151)
-template <int W>
-__device__ __forceinline__ uint32_t pattern_of(const RotLayer<W>& L, const uint64_t* k) {
-    uint32_t s = (uint32_t)((pick<W>(k, L.qw[0]) >> L.qb[0]) & 1u) |
-                 (uint32_t)((pick<W>(k, W + L.qw[0]) >> L.qb[0]) & 1u) << 1 |
-                 (uint32_t)((pick<W>(k, L.qw[1]) >> L.qb[1]) & 1u) << 2 |
-                 (uint32_t)((pick<W>(k, W + L.qw[1]) >> L.qb[1]) & 1u) << 3;
-    return s & L.pattern_mask;
-}
-
-template <typename T>
-struct Amp;
-template <>
-struct Amp<double> {
-    template <int W>
-    __device__ static double a0(const RotLayer<W>& L, uint32_t s) { return L.a0[s]; }
-    template <int W>
-    __device__ static double a1(const RotLayer<W>& L, uint32_t s) { return L.a1[s]; }
-    template <int W>
-    __device__ static double cs(const RotLayer<W>& L) { return L.cos64; }
-    template <int W>
-    __device__ static double sn(const RotLayer<W>& L) { return L.sin64; }
-};
-template <>
-struct Amp<float> {
-    template <int W>
-    __device__ static float a0(const RotLayer<W>& L, uint32_t s) { return L.a0f[s]; }
-    template <int W>
-    __device__ static float a1(const RotLayer<W>& L, uint32_t s) { return L.a1f[s]; }
-    template <int W>
-    __device__ static float cs(const RotLayer<W>& L) { return L.cos32; }
-    template <int W>
-    __device__ static float sn(const RotLayer<W>& L) { return L.sin32; }
-};
-
-// The layer's per-pattern amplitudes staged in shared memory: indexing the kernel-parameter
-// copy with a per-lane pattern would serialize on the constant cache.
-template <typename T>
-struct AmpTab {
-    T a0[16];
-    T a1[16];
-};
-
-template <int W, typename T>
-__device__ __forceinline__ void stage_amps(const RotLayer<W>& L, AmpTab<T>& t) {
-    if (threadIdx.x < 16) {
-        t.a0[threadIdx.x] = Amp<T>::a0(L, threadIdx.x);
-        t.a1[threadIdx.x] = Amp<T>::a1(L, threadIdx.x);
-    }
-}
-
 // Does term k emit a partner?
 template <int W, typename T>
 __device__ __forceinline__ bool emits_partner(const RotLayer<W>& L, const AmpTab<T>& A, const uint64_t* k) {
     if (L.wide) return anticommutes<W>(k, L.gx, L.gz);
     return A.a1[pattern_of<W>(L, k)] != T(0);
-}
-
-template <int W, typename T>
-__device__ __forceinline__ bool emits_partner_regs(const RotLayer<W>& L, const AmpTab<T>& A,
-                                                   const uint64_t (&k)[2 * W]) {
-    if (L.wide) {
-        uint64_t f = 0;
-#pragma unroll
-        for (int i = 0; i < W; ++i) f ^= (k[i] & L.gz[i]) ^ (k[W + i] & L.gx[i]);
-        return (__popcll(f) & 1) != 0;
-    }
-    return A.a1[pattern_of<W>(L, k)] != T(0);
-}
-
-template <int W>
-__device__ __forceinline__ uint32_t div_regs(const uint64_t (&a)[2 * W], const uint64_t (&b)[2 * W]) {
-    uint32_t r = 0xFFFFu;
-#pragma unroll
-    for (int i = 2 * W - 1; i >= 0; --i) {
-        uint64_t d = a[i] ^ b[i];
-        if (d) r = 64u * i + (uint32_t)__clzll((long long)d);
-    }
-    return r;
 }
 
 // Own-row coefficient after the layer.
@@ -1005,14 +922,15 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
     if (tid == 0) bulk_wait_read_all();  // shared memory stays valid until the last copy has read it
 }
 
-// One launch resets what a rotation layer's kernels count on: the partner and output counts,
+// One launch resets what a rotation layer's kernels count on: the partner count (unless the
+// partner list is already there) and the output count,
 // the tile dispensers (the merge's starts at `merge_start`, 1 under failure injection), the
 // look-back words of the classify and the merge (disjoint ranges of `status`) and the folded
 // noise's drop counters.
 __global__ void k_layer_prep(Ctl* ctl, unsigned long long* __restrict__ status, uint32_t nstatus,
-                             unsigned int merge_start, unsigned long long* __restrict__ noise_drops) {
+                             unsigned int merge_start, unsigned long long* __restrict__ noise_drops, int keep_m) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < 2) ctl->count[t] = 0;
+    if (t < 2 && !(t == 0 && keep_m)) ctl->count[t] = 0;
     if (t < 4) ctl->tile_counter[t] = t == 3 ? merge_start : 0u;
     if (noise_drops && t <= (uint32_t)kMaxNoise) noise_drops[t] = 0;
     for (uint32_t i = t; i < nstatus; i += gridDim.x * blockDim.x) status[i] = 0;
@@ -1053,16 +971,18 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
         const uint32_t nstatus = ctiles + (a.slot_count ? 0u : mtiles_max);
         const uint32_t blocks = std::max<uint32_t>(1u, std::min<uint32_t>((nstatus + 255) / 256, 4u * (uint32_t)a.sms));
         k_layer_prep<<<blocks, 256, 0, st>>>(ctl, a.status, nstatus, a.inject_stall ? 1u : 0u,
-                                             a.noise ? a.noise_drops : nullptr);
+                                             a.noise ? a.noise_drops : nullptr, a.preclassified);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if (m_hi > 0) {
-        // 1. classify
-        const uint32_t tiles = ctiles;
-        a.prof->begin(K_CLASSIFY, (double)a.n * 16 * W, st);
-        k_classify<W, T><<<tiles, kBlock, 0, st>>>(a.Sk, a.n, a.L, a.idx, a.D, a.status, ctl);
-        a.prof->end(st);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        // 1. classify (unless the TopN compaction before this layer listed the partners)
+        if (!a.preclassified) {
+            const uint32_t tiles = ctiles;
+            a.prof->begin(K_CLASSIFY, (double)a.n * 16 * W, st);
+            k_classify<W, T><<<tiles, kBlock, 0, st>>>(a.Sk, a.n, a.L, a.idx, a.D, a.status, ctl);
+            a.prof->end(st);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
         // 2-3. level scans (batches of kMaxLevels; one batch of four covers every gate on at
         // most two qubits), scatter on the last batch
         const uint32_t stiles = (uint32_t)((m_hi + kScanTile - 1) / kScanTile);

@@ -18,6 +18,7 @@
 //   k_expect_*             <psi|O|psi> in a product state, float64 partial sums reduced in a
 //                          fixed order (readout/product_state.rs:84-101)
 #include "ps_device.cuh"
+#include "ps_rotlayer.cuh"
 #include "ps_store.h"
 
 #include <algorithm>
@@ -512,7 +513,8 @@ __device__ __forceinline__ void block_select(unsigned int* __restrict__ hist, in
 // Block-wide: the boundary of `total` candidate keys in sk (shared memory, room for the next
 // power of two) at rank r from the top (1 <= r <= total): pads with zeros (the lowest key),
 // sorts descending (bitonic), and sets the select's final prefix (the boundary key itself, full
-// mask), remaining rank and count above ("above" counts the candidates strictly larger).
+// mask), remaining rank and count above ("above" counts the candidates strictly larger) and
+// the number of candidates equal to the boundary (aux[4]).
 __device__ __forceinline__ void block_sort_boundary(uint64_t* sk, unsigned int total, unsigned long long r,
                                                     Ctl* ctl) {
     const int tid = threadIdx.x;
@@ -537,13 +539,19 @@ __device__ __forceinline__ void block_sort_boundary(uint64_t* sk, unsigned int t
         }
     }
     const uint64_t B = sk[r - 1];
-    for (unsigned int i = tid; i < total; i += kSelThreads)
-        if (sk[i] == B && (i == 0 || sk[i - 1] != B)) {
-            ctl->aux[0] = B;
-            ctl->aux[1] = ~0ull;
-            ctl->aux[2] = r - i;
-            ctl->aux[3] += i;
-        }
+    __shared__ unsigned int s_first, s_last;
+    for (unsigned int i = tid; i < total; i += kSelThreads) {
+        if (sk[i] == B && (i == 0 || sk[i - 1] != B)) s_first = i;
+        if (sk[i] == B && (i + 1 == total || sk[i + 1] != B)) s_last = i;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        ctl->aux[0] = B;
+        ctl->aux[1] = ~0ull;
+        ctl->aux[2] = r - s_first;
+        ctl->aux[3] += s_first;
+        ctl->aux[4] = s_last - s_first + 1;
+    }
 }
 
 // SCORE: the learned pass's variant (select keys from score_key of the coefficient and the
@@ -571,7 +579,7 @@ __global__ void __launch_bounds__(kSelThreads, SCORE ? 3 : 4) k_topn_select_all(
     for (uint32_t i = blockIdx.x * kSelThreads + tid; i < ncstatus; i += gridDim.x * kSelThreads) cstatus[i] = 0;
     // digit 1 (block 0 first sets the select's state: no prefix, rank keep_n from the top)
     if (blockIdx.x == 0) {
-        if (tid < 7) ctl->aux[tid] = tid == 2 ? keep_n : 0ull;
+        if (tid < 8) ctl->aux[tid] = tid == 2 ? keep_n : 0ull;
         if (tid == 0) ctl->tile_counter[6] = 0;
         __syncthreads();
         block_select<kTopnBins1>(hist, window ? 48 : 52, window ? 11 : 12, ctl, s_part);
@@ -870,16 +878,13 @@ __global__ void __launch_bounds__(kThreads) k_topn_hist_cand(const uint64_t* __r
 // key_mode 3 keeps every row.  Rows outside the slots of a slotted store are skipped.
 // SCORE: the learned pass's variant (score keys from the prediction column, which the kept rows
 // carry); the plain variant keeps its registers, and with them its residency, free of the log.
+// One tile (the tile dispenser's next) per call.
 template <int W, typename T, bool SCORE>
-__global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __restrict__ keys, const T* __restrict__ coef,
-                                                           const uint64_t* __restrict__ sel, int key_mode,
-                                                           uint64_t base, uint64_t n, unsigned long long keep_n,
-                                                           uint64_t* __restrict__ okeys, T* __restrict__ ocoef,
-                                                           unsigned long long* status, Ctl* ctl, SlotMap slots,
-                                                           const float* __restrict__ fin, float* __restrict__ fout) {
-    // A select whose windowed boundary left the window writes nothing: the pass reruns in full
-    // range and rewrites the output.
-    if (key_mode != 2 && key_mode != 3 && ctl->aux[5]) return;
+__device__ __forceinline__ void compact_tile(const uint64_t* __restrict__ keys, const T* __restrict__ coef,
+                                             const uint64_t* __restrict__ sel, int key_mode, uint64_t base,
+                                             uint64_t n, unsigned long long keep_n, uint64_t* __restrict__ okeys,
+                                             T* __restrict__ ocoef, unsigned long long* status, Ctl* ctl,
+                                             SlotMap slots, const float* __restrict__ fin, float* __restrict__ fout) {
     const unsigned long long quota = ctl->aux[0] == 0 ? 0ull : keep_n - ctl->aux[3];
     constexpr int ITEMS = 16;
     constexpr int TILE = kThreads * ITEMS;
@@ -974,6 +979,164 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
         }
         arank += __popc(ba[i]);
         trank += __popc(bt[i]);
+    }
+}
+
+template <int W, typename T, bool SCORE>
+__global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __restrict__ keys, const T* __restrict__ coef,
+                                                           const uint64_t* __restrict__ sel, int key_mode,
+                                                           uint64_t base, uint64_t n, unsigned long long keep_n,
+                                                           uint64_t* __restrict__ okeys, T* __restrict__ ocoef,
+                                                           unsigned long long* status, Ctl* ctl, SlotMap slots,
+                                                           const float* __restrict__ fin, float* __restrict__ fout) {
+    // A select whose windowed boundary left the window writes nothing: the pass reruns in full
+    // range and rewrites the output.
+    if (key_mode != 2 && key_mode != 3 && ctl->aux[5]) return;
+    compact_tile<W, T, SCORE>(keys, coef, sel, key_mode, base, n, keep_n, okeys, ocoef, status, ctl, slots, fin, fout);
+}
+
+// Plain TopN compaction that also classifies the kept rows for the next rotation layer (the work
+// of that layer's k_classify, done while the keys are in registers).  When every key equal to the
+// boundary is kept (the select's tie count aux[4] equals the rank left for the ties, aux[2]), a
+// row is kept iff it is live and its key is at least the boundary, so a tile's kept count and its
+// count of kept rows that emit a partner under the next layer are both local, and one look-back
+// word carries the two (31 bits each).  The kept row goes to position pos; the j-th kept row that
+// emits a partner gets idx[j] = pos and D[j] = its divergence rank from the (j-1)-th (unknown for
+// the first of a warp, which k_level_reduce resolves), and the last tile publishes the partner
+// count in count[0], as k_classify does.  Otherwise (the quota cuts the ties, or the boundary is
+// NaN) the plain compaction runs and aux[7] tells the host that the next layer classifies itself.
+template <int W, typename T>
+__global__ void __launch_bounds__(kThreads, W == 1 ? 8 : (W == 2 ? 4 : 2)) k_topn_compact_cls(const uint64_t* __restrict__ keys,
+                                                               const T* __restrict__ coef, uint64_t base, uint64_t n,
+                                                               unsigned long long keep_n, uint64_t* __restrict__ okeys,
+                                                               T* __restrict__ ocoef, unsigned long long* status,
+                                                               Ctl* ctl, SlotMap slots, const RotLayer<W> L,
+                                                               uint32_t* __restrict__ idx, uint16_t* __restrict__ D) {
+    if (ctl->aux[5]) return;  // the windowed boundary left the window: the pass reruns in full range
+    if (!(ctl->aux[0] != 0 && ctl->aux[4] == ctl->aux[2])) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->aux[7] = 1;
+        compact_tile<W, T, false>(keys, coef, nullptr, 0, base, n, keep_n, okeys, ocoef, status, ctl, slots, nullptr,
+                                  nullptr);
+        return;
+    }
+    constexpr int ITEMS = 16;
+    constexpr int TILE = kThreads * ITEMS;
+    constexpr unsigned long long kLow31 = (1ull << 31) - 1;
+    __shared__ unsigned int s_tile;
+    __shared__ unsigned int s_wk[kThreads / 32], s_wp[kThreads / 32];
+    __shared__ unsigned long long s_kept, s_part;
+    __shared__ AmpTab<T> A;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned int lt = (1u << lane) - 1u;
+    if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[6], 1u);
+    stage_amps<W, T>(L, A);
+    __syncthreads();
+    const unsigned int tile = s_tile;
+    const uint64_t boundary = ctl->aux[0] + base;  // a windowed select's key back in full range
+    const uint64_t wbase = (uint64_t)tile * TILE + (uint64_t)warp * 32 * ITEMS;
+    unsigned int bk[ITEMS], bp[ITEMS];
+    unsigned int wk = 0, wp = 0;
+    SlotWalk sw(slots, wbase + lane);
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const uint64_t e = wbase + (uint64_t)i * 32 + lane;
+        bool kept = false, part = false;
+        if (e < n) {
+            // neither load waits for the liveness test (a slot's tail is allocated)
+            const uint64_t mk = mag_key<T>(coef[e]);
+            uint64_t k[2 * W];
+            load_key<W>(keys, e, k);
+            if (sw.live(slots) && mk >= boundary) {
+                kept = true;
+                part = emits_partner_regs<W, T>(L, A, k);
+            }
+        }
+        sw.step32(slots);
+        bk[i] = __ballot_sync(0xffffffffu, kept);
+        bp[i] = __ballot_sync(0xffffffffu, part);
+        wk += __popc(bk[i]);
+        wp += __popc(bp[i]);
+    }
+    if (lane == 0) {
+        s_wk[warp] = wk;
+        s_wp[warp] = wp;
+    }
+    __syncthreads();
+    unsigned int xk = 0, xp = 0, tk = 0, tp = 0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) {
+        xk += w < warp ? s_wk[w] : 0u;
+        xp += w < warp ? s_wp[w] : 0u;
+        tk += s_wk[w];
+        tp += s_wp[w];
+    }
+    if (tid < 32) {
+        const unsigned long long agg = (unsigned long long)tk | ((unsigned long long)tp << 31);
+        unsigned long long pre = 0;
+        if (tile == 0) {
+            if (tid == 0) st_release_u64(status + tile, kFlagInc | agg);
+        } else {
+            if (tid == 0) st_release_u64(status + tile, kFlagAgg | agg);
+            pre = lookback_sum_warp(status, tile, ctl, 704);
+            if (tid == 0) st_release_u64(status + tile, kFlagInc | (pre + agg));
+        }
+        if (tid == 0) {
+            s_kept = pre & kLow31;
+            s_part = pre >> 31;
+            if ((uint64_t)(tile + 1) * TILE >= n) {
+                ctl->count[3] = s_kept + tk;
+                ctl->count[0] = s_part + tp;
+            }
+        }
+    }
+    __syncthreads();
+    unsigned long long kr = s_kept + xk, pr = s_part + xp;
+    uint64_t prev[2 * W];
+#pragma unroll
+    for (int w = 0; w < 2 * W; ++w) prev[w] = 0;
+    bool have_prev = false;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const unsigned int b = bk[i], bq = bp[i];
+        const uint64_t e = wbase + (uint64_t)i * 32 + lane;
+        const unsigned long long pos = kr + __popc(b & lt);
+        uint64_t k[2 * W];
+#pragma unroll
+        for (int w = 0; w < 2 * W; ++w) k[w] = 0;
+        if ((b >> lane) & 1u) {
+            load_key<W>(keys, e, k);
+            if (PS_GUARD(ctl, pos < n, 702)) {
+                store_key<W>(okeys, pos, k);
+                ocoef[pos] = coef[e];
+            }
+        }
+        if (bq != 0) {  // warp-uniform: the rows that emit a partner, in order, with their ranks
+            const unsigned int lower = bq & lt;
+            const int src = lower ? 31 - __clz(lower) : lane;
+            const int hi = 31 - __clz(bq);
+            uint64_t pk[2 * W];
+#pragma unroll
+            for (int w = 0; w < 2 * W; ++w) pk[w] = __shfl_sync(0xffffffffu, k[w], src);
+            if ((bq >> lane) & 1u) {
+                const unsigned long long j = pr + __popc(lower);
+                if (PS_BOUNDS(ctl, j < n, 705)) {
+                    idx[j] = (uint32_t)pos;
+                    uint16_t d;
+                    if (lower)
+                        d = (uint16_t)div_regs<W>(pk, k);
+                    else if (have_prev)
+                        d = (uint16_t)div_regs<W>(prev, k);
+                    else
+                        d = j == 0 ? kDivStart : kDivUnknown;
+                    D[j] = d;
+                }
+            }
+#pragma unroll
+            for (int w = 0; w < 2 * W; ++w) prev[w] = __shfl_sync(0xffffffffu, k[w], hi);
+            have_prev = true;
+            pr += __popc(bq);
+        }
+        kr += __popc(b);
     }
 }
 
@@ -1290,9 +1453,11 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
                                  T* ocoef, unsigned int* hist, bool hist_ready, uint64_t* cand, uint64_t cand_cap,
                                  unsigned long long* status, Ctl* ctl, unsigned long long* host_count,
                                  uint64_t* out_n, int sms, cudaStream_t st, KernelProf* prof, const uint64_t* sel,
-                                 bool window, uint64_t base, SlotMap slots, const float* fpred, float* fout) {
-    // aux: prefix, mask, remaining rank, above, keys in the last chosen bin, window miss, keys
-    // gathered for the in-block sort (cooperative select); count[4]: candidates
+                                 bool window, uint64_t base, SlotMap slots, const float* fpred, float* fout,
+                                 const RotLayer<W>* next, uint32_t* next_idx, uint16_t* next_D) {
+    // aux: prefix, mask, remaining rank, above, keys in the last chosen bin (after the select:
+    // the keys equal to the boundary), window miss, keys gathered for the in-block sort
+    // (cooperative select), next layer not classified by the compaction; count[4]: candidates
     window = window && hist_ready && !sel;
     if (!window) base = 0;
     const unsigned int cgrid = grid_for(n, sms);
@@ -1358,7 +1523,9 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
         init[3] = 0ull;
         init[4] = 0ull;
         init[5] = 0ull;
-        cudaMemcpyAsync(ctl->aux, init, 6 * sizeof(unsigned long long), cudaMemcpyHostToDevice, st);
+        init[6] = 0ull;
+        init[7] = 0ull;
+        cudaMemcpyAsync(ctl->aux, init, 8 * sizeof(unsigned long long), cudaMemcpyHostToDevice, st);
         // digit 1: the select key's top 12 bits (key >> 52), or in a window the bin of 2^48 units;
         // then 13-bit digits down to bit 0 (a window's last digit overlaps bits already fixed)
         prof->begin(K_TOPN_STEP, kTopnBins1 * 8.0, st);
@@ -1390,7 +1557,11 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
         cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     }
     prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
-    if (fout)
+    const bool classify = next && next_idx && next_D && !sel && !fpred && !fout;
+    if (classify)
+        k_topn_compact_cls<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, base, n, (unsigned long long)keep_n, okeys,
+                                                             ocoef, status, ctl, slots, *next, next_idx, next_D);
+    else if (fout)
         k_topn_compact<W, T, true><<<tiles, kThreads, 0, st>>>(keys, coef, sel, sel ? 1 : (fpred ? 4 : 0), base, n,
                                                                (unsigned long long)keep_n, okeys, ocoef, status, ctl,
                                                                slots, fpred, fout);
@@ -1405,6 +1576,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     if ((e = spin_sync(st)) != cudaSuccess) return e;
     *out_n = host_count[3];
     prof->add_bytes(K_TOPN_COMPACT, (double)*out_n * (2 * 16 * W + sizeof(T)));
+    if (classify && !topn_unclassified(host_count)) prof->add_bytes(K_TOPN_COMPACT, (double)host_count[0] * 6.0);
     return cudaSuccess;
 }
 

@@ -409,3 +409,32 @@ def test_skip_covers_noise_and_general_tables_outside_the_support():
     o.propagate(oracle_channels(first), {"keep": [("coeff", 1e-12)]}, "forward")
     o.propagate(oracle_channels(circ), {"keep": [("coeff", 1e-12)]}, "forward")
     assert_same_terms(got, oracle_arrays(o), what="skip-noise-general")
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("ties", [False, True])
+def test_topn_compaction_lists_the_next_layers_partners(dtype, ties):
+    """A TopN pass followed by a rotation layer writes that layer's partner list while it
+    compacts (the layer then launches no classify pass) when every key equal to the boundary is
+    kept; when the quota cuts the ties it compacts plainly and the layer classifies itself.
+    Either way every layer is bit-exact against the oracle."""
+    nq = 20
+    x, z, c = workloads.random_observable(nq, 5000, seed=13)
+    if ties:
+        c = np.random.default_rng(3).choice([0.25, -0.25, 0.5, 0.125, -0.0625], size=len(x))
+    circ = workloads.random_pair_layers(nq, 2, seed=9)
+    pol = truncation.topn(4000)
+    g = ps.GpuPauliSum(nq, dtype)
+    g.upload(x, z, c)
+    g.set_profiling(True)
+    st = g.propagate(circ, pol, "heisenberg", with_stats=True)
+    prof = g.read_profile()
+    o = oracle_sum(nq, x, z, c, dtype)
+    after = o.propagate(oracle_channels(circ), oracle_policy(pol), "heisenberg")
+    assert st.terms_after == [int(v) for v in after]
+    assert_same_terms(g.download(), oracle_arrays(o), what=f"listed-partners-{dtype}-{ties}")
+    classify = prof["k_classify"]["launches"]
+    assert classify > 0  # the first layer classifies for itself
+    if not ties:
+        # the layers after a TopN pass take their partner lists from its compaction
+        assert classify < len(circ) // 2, (classify, len(circ))
