@@ -113,6 +113,11 @@ struct ps_sum {
     bool pre_valid = false;
     const ps_table* pre_table = nullptr;
     uint64_t pre_n = 0;
+    // the merge before such a TopN pass: each output row's partner test under next_table
+    Buf nflag;
+    bool nflag_valid = false;
+    const ps_table* nflag_table = nullptr;
+    LevelList* levels_next = nullptr;  // host scratch for the next layer's table
     Buf noise_drops;                      // folded noise: own rows first dropped after channel j
     unsigned long long* hnoise = nullptr; // pinned, kMaxNoise + 1 words
     KeepProg clean_keep{};
@@ -1146,6 +1151,21 @@ struct Engine {
         if (e == cudaSuccess && slotted)
             e = ensure(s, s->slot_count, (span_rows / merge_slot_rows<W>() + 1) * sizeof(unsigned int));
         if (e != cudaSuccess) return cuda_fail(s, e, "apply: output store");
+        // a plain TopN pass alone follows and a rotation layer (with partners) comes next: the
+        // merge also writes each output row's partner test under that layer, for the compaction
+        s->nflag_valid = false;
+        if (slotted && first_pass == PS_PASS_TOPN && policy->num_passes == 1 && s->next_table && !carry_f &&
+            !(noise && noise->n > 0) && a.L.partners && policy->passes[0].n < (1ull << 31) - 1) {
+            std::string why_next;
+            bool general_next = false;
+            if (to_rot_layer<W, T>(*s->next_table, a.next_L, *s->levels_next, why_next, &general_next) == PS_OK &&
+                !general_next && a.next_L.partners) {
+                if ((e = ensure(s, s->nflag, span_rows)) != cudaSuccess) return cuda_fail(s, e, "apply: partner flags");
+                a.next_flags = static_cast<uint8_t*>(s->nflag.p);
+                s->nflag_valid = true;
+                s->nflag_table = s->next_table;
+            }
+        }
         const uint64_t tiles_hi = out_rows / kMinTileRows + 4;
         if ((e = ensure(s, s->status, tiles_hi * sizeof(unsigned long long))) != cudaSuccess ||
             (e = ensure(s, s->bounds, (tiles_hi + 2) * sizeof(ulonglong2))) != cudaSuccess)
@@ -1400,6 +1420,9 @@ struct Engine {
                 if (use_hist) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
                 return cuda_fail(s, e, "topn: scratch");
             }
+            // the merge wrote the rows' partner tests under that layer
+            const bool flags_ok = classify && i == 0 && s->slotted && s->nflag_valid && s->nflag_table == s->next_table;
+            s->nflag_valid = false;
             uint64_t out_n = 0;
             // a histogram binned in the window around the last boundary selects in 1/16 octaves
             // (few candidates); when the boundary left the window, the pass reruns in full range
@@ -1413,7 +1436,8 @@ struct Engine {
                                          s->stream, &s->prof, nullptr, win, win ? s->hist_base : 0, slot_map(s),
                                          nullptr, nullptr, classify ? &next_L : nullptr,
                                          classify ? (uint32_t*)s->idx.p : nullptr,
-                                         classify ? (uint16_t*)s->dv.p : nullptr);
+                                         classify ? (uint16_t*)s->dv.p : nullptr, classify && flags_ok ?
+                                         static_cast<const uint8_t*>(s->nflag.p) : nullptr);
                 s->prof.resolve();
                 if (e != cudaSuccess) return cuda_fail(s, e, "topn");
                 unsigned int fl = 0, fi = 0;
@@ -1821,6 +1845,7 @@ ps_status ps_create(int32_t device, int32_t num_qubits, int32_t dtype, ps_sum** 
         return e == cudaErrorMemoryAllocation ? PS_ERR_OOM : PS_ERR_DEVICE;
     }
     s->levels = new LevelList();
+    s->levels_next = new LevelList();
     *out = s;
     return PS_OK;
 }
@@ -1834,7 +1859,7 @@ ps_status ps_destroy(ps_sum* s) {
     for (Buf* b : {&s->keys[0], &s->keys[1], &s->coef[0], &s->coef[1], &s->pk, &s->pc, &s->idx, &s->dv, &s->fv,
                    &s->slots, &s->status, &s->bounds, &s->hist, &s->cand, &s->partial, &s->dout, &s->sort_status,
                    &s->up_x, &s->up_z, &s->up_c, &s->up_k, &s->up_v0, &s->up_v1, &s->up_c0, &s->up_st, &s->sel,
-                   &s->cnorms, &s->cfirst, &s->slot_count, &s->noise_drops})
+                   &s->cnorms, &s->cfirst, &s->slot_count, &s->noise_drops, &s->nflag})
         release(*b);
     if (s->ctl) cudaFree(s->ctl);
     if (s->sort.hist) cudaFree(s->sort.hist);
@@ -1849,6 +1874,7 @@ ps_status ps_destroy(ps_sum* s) {
     s->prof.destroy();
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s->levels;
+    delete s->levels_next;
     delete s;
     return PS_OK;
 }
@@ -1924,7 +1950,8 @@ ps_status ps_propagate(ps_sum* s, const ps_channel* channels, uint64_t num_chann
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, s->stream);
-    s->pre_valid = false;  // a partner list names a table of this call only
+    s->pre_valid = false;  // a partner list (or flags) names a table of this call only
+    s->nflag_valid = false;
     ps_run_stats rs;
     std::memset(&rs, 0, sizeof rs);
     rs.peak_terms = s->n;
@@ -1954,10 +1981,10 @@ ps_status ps_propagate(ps_sum* s, const ps_channel* channels, uint64_t num_chann
             }
             uint64_t after[kMaxNoise];
             const uint64_t n0 = s->n;
+            s->next_table = fj + 1 < num_channels ? &tables[fj + 1] : nullptr;
             ps = dispatch<Engine>(s, [&](auto op) { return decltype(op)::apply(s, tables[fj], policy, &ls, &N, after); });
             if (ps == PS_OK && s->scorer) s->scorer_remaining -= (double)(fj - li);  // the folded layers' count-downs
             s->pass_call = fj;
-            s->next_table = fj + 1 < num_channels ? &tables[fj + 1] : nullptr;
             if (ps == PS_OK) ps = ps_finalize_layer(s, policy);
             s->next_table = nullptr;
             s->pass_call = 0;
@@ -1980,13 +2007,13 @@ ps_status ps_propagate(ps_sum* s, const ps_channel* channels, uint64_t num_chann
         }
         rs.total_terms_in += s->n;
         const uint64_t skipped0 = s->layers_skipped, n_in = s->n;
+        s->next_table = li + 1 < num_channels ? &tables[li + 1] : nullptr;
         ps = ps_apply_layer(s, &tables[li], policy, &ls);
         if (s->layers_skipped != skipped0) {
             ++rs.layers_skipped;
             rs.skipped_terms_in += n_in;
         }
         s->pass_call = li;  // CollapseSample's pass index of this layer
-        s->next_table = li + 1 < num_channels ? &tables[li + 1] : nullptr;
         if (ps == PS_OK) ps = ps_finalize_layer(s, policy);
         s->next_table = nullptr;
         s->pass_call = 0;
@@ -1999,6 +2026,8 @@ ps_status ps_propagate(ps_sum* s, const ps_channel* channels, uint64_t num_chann
         ++rs.layers;
     }
     s->pre_valid = false;
+    s->nflag_valid = false;
+    s->next_table = nullptr;
     cudaEventRecord(e1, s->stream);
     cudaEventSynchronize(e1);
     float ms = 0.f;

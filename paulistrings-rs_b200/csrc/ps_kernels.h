@@ -232,6 +232,8 @@ struct RotationArgs {
     int inject_stall;         // failure injection: the merge skips its first tile
     int preclassified;        // idx, D and count[0] already hold this layer's partner list (written
                               // by the TopN compaction before it): no classify pass
+    RotLayer<W> next_L;       // with next_flags (slotted output only): the next rotation layer,
+    uint8_t* next_flags;      // and per output row whether it emits a partner under it
     unsigned long long stall_limit;  // ... and its look-back waits give up after this many polls
     unsigned int* slot_count; // when set, the merge writes tile t at rows t * merge_slot_rows<W>()
                               // and its row count to slot_count[t], with no look-back (slotted

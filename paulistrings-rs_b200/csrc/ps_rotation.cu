@@ -92,6 +92,18 @@ struct NoNoise {};
 template <bool NOISE>
 using NoiseArg = typename std::conditional<NOISE, NoiseList, NoNoise>::type;
 
+// Before a TopN pass whose compaction lists the next rotation layer's partners: the merge
+// writes, per output row (slot layout), whether the row emits a partner under that layer, so the
+// compaction decides from one byte instead of reading the key twice.
+template <int W>
+struct NextFlagArg {
+    RotLayer<W> L;
+    uint8_t* flags;
+};
+struct NoNextFlag {};
+template <int W, bool ON>
+using NextArg = typename std::conditional<ON, NextFlagArg<W>, NoNextFlag>::type;
+
 // Shared storage for the staged channels only in the kernels that fold noise.
 template <typename T, bool ON>
 struct NoiseShared {
@@ -705,7 +717,7 @@ __device__ __forceinline__ uint32_t merge_walk(const uint64_t* sSk, const T* sSc
     return mask;
 }
 
-template <int W, typename T, bool NOISE, bool HASF>
+template <int W, typename T, bool NOISE, bool HASF, bool NEXTF = false>
 __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t* __restrict__ Sk, const T* __restrict__ Sc,
                                                   uint64_t n, const uint64_t* __restrict__ Pk,
                                                   const T* __restrict__ Pc, const ulonglong2* __restrict__ bounds,
@@ -717,7 +729,7 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
                                                   long long stall_limit, const NoiseArg<NOISE> N,
                                                   unsigned long long* __restrict__ noise_drops,
                                                   const float* __restrict__ Sf, const float* __restrict__ Pf,
-                                                  float* __restrict__ Of) {
+                                                  float* __restrict__ Of, const NextArg<W, NEXTF> NX = {}) {
     using SM = MergeSmem<W, T>;
     constexpr int ITEMS = RotTile<W>::kMergeItems;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -731,6 +743,7 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
     __shared__ unsigned long long s_outoff;
     __shared__ unsigned int s_hist[kTopnHistBins];
     __shared__ AmpTab<T> A;
+    __shared__ AmpTab<T> NA;  // the next layer's amplitudes (NEXTF)
     __shared__ NoiseShared<T, NOISE> NSH;
     NoiseSmem<T>* NS = NSH.tab();
     unsigned int* s_drop = NSH.drops();
@@ -740,6 +753,7 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
     if (topn_hist)
         for (int q = tid; q < kTopnHistBins; q += kBlock) s_hist[q] = 0;
     stage_amps<W, T>(L, A);
+    if constexpr (NEXTF) stage_amps<W, T>(NX.L, NA);
     if constexpr (NOISE) {
         stage_noise<T>(N, *NS);
         for (int q = tid; q <= kMaxNoise; q += kBlock) s_drop[q] = 0;
@@ -888,6 +902,11 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
         for (uint32_t q = tid; q < total; q += kBlock) {
             const T v = sC[q];
             Oc[off + q] = v;
+            if constexpr (NEXTF) {
+                uint64_t k[2 * W];
+                ld_row<W>(sK, q, k);
+                NX.flags[off + q] = emits_partner_regs<W, T>(NX.L, NA, k) ? 1 : 0;
+            }
             float fv = 0.0f;
             if constexpr (HASF) {
                 fv = sF[q];
@@ -1062,7 +1081,7 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     // injection the dispenser starts at tile 1, so tile 0 never publishes and tile 1's bounded
     // look-back gives up)
     const size_t smem = MergeSmem<W, T>::bytes;
-    static std::atomic<int> merge_per_sm[3];
+    static std::atomic<int> merge_per_sm[4];
     const long long stall = a.inject_stall ? (long long)a.stall_limit : 0ll;
     a.prof->begin(K_MERGE, 0.0, st);
     if (a.noise) {
@@ -1078,6 +1097,15 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
         k_merge<W, T, false, true><<<mgrid, kBlock, fsmem, st>>>(
             a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc, a.out_cap, merge_status, ctl, a.topn_hist,
             a.topn_hist_mode, a.topn_hist_base, a.slot_count, stall, NoNoise{}, nullptr, a.Sf, a.Pf, a.Of);
+    } else if (a.next_flags) {
+        const int mper = resident_blocks(k_merge<W, T, false, false, true>, kBlock, smem, merge_per_sm[3]);
+        const uint32_t mgrid = (uint32_t)std::min<uint64_t>(mtiles_hi, (uint64_t)mper * (a.sms > 0 ? a.sms : 1));
+        NextFlagArg<W> nx;
+        nx.L = a.next_L;
+        nx.flags = a.next_flags;
+        k_merge<W, T, false, false, true><<<mgrid, kBlock, smem, st>>>(
+            a.Sk, a.Sc, a.n, a.Pk, a.Pc, a.bounds, a.L, a.keep, a.Ok, a.Oc, a.out_cap, merge_status, ctl, a.topn_hist,
+            a.topn_hist_mode, a.topn_hist_base, a.slot_count, stall, NoNoise{}, nullptr, nullptr, nullptr, nullptr, nx);
     } else {
         const int mper = resident_blocks(k_merge<W, T, false, false>, kBlock, smem, merge_per_sm[0]);
         const uint32_t mgrid = (uint32_t)std::min<uint64_t>(mtiles_hi, (uint64_t)mper * (a.sms > 0 ? a.sms : 1));
@@ -1136,8 +1164,8 @@ template uint64_t merge_span_rows<4>(uint64_t);
 template <int W, typename T>
 cudaError_t configure_rotation_kernels() {
     cudaError_t e = cudaSuccess;
-    const void* kernels[3] = {(const void*)k_merge<W, T, false, false>, (const void*)k_merge<W, T, true, false>,
-                              (const void*)k_merge<W, T, false, true>};
+    const void* kernels[4] = {(const void*)k_merge<W, T, false, false>, (const void*)k_merge<W, T, true, false>,
+                              (const void*)k_merge<W, T, false, true>, (const void*)k_merge<W, T, false, false, true>};
     for (const void* k : kernels) {
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,

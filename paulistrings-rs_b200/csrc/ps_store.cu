@@ -1005,13 +1005,16 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
 // the first of a warp, which k_level_reduce resolves), and the last tile publishes the partner
 // count in count[0], as k_classify does.  Otherwise (the quota cuts the ties, or the boundary is
 // NaN) the plain compaction runs and aux[7] tells the host that the next layer classifies itself.
-template <int W, typename T>
+// FLAGS: the layer's merge wrote each row's partner test under the next layer (nflag, one byte
+// per row of the slotted store), so the first pass reads a byte instead of the key.
+template <int W, typename T, bool FLAGS>
 __global__ void __launch_bounds__(kThreads, W == 1 ? 8 : (W == 2 ? 4 : 2)) k_topn_compact_cls(const uint64_t* __restrict__ keys,
                                                                const T* __restrict__ coef, uint64_t base, uint64_t n,
                                                                unsigned long long keep_n, uint64_t* __restrict__ okeys,
                                                                T* __restrict__ ocoef, unsigned long long* status,
                                                                Ctl* ctl, SlotMap slots, const RotLayer<W> L,
-                                                               uint32_t* __restrict__ idx, uint16_t* __restrict__ D) {
+                                                               uint32_t* __restrict__ idx, uint16_t* __restrict__ D,
+                                                               const uint8_t* __restrict__ nflag) {
     if (ctl->aux[5]) return;  // the windowed boundary left the window: the pass reruns in full range
     if (!(ctl->aux[0] != 0 && ctl->aux[4] == ctl->aux[2])) {
         if (blockIdx.x == 0 && threadIdx.x == 0) ctl->aux[7] = 1;
@@ -1044,11 +1047,19 @@ __global__ void __launch_bounds__(kThreads, W == 1 ? 8 : (W == 2 ? 4 : 2)) k_top
         if (e < n) {
             // neither load waits for the liveness test (a slot's tail is allocated)
             const uint64_t mk = mag_key<T>(coef[e]);
-            uint64_t k[2 * W];
-            load_key<W>(keys, e, k);
-            if (sw.live(slots) && mk >= boundary) {
-                kept = true;
-                part = emits_partner_regs<W, T>(L, A, k);
+            if constexpr (FLAGS) {
+                const bool f = nflag[e] != 0;
+                if (sw.live(slots) && mk >= boundary) {
+                    kept = true;
+                    part = f;
+                }
+            } else {
+                uint64_t k[2 * W];
+                load_key<W>(keys, e, k);
+                if (sw.live(slots) && mk >= boundary) {
+                    kept = true;
+                    part = emits_partner_regs<W, T>(L, A, k);
+                }
             }
         }
         sw.step32(slots);
@@ -1454,7 +1465,8 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
                                  unsigned long long* status, Ctl* ctl, unsigned long long* host_count,
                                  uint64_t* out_n, int sms, cudaStream_t st, KernelProf* prof, const uint64_t* sel,
                                  bool window, uint64_t base, SlotMap slots, const float* fpred, float* fout,
-                                 const RotLayer<W>* next, uint32_t* next_idx, uint16_t* next_D) {
+                                 const RotLayer<W>* next, uint32_t* next_idx, uint16_t* next_D,
+                                 const uint8_t* next_flags) {
     // aux: prefix, mask, remaining rank, above, keys in the last chosen bin (after the select:
     // the keys equal to the boundary), window miss, keys gathered for the in-block sort
     // (cooperative select), next layer not classified by the compaction; count[4]: candidates
@@ -1558,9 +1570,14 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     }
     prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
     const bool classify = next && next_idx && next_D && !sel && !fpred && !fout;
-    if (classify)
-        k_topn_compact_cls<W, T><<<tiles, kThreads, 0, st>>>(keys, coef, base, n, (unsigned long long)keep_n, okeys,
-                                                             ocoef, status, ctl, slots, *next, next_idx, next_D);
+    if (classify && next_flags)
+        k_topn_compact_cls<W, T, true><<<tiles, kThreads, 0, st>>>(keys, coef, base, n, (unsigned long long)keep_n,
+                                                                   okeys, ocoef, status, ctl, slots, *next, next_idx,
+                                                                   next_D, next_flags);
+    else if (classify)
+        k_topn_compact_cls<W, T, false><<<tiles, kThreads, 0, st>>>(keys, coef, base, n, (unsigned long long)keep_n,
+                                                                    okeys, ocoef, status, ctl, slots, *next, next_idx,
+                                                                    next_D, nullptr);
     else if (fout)
         k_topn_compact<W, T, true><<<tiles, kThreads, 0, st>>>(keys, coef, sel, sel ? 1 : (fpred ? 4 : 0), base, n,
                                                                (unsigned long long)keep_n, okeys, ocoef, status, ctl,

@@ -81,14 +81,16 @@ struct StoreOps {
     // the select key is then score_key(c, f) (windowed like mag_key when window), and the kept
     // rows' predictions are written to fout.  next (plain TopN only): the next rotation layer;
     // the compaction then also writes that layer's partner list (next_idx, next_D, n words each)
-    // and its partner count in count[0], unless topn_unclassified says it could not.
+    // and its partner count in count[0], unless topn_unclassified says it could not; next_flags:
+    // each row's partner test under that layer, written by the layer's merge (or nullptr).
     static cudaError_t topn(const uint64_t* keys, const T* coef, uint64_t n, uint64_t keep_n, uint64_t* okeys, T* ocoef,
                             unsigned int* hist, bool hist_ready, uint64_t* cand, uint64_t cand_cap,
                             unsigned long long* status, Ctl* ctl, unsigned long long* host_count, uint64_t* out_n,
                             int sms, cudaStream_t st, KernelProf* prof, const uint64_t* sel = nullptr,
                             bool window = false, uint64_t base = 0, SlotMap slots = SlotMap{nullptr, 0u},
                             const float* fpred = nullptr, float* fout = nullptr, const RotLayer<W>* next = nullptr,
-                            uint32_t* next_idx = nullptr, uint16_t* next_D = nullptr);
+                            uint32_t* next_idx = nullptr, uint16_t* next_D = nullptr,
+                            const uint8_t* next_flags = nullptr);
     // Compact the live rows of a slotted store of n rows (its span) into okeys / ocoef, in order;
     // *out_n = rows kept.  Reads the counts and error words into host_count (synchronizes).
     static cudaError_t densify(const uint64_t* keys, const T* coef, uint64_t n, SlotMap slots, uint64_t* okeys,
