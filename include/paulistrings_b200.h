@@ -299,9 +299,13 @@ ps_status ps_expectation_device_noalloc(const uint64_t* keys, const void* coeffs
  * merge skips its first tile, so the following tile's output-offset wait sees a flag nothing
  * sets and gives up after `arg` polls (0: the default limit), reporting PS_ERR_TIMEOUT; the
  * shortened limit applies to that merge's output-offset waits only, and every other bounded
- * wait keeps the default.  PS_FAULT_NONE disarms both.  Either way the layer fails and the
- * store keeps the last completed layer. */
-typedef enum ps_fault_kind { PS_FAULT_NONE = 0, PS_FAULT_OOM = 1, PS_FAULT_STALL = 2 } ps_fault_kind;
+ * wait keeps the default.  PS_FAULT_FLAG: the next rotation layer's device error word is set
+ * from the host, in stream order after its kernels, as a failed device check would set it
+ * (`arg`: the flag bits, 0 for an internal-check failure); the layer reports PS_ERR_DEVICE (or
+ * PS_ERR_TIMEOUT for the timeout bit), including a layer whose TopN pass was already queued
+ * behind it.  PS_FAULT_NONE disarms them all.  Either way the layer fails and the store keeps
+ * the last completed layer. */
+typedef enum ps_fault_kind { PS_FAULT_NONE = 0, PS_FAULT_OOM = 1, PS_FAULT_STALL = 2, PS_FAULT_FLAG = 3 } ps_fault_kind;
 ps_status ps_inject_fault(ps_sum* sum, int32_t kind, uint64_t arg);
 
 /* Wait for the handle's stream.  PartitionStorage::settle. */

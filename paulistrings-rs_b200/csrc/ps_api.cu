@@ -118,6 +118,17 @@ struct ps_sum {
     bool nflag_valid = false;
     const ps_table* nflag_table = nullptr;
     LevelList* levels_next = nullptr;  // host scratch for the next layer's table
+    // A rotation layer whose plain TopN pass follows at once (inside ps_propagate) does not wait
+    // for its counts: the pass reads the span and live count on the device, and one
+    // synchronization after it serves both.  def_*: what the pass needs to finish the layer.
+    unsigned int fault_flag = 0;  // PS_FAULT_FLAG: error bits the next rotation layer reports
+    bool in_propagate = false;
+    bool deferred = false;
+    int def_prev_cur = 0;
+    uint64_t def_n_in = 0;
+    int def_nlv = 0;
+    bool def_classified = false;
+    ps_layer_stats* def_stats = nullptr;
     Buf noise_drops;                      // folded noise: own rows first dropped after channel j
     unsigned long long* hnoise = nullptr; // pinned, kMaxNoise + 1 words
     KeepProg clean_keep{};
@@ -1236,6 +1247,15 @@ struct Engine {
             a.noise_drops = static_cast<unsigned long long*>(s->noise_drops.p);
             a.host_noise_drops = s->hnoise;
         }
+        // the TopN pass that follows reads the span and live count on the device and waits once
+        // for both (one cooperative select, the merge's histogram and slots; no folded noise)
+        const bool defer = s->in_propagate && slotted && fuse_topn && first_pass == PS_PASS_TOPN &&
+                           policy->num_passes == 1 && policy->passes[0].n > 0 && !carry_f && !a.noise &&
+                           a.L.partners && StoreOps<W, T>::cooperative_select();
+        if (defer) a.defer_counts = s->hcount + 32;
+        a.inject_flag = s->fault_flag;
+        s->fault_flag = 0;
+        s->deferred = false;
         e = launch_rotation_layer<W, T>(a, s->stream);
         s->prof.resolve();
         if (e != cudaSuccess) return cuda_fail(s, e, "apply: rotation layer");
@@ -1262,12 +1282,53 @@ struct Engine {
             stats->terms_after_passes = out_n;
             stats->path = a.L.partners ? PS_PATH_ROTATION : PS_PATH_RESCALE;
         }
+        if (defer) {
+            // counts, statistics and the error check come with the TopN pass's synchronization
+            s->deferred = true;
+            s->def_prev_cur = s->cur;
+            s->def_n_in = n;
+            s->def_nlv = s->levels->n;
+            s->def_classified = !a.preclassified;
+            s->def_stats = stats;
+            if (stats) std::memset(stats, 0, sizeof *stats);
+        }
         s->cur = spare;
-        s->n = slotted ? span : out_n;
+        s->n = slotted ? span : out_n;  // deferred: a bound on the span
         s->slotted = slotted;
-        s->live_n = out_n;
+        s->live_n = out_n;              // deferred: not known yet
         s->slot_rows = slotted ? merge_slot_rows<W>() : 0u;
         layer_done(s, lsup, keep, a.L.partners != 0);
+        return PS_OK;
+    }
+
+    // The deferred layer's counts, read after the TopN pass's synchronization (host_count + 32
+    // holds the copy the layer queued before the pass): statistics, byte bookkeeping and its
+    // error check.  A failed layer's pass wrote nothing, so its input is restored as the store.
+    static ps_status finish_deferred(ps_sum* s, uint64_t span) {
+        s->deferred = false;
+        const unsigned long long* c = s->hcount + 32;
+        const unsigned int* f = reinterpret_cast<const unsigned int*>(reinterpret_cast<const unsigned char*>(c) +
+                                                                      offsetof(Ctl, err));
+        if (f[0]) {
+            s->cur = s->def_prev_cur;
+            s->n = s->def_n_in;
+            s->slotted = false;
+            s->live_n = 0;
+            cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);  // the pass left it
+            s->hist_ready = false;
+            return flags_status(s, f[0], f[1], "apply");
+        }
+        const uint64_t m = c[0], out = c[1];
+        book_rotation_bytes<W, T>(&s->prof, s->def_n_in, m, out, s->def_nlv, s->def_classified);
+        if (s->def_stats) {
+            s->def_stats->terms_in = s->def_n_in;
+            s->def_stats->partners = m;
+            s->def_stats->terms_out = out;
+            s->def_stats->terms_after_passes = out;
+            s->def_stats->path = PS_PATH_ROTATION;
+        }
+        s->n = span;
+        s->live_n = out;
         return PS_OK;
     }
 
@@ -1388,7 +1449,10 @@ struct Engine {
                 ready = false;
             }
             const bool use_hist = ready && i == 0;
-            if ((s->slotted ? s->live_n : s->n) <= p.n) {
+            // the layer before did not wait for its counts: the select decides on the device
+            // whether the live rows fit (the layer keeps a pass of n > 0 only, with its histogram)
+            const bool dfr = s->deferred && i == 0 && use_hist;
+            if (!dfr && (s->slotted ? s->live_n : s->n) <= p.n) {
                 if (use_hist) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
                 ps_status ps = densify(s, "topn");
                 if (ps != PS_OK) return ps;
@@ -1427,8 +1491,10 @@ struct Engine {
             // a histogram binned in the window around the last boundary selects in 1/16 octaves
             // (few candidates); when the boundary left the window, the pass reruns in full range
             const bool window = use_hist && s->hist_window;
+            bool kept_all = false;
             for (int attempt = 0; attempt < 2; ++attempt) {
                 const bool win = window && attempt == 0;
+                const bool dfr_now = dfr && attempt == 0;
                 e = StoreOps<W, T>::topn(K(s, s->cur), C(s, s->cur), s->n, p.n, K(s, spare), C(s, spare),
                                          (unsigned int*)s->hist.p, use_hist && attempt == 0, (uint64_t*)s->cand.p,
                                          topn_cand_words(s->n, s->sms), (unsigned long long*)s->status.p, s->ctl,
@@ -1437,9 +1503,14 @@ struct Engine {
                                          nullptr, nullptr, classify ? &next_L : nullptr,
                                          classify ? (uint32_t*)s->idx.p : nullptr,
                                          classify ? (uint16_t*)s->dv.p : nullptr, classify && flags_ok ?
-                                         static_cast<const uint8_t*>(s->nflag.p) : nullptr);
+                                         static_cast<const uint8_t*>(s->nflag.p) : nullptr, dfr_now);
                 s->prof.resolve();
                 if (e != cudaSuccess) return cuda_fail(s, e, "topn");
+                if (dfr_now) {  // the layer's own counts and error check, then the pass's
+                    ps_status ps = finish_deferred(s, s->hcount[22]);
+                    if (ps != PS_OK) return ps;
+                    kept_all = s->hcount[23] != 0;
+                }
                 unsigned int fl = 0, fi = 0;
                 topn_flags(s->hcount, &fl, &fi);
                 ps_status ps = flags_status(s, fl, fi, "topn");
@@ -1447,6 +1518,7 @@ struct Engine {
                     cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
                     return ps;
                 }
+                if (kept_all) break;  // no boundary: the window stays where it was
                 if (!(win && topn_window_missed(s->hcount))) {
                     const uint64_t boundary = topn_boundary(s->hcount, win ? s->hist_base : 0);
                     const uint64_t half = 1024ull << 48;
@@ -1952,6 +2024,7 @@ ps_status ps_propagate(ps_sum* s, const ps_channel* channels, uint64_t num_chann
     cudaEventRecord(e0, s->stream);
     s->pre_valid = false;  // a partner list (or flags) names a table of this call only
     s->nflag_valid = false;
+    s->in_propagate = true;
     ps_run_stats rs;
     std::memset(&rs, 0, sizeof rs);
     rs.peak_terms = s->n;
@@ -2028,6 +2101,8 @@ ps_status ps_propagate(ps_sum* s, const ps_channel* channels, uint64_t num_chann
     s->pre_valid = false;
     s->nflag_valid = false;
     s->next_table = nullptr;
+    s->in_propagate = false;
+    s->deferred = false;
     cudaEventRecord(e1, s->stream);
     cudaEventSynchronize(e1);
     float ms = 0.f;
@@ -2087,6 +2162,10 @@ ps_status ps_inject_fault(ps_sum* s, int32_t kind, uint64_t arg) {
         s->fault_oom_after = -1;
         s->fault_stall = false;
         s->stall_limit = 0;
+        s->fault_flag = 0;
+        break;
+    case PS_FAULT_FLAG:
+        s->fault_flag = arg ? (unsigned int)arg : 8u;  // ERR_INTERNAL
         break;
     case PS_FAULT_OOM:
         s->fault_oom_after = (long long)arg;

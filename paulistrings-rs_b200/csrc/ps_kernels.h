@@ -1,27 +1,55 @@
 // ps_kernels.h -- plain data shapes shared by the host driver and the kernel launchers.
 #pragma once
 
+#include <chrono>
 #include <cstddef>
 #include <cstdint>
+#include <cstdlib>
+#include <sys/prctl.h>
+#include <thread>
 #include <cuda_runtime.h>
 
 namespace psb {
 
-// Wait for everything queued on `st`, the calling thread spinning on an event instead of
-// sleeping in the driver: a layer waits for its counts once or twice, and a sleeping thread's
-// wake-up on a busy host can cost more than the kernels it waited for.  One event per device
-// and host thread.
+// Wait for everything queued on `st`: the calling thread spins on an event for up to the spin
+// budget (a layer's short waits end within it, where a sleeping thread's wake-up would cost more
+// than the kernels it waited for), then polls the event between sleeps of 20 us with the
+// thread's timer slack at 1 us (a thread that keeps spinning through a millisecond wait on a
+// busy host is preempted and returns late; a blocking wait in the driver wakes up later still).
+// The budget is PAULISTRINGS_B200_SPIN_US microseconds, read once (default 200; negative: spin
+// without bound).  One event per device and host thread.
+inline long long spin_budget_ns() {
+    static const long long ns = [] {
+        const char* v = std::getenv("PAULISTRINGS_B200_SPIN_US");
+        const long long us = v && *v ? std::atoll(v) : 200;
+        return us < 0 ? -1ll : us * 1000;
+    }();
+    return ns;
+}
 inline cudaError_t spin_sync(cudaStream_t st) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaStreamSynchronize(st);
     thread_local cudaEvent_t events[64] = {};
+    thread_local bool slack_set = false;
     if (!events[dev] && cudaEventCreateWithFlags(&events[dev], cudaEventDisableTiming) != cudaSuccess) {
         events[dev] = nullptr;
         return cudaStreamSynchronize(st);
     }
     cudaError_t e = cudaEventRecord(events[dev], st);
     if (e != cudaSuccess) return e;
+    const long long budget = spin_budget_ns();
+    const auto t0 = std::chrono::steady_clock::now();
+    bool sleeping = false;
     while ((e = cudaEventQuery(events[dev])) == cudaErrorNotReady) {
+        if (!sleeping && budget >= 0 &&
+            std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count() > budget) {
+            sleeping = true;
+            if (!slack_set) {
+                prctl(PR_SET_TIMERSLACK, 1000ul, 0ul, 0ul, 0ul);  // this thread's sleeps end within ~1 us
+                slack_set = true;
+            }
+        }
+        if (sleeping) std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
     return e;
 }
@@ -35,6 +63,8 @@ struct Ctl {
     unsigned long long aux[8];     // small per-pass values (TopN boundary, quota, ...)
     unsigned long long spin_limit; // polls before a bounded device wait gives up
     unsigned long long support[4]; // ingest: OR of every key's x | z words (the qubits any term touches)
+    unsigned long long span;       // a slotted merge's output: rows its slots span
+    unsigned long long topn_all;   // a TopN select found the live rows within its quota: keep them all
 };
 
 // Lowered keep program (postfix), KeepProgram in the reference's device path.
@@ -234,6 +264,10 @@ struct RotationArgs {
                               // by the TopN compaction before it): no classify pass
     RotLayer<W> next_L;       // with next_flags (slotted output only): the next rotation layer,
     uint8_t* next_flags;      // and per output row whether it emits a partner under it
+    unsigned int inject_flag;          // failure injection: error bits written after the kernels
+    unsigned long long* defer_counts;  // pinned: when set, the counts and error words are copied here
+                                       // and the launcher returns without waiting (slotted output: the
+                                       // TopN pass reads the span and live count on the device)
     unsigned long long stall_limit;  // ... and its look-back waits give up after this many polls
     unsigned int* slot_count; // when set, the merge writes tile t at rows t * merge_slot_rows<W>()
                               // and its row count to slot_count[t], with no look-back (slotted
@@ -257,6 +291,8 @@ uint64_t merge_span_rows(uint64_t rows_in);
 
 template <int W, typename T>
 cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st);
+template <int W, typename T>
+void book_rotation_bytes(KernelProf* prof, uint64_t n, uint64_t m, uint64_t out_count, int nlv, bool classified);
 template <int W, typename T>
 cudaError_t configure_rotation_kernels();
 

@@ -760,6 +760,8 @@ __global__ void __launch_bounds__(kBlock, W == 1 ? 4 : 1) k_merge(const uint64_t
     }
     const uint64_t m = ctl->count[0];  // partners, published by k_classify (0 without partners)
     const uint32_t num_tiles = (uint32_t)((n + m + SM::TILE - 1) / SM::TILE);
+    // a slotted output's span, for the TopN pass that reads it without the host knowing m
+    if (slot_count && blockIdx.x == 0 && tid == 0) ctl->span = (unsigned long long)num_tiles * (SM::TILE + 2);
     uint32_t phase = 0;  // completed phases of `bar`
     // Persistent: each block takes tiles from the dispenser until none is left (the grid is
     // sized by residency, not by the tile count, which only the device knows).
@@ -1115,6 +1117,21 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     }
     a.prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (a.inject_flag) {  // as a failed device check would leave it (stream order: after the kernels)
+        *reinterpret_cast<unsigned int*>(a.host_count + 60) = a.inject_flag;  // pinned, otherwise unused
+        cudaMemcpyAsync(&ctl->err, a.host_count + 60, sizeof(unsigned int), cudaMemcpyHostToDevice, st);
+    }
+    if (a.defer_counts) {
+        // the caller reads them after the TopN pass's synchronization (and books the bytes then)
+        cudaMemcpyAsync(a.defer_counts, &ctl->count[0], offsetof(Ctl, err_info) + sizeof(unsigned int),
+                        cudaMemcpyDeviceToHost, st);
+        *a.partners_out = 0;
+        *a.out_count = 0;
+        *a.span_out = (a.n + m_hi + MT - 1) / MT * (uint64_t)(MT + 2);  // a bound: m is not known here
+        *a.err_flags = 0;
+        *a.err_info = 0;
+        return cudaGetLastError();
+    }
     // counts and error flags in one copy: count[0..7], tile_counter[0..7], err, err_info
     cudaMemcpyAsync(a.host_count, &ctl->count[0], offsetof(Ctl, err_info) + sizeof(unsigned int),
                     cudaMemcpyDeviceToHost, st);
@@ -1130,20 +1147,26 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
         reinterpret_cast<const unsigned char*>(a.host_count) + offsetof(Ctl, err));
     *a.err_flags = flags[0];
     *a.err_info = flags[1];
-    // algorithmic bytes, booked now that m and the output count are known
-    a.prof->add_bytes(K_CLASSIFY, (double)m * 6);  // idx + divergence writes
-    const int nlv = a.levels->n;
+    book_rotation_bytes<W, T>(a.prof, a.n, m, *a.out_count, a.levels->n, !a.preclassified);
+    return cudaSuccess;
+}
+
+// The algorithmic bytes of a rotation layer's kernels, booked once m and the output count are
+// known (after the layer's synchronization, or the TopN pass's when the layer did not wait).
+template <int W, typename T>
+void book_rotation_bytes(KernelProf* prof, uint64_t n, uint64_t m, uint64_t out_count, int nlv, bool classified) {
+    constexpr int MT = RotTile<W>::kMergeTile;
+    if (classified) prof->add_bytes(K_CLASSIFY, (double)m * 6);  // idx + divergence writes
     const int per = nlv <= 4 ? 4 : kMaxLevels;
     const int nb = m ? (nlv + per - 1) / per : 0;
     for (int b = 0; b < nb; ++b) {
         const bool last = b == nb - 1;
-        a.prof->add_bytes(K_LEVEL_SCAN, (double)m * 2);  // divergence reads
+        prof->add_bytes(K_LEVEL_SCAN, (double)m * 2);  // divergence reads
         // divergence reads, earlier batches' F, then F written or (last) index, gather and place
-        a.prof->add_bytes(K_LEVEL_APPLY, (double)m * (2 + (b > 0 ? 4 : 0) + (last ? 4 + 2.0 * (16 * W + sizeof(T)) : 4)));
+        prof->add_bytes(K_LEVEL_APPLY, (double)m * (2 + (b > 0 ? 4 : 0) + (last ? 4 + 2.0 * (16 * W + sizeof(T)) : 4)));
     }
-    a.prof->add_bytes(K_PARTITION, (double)((a.n + m + MT - 1) / MT + 1) * 16);
-    a.prof->add_bytes(K_MERGE, (double)(a.n + m + *a.out_count) * (16 * W + sizeof(T)));
-    return cudaSuccess;
+    prof->add_bytes(K_PARTITION, (double)((n + m + MT - 1) / MT + 1) * 16);
+    prof->add_bytes(K_MERGE, (double)(n + m + out_count) * (16 * W + sizeof(T)));
 }
 
 template <int W>
@@ -1180,6 +1203,7 @@ cudaError_t configure_rotation_kernels() {
 
 #define PS_INSTANTIATE_ROT(W, T)                                                                 \
     template cudaError_t launch_rotation_layer<W, T>(const RotationArgs<W, T>&, cudaStream_t); \
+    template void book_rotation_bytes<W, T>(KernelProf*, uint64_t, uint64_t, uint64_t, int, bool); \
     template cudaError_t configure_rotation_kernels<W, T>();
 
 PS_INSTANTIATE_ROT(1, double)

@@ -559,7 +559,7 @@ __device__ __forceinline__ void block_sort_boundary(uint64_t* sk, unsigned int t
 template <typename T, bool SCORE>
 __global__ void __launch_bounds__(kSelThreads, SCORE ? 3 : 4) k_topn_select_all(const T* __restrict__ coef,
                                                                  const uint64_t* __restrict__ sel, int window,
-                                                                 uint64_t base, uint64_t n, Ctl* ctl,
+                                                                 uint64_t base, uint64_t n_arg, Ctl* ctl,
                                                                  unsigned int* __restrict__ hist,
                                                                  uint64_t* __restrict__ cand, uint64_t cand_cap,
                                                                  uint64_t seg_cap, unsigned int* __restrict__ seg_count,
@@ -567,9 +567,14 @@ __global__ void __launch_bounds__(kSelThreads, SCORE ? 3 : 4) k_topn_select_all(
                                                                  const float* __restrict__ fpred,
                                                                  unsigned long long keep_n,
                                                                  unsigned long long* __restrict__ cstatus,
-                                                                 uint32_t ncstatus) {
+                                                                 uint32_t ncstatus, int deferred) {
     constexpr int ITEMS = 16;
     constexpr int CHUNK = kSelThreads * ITEMS;
+    // deferred: the host launched this pass without reading the layer's counts; n_arg bounds the
+    // rows (it sized the grid and the segments), the merge left the span, and a failed layer
+    // (an error flag already set) writes nothing more
+    if (deferred && ctl->err) return;
+    const uint64_t n = deferred ? ctl->span : n_arg;
     __shared__ unsigned int sh[kTopnBinsN];
     __shared__ unsigned long long s_part[kSelThreads];
     __shared__ unsigned long long s_base;
@@ -577,13 +582,26 @@ __global__ void __launch_bounds__(kSelThreads, SCORE ? 3 : 4) k_topn_select_all(
     const unsigned int lt = (1u << lane) - 1u;
     // the compaction's look-back words and dispenser, reset here for the launch that follows
     for (uint32_t i = blockIdx.x * kSelThreads + tid; i < ncstatus; i += gridDim.x * kSelThreads) cstatus[i] = 0;
-    // digit 1 (block 0 first sets the select's state: no prefix, rank keep_n from the top)
+    // digit 1 (block 0 first sets the select's state: no prefix, rank keep_n from the top).
+    // Deferred, the live rows may fit the quota (the host checks that itself otherwise): then
+    // every live row is kept, the histogram is cleared and nothing is selected.
+    const bool keep_all = deferred && ctl->count[1] <= keep_n;
     if (blockIdx.x == 0) {
         if (tid < 8) ctl->aux[tid] = tid == 2 ? keep_n : 0ull;
-        if (tid == 0) ctl->tile_counter[6] = 0;
+        if (tid == 0) {
+            ctl->tile_counter[6] = 0;
+            ctl->topn_all = keep_all ? 1ull : 0ull;
+            ctl->count[0] = 0;  // the compaction's partner count for the next layer (none when it lists none)
+            ctl->count[3] = 0;  // its output count (no tile writes it when the span is empty)
+        }
         __syncthreads();
-        block_select<kTopnBins1>(hist, window ? 48 : 52, window ? 11 : 12, ctl, s_part);
+        if (keep_all) {
+            for (int q = tid; q < kTopnBins1; q += kSelThreads) hist[q] = 0;
+        } else {
+            block_select<kTopnBins1>(hist, window ? 48 : 52, window ? 11 : 12, ctl, s_part);
+        }
     }
+    if (keep_all) return;  // every block: the same decision, before any barrier
     if (!grid_barrier(bar, ctl, 720)) return;
     // the boundary bin's keys into this block's segment
     {
@@ -896,6 +914,7 @@ __device__ __forceinline__ void compact_tile(const uint64_t* __restrict__ keys, 
     if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[6], 1u);
     __syncthreads();
     const unsigned int tile = s_tile;
+    if (tile > 0 && (uint64_t)tile * TILE >= n) return;  // past the span (a grid sized by a bound)
     const uint64_t boundary = ctl->aux[0] == 0 ? 0ull : ctl->aux[0] + base;  // a windowed select's key back in full range
     const uint64_t wbase = (uint64_t)tile * TILE + (uint64_t)warp * 32 * ITEMS;
     unsigned int ba[ITEMS], bt[ITEMS];
@@ -988,9 +1007,17 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
                                                            uint64_t base, uint64_t n, unsigned long long keep_n,
                                                            uint64_t* __restrict__ okeys, T* __restrict__ ocoef,
                                                            unsigned long long* status, Ctl* ctl, SlotMap slots,
-                                                           const float* __restrict__ fin, float* __restrict__ fout) {
+                                                           const float* __restrict__ fin, float* __restrict__ fout,
+                                                           int deferred) {
     // A select whose windowed boundary left the window writes nothing: the pass reruns in full
-    // range and rewrites the output.
+    // range and rewrites the output.  Deferred (see k_topn_select_all): the merge's span, no
+    // write after a failed layer, and every live row kept when the select found them within the
+    // quota.
+    if (deferred) {
+        if (ctl->err) return;
+        n = ctl->span;
+        if (ctl->topn_all) key_mode = 3;
+    }
     if (key_mode != 2 && key_mode != 3 && ctl->aux[5]) return;
     compact_tile<W, T, SCORE>(keys, coef, sel, key_mode, base, n, keep_n, okeys, ocoef, status, ctl, slots, fin, fout);
 }
@@ -1014,9 +1041,16 @@ __global__ void __launch_bounds__(kThreads, W == 1 ? 8 : (W == 2 ? 4 : 2)) k_top
                                                                T* __restrict__ ocoef, unsigned long long* status,
                                                                Ctl* ctl, SlotMap slots, const RotLayer<W> L,
                                                                uint32_t* __restrict__ idx, uint16_t* __restrict__ D,
-                                                               const uint8_t* __restrict__ nflag) {
-    if (ctl->aux[5]) return;  // the windowed boundary left the window: the pass reruns in full range
-    if (!(ctl->aux[0] != 0 && ctl->aux[4] == ctl->aux[2])) {
+                                                               const uint8_t* __restrict__ nflag, int deferred) {
+    // deferred: as k_topn_compact
+    bool all = false;
+    if (deferred) {
+        if (ctl->err) return;
+        n = ctl->span;
+        all = ctl->topn_all != 0;
+    }
+    if (!all && ctl->aux[5]) return;  // the windowed boundary left the window: the pass reruns in full range
+    if (!all && !(ctl->aux[0] != 0 && ctl->aux[4] == ctl->aux[2])) {
         if (blockIdx.x == 0 && threadIdx.x == 0) ctl->aux[7] = 1;
         compact_tile<W, T, false>(keys, coef, nullptr, 0, base, n, keep_n, okeys, ocoef, status, ctl, slots, nullptr,
                                   nullptr);
@@ -1035,7 +1069,9 @@ __global__ void __launch_bounds__(kThreads, W == 1 ? 8 : (W == 2 ? 4 : 2)) k_top
     stage_amps<W, T>(L, A);
     __syncthreads();
     const unsigned int tile = s_tile;
-    const uint64_t boundary = ctl->aux[0] + base;  // a windowed select's key back in full range
+    if (tile > 0 && (uint64_t)tile * TILE >= n) return;  // past the span (a grid sized by a bound)
+    // a windowed select's key back in full range; every live row when all are kept
+    const uint64_t boundary = all ? 0ull : ctl->aux[0] + base;
     const uint64_t wbase = (uint64_t)tile * TILE + (uint64_t)warp * 32 * ITEMS;
     unsigned int bk[ITEMS], bp[ITEMS];
     unsigned int wk = 0, wp = 0;
@@ -1459,6 +1495,31 @@ cudaError_t StoreOps<W, T>::dedup(const uint64_t* keys, const uint32_t* vals, co
     return cudaSuccess;
 }
 
+// Resident blocks per SM of the cooperative select (its plain or scored variant), looked up on
+// first use; -1 when the device cannot run it.
+template <typename T>
+int select_blocks_per_sm(bool score) {
+    static std::atomic<int> per_sm[2] = {{0}, {0}};
+    std::atomic<int>& per_v = per_sm[score ? 1 : 0];
+    int per = per_v.load(std::memory_order_relaxed);
+    if (per == 0) {
+        const void* kern = score ? (const void*)k_topn_select_all<T, true> : (const void*)k_topn_select_all<T, false>;
+        int dev = 0, coop = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kSelThreads, 0) != cudaSuccess || per < 1)
+            per = -1;
+        cudaGetLastError();
+        per_v.store(per, std::memory_order_relaxed);
+    }
+    return per;
+}
+
+template <int W, typename T>
+bool StoreOps<W, T>::cooperative_select() {
+    return select_blocks_per_sm<T>(false) > 0;
+}
+
 template <int W, typename T>
 cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n, uint64_t keep_n, uint64_t* okeys,
                                  T* ocoef, unsigned int* hist, bool hist_ready, uint64_t* cand, uint64_t cand_cap,
@@ -1466,7 +1527,8 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
                                  uint64_t* out_n, int sms, cudaStream_t st, KernelProf* prof, const uint64_t* sel,
                                  bool window, uint64_t base, SlotMap slots, const float* fpred, float* fout,
                                  const RotLayer<W>* next, uint32_t* next_idx, uint16_t* next_D,
-                                 const uint8_t* next_flags) {
+                                 const uint8_t* next_flags, bool deferred) {
+    const int dfr = deferred ? 1 : 0;
     // aux: prefix, mask, remaining rank, above, keys in the last chosen bin (after the select:
     // the keys equal to the boundary), window miss, keys gathered for the in-block sort
     // (cooperative select), next layer not classified by the compaction; count[4]: candidates
@@ -1478,6 +1540,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     if (key_cap + (cgrid + 1) / 2 > cand_cap) return cudaErrorInvalidValue;  // sized by topn_cand_words
     unsigned int* seg_count = reinterpret_cast<unsigned int*>(cand + key_cap);
     cudaError_t e;
+    if (deferred && (!hist_ready || !slots.count)) return cudaErrorInvalidValue;  // needs the merge's histogram and slots
     if (!hist_ready) {
         cudaMemsetAsync(hist, 0, kTopnBins1 * sizeof(unsigned int), st);
         prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
@@ -1492,15 +1555,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     {
         const float* fp = sel ? nullptr : fpred;
         const void* kern = fp ? (const void*)k_topn_select_all<T, true> : (const void*)k_topn_select_all<T, false>;
-        static std::atomic<int> per_sm[2] = {{0}, {0}};
-        std::atomic<int>& per_v = per_sm[fp ? 1 : 0];
-        int per = per_v.load(std::memory_order_relaxed);
-        if (per == 0) {
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kSelThreads, 0) != cudaSuccess || per < 1)
-                per = -1;
-            cudaGetLastError();
-            per_v.store(per, std::memory_order_relaxed);
-        }
+        const int per = select_blocks_per_sm<T>(fp != nullptr);
         if (per > 0) {
             const uint64_t nchunks = (n + kSelThreads * 16 - 1) / (kSelThreads * 16);
             const unsigned int G =
@@ -1518,12 +1573,13 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
                 void* args[] = {(void*)&coef, (void*)&sel,  (void*)&win,   (void*)&base, (void*)&n,
                                 (void*)&ctl,  (void*)&hist, (void*)&cand,  (void*)&gkey, (void*)&gseg,
                                 (void*)&gcount, (void*)&slots, (void*)&bar, (void*)&fp, (void*)&kn,
-                                (void*)&status, (void*)&ctiles};
+                                (void*)&status, (void*)&ctiles, (void*)&dfr};
                 prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
                 e = cudaLaunchCooperativeKernel(kern, dim3(G), dim3(kSelThreads), args, 0, st);
                 prof->end(st);
                 selected = e == cudaSuccess;
                 if (!selected) cudaGetLastError();  // not launched: the multi-launch path selects instead
+                if (!selected && deferred) return cudaErrorNotSupported;  // the host does not know the span
             }
         }
     }
@@ -1573,23 +1629,25 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     if (classify && next_flags)
         k_topn_compact_cls<W, T, true><<<tiles, kThreads, 0, st>>>(keys, coef, base, n, (unsigned long long)keep_n,
                                                                    okeys, ocoef, status, ctl, slots, *next, next_idx,
-                                                                   next_D, next_flags);
+                                                                   next_D, next_flags, dfr);
     else if (classify)
         k_topn_compact_cls<W, T, false><<<tiles, kThreads, 0, st>>>(keys, coef, base, n, (unsigned long long)keep_n,
                                                                     okeys, ocoef, status, ctl, slots, *next, next_idx,
-                                                                    next_D, nullptr);
+                                                                    next_D, nullptr, dfr);
     else if (fout)
         k_topn_compact<W, T, true><<<tiles, kThreads, 0, st>>>(keys, coef, sel, sel ? 1 : (fpred ? 4 : 0), base, n,
                                                                (unsigned long long)keep_n, okeys, ocoef, status, ctl,
-                                                               slots, fpred, fout);
+                                                               slots, fpred, fout, dfr);
     else
         k_topn_compact<W, T, false><<<tiles, kThreads, 0, st>>>(keys, coef, sel, sel ? 1 : 0, base, n,
                                                                 (unsigned long long)keep_n, okeys, ocoef, status, ctl,
-                                                                slots, nullptr, nullptr);
+                                                                slots, nullptr, nullptr, dfr);
     prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // the one host synchronization of the pass: counts, error flags and the select's aux words
+    // (and, deferred, the span the select read and whether it kept every live row)
     cudaMemcpyAsync(host_count, &ctl->count[0], offsetof(Ctl, spin_limit), cudaMemcpyDeviceToHost, st);
+    if (deferred) cudaMemcpyAsync(host_count + 22, &ctl->span, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
     if ((e = spin_sync(st)) != cudaSuccess) return e;
     *out_n = host_count[3];
     prof->add_bytes(K_TOPN_COMPACT, (double)*out_n * (2 * 16 * W + sizeof(T)));
@@ -1614,10 +1672,10 @@ cudaError_t StoreOps<W, T>::densify(const uint64_t* keys, const T* coef, uint64_
     prof->begin(K_TOPN_COMPACT, 0.0, st);
     if (fout)
         k_topn_compact<W, T, true><<<tiles, kThreads, 0, st>>>(keys, coef, nullptr, 3, 0ull, n, 0ull, okeys, ocoef,
-                                                               status, ctl, slots, fin, fout);
+                                                               status, ctl, slots, fin, fout, 0);
     else
         k_topn_compact<W, T, false><<<tiles, kThreads, 0, st>>>(keys, coef, nullptr, 3, 0ull, n, 0ull, okeys, ocoef,
-                                                                status, ctl, slots, nullptr, nullptr);
+                                                                status, ctl, slots, nullptr, nullptr, 0);
     prof->end(st);
     cudaError_t e;
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1672,7 +1730,7 @@ cudaError_t StoreOps<W, T>::approx_topn(const uint64_t* keys, const T* coef, uin
     cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
     k_topn_compact<W, T, false><<<tiles, kThreads, 0, st>>>(keys, coef, nullptr, 2, 0ull, n, (unsigned long long)keep_n,
-                                                     okeys, ocoef, status, ctl, SlotMap{nullptr, 0u}, nullptr, nullptr);
+                                                     okeys, ocoef, status, ctl, SlotMap{nullptr, 0u}, nullptr, nullptr, 0);
     prof->end(st);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     cudaMemcpyAsync(host_count, &ctl->count[0], offsetof(Ctl, err_info) + sizeof(unsigned int),

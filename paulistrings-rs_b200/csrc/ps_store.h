@@ -83,6 +83,10 @@ struct StoreOps {
     // the compaction then also writes that layer's partner list (next_idx, next_D, n words each)
     // and its partner count in count[0], unless topn_unclassified says it could not; next_flags:
     // each row's partner test under that layer, written by the layer's merge (or nullptr).
+    // deferred: the host has not read the layer's counts; n (and the scratch) bound the span,
+    // which the kernels read from the control block with the live count (when it is within
+    // keep_n every live row is kept), and a layer that failed is left alone; host_count[22] and
+    // [23] receive the span and whether every live row was kept.  Needs cooperative_select().
     static cudaError_t topn(const uint64_t* keys, const T* coef, uint64_t n, uint64_t keep_n, uint64_t* okeys, T* ocoef,
                             unsigned int* hist, bool hist_ready, uint64_t* cand, uint64_t cand_cap,
                             unsigned long long* status, Ctl* ctl, unsigned long long* host_count, uint64_t* out_n,
@@ -90,7 +94,9 @@ struct StoreOps {
                             bool window = false, uint64_t base = 0, SlotMap slots = SlotMap{nullptr, 0u},
                             const float* fpred = nullptr, float* fout = nullptr, const RotLayer<W>* next = nullptr,
                             uint32_t* next_idx = nullptr, uint16_t* next_D = nullptr,
-                            const uint8_t* next_flags = nullptr);
+                            const uint8_t* next_flags = nullptr, bool deferred = false);
+    // Can topn run deferred (the whole select in one cooperative launch on this device)?
+    static bool cooperative_select();
     // Compact the live rows of a slotted store of n rows (its span) into okeys / ocoef, in order;
     // *out_n = rows kept.  Reads the counts and error words into host_count (synchronizes).
     static cudaError_t densify(const uint64_t* keys, const T* coef, uint64_t n, SlotMap slots, uint64_t* okeys,

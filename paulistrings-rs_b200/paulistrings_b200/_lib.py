@@ -67,7 +67,7 @@ EXPORTED = (
     "ps_set_scorer",
 )
 
-PS_FAULT_NONE, PS_FAULT_OOM, PS_FAULT_STALL = 0, 1, 2
+PS_FAULT_NONE, PS_FAULT_OOM, PS_FAULT_STALL, PS_FAULT_FLAG = 0, 1, 2, 3
 
 NOALLOC_MAX_TERMS = 1 << 30
 
