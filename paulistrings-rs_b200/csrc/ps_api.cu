@@ -128,6 +128,7 @@ struct ps_sum {
     uint64_t def_n_in = 0;
     int def_nlv = 0;
     bool def_classified = false;
+    bool def_flags = false;
     ps_layer_stats* def_stats = nullptr;
     Buf noise_drops;                      // folded noise: own rows first dropped after channel j
     unsigned long long* hnoise = nullptr; // pinned, kMaxNoise + 1 words
@@ -159,19 +160,26 @@ ps_status cuda_fail(ps_sum* s, cudaError_t e, const char* where) {
     return set_err(s, st, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
-// Grow-only buffer; contents are not preserved.
+// Grow-only buffer; contents are not preserved.  A buffer that must grow grows by half again
+// at least (exactly to the request when that much does not fit), so a sum that grows a little
+// every layer does not free and allocate -- two device-wide synchronizations -- every layer.
 cudaError_t ensure(Buf& b, size_t bytes) {
     if (b.bytes >= bytes && b.p) return cudaSuccess;
+    size_t cap = b.p && b.bytes ? std::max(bytes, b.bytes + b.bytes / 2) : bytes;
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.bytes = 0;
-    size_t want = bytes + kPad;
-    cudaError_t e = cudaMalloc(&b.p, want);
+    cudaError_t e = cudaMalloc(&b.p, cap + kPad);
+    if (e == cudaErrorMemoryAllocation && cap > bytes) {
+        cudaGetLastError();
+        cap = bytes;
+        e = cudaMalloc(&b.p, cap + kPad);
+    }
     if (e != cudaSuccess) {
         b.p = nullptr;
         return e;
     }
-    b.bytes = bytes;
+    b.bytes = cap;
     return cudaSuccess;
 }
 
@@ -1289,6 +1297,7 @@ struct Engine {
             s->def_n_in = n;
             s->def_nlv = s->levels->n;
             s->def_classified = !a.preclassified;
+            s->def_flags = a.next_flags != nullptr;
             s->def_stats = stats;
             if (stats) std::memset(stats, 0, sizeof *stats);
         }
@@ -1320,6 +1329,7 @@ struct Engine {
         }
         const uint64_t m = c[0], out = c[1];
         book_rotation_bytes<W, T>(&s->prof, s->def_n_in, m, out, s->def_nlv, s->def_classified);
+        if (s->def_flags) s->prof.add_bytes(K_MERGE, (double)out);  // the partner-test bytes
         if (s->def_stats) {
             s->def_stats->terms_in = s->def_n_in;
             s->def_stats->partners = m;

@@ -1148,6 +1148,7 @@ cudaError_t launch_rotation_layer(const RotationArgs<W, T>& a, cudaStream_t st) 
     *a.err_flags = flags[0];
     *a.err_info = flags[1];
     book_rotation_bytes<W, T>(a.prof, a.n, m, *a.out_count, a.levels->n, !a.preclassified);
+    if (a.next_flags) a.prof->add_bytes(K_MERGE, (double)*a.out_count);  // the partner-test bytes
     return cudaSuccess;
 }
 

@@ -1574,7 +1574,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
                                 (void*)&ctl,  (void*)&hist, (void*)&cand,  (void*)&gkey, (void*)&gseg,
                                 (void*)&gcount, (void*)&slots, (void*)&bar, (void*)&fp, (void*)&kn,
                                 (void*)&status, (void*)&ctiles, (void*)&dfr};
-                prof->begin(K_TOPN_HIST, (double)n * sizeof(T), st);
+                prof->begin(K_TOPN_HIST, deferred ? 0.0 : (double)n * sizeof(T), st);
                 e = cudaLaunchCooperativeKernel(kern, dim3(G), dim3(kSelThreads), args, 0, st);
                 prof->end(st);
                 selected = e == cudaSuccess;
@@ -1624,7 +1624,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
         cudaMemsetAsync(status, 0, (size_t)tiles * sizeof(unsigned long long), st);
         cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     }
-    prof->begin(K_TOPN_COMPACT, (double)n * sizeof(T), st);
+    prof->begin(K_TOPN_COMPACT, deferred ? 0.0 : (double)n * sizeof(T), st);
     const bool classify = next && next_idx && next_D && !sel && !fpred && !fout;
     if (classify && next_flags)
         k_topn_compact_cls<W, T, true><<<tiles, kThreads, 0, st>>>(keys, coef, base, n, (unsigned long long)keep_n,
@@ -1650,6 +1650,11 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
     if (deferred) cudaMemcpyAsync(host_count + 22, &ctl->span, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
     if ((e = spin_sync(st)) != cudaSuccess) return e;
     *out_n = host_count[3];
+    if (deferred) {  // the rows the select and the compaction read: the span, known now
+        prof->add_bytes(K_TOPN_HIST, (double)host_count[22] * sizeof(T));
+        prof->add_bytes(K_TOPN_COMPACT, (double)host_count[22] * sizeof(T));
+    }
+    if (classify && next_flags) prof->add_bytes(K_TOPN_COMPACT, (double)(deferred ? host_count[22] : n));
     prof->add_bytes(K_TOPN_COMPACT, (double)*out_n * (2 * 16 * W + sizeof(T)));
     if (classify && !topn_unclassified(host_count)) prof->add_bytes(K_TOPN_COMPACT, (double)host_count[0] * 6.0);
     return cudaSuccess;
