@@ -814,21 +814,21 @@ def main():
                     help="the other configurations measured after the headline (comma list of "
                          f"{','.join(CONFIGS)}; 'none' for the headline alone)")
     ap.add_argument("--configs-only", action="store_true", help="print only the configurations' object")
-    # the learned comparisons run in reduced form by default (two fields, smaller budgets) so the
-    # whole line takes minutes; the full sets: --learn-fields 0.5 1 2 3 --learn-plain-budgets 20 22
-    # 24 --learn-budgets 16 18 20 22 24 --learn-ref-cap 29 --xxz-budget 24 --xxz-steps 50
-    ap.add_argument("--learn-fields", type=float, nargs="+", default=[0.5, 2.0])
-    ap.add_argument("--learn-plain-budgets", type=int, nargs="+", default=[20, 22], help="log2 TopN budgets")
-    ap.add_argument("--learn-budgets", type=int, nargs="+", default=[16, 18, 20],
+    # the learned comparisons: config 3's fields and plain budgets, the learned form from 2^16 up;
+    # config 4 at 50 steps and 2^20 terms against a 2^22 reference (--xxz-budget 22: about five
+    # minutes; the 2^28 budget of its definition: --xxz-budget 28, much longer)
+    ap.add_argument("--learn-fields", type=float, nargs="+", default=[0.5, 1.0, 2.0, 3.0])
+    ap.add_argument("--learn-plain-budgets", type=int, nargs="+", default=[20, 22, 24], help="log2 TopN budgets")
+    ap.add_argument("--learn-budgets", type=int, nargs="+", default=[16, 18, 20, 22],
                     help="log2 budgets of the learned form")
     ap.add_argument("--learn-ref-eps", type=float, default=1e-7)
     ap.add_argument("--learn-ref-cap", type=int, default=28, help="log2 TopN cap of the reference run")
     ap.add_argument("--learn-train-eps", type=float, default=1e-5, help="threshold of the attribution runs")
-    ap.add_argument("--learn-samples", type=int, default=512, help="attribution samples per step boundary")
+    ap.add_argument("--learn-samples", type=int, default=1024, help="attribution samples per step boundary")
     ap.add_argument("--learn-rescore", type=int, default=0,
                     help="layers between the learned pass's fresh predictions (0: one Trotter step)")
     ap.add_argument("--xxz-budget", type=int, default=20, help="log2 TopN budget of the L=256 XXZ comparison")
-    ap.add_argument("--xxz-steps", type=int, default=20)
+    ap.add_argument("--xxz-steps", type=int, default=50)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")

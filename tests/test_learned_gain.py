@@ -4,9 +4,9 @@ A 4 x 4 periodic transverse-field Ising quench (J = 1, dt = 0.05, 10 Trotter ste
 (1/16) sum X_i, readout in |0...0>, Heisenberg picture, f32 coefficients for the truncated
 runs) — the 8 x 8 learned-truncation configuration shrunk to what a test can afford.  The scorer
 is trained on attribution data the engine generates from tight-threshold (1e-6) runs at
-h in {0.75, 1.5, 2.5} and judged, against plain coefficient-magnitude TopN at budgets of 2^7,
+h in {0.75, 1.5, 2.5} and compared with plain coefficient-magnitude TopN at budgets of 2^7,
 2^9 and 2^11 terms, by |<O> - <O>_ref| at h in {0.5, 1, 2, 3}, the reference being the
-threshold-1e-6 run in f64.  Plain TopN is the judge: the test asserts the scored policy's
+threshold-1e-6 run in f64.  Plain TopN is the yardstick: the test asserts the scored policy's
 summed error is below plain TopN's.
 """
 
