@@ -1257,9 +1257,12 @@ struct Engine {
         }
         // the TopN pass that follows reads the span and live count on the device and waits once
         // for both (one cooperative select, the merge's histogram and slots; no folded noise)
-        const bool defer = s->in_propagate && slotted && fuse_topn && first_pass == PS_PASS_TOPN &&
-                           policy->num_passes == 1 && policy->passes[0].n > 0 && !carry_f && !a.noise &&
-                           a.L.partners && StoreOps<W, T>::cooperative_select();
+        // (or an inherited learned pass between rescorings, whose select reads the carried scores)
+        const bool defer_pass = (first_pass == PS_PASS_TOPN && !carry_f) ||
+                                (scored_fuse && s->f_age + 1 < inherit_interval(policy, s));
+        const bool defer = s->in_propagate && slotted && fuse_topn && defer_pass && policy->num_passes == 1 &&
+                           policy->passes[0].n > 0 && !a.noise && a.L.partners &&
+                           StoreOps<W, T>::cooperative_select();
         if (defer) a.defer_counts = s->hcount + 32;
         a.inject_flag = s->fault_flag;
         s->fault_flag = 0;
@@ -1342,6 +1345,14 @@ struct Engine {
         return PS_OK;
     }
 
+    // A deferred layer whose pass cannot run on the device's counts: wait for them here.
+    static ps_status settle_deferred(ps_sum* s) {
+        cudaMemcpyAsync(s->hcount + 22, &s->ctl->span, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s->stream);
+        cudaError_t e = spin_sync(s->stream);
+        if (e != cudaSuccess) return cuda_fail(s, e, "apply: counts");
+        return finish_deferred(s, s->hcount[22]);
+    }
+
     // The sort path: branch records, LSD radix sort of (key, record index), run-summing dedup
     // with the keep program (apply_layer_body's general tables, engine/gpu/layer.rs:614-763).
     static ps_status apply_general(ps_sum* s, const ps_table& t, const KeepProg& keep, const ps_policy* policy,
@@ -1419,6 +1430,13 @@ struct Engine {
 
     static ps_status finalize(ps_sum* s, const ps_policy* policy) {
         const uint64_t interval = inherit_interval(policy, s);
+        const bool deferrable = policy && policy->num_passes > 0 &&
+                                (policy->passes[0].kind == PS_PASS_TOPN ||
+                                 (policy->passes[0].kind == PS_PASS_SCORED_TOPN && interval > 1));
+        if (s->deferred && !deferrable) {  // a pass that needs the layer's counts on the host
+            ps_status ps = settle_deferred(s);
+            if (ps != PS_OK) return ps;
+        }
         if (!(policy && policy->num_passes > 0 && (policy->passes[0].kind == PS_PASS_TOPN || interval > 1))) {
             ps_status ps = densify(s, "finalize");
             if (ps != PS_OK) return ps;
@@ -1462,6 +1480,10 @@ struct Engine {
             // the layer before did not wait for its counts: the select decides on the device
             // whether the live rows fit (the layer keeps a pass of n > 0 only, with its histogram)
             const bool dfr = s->deferred && i == 0 && use_hist;
+            if (s->deferred && !dfr) {
+                ps_status ps = settle_deferred(s);
+                if (ps != PS_OK) return ps;
+            }
             if (!dfr && (s->slotted ? s->live_n : s->n) <= p.n) {
                 if (use_hist) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
                 ps_status ps = densify(s, "topn");
@@ -1645,6 +1667,12 @@ struct Engine {
     static ps_status scored_inherited(ps_sum* s, uint64_t keep_n, uint64_t interval, bool hist_ok) {
         ps_scorer* sc = s->scorer;
         const bool rescore = !s->f_valid || s->f_age + 1 >= interval;
+        // the layer did not wait for its counts: the select reads them (between rescorings)
+        const bool dfr = s->deferred && !rescore && hist_ok && keep_n > 0;
+        if (s->deferred && !dfr) {
+            ps_status ps = settle_deferred(s);
+            if (ps != PS_OK) return ps;
+        }
         const uint64_t live = s->slotted ? s->live_n : s->n;
         auto drop_hist = [&]() {
             if (hist_ok) cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
@@ -1680,7 +1708,7 @@ struct Engine {
         } else {
             ++s->f_age;
         }
-        if (live <= keep_n || keep_n == 0) {
+        if (!dfr && (live <= keep_n || keep_n == 0)) {
             drop_hist();
             if (keep_n == 0 && live > 0) {
                 s->n = 0;
@@ -1700,15 +1728,23 @@ struct Engine {
         }
         uint64_t out_n = 0;
         const bool window = !rescore && hist_ok && s->score_window;
+        bool kept_all = false;
         for (int attempt = 0; attempt < 2; ++attempt) {
             const bool win = window && attempt == 0;
+            const bool dfr_now = dfr && attempt == 0;
             e = StoreOps<W, T>::topn(K(s, s->cur), C(s, s->cur), s->n, keep_n, K(s, spare), C(s, spare),
                                      (unsigned int*)s->hist.p, hist_ok && attempt == 0, (uint64_t*)s->cand.p,
                                      topn_cand_words(s->n, s->sms), (unsigned long long*)s->status.p, s->ctl, s->hcount,
                                      &out_n, s->sms, s->stream, &s->prof, rescore ? (const uint64_t*)s->sel.p : nullptr,
-                                     win, win ? s->score_base : 0, slot_map(s), F(s, s->cur), F(s, spare));
+                                     win, win ? s->score_base : 0, slot_map(s), F(s, s->cur), F(s, spare), nullptr,
+                                     nullptr, nullptr, nullptr, dfr_now);
             s->prof.resolve();
             if (e != cudaSuccess) return cuda_fail(s, e, "scored TopN");
+            if (dfr_now) {  // the layer's own counts and error check, then the pass's
+                ps_status ps = finish_deferred(s, s->hcount[22]);
+                if (ps != PS_OK) return ps;
+                kept_all = s->hcount[23] != 0;
+            }
             unsigned int fl = 0, fi = 0;
             topn_flags(s->hcount, &fl, &fi);
             ps_status ps = flags_status(s, fl, fi, "scored TopN");
@@ -1716,6 +1752,7 @@ struct Engine {
                 cudaMemsetAsync(s->hist.p, 0, kTopnBinsN * sizeof(unsigned int), s->stream);
                 return ps;
             }
+            if (kept_all) break;  // no boundary: the window stays where it was
             if (!(win && topn_window_missed(s->hcount))) {
                 const uint64_t boundary = topn_boundary(s->hcount, win ? s->score_base : 0);
                 const uint64_t half = 1024ull << 48;
