@@ -510,47 +510,82 @@ __device__ __forceinline__ void block_select(unsigned int* __restrict__ hist, in
     __syncthreads();
 }
 
-// Block-wide: the boundary of `total` candidate keys in sk (shared memory, room for the next
-// power of two) at rank r from the top (1 <= r <= total): pads with zeros (the lowest key),
-// sorts descending (bitonic), and sets the select's final prefix (the boundary key itself, full
-// mask), remaining rank and count above ("above" counts the candidates strictly larger) and
-// the number of candidates equal to the boundary (aux[4]).
-__device__ __forceinline__ void block_sort_boundary(uint64_t* sk, unsigned int total, unsigned long long r,
+// Block-wide (kSelThreads threads): the boundary of the `total` candidate keys in sk (shared
+// memory) at rank r from the top (1 <= r <= total), by an in-block radix select of eight 8-bit
+// digits (a histogram of the keys that match the digits fixed so far, and one warp finding the
+// digit that holds the remaining rank).  Sets the select's final prefix (the boundary key
+// itself, full mask), the rank left within the keys equal to it, adds the count of candidates
+// strictly larger to the count above, and records the number of candidates equal to the
+// boundary (aux[4]).
+__device__ __forceinline__ void block_sort_boundary(const uint64_t* sk, unsigned int total, unsigned long long r,
                                                     Ctl* ctl) {
-    const int tid = threadIdx.x;
-    unsigned int np = 1;
-    while (np < total) np <<= 1;
-    for (unsigned int i = total + tid; i < np; i += kSelThreads) sk[i] = 0ull;
+    static_assert(kSelThreads == 256, "one histogram bin per thread");
+    __shared__ unsigned int h[256];
+    __shared__ unsigned long long s_prefix, s_mask, s_r, s_above, s_pass_above;
+    __shared__ unsigned int s_bin, s_cnt;
+    const int tid = threadIdx.x, lane = tid & 31;
+    if (tid == 0) {
+        s_prefix = 0;
+        s_mask = 0;
+        s_r = r;
+        s_above = 0;
+        s_cnt = 0;
+    }
     __syncthreads();
-    for (unsigned int k = 2; k <= np; k <<= 1) {
-        for (unsigned int j = k >> 1; j > 0; j >>= 1) {
-            for (unsigned int i = tid; i < np; i += kSelThreads) {
-                const unsigned int l = i ^ j;
-                if (l > i) {
-                    const uint64_t a = sk[i], b = sk[l];
-                    const bool desc = (i & k) == 0;
-                    if (desc ? a < b : a > b) {
-                        sk[i] = b;
-                        sk[l] = a;
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        h[tid] = 0;
+        __syncthreads();
+        const uint64_t pfx = s_prefix, msk = s_mask;
+        for (unsigned int i = tid; i < total; i += kSelThreads) {
+            const uint64_t k = sk[i];
+            if ((k & msk) == pfx) atomicAdd(&h[(unsigned int)(k >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        if (tid < 32) {
+            // lane l holds the bins 255 - 8 l - j (j < 8), counted from the top
+            unsigned int c[8], tot = 0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                c[j] = h[255 - (8 * lane + j)];
+                tot += c[j];
+            }
+            unsigned int incl = tot;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const unsigned long long rr = s_r;
+            const unsigned int excl = incl - tot;
+            if (excl < rr && incl >= rr) {  // exactly one lane: its bins hold the remaining rank
+                unsigned int acc = excl;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    if (acc + c[j] >= rr) {
+                        s_bin = 255u - (unsigned int)(8 * lane + j);
+                        s_pass_above = acc;
+                        s_cnt = c[j];
+                        break;
                     }
+                    acc += c[j];
                 }
             }
-            __syncthreads();
         }
+        __syncthreads();
+        if (tid == 0) {
+            s_prefix |= (unsigned long long)s_bin << shift;
+            s_mask |= 0xFFull << shift;
+            s_r -= s_pass_above;
+            s_above += s_pass_above;
+        }
+        __syncthreads();
     }
-    const uint64_t B = sk[r - 1];
-    __shared__ unsigned int s_first, s_last;
-    for (unsigned int i = tid; i < total; i += kSelThreads) {
-        if (sk[i] == B && (i == 0 || sk[i - 1] != B)) s_first = i;
-        if (sk[i] == B && (i + 1 == total || sk[i + 1] != B)) s_last = i;
-    }
-    __syncthreads();
     if (tid == 0) {
-        ctl->aux[0] = B;
+        ctl->aux[0] = s_prefix;
         ctl->aux[1] = ~0ull;
-        ctl->aux[2] = r - s_first;
-        ctl->aux[3] += s_first;
-        ctl->aux[4] = s_last - s_first + 1;
+        ctl->aux[2] = s_r;
+        ctl->aux[3] += s_above;
+        ctl->aux[4] = s_cnt;
     }
 }
 
@@ -659,8 +694,8 @@ __global__ void __launch_bounds__(kSelThreads, SCORE ? 3 : 4) k_topn_select_all(
         if (tid == 0) seg_count[blockIdx.x] = (unsigned int)s_base;
     }
     if (!grid_barrier(bar, ctl, 722)) return;
-    // Few candidates (the usual case at small sums): block 0 sorts them all in shared memory and
-    // reads the boundary off the sorted order; no further grid barrier.  Every block sums the
+    // Few candidates (the usual case at small sums): block 0 gathers them all into shared memory
+    // and radix-selects the boundary there; no further grid barrier.  Every block sums the
     // segment lengths, so all take the same branch.
     {
         constexpr int kSortCap = kTopnBinsN / 2;  // 64-bit keys in the 8192-word histogram's space
@@ -735,8 +770,8 @@ __global__ void __launch_bounds__(kSelThreads, SCORE ? 3 : 4) k_topn_select_all(
         if (blockIdx.x == 0) block_select<kTopnBinsN>(hist, shift, 13, ctl, s_part);
         if (!grid_barrier(bar, ctl, 724)) return;
         // Once the chosen bin holds at most kSortCap keys, the remaining digits give way to one
-        // block's sort: every block appends its keys of the bin to a list in the (now zero)
-        // histogram's space, and block 0 sorts them, then zeroes the words it used.
+        // block's select: every block appends its keys of the bin to a list in the (now zero)
+        // histogram's space, and block 0 radix-selects among them, then zeroes the words it used.
         constexpr unsigned int kSortCap = kTopnBinsN / 2;
         const unsigned long long cnt = __ldcg(&ctl->aux[4]), r = __ldcg(&ctl->aux[2]);
         if (d < 3 && cnt <= kSortCap && r >= 1 && r <= cnt) {
@@ -1530,7 +1565,7 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
                                  const uint8_t* next_flags, bool deferred) {
     const int dfr = deferred ? 1 : 0;
     // aux: prefix, mask, remaining rank, above, keys in the last chosen bin (after the select:
-    // the keys equal to the boundary), window miss, keys gathered for the in-block sort
+    // the keys equal to the boundary), window miss, keys gathered for the in-block select
     // (cooperative select), next layer not classified by the compaction; count[4]: candidates
     window = window && hist_ready && !sel;
     if (!window) base = 0;
