@@ -749,7 +749,7 @@ def config_learned_xxz256(args):
     obs64 = {"I" * 32 + "Z" + "I" * 31: 1.0}
     sc, losses, rows, t_data, t_train = learned.train_scorer(
         obs64, 64, lambda _h: workloads.xxz_chain(64, 1, Jz=jz, dt=dt), (jz,), steps, workloads.neel_state(64),
-        args.learn_train_eps, samples_per_step=args.learn_samples, every=5, chunk=256, epochs=40, batch=1024,
+        args.learn_train_eps, samples_per_step=args.xxz_samples, every=5, chunk=256, epochs=40, batch=1024,
         lr=1e-3)
     sc.set_site_map(np.clip(np.arange(L) - 128 + 32, 0, 63))
     b = args.xxz_budget
@@ -829,6 +829,8 @@ def main():
                     help="layers between the learned pass's fresh predictions (0: one Trotter step)")
     ap.add_argument("--xxz-budget", type=int, default=20, help="log2 TopN budget of the L=256 XXZ comparison")
     ap.add_argument("--xxz-steps", type=int, default=50)
+    ap.add_argument("--xxz-samples", type=int, default=256,
+                    help="attribution samples per step boundary of the L=64 XXZ training runs")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
