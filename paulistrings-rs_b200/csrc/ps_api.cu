@@ -1450,7 +1450,8 @@ struct Engine {
             if (p.kind == PS_PASS_SCORED_TOPN) {
                 if (interval > 1) {
                     ps_status ps = scored_inherited(s, p.n, interval,
-                                                    ready && i == 0 && s->hist_kind == PS_PASS_SCORED_TOPN);
+                                                    ready && i == 0 && s->hist_kind == PS_PASS_SCORED_TOPN,
+                                                    i == policy->num_passes - 1);
                     if (ps != PS_OK) return ps;
                     continue;
                 }
@@ -1664,7 +1665,7 @@ struct Engine {
     // histogrammed log|c| + f, and the select computes the same score from the coefficient and
     // the prediction.  Either way the compaction carries the predictions with the kept rows.
     // hist_ok: the layer's merge left a histogram of the scores in s->hist.
-    static ps_status scored_inherited(ps_sum* s, uint64_t keep_n, uint64_t interval, bool hist_ok) {
+    static ps_status scored_inherited(ps_sum* s, uint64_t keep_n, uint64_t interval, bool hist_ok, bool last_pass) {
         ps_scorer* sc = s->scorer;
         const bool rescore = !s->f_valid || s->f_age + 1 >= interval;
         // the layer did not wait for its counts: the select reads them (between rescorings)
@@ -1726,6 +1727,22 @@ struct Engine {
             drop_hist();
             return cuda_fail(s, e, "scored TopN: scratch");
         }
+        // the layer's last pass between rescorings, a rotation layer (with partners) next: the
+        // compaction also lists that layer's partners (as the plain TopN pass's does)
+        RotLayer<W> next_L;
+        bool classify = false;
+        if (last_pass && !rescore && s->next_table && keep_n < (1ull << 31) - 1) {
+            std::string why_next;
+            bool general = false;
+            classify = to_rot_layer<W, T>(*s->next_table, next_L, *s->levels, why_next, &general) == PS_OK &&
+                       !general && next_L.partners;
+            if (classify) e = ensure(s, s->idx, keep_n * 4);
+            if (classify && e == cudaSuccess) e = ensure(s, s->dv, keep_n * 2);
+            if (e != cudaSuccess) {
+                drop_hist();
+                return cuda_fail(s, e, "scored TopN: scratch");
+            }
+        }
         uint64_t out_n = 0;
         const bool window = !rescore && hist_ok && s->score_window;
         bool kept_all = false;
@@ -1736,8 +1753,9 @@ struct Engine {
                                      (unsigned int*)s->hist.p, hist_ok && attempt == 0, (uint64_t*)s->cand.p,
                                      topn_cand_words(s->n, s->sms), (unsigned long long*)s->status.p, s->ctl, s->hcount,
                                      &out_n, s->sms, s->stream, &s->prof, rescore ? (const uint64_t*)s->sel.p : nullptr,
-                                     win, win ? s->score_base : 0, slot_map(s), F(s, s->cur), F(s, spare), nullptr,
-                                     nullptr, nullptr, nullptr, dfr_now);
+                                     win, win ? s->score_base : 0, slot_map(s), F(s, s->cur), F(s, spare),
+                                     classify ? &next_L : nullptr, classify ? (uint32_t*)s->idx.p : nullptr,
+                                     classify ? (uint16_t*)s->dv.p : nullptr, nullptr, dfr_now);
             s->prof.resolve();
             if (e != cudaSuccess) return cuda_fail(s, e, "scored TopN");
             if (dfr_now) {  // the layer's own counts and error check, then the pass's
@@ -1764,6 +1782,11 @@ struct Engine {
         s->cur = spare;
         s->n = out_n;
         s->slotted = false;
+        if (classify && !topn_unclassified(s->hcount)) {
+            s->pre_valid = true;
+            s->pre_table = s->next_table;
+            s->pre_n = out_n;
+        }
         return PS_OK;
     }
 

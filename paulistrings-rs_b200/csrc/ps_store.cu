@@ -1069,14 +1069,18 @@ __global__ void __launch_bounds__(kThreads) k_topn_compact(const uint64_t* __res
 // NaN) the plain compaction runs and aux[7] tells the host that the next layer classifies itself.
 // FLAGS: the layer's merge wrote each row's partner test under the next layer (nflag, one byte
 // per row of the slotted store), so the first pass reads a byte instead of the key.
-template <int W, typename T, bool FLAGS>
-__global__ void __launch_bounds__(kThreads, W == 1 ? 8 : (W == 2 ? 4 : 2)) k_topn_compact_cls(const uint64_t* __restrict__ keys,
+// SCORE: the inherited learned pass (keys score_key(c, f) from the carried predictions fin,
+// which the kept rows carry to fout).
+template <int W, typename T, bool FLAGS, bool SCORE = false>
+__global__ void __launch_bounds__(kThreads, W == 1 ? (SCORE ? 4 : 8) : (W == 2 ? 4 : 2)) k_topn_compact_cls(const uint64_t* __restrict__ keys,
                                                                const T* __restrict__ coef, uint64_t base, uint64_t n,
                                                                unsigned long long keep_n, uint64_t* __restrict__ okeys,
                                                                T* __restrict__ ocoef, unsigned long long* status,
                                                                Ctl* ctl, SlotMap slots, const RotLayer<W> L,
                                                                uint32_t* __restrict__ idx, uint16_t* __restrict__ D,
-                                                               const uint8_t* __restrict__ nflag, int deferred) {
+                                                               const uint8_t* __restrict__ nflag, int deferred,
+                                                               const float* __restrict__ fin = nullptr,
+                                                               float* __restrict__ fout = nullptr) {
     // deferred: as k_topn_compact
     bool all = false;
     if (deferred) {
@@ -1087,8 +1091,8 @@ __global__ void __launch_bounds__(kThreads, W == 1 ? 8 : (W == 2 ? 4 : 2)) k_top
     if (!all && ctl->aux[5]) return;  // the windowed boundary left the window: the pass reruns in full range
     if (!all && !(ctl->aux[0] != 0 && ctl->aux[4] == ctl->aux[2])) {
         if (blockIdx.x == 0 && threadIdx.x == 0) ctl->aux[7] = 1;
-        compact_tile<W, T, false>(keys, coef, nullptr, 0, base, n, keep_n, okeys, ocoef, status, ctl, slots, nullptr,
-                                  nullptr);
+        compact_tile<W, T, SCORE>(keys, coef, nullptr, SCORE ? 4 : 0, base, n, keep_n, okeys, ocoef, status, ctl,
+                                  slots, fin, fout);
         return;
     }
     constexpr int ITEMS = 16;
@@ -1117,7 +1121,11 @@ __global__ void __launch_bounds__(kThreads, W == 1 ? 8 : (W == 2 ? 4 : 2)) k_top
         bool kept = false, part = false;
         if (e < n) {
             // neither load waits for the liveness test (a slot's tail is allocated)
-            const uint64_t mk = mag_key<T>(coef[e]);
+            uint64_t mk;
+            if constexpr (SCORE)
+                mk = score_key<T>(coef[e], fin[e]);
+            else
+                mk = mag_key<T>(coef[e]);
             if constexpr (FLAGS) {
                 const bool f = nflag[e] != 0;
                 if (sw.live(slots) && mk >= boundary) {
@@ -1190,6 +1198,7 @@ __global__ void __launch_bounds__(kThreads, W == 1 ? 8 : (W == 2 ? 4 : 2)) k_top
             if (PS_GUARD(ctl, pos < n, 702)) {
                 store_key<W>(okeys, pos, k);
                 ocoef[pos] = coef[e];
+                if constexpr (SCORE) fout[pos] = fin[e];
             }
         }
         if (bq != 0) {  // warp-uniform: the rows that emit a partner, in order, with their ranks
@@ -1660,8 +1669,13 @@ cudaError_t StoreOps<W, T>::topn(const uint64_t* keys, const T* coef, uint64_t n
         cudaMemsetAsync(&ctl->tile_counter[6], 0, sizeof(unsigned int), st);
     }
     prof->begin(K_TOPN_COMPACT, deferred ? 0.0 : (double)n * sizeof(T), st);
-    const bool classify = next && next_idx && next_D && !sel && !fpred && !fout;
-    if (classify && next_flags)
+    const bool classify = next && next_idx && next_D && !sel && (fpred != nullptr) == (fout != nullptr);
+    if (classify && fpred)
+        k_topn_compact_cls<W, T, false, true><<<tiles, kThreads, 0, st>>>(keys, coef, base, n,
+                                                                          (unsigned long long)keep_n, okeys, ocoef,
+                                                                          status, ctl, slots, *next, next_idx, next_D,
+                                                                          nullptr, dfr, fpred, fout);
+    else if (classify && next_flags)
         k_topn_compact_cls<W, T, true><<<tiles, kThreads, 0, st>>>(keys, coef, base, n, (unsigned long long)keep_n,
                                                                    okeys, ocoef, status, ctl, slots, *next, next_idx,
                                                                    next_D, next_flags, dfr);
