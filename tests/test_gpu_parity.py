@@ -438,3 +438,32 @@ def test_topn_compaction_lists_the_next_layers_partners(dtype, ties):
     if not ties:
         # the layers after a TopN pass take their partner lists from its compaction
         assert classify < len(circ) // 2, (classify, len(circ))
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_layer_within_the_cap_keeps_every_row_on_the_device(dtype):
+    """A sum at its TopN cap meets a rotation that commutes with every term (no partners): the
+    layer does not wait for its counts, so the select finds on the device that the live rows fit
+    the quota and keeps them all; the next layer, which does split terms, takes its partner list
+    from that compaction.  Bit-exact against the oracle throughout."""
+    nq = 20
+    rng = np.random.default_rng(17)
+    W = ps.width_for(nq)
+    zs = set()
+    while len(zs) < 3000:
+        zs.add(int(rng.integers(1, 1 << nq)))
+    x = np.zeros((len(zs), W), np.uint64)
+    z = np.array(sorted(zs), np.uint64).reshape(-1, W)
+    c = rng.standard_normal(len(zs))
+    pol = truncation.topn(3000)
+    circ = ps.Circuit(nq)
+    circ.pauli_rotation("ZZ", [0, 1], 0.3)   # commutes with every Z string: no partners
+    circ.pauli_rotation("XY", [2, 3], 0.4)   # splits the terms with Z on exactly one of 2, 3
+    circ.pauli_rotation("ZZ", [4, 5], 0.2)
+    g = ps.GpuPauliSum(nq, dtype)
+    g.upload(x, z, c)
+    st = g.propagate(circ, pol, "heisenberg", with_stats=True)
+    o = oracle_sum(nq, x, z, c, dtype)
+    after = o.propagate(oracle_channels(circ), oracle_policy(pol), "heisenberg")
+    assert st.terms_after == [int(v) for v in after]
+    assert_same_terms(g.download(), oracle_arrays(o), what=f"keep-all-{dtype}")
