@@ -8,20 +8,22 @@
 // keys first differ on a bit of g (crates/paulistrings/src/engine/bucketed/
 // partner_order.rs:10-14).  So the layer is:
 //
+//   k_layer_prep reset the layer's counts, tile dispensers and look-back words;
 //   k_classify   stream the store keys (warp-striped coalesced loads), list
 //                anticommuting rows with a decoupled look-back count and record
-//                each one's divergence rank from its predecessor;
-//   forward level scan (k_level_reduce, k_level_scan, k_fwd_apply): max-scan
-//                per bit of g, the upper half of each group moves down by the
-//                lower half's size;
-//   backward level scan (k_level_reduce, k_level_scan, k_bwd_apply): min-scan
-//                per bit of g, the lower half moves up by the upper half's size;
-//                writes each partner at its sorted slot;
+//                each one's divergence rank from its predecessor (skipped when the
+//                TopN compaction before the layer already wrote that list);
+//   level scans  (k_level_reduce per tile, k_level_scan over the tiles,
+//                k_level_apply per partner): forward max-scan per bit of g (the
+//                upper half of each group moves down by the lower half's size) and
+//                backward min-scan (the lower half moves up by the upper half's
+//                size); the last batch writes each partner at its sorted slot;
 //   k_partition  merge-path split points (a warp per run of tiles, 32-way search);
 //   k_merge      merge own rows and partners (TMA bulk copies into shared
 //                memory), sum equal keys, drop exact zeros and keep-program
 //                rejects, and write the tile at its look-back offset or, before
-//                a TopN pass, at its fixed slot.
+//                a TopN pass, at its fixed slot (with the first select digit, and
+//                before a rotation layer each row's partner test under it).
 //
 // Key-preserving tables (depolarizing noise, quarter turns with sin = 0) run
 // k_partition + k_merge with an empty partner stream.

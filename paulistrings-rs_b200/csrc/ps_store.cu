@@ -10,11 +10,17 @@
 //   k_dedup                sum runs of equal keys in input order, drop exact zeros (and keep
 //                          rejects), compact with a look-back (BuildAccumulator::finalize,
 //                          crates/paulistrings/src/pauli_sum/accumulator.rs:35-56)
-//   k_topn_hist/_step/_compact
-//                          TopN by 8-bit radix-select on the bit pattern of |c|^2 (NaN lowest),
-//                          then an order-preserving compaction keeping everything above the
-//                          boundary and the first `quota` boundary ties in key order
-//                          (TopN::finalize_layer, crates/paulistrings/src/truncation/builtin.rs:73-129)
+//   k_topn_select_all      TopN select on the bit pattern of |c|^2 (NaN lowest) in one
+//                          cooperative launch: a digit-1 bin from the merge's histogram, the bin's
+//                          keys gathered, 13-bit digit rounds until at most 4096 keys remain, then
+//                          an in-block radix select (TopN::finalize_layer,
+//                          crates/paulistrings/src/truncation/builtin.rs:73-129); the multi-launch
+//                          k_topn_hist1 / k_topn_cand / k_topn_hist_cand / k_topn_select path when
+//                          the device cannot run it
+//   k_topn_compact         order-preserving compaction keeping everything above the boundary and
+//                          the first `quota` boundary ties in key order
+//   k_topn_compact_cls     the same when every tie is kept, also listing the next rotation
+//                          layer's partners (its idx, divergence ranks and partner count)
 //   k_expect_*             <psi|O|psi> in a product state, float64 partial sums reduced in a
 //                          fixed order (readout/product_state.rs:84-101)
 #include "ps_device.cuh"
